@@ -1,0 +1,487 @@
+"""Python driver of the CPU oracle (test infrastructure only).
+
+Restates the reference's host-side pieces around the C kernels of
+``iblbm_oracle.c``:
+
+- ``init_state``   iblbm/init.py:116-265 (grid, tau, markers, feq -> fstar) and
+                   iblbm/physics/sedimentation.py:94-219 (particles);
+- ``OracleSim``    the time loop of iblbm/runtime/loop.py:44-151 for the fixed /
+                   oscillating cylinder runtime (runtime/scenarios/fixed_cylinder.py)
+                   and the multi-particle sedimentation runtime
+                   (runtime/scenarios/sedimentation_multi.py), with the IBM
+                   strategies of iblbm/ibm/strategies/{df,mdf,dfc}.py;
+- ``mdf_omega``    iblbm/ibm/a_norm.py:204-266.
+
+The configuration object is duck-typed: any object with the reference
+``SimConfig`` attribute names works (the reference's own or the product's).
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use this
+module; it is the checker, never the thing measured or shipped.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from types import SimpleNamespace
+
+import numpy as np
+
+from .build import build_oracle
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+BC_IDS = {"dirichlet_neumann": 0, "open_boundary": 1, "settling_channel": 2, "velocity_inlet": 3}
+DELTA_IDS = {"peskin4pt": 0, "hat": 1}
+MDF_COUPLED_OMEGA_MAX = 0.8  # iblbm/ibm/multi_particle.py:33
+
+
+def lib():
+    """Load (building first if needed) the oracle shared library."""
+    global _lib
+    if _lib is None:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "liboracle.so")
+        if not os.path.exists(path):
+            path = build_oracle()
+        _lib = ctypes.CDLL(path)
+        _lib.orc_a_norm_inf.restype = ctypes.c_double
+        _lib.orc_bc.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a):
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_D)
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(_I)
+    raise TypeError(a.dtype)
+
+
+# --------------------------------------------------------------------------
+# Kernel wrappers (AoS arrays, the reference's layout)
+# --------------------------------------------------------------------------
+def feq(ro, U, incompressible=False):
+    out = np.empty((ro.shape[0], 9))
+    lib().orc_feq(ctypes.c_int(ro.shape[0]), _p(ro), _p(U), ctypes.c_int(int(incompressible)), _p(out))
+    return out
+
+
+def macroscopic(fstar, incompressible=False):
+    N = fstar.shape[0]
+    ro = np.empty(N)
+    U = np.empty((N, 2))
+    lib().orc_macro(ctypes.c_int(N), _p(fstar), ctypes.c_int(int(incompressible)), _p(ro), _p(U))
+    return ro, U
+
+
+def collide_bgk(fstar, feq_, U, fib, tau, dt):
+    f = np.empty_like(fstar)
+    lib().orc_collide_bgk(ctypes.c_int(fstar.shape[0]), _p(fstar), _p(feq_), _p(U), _p(fib),
+                          ctypes.c_double(tau), ctypes.c_double(dt), _p(f))
+    return f
+
+
+def collide_trt(fstar, feq_, U, fib, tau, tau_minus, dt):
+    f = np.empty_like(fstar)
+    lib().orc_collide_trt(ctypes.c_int(fstar.shape[0]), _p(fstar), _p(feq_), _p(U), _p(fib),
+                          ctypes.c_double(1.0 / tau), ctypes.c_double(1.0 / tau_minus),
+                          ctypes.c_double(dt), _p(f))
+    return f
+
+
+def collide_cmmrt(fstar, U, fib, S_diag, dt):
+    f = np.empty_like(fstar)
+    S = np.ascontiguousarray(S_diag, dtype=np.float64)
+    lib().orc_collide_cmmrt(ctypes.c_int(fstar.shape[0]), _p(fstar), _p(U), _p(fib), _p(S),
+                            ctypes.c_double(dt), _p(f))
+    return f
+
+
+def stream(fstar_old, f, nx, ny):
+    out = np.empty_like(fstar_old)
+    lib().orc_stream(ctypes.c_int(nx), ctypes.c_int(ny), _p(fstar_old), _p(f), _p(out))
+    return out
+
+
+def apply_bc(bc_type, nx, ny, fstar, ro, U, inflow_u, dens, incompressible=False):
+    rc = lib().orc_bc(ctypes.c_int(BC_IDS[bc_type]), ctypes.c_int(nx), ctypes.c_int(ny), _p(fstar),
+                      _p(ro), _p(U), ctypes.c_double(inflow_u), ctypes.c_double(dens),
+                      ctypes.c_int(int(incompressible)))
+    if rc != 0:
+        raise KeyError(bc_type)
+
+
+def velocity_correction(U, fib, ro, dt, incompressible=False):
+    lib().orc_velocity_correction(ctypes.c_int(U.shape[0]), _p(U), _p(fib), _p(ro),
+                                  ctypes.c_double(dt), ctypes.c_int(int(incompressible)))
+
+
+def ibm_df(Lx, Ly, dvel, Eux, Euy, Ro, dx, dy, dt, Larea, ny, nx, delta_type, incompressible=False):
+    Lb = len(Lx)
+    fib = np.empty((nx * ny, 2))
+    out = [np.empty(Lb) for _ in range(5)]
+    lib().orc_ibm_df(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(Lb), _p(Lx), _p(Ly), _p(dvel),
+                     _p(Eux), _p(Euy), _p(Ro), ctypes.c_double(dx), ctypes.c_double(dy),
+                     ctypes.c_double(dt), ctypes.c_double(Larea), ctypes.c_int(DELTA_IDS[delta_type]),
+                     ctypes.c_int(int(incompressible)), _p(fib), *[_p(o) for o in out])
+    return (fib, *out)
+
+
+def ibm_mdf(Lx, Ly, dvel, U, ro, dx, dy, dt, Larea, ny, nx, n_iter, min_iter, delta_type, omega, tol):
+    fib = np.empty((nx * ny, 2))
+    stats = np.zeros(3, dtype=np.int32)
+    res = np.zeros(1)
+    lib().orc_ibm_mdf(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(len(Lx)), _p(Lx), _p(Ly),
+                      _p(dvel), _p(U), _p(ro), ctypes.c_double(dx), ctypes.c_double(dy),
+                      ctypes.c_double(dt), ctypes.c_double(Larea), ctypes.c_int(int(n_iter)),
+                      ctypes.c_int(int(min_iter)), ctypes.c_int(DELTA_IDS[delta_type]),
+                      ctypes.c_double(omega), ctypes.c_double(tol), _p(fib), _p(stats), _p(res))
+    return fib, {"iter_count": int(stats[0]), "last_residual": float(res[0]),
+                 "diverged": bool(stats[1]), "converged": bool(stats[2])}
+
+
+def mdf_coupled(parts, U, ro, dx, dy, dt, ny, nx, n_iter, min_iter, delta_type, omega_opt, tol,
+                incompressible):
+    """parts: list of (Lx, Ly, desired_velocity, Larea)."""
+    P = len(parts)
+    moff = np.zeros(P + 1, dtype=np.int32)
+    for p, (lx, _, _, _) in enumerate(parts):
+        moff[p + 1] = moff[p] + len(lx)
+    Lx = np.ascontiguousarray(np.concatenate([p[0] for p in parts]))
+    Ly = np.ascontiguousarray(np.concatenate([p[1] for p in parts]))
+    dv = np.ascontiguousarray(np.concatenate([p[2] for p in parts]))
+    La = np.array([float(p[3]) for p in parts])
+    N = nx * ny
+    fib = np.empty((N, 2))
+    fpart = np.empty((P, N, 2))
+    stats = np.zeros(4, dtype=np.int32)
+    dstats = np.zeros(2)
+    lib().orc_mdf_coupled(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(P), _p(moff), _p(Lx), _p(Ly),
+                          _p(dv), _p(La), _p(U), _p(ro), ctypes.c_double(dx), ctypes.c_double(dy),
+                          ctypes.c_double(dt), ctypes.c_int(int(n_iter)), ctypes.c_int(int(min_iter)),
+                          ctypes.c_int(DELTA_IDS[delta_type]), ctypes.c_double(omega_opt),
+                          ctypes.c_double(MDF_COUPLED_OMEGA_MAX), ctypes.c_double(tol),
+                          ctypes.c_int(int(incompressible)), _p(fib), _p(fpart), _p(stats), _p(dstats))
+    return fib, fpart, {"iter_count": int(stats[0]), "last_residual": float(dstats[0]),
+                        "diverged": bool(stats[1]), "converged": bool(stats[2]),
+                        "guard_trips": int(stats[3]), "omega_used": float(dstats[1])}
+
+
+def dfc_lambda(Lx, Ly, Larea, dx, dy, ny, nx, delta_type, rho_f=1.0):
+    lam = np.empty(len(Lx))
+    lib().orc_dfc_lambda(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(len(Lx)), _p(Lx), _p(Ly),
+                         ctypes.c_double(rho_f), ctypes.c_double(Larea), ctypes.c_double(dx),
+                         ctypes.c_double(dy), ctypes.c_int(DELTA_IDS[delta_type]), _p(lam))
+    return lam
+
+
+def dfc_correction(Lx, Ly, dvel, fstar, lambda_k, dx, dy, Larea, ny, nx, delta_type, scale=1.0):
+    """In-place on a copy of fstar; returns (fstar_corrected, dfc_force)."""
+    fs = fstar.copy()
+    force = np.empty((len(Lx), 2))
+    lib().orc_dfc_correction(ctypes.c_int(nx), ctypes.c_int(ny), ctypes.c_int(len(Lx)), _p(Lx), _p(Ly),
+                             _p(dvel), _p(fs), _p(lambda_k), ctypes.c_double(dx), ctypes.c_double(dy),
+                             ctypes.c_double(Larea), ctypes.c_int(DELTA_IDS[delta_type]),
+                             ctypes.c_double(scale), _p(force))
+    return fs, force
+
+
+def mdf_omega(Lx, Ly, delta_type, Larea, dx):
+    """omega = 1/||A||_inf — iblbm/ibm/a_norm.py:204-266 (coordinates /dx)."""
+    Lx_lu = np.ascontiguousarray(np.asarray(Lx, dtype=np.float64) / float(dx))
+    Ly_lu = np.ascontiguousarray(np.asarray(Ly, dtype=np.float64) / float(dx))
+    norm = lib().orc_a_norm_inf(ctypes.c_int(len(Lx_lu)), _p(Lx_lu), _p(Ly_lu),
+                                ctypes.c_int(DELTA_IDS[delta_type]), ctypes.c_double(float(Larea)))
+    return 1.0 / norm
+
+
+# --------------------------------------------------------------------------
+# Initialisation — iblbm/init.py:116-265
+# --------------------------------------------------------------------------
+def circle_markers(cx, cy, r, lattice_r, dx, spacing, retraction_dx):
+    """iblbm/init.py:211-243 and iblbm/physics/markers.py:61-85 (identical arithmetic)."""
+    dd = 2.0 * np.pi * lattice_r / spacing
+    step = 1.0 / dd
+    Ldx = np.arange(0, 1.0 + step * 0.5, step)
+    Ldx = Ldx[Ldx <= 1.0 + 1e-12]
+    if len(Ldx) > 1 and np.abs(Ldx[-1] - 1.0) < step * 0.5:
+        Ldx = Ldx[:-1]
+    theta = 2.0 * np.pi * Ldx
+    r_ret = r - retraction_dx * dx
+    Lx = r_ret * np.cos(theta) + cx
+    Ly = r_ret * np.sin(theta) + cy
+    Lb = len(Lx)
+    Larea = 2.0 * np.pi * (lattice_r - retraction_dx) / Lb
+    return np.ascontiguousarray(Lx), np.ascontiguousarray(Ly), Lb, Larea
+
+
+def init_state(cfg):
+    if cfg.nx_formula == "standard":
+        nx = int(cfg.NN * cfg.xmax - (cfg.xmax - 1))
+    else:
+        nx = int(cfg.NN * cfg.xmax)
+    dx = 1.0 / (cfg.NN - 1)
+    ny = round(cfg.ymax / dx) + 1
+    dy = cfg.ymax / (ny - 1)
+    if abs(dx - dy) / dx > 1e-6:
+        raise ValueError("non-square lattice")
+    N = nx * ny
+    phy_char = cfg.phy_l * cfg.cylinder_D_ratio
+    Cx = (cfg.phy_l / (cfg.NN - 1)) / 1.0
+    r = phy_char / 2.0 / cfg.phy_l
+    lattice_r = (phy_char / Cx) / 2.0
+    tau = 3.0 * (cfg.lattice_u * 2.0 * lattice_r / cfg.Re) + 0.5
+    U = np.zeros((N, 2))
+    if cfg.motion_type not in ("oscillating", "sedimentation"):
+        U[:, 0] = cfg.inflow_u
+    ro = np.ones(N)
+    fe = feq(ro, U, cfg.incompressible_lbgk)
+    cx, cy = cfg.cylinder_center
+    if cx - r < 0 or cx + r > cfg.xmax or cy - r < 0 or cy + r > cfg.ymax:
+        raise ValueError("cylinder outside the domain")
+    Lx, Ly, Lb, Larea = circle_markers(cx, cy, r, lattice_r, dx, cfg.marker_spacing_factor,
+                                       cfg.retraction_dx)
+    s = SimpleNamespace(nx=nx, ny=ny, N=N, dx=dx, dy=dy, dt=1.0, tau=tau, r=r, lattice_r=lattice_r,
+                        in_u=cfg.inflow_u, dens=1.0, fstar=fe.copy(), feq=fe, ro=ro, U=U,
+                        fib=np.zeros((N, 2)), Lx=Lx, Ly=Ly, Lb=Lb, Larea=Larea,
+                        desired_velocity=np.zeros((Lb, 2)), lambda_cache=None, dfc_force_lagr=None,
+                        particles=None, mdf_omega=None, mdf_stats=None)
+    if cfg.collision_model == "TRT":
+        s.tau_minus = 0.5 + cfg.trt_magic_param / (tau - 0.5)
+    if cfg.collision_model == "CM_MRT":
+        s_eps = cfg.mrt_s_eps if cfg.mrt_s_eps is not None else 1.4
+        s_q = cfg.mrt_s_q if cfg.mrt_s_q is not None else 1.2
+        s_nu = 1.0 / tau
+        s.S_diag = np.array([0.0, 0.0, 0.0, s_nu, s_nu, s_nu, s_q, s_q, s_eps])
+    if cfg.motion_type == "sedimentation":
+        if cfg.gravity <= 0.0 or cfg.rho_ratio <= 1.0:
+            raise ValueError("sedimentation needs gravity > 0 and rho_ratio > 1")
+        s.gravity_lattice = cfg.gravity
+        if cfg.particles_config is not None:
+            parts = []
+            for pc in cfg.particles_config:
+                pcx, pcy = pc["center"]
+                rho_p = pc["rho_ratio"]
+                mass = rho_p * np.pi * lattice_r ** 2
+                plx, ply, plb, pla = circle_markers(pcx, pcy, r, lattice_r, dx,
+                                                    cfg.marker_spacing_factor, cfg.retraction_dx)
+                parts.append(SimpleNamespace(
+                    pos=np.array([pcx, pcy], dtype=float), vel=np.zeros(2), vel_prev=np.zeros(2),
+                    force=np.zeros(2), mass=mass, rho_ratio=rho_p, lattice_r=lattice_r, r_domain=r,
+                    I_particle=0.5 * mass * lattice_r ** 2, Lx_c=plx.copy(), Ly_c=ply.copy(),
+                    Lx=plx, Ly=ply, Lb=plb, Larea=pla, desired_velocity=np.zeros((plb, 2)),
+                    cx_init=pcx, cy_init=pcy))
+            s.particles = parts
+    return s
+
+
+# --------------------------------------------------------------------------
+# Rigid-body helpers — iblbm/physics/{gravity,rigid_body,markers}.py and
+# iblbm/physics/inertia/{none,explicit_history,feng_b2}.py
+# --------------------------------------------------------------------------
+def _net_gravity(rho_ratio, r_lat, g, direction):
+    mag = (rho_ratio - 1.0) * (np.pi * r_lat ** 2) * g
+    return np.array([mag, 0.0]) if direction == "right" else np.array([0.0, -mag])
+
+
+def _history_dv(model, vel, vel_prev, mass, r_lat):
+    if model == "explicit_history":
+        return (np.pi * r_lat ** 2 / mass) * (vel - vel_prev)
+    return None
+
+
+def _update_markers(Lx_c, Ly_c, cx0, cy0, pos, angle=0.0):
+    cos_a = np.cos(angle)
+    sin_a = np.sin(angle)
+    rx = Lx_c - cx0
+    ry = Ly_c - cy0
+    return cos_a * rx - sin_a * ry + pos[0], sin_a * rx + cos_a * ry + pos[1]
+
+
+# --------------------------------------------------------------------------
+# Time loop — iblbm/runtime/loop.py:44-151
+# --------------------------------------------------------------------------
+class OracleSim:
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.s = init_state(cfg)
+        if cfg.motion_type == "sedimentation" and cfg.settling_inertia_model == "full_volume":
+            raise NotImplementedError("full_volume inertia is outside the hot path")
+        self.force_level = cfg.ibm_method in ("DF", "MDF")
+        self.ttt = 1
+        self.Cd_history = []
+        self.Cl_history = []
+        self.history = []
+        self.Lx_c = self.s.Lx.copy()
+        self.Ly_c = self.s.Ly.copy()
+        if cfg.ibm_method == "MDF":
+            s = self.s
+            s.mdf_omega = mdf_omega(s.Lx, s.Ly, cfg.delta_type, float(s.Larea), float(s.dx))
+            if cfg.motion_type == "sedimentation" and cfg.enable_rotation:
+                s.mdf_omega = min(float(s.mdf_omega), 1.0)
+        self.f = None
+        if cfg.stream_first or self.force_level:
+            self.f = self.collide()
+
+    # iblbm/runtime/step.py:26-46 + iblbm/lbm/collision/*.py step_cpu
+    def collide(self):
+        s, cfg = self.s, self.cfg
+        if cfg.collision_model == "BGK":
+            return collide_bgk(s.fstar, s.feq, s.U, s.fib, s.tau, s.dt)
+        if cfg.collision_model == "TRT":
+            return collide_trt(s.fstar, s.feq, s.U, s.fib, s.tau, s.tau_minus, s.dt)
+        if cfg.collision_model == "CM_MRT":
+            return collide_cmmrt(s.fstar, s.U, s.fib, s.S_diag, s.dt)
+        raise KeyError(cfg.collision_model)
+
+    # iblbm/runtime/step.py:49-60
+    def stream_boundary_macro(self):
+        s, cfg = self.s, self.cfg
+        s.fstar = stream(s.fstar, self.f, s.nx, s.ny)
+        apply_bc(cfg.bc_type, s.nx, s.ny, s.fstar, s.ro, s.U, s.in_u, s.dens, cfg.incompressible_lbgk)
+        s.ro, s.U = macroscopic(s.fstar, cfg.incompressible_lbgk)
+
+    def apply_ibm(self):
+        s, cfg = self.s, self.cfg
+        if s.particles is not None:
+            return self._apply_ibm_multi()
+        if cfg.ibm_method == "DF":
+            s.fib, s.Lux, s.Luy, s.Lfx, s.Lfy, s.R = ibm_df(
+                s.Lx, s.Ly, np.ascontiguousarray(s.desired_velocity), np.ascontiguousarray(s.U[:, 0]),
+                np.ascontiguousarray(s.U[:, 1]), s.ro, s.dx, s.dy, s.dt, s.Larea, s.ny, s.nx,
+                cfg.delta_type, cfg.incompressible_lbgk)
+            velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
+        elif cfg.ibm_method == "MDF":
+            s.fib, s.mdf_stats = ibm_mdf(
+                s.Lx, s.Ly, np.ascontiguousarray(s.desired_velocity), s.U, s.ro, s.dx, s.dy, s.dt,
+                s.Larea, s.ny, s.nx, cfg.mdf_iterations, cfg.mdf_min_iterations, cfg.delta_type,
+                s.mdf_omega, cfg.mdf_tolerance)
+            velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
+        elif cfg.ibm_method == "DFC":
+            lam = s.lambda_cache if cfg.motion_type is None else None
+            if lam is None:
+                lam = dfc_lambda(s.Lx, s.Ly, s.Larea, s.dx, s.dy, s.ny, s.nx, cfg.delta_type)
+            s.fstar, s.dfc_force_lagr = dfc_correction(
+                s.Lx, s.Ly, np.ascontiguousarray(s.desired_velocity), s.fstar, lam, s.dx, s.dy,
+                s.Larea, s.ny, s.nx, cfg.delta_type)
+            if cfg.motion_type is None:
+                s.lambda_cache = lam
+            s.ro, s.U = macroscopic(s.fstar, cfg.incompressible_lbgk)
+        else:
+            raise KeyError(cfg.ibm_method)
+
+    # iblbm/ibm/multi_particle.py:424-455 (MDF) and 347-421 (DF, uncoupled)
+    def _apply_ibm_multi(self):
+        s, cfg = self.s, self.cfg
+        if cfg.ibm_method != "MDF" or len(s.particles) < 2:
+            raise NotImplementedError("multi-particle oracle covers coupled MDF")
+        parts = [(np.ascontiguousarray(p.Lx), np.ascontiguousarray(p.Ly),
+                  np.ascontiguousarray(p.desired_velocity), p.Larea) for p in s.particles]
+        fib, fpart, stats = mdf_coupled(parts, s.U, s.ro, s.dx, s.dy, s.dt, s.ny, s.nx,
+                                        cfg.mdf_iterations, cfg.mdf_min_iterations, cfg.delta_type,
+                                        s.mdf_omega, cfg.mdf_tolerance, cfg.incompressible_lbgk)
+        s.fib = fib
+        s.mdf_stats = stats
+        for p, particle in enumerate(s.particles):
+            fp = fpart[p]
+            particle._fib_force = np.array([-float(fp[:, 0].sum()), -float(fp[:, 1].sum())])
+        velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
+
+    # runtime/scenarios/sedimentation_multi.py:36-80 (Verlet half step, no rotation)
+    def _half_step(self):
+        s, cfg = self.s, self.cfg
+        for p in s.particles:
+            F = p.force + _net_gravity(p.rho_ratio, p.lattice_r, s.gravity_lattice, cfg.gravity_direction)
+            hist = _history_dv(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            vel_half = p.vel + 0.5 * s.dt * F / p.mass
+            if hist is not None:
+                vel_half = vel_half + 0.5 * hist
+            p.pos = p.pos + s.dt * vel_half * s.dx
+            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=0.0)
+            dv = np.empty((p.Lb, 2))
+            dv[:, 0] = float(vel_half[0])
+            dv[:, 1] = float(vel_half[1])
+            p.desired_velocity = dv
+            p._vel_half = vel_half
+
+    # runtime/scenarios/sedimentation_multi.py:83-111
+    def _full_step(self):
+        s, cfg = self.s, self.cfg
+        for p in s.particles:
+            F = p._fib_force + _net_gravity(p.rho_ratio, p.lattice_r, s.gravity_lattice,
+                                            cfg.gravity_direction)
+            vel_new = p._vel_half + 0.5 * s.dt * F / p.mass
+            hist = _history_dv(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            if hist is not None:
+                vel_new = vel_new + 0.5 * hist
+            if cfg.settling_inertia_model == "feng_b2":
+                vel_new = vel_new + (1.0 / p.rho_ratio) * (p.vel - p.vel_prev)
+            p.vel_prev = p.vel.copy()
+            p.vel = vel_new
+            p.force = p._fib_force
+
+    def cd_cl(self):
+        """iblbm/diagnostics/core.py:53-113 via the strategies' compute_cd_cl."""
+        s, cfg = self.s, self.cfg
+        u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else s.in_u
+        if cfg.ibm_method == "DFC":
+            total = np.sum(s.dfc_force_lagr, axis=0)
+            denom = float(s.ro.mean()) * u_ref ** 2 * s.lattice_r
+            return float(np.abs(total[0])) / denom, float(total[1]) / denom
+        denom = np.mean(s.ro) * u_ref ** 2 * s.lattice_r
+        return float(np.abs(np.sum(s.fib[:, 0])) / denom), float(np.sum(s.fib[:, 1]) / denom)
+
+    def step(self):
+        """One iteration of iblbm/runtime/loop.py:63-138 (without the stop checks)."""
+        s, cfg, ttt = self.s, self.cfg, self.ttt
+        if s.particles is not None and cfg.time_integrator != "euler_explicit":
+            self._half_step()
+        if not cfg.stream_first and not self.force_level:
+            self.f = self.collide()
+        self.stream_boundary_macro()
+        self.apply_ibm()
+        if s.particles is not None:
+            self._full_step()
+        s.feq = feq(s.ro, s.U, cfg.incompressible_lbgk)
+        if cfg.stream_first or self.force_level:
+            self.f = self.collide()
+        if cfg.motion_type == "oscillating":
+            # iblbm/physics/motion.py:15-52 (desired velocity = displacement)
+            f0 = cfg.lattice_u / (cfg.KC * 2.0 * s.lattice_r)
+            A = cfg.KC * 2.0 * s.r / (2.0 * np.pi)
+            xt = A * np.sin(f0 * 2.0 * np.pi * ttt)
+            s.Lx = np.ascontiguousarray(self.Lx_c - xt)
+            s.Ly = self.Ly_c.copy()
+            s.desired_velocity[:, 0] = xt
+            s.desired_velocity[:, 1] = 0.0
+        if ttt % cfg.check_interval == 0:
+            if s.particles is not None:
+                self.history.append([(p.pos.copy(), p.vel.copy()) for p in s.particles])
+                self.Cd_history.append(0.0)
+                self.Cl_history.append(0.0)
+            else:
+                Cd, Cl = self.cd_cl()
+                self.Cd_history.append(Cd)
+                self.Cl_history.append(Cl)
+        self.ttt += 1
+
+    def run(self, max_steps=None):
+        steps = self.cfg.max_steps if max_steps is None else max_steps
+        while self.ttt <= steps:
+            self.step()
+        return {"Cd_history": np.array(self.Cd_history), "Cl_history": np.array(self.Cl_history),
+                "state": self.s, "final_step": self.ttt - 1}
+
+
+def run(cfg, max_steps=None):
+    return OracleSim(cfg).run(max_steps)
+
+
+def collide_post(sim):
+    """Post-collision populations of the last completed step (force-level schedule)."""
+    return sim.f
+
+
+__all__ = ["OracleSim", "run", "init_state", "mdf_omega", "math"]

@@ -1,0 +1,135 @@
+"""Pin the CPU oracle against the reference solver's own outputs.
+
+The fixtures in tests/golden/ were produced by running the reference's CPU path
+(tests/golden/make_golden.py).  The oracle restates the same FP64 arithmetic in
+the same order, so the comparison is bit for bit (`assert_array_equal` and
+SHA-256 digests); the only exception is the DFC marker force, where the
+reference sums 9 terms through a BLAS matrix product whose order is
+implementation-defined, checked to 1e-14 relative.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from iblbm_b200.config import SimConfig
+from oracle import harness as H
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _sha(a):
+    return hashlib.sha256(np.ascontiguousarray(np.asarray(a, dtype=np.float64)).tobytes()).hexdigest()
+
+
+@pytest.fixture(scope="module")
+def units():
+    return dict(np.load(os.path.join(GOLD, "units.npz")))
+
+
+def test_feq_macro(units):
+    u = units
+    np.testing.assert_array_equal(H.feq(u["u_ro"], u["u_U"], False), u["u_feq"])
+    np.testing.assert_array_equal(H.feq(u["u_ro"], u["u_U"], True), u["u_feq_inc"])
+    ro, U = H.macroscopic(u["u_fstar"], False)
+    np.testing.assert_array_equal(ro, u["u_macro_ro"])
+    np.testing.assert_array_equal(U, u["u_macro_U"])
+    _, Ui = H.macroscopic(u["u_fstar"], True)
+    np.testing.assert_array_equal(Ui, u["u_macro_U_inc"])
+
+
+def test_collisions(units):
+    u = units
+    tau, taum = float(u["u_tau"][0]), float(u["u_tau_minus"][0])
+    np.testing.assert_array_equal(H.collide_bgk(u["u_fstar"], u["u_feq"], u["u_U"], u["u_fib"], tau, 1.0),
+                                  u["u_bgk"])
+    np.testing.assert_array_equal(
+        H.collide_trt(u["u_fstar"], u["u_feq"], u["u_U"], u["u_fib"], tau, taum, 1.0), u["u_trt"])
+    np.testing.assert_array_equal(H.collide_cmmrt(u["u_fstar"], u["u_U"], u["u_fib"], u["u_S"], 1.0),
+                                  u["u_cmmrt"])
+
+
+@pytest.mark.parametrize("bc", ["dirichlet_neumann", "open_boundary", "settling_channel", "velocity_inlet"])
+def test_stream_and_boundaries(units, bc):
+    u = units
+    nx, ny = int(u["g_nx"][0]), int(u["g_ny"][0])
+    fs = H.stream(u["g_fold"], u["g_fpost"], nx, ny)
+    np.testing.assert_array_equal(fs, u["g_stream"])
+    ro, U = u["g_ro"].copy(), u["g_U"].copy()
+    H.apply_bc(bc, nx, ny, fs, ro, U, 0.05, 1.0, False)
+    np.testing.assert_array_equal(fs, u[f"bc_{bc}_f"])
+    np.testing.assert_array_equal(ro, u[f"bc_{bc}_ro"])
+    np.testing.assert_array_equal(U, u[f"bc_{bc}_U"])
+
+
+@pytest.mark.parametrize("delta", ["hat", "peskin4pt"])
+def test_ibm_kernels(units, delta):
+    u = units
+    nx, ny, dx = int(u["i_nx"][0]), int(u["i_ny"][0]), float(u["i_dx"][0])
+    Lx, Ly, dv, La = u["i_Lx"], u["i_Ly"], np.ascontiguousarray(u["i_dv"]), float(u["i_Larea"][0])
+    Eux, Euy, Ro = (np.ascontiguousarray(u[k].ravel()) for k in ("i_Eux", "i_Euy", "i_Ro"))
+    for inc in (0, 1):
+        fib, Lux, Luy, Lfx, Lfy, R = H.ibm_df(Lx, Ly, dv, Eux, Euy, Ro, dx, dx, 1.0, La, ny, nx, delta, inc)
+        k = f"df_{delta}_{inc}"
+        np.testing.assert_array_equal(fib, u[k + "_fib"])
+        np.testing.assert_array_equal(Lux, u[k + "_Lux"])
+        np.testing.assert_array_equal(Luy, u[k + "_Luy"])
+        np.testing.assert_array_equal(Lfx, u[k + "_Lfx"])
+        np.testing.assert_array_equal(R, u[k + "_R"])
+    om = H.mdf_omega(Lx, Ly, delta, La, dx)
+    assert om == float(u[f"omega_{delta}"][0])
+    Uf = np.ascontiguousarray(np.stack([Eux, Euy], axis=1))
+    fibm, st = H.ibm_mdf(Lx, Ly, dv, Uf, Ro, dx, dx, 1.0, La, ny, nx, 20, 5, delta, om, 1e-6)
+    np.testing.assert_array_equal(fibm, u[f"mdf_{delta}_fib"])
+    ref = u[f"mdf_{delta}_stats"]
+    assert st["iter_count"] == int(ref[0]) and st["last_residual"] == ref[1]
+    lam = H.dfc_lambda(Lx, Ly, La, dx, dx, ny, nx, delta)
+    np.testing.assert_array_equal(lam, u[f"lam_{delta}"])
+    fc, force = H.dfc_correction(Lx, Ly, dv, u[f"dfc_{delta}_fstar"], lam, dx, dx, La, ny, nx, delta)
+    np.testing.assert_array_equal(fc, u[f"dfc_{delta}_fc"])
+    np.testing.assert_allclose(force, u[f"dfc_{delta}_force"], rtol=1e-14, atol=1e-18)
+
+
+@pytest.mark.parametrize("name", ["C1", "C2", "C3", "C5"])
+def test_initial_state(units, name):
+    from tests.golden.make_golden import INIT_CASES
+    s = H.init_state(SimConfig(**INIT_CASES[name]))
+    scal = units[f"init_{name}_scal"]
+    got = np.array([s.nx, s.ny, s.dx, s.dy, s.tau, s.Larea, s.lattice_r, s.r, s.Lb], dtype=np.float64)
+    np.testing.assert_array_equal(got, scal)
+    np.testing.assert_array_equal(s.Lx, units[f"init_{name}_Lx"])
+    np.testing.assert_array_equal(s.Ly, units[f"init_{name}_Ly"])
+    assert _sha(s.feq) == bytes(units[f"init_{name}_feq_sha"]).hex()
+    for p, part in enumerate(s.particles or []):
+        np.testing.assert_array_equal(part.Lx, units[f"init_{name}_p{p}_Lx"])
+        np.testing.assert_array_equal(np.array([part.mass, part.I_particle, part.Larea, part.Lb]),
+                                      units[f"init_{name}_p{p}_scal"])
+
+
+RUNS = sorted(f[4:-4] for f in os.listdir(GOLD) if f.startswith("run_") and f.endswith(".npz"))
+
+
+@pytest.mark.parametrize("name", RUNS)
+def test_oracle_runs_match_reference(name):
+    g = dict(np.load(os.path.join(GOLD, f"run_{name}.npz")))
+    kw = json.loads(bytes(g["config_json"]).decode())
+    if "particles_config" in kw and kw["particles_config"]:
+        kw["particles_config"] = [dict(p, center=tuple(p["center"])) for p in kw["particles_config"]]
+    kw["cylinder_center"] = tuple(kw["cylinder_center"])
+    res = H.run(SimConfig(**kw))
+    s = res["state"]
+    arrays = {"ro": s.ro, "U": s.U, "fib": s.fib, "fstar": s.fstar, "feq": s.feq}
+    for k, a in arrays.items():
+        np.testing.assert_array_equal(np.asarray(a).reshape(a.shape[0], -1)[::97], g[f"sample_{k}"], err_msg=k)
+        assert _sha(a) == bytes(g[f"sha_{k}"]).hex(), k
+    if kw.get("ibm_method") == "DFC":
+        np.testing.assert_allclose(res["Cd_history"], g["Cd_history"], rtol=1e-13)
+        np.testing.assert_allclose(res["Cl_history"], g["Cl_history"], rtol=1e-12, atol=1e-15)
+    else:
+        np.testing.assert_array_equal(res["Cd_history"], g["Cd_history"])
+        np.testing.assert_array_equal(res["Cl_history"], g["Cl_history"])
+    if "particles" in g:
+        got = np.array([[*p.pos, *p.vel, *p.force] for p in s.particles])
+        np.testing.assert_array_equal(got, g["particles"])
