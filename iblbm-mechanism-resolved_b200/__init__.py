@@ -8,4 +8,11 @@ ctypes; PyTorch CUDA tensors hold the device buffers.
 """
 from .config import SimConfig
 
-__all__ = ["SimConfig"]
+
+def run(cfg, verbose=True, callback=None, save_dir=None, engine=None):
+    """iblbm.run drop-in: see loop.run."""
+    from .loop import run as _run
+    return _run(cfg, verbose=verbose, callback=callback, save_dir=save_dir, engine=engine)
+
+
+__all__ = ["SimConfig", "run"]

@@ -1,0 +1,399 @@
+"""Fused-step engine: device state in HBM and the per-step launch sequence.
+
+Per timestep the engine launches, on one CUDA stream:
+
+1. ``iblbm_ibm_step_f64`` (one CTA) — band rebuild when markers move, band
+   moments, DF / MDF / coupled MDF / DFC;
+2. ``iblbm_dense_step_f64`` — pull-stream + closure + band correction +
+   moments + collision over the whole lattice, ping-ponging two population
+   buffers.
+
+Steps between diagnostics are captured once into CUDA graphs and replayed, so
+the host issues one graph launch per chunk instead of two kernel launches per
+step.  Device layout: populations are pitched structure-of-arrays planes
+(q, j, i) with the row pitch rounded up to 32 elements (256-byte rows in FP64).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView, Case, DenseArgs, Geom,
+                   IbmArgs, check, lib, ptr)
+from .physics import (history_increment, mdf_relaxation_factor, net_gravity, oscillation_table,
+                      rigid_markers)
+from .state import initial_velocity, initialize
+
+MDF_COUPLED_OMEGA_MAX = 0.8  # iblbm/ibm/multi_particle.py:33
+MOVING_ROTATION_OMEGA_MAX = 1.0  # iblbm/ibm/strategies/mdf.py:23
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("iblbm_b200 needs a CUDA device; this package has no CPU fallback")
+    return torch
+
+
+class Engine:
+    """One lattice case on one GPU (FP64 form, the reference's arithmetic)."""
+
+    def __init__(self, cfg, device=None):
+        torch = _torch()
+        self.torch = torch
+        self.cfg = cfg
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.L = lib()
+        st = self.st = initialize(cfg)
+        if cfg.ibm_method not in ("DF", "MDF", "DFC"):
+            raise KeyError(f"unregistered ibm_method='{cfg.ibm_method}' (DF, MDF, DFC)")
+        if cfg.bc_type not in BC_IDS:
+            raise KeyError(f"bc_type='{cfg.bc_type}' is not on the accelerated path ({sorted(BC_IDS)})")
+        if cfg.delta_type not in DELTA_IDS:
+            raise KeyError(f"unknown delta_type='{cfg.delta_type}'")
+        if cfg.motion_type not in (None, "oscillating", "sedimentation"):
+            raise ValueError(f"motion_type='{cfg.motion_type}' is not supported")
+        if cfg.motion_type == "sedimentation":
+            if st.particles is None:
+                raise NotImplementedError("single-particle sedimentation runtime is not on the accelerated path")
+            if cfg.settling_inertia_model == "full_volume" or cfg.enable_rotation:
+                raise NotImplementedError("full_volume inertia and particle rotation are not on the accelerated path")
+            if cfg.time_integrator != "verlet":
+                raise NotImplementedError("only the Velocity-Verlet integrator is on the accelerated path")
+            if cfg.ibm_method != "MDF":
+                raise NotImplementedError("multi-particle sedimentation is accelerated for MDF")
+        if cfg.stream_first:
+            raise NotImplementedError("stream_first=True is not on the accelerated path")
+        nx, ny = st.nx, st.ny
+        self.N = N = nx * ny
+        pitch = (nx + 31) // 32 * 32
+        self.geom = Geom(nx, ny, pitch, pitch * ny)
+        self.qstride = pitch * ny
+        dev, f64, i32 = self.dev, torch.float64, torch.int32
+        self.stream = lambda: torch.cuda.current_stream(self.dev).cuda_stream
+        self.case = Case()
+        c = self.case
+        c.collision = COLL_IDS[cfg.collision_model]
+        c.bc = BC_IDS[cfg.bc_type]
+        c.incompressible = int(bool(cfg.incompressible_lbgk))
+        c.tau = st.tau
+        c.dt = st.dt
+        c.s_minus = (1.0 / st.tau_minus) if st.tau_minus is not None else 0.0
+        for q in range(9):
+            c.S[q] = float(st.S_diag[q]) if st.S_diag is not None else 0.0
+        c.inflow_u = st.in_u
+        c.dens = st.dens
+
+        # ---- initial populations: feq(1, U0), then the first collision ----------
+        U0 = torch.as_tensor(initial_velocity(cfg, N), device=dev).contiguous()
+        ro0 = torch.ones(N, dtype=f64, device=dev)
+        feq0 = torch.empty(N * 9, dtype=f64, device=dev)
+        s = self.stream()
+        check(self.L.iblbm_feq(ptr(ro0), ptr(U0), N, c.incompressible, ptr(feq0), s), "iblbm_feq")
+        fib0 = torch.zeros(N * 2, dtype=f64, device=dev)
+        fpost0 = torch.empty_like(feq0)
+        self._collide_aos(feq0, feq0, U0, fib0, fpost0)
+        self.f = [torch.empty(9 * self.qstride, dtype=f64, device=dev) for _ in range(2)]
+        check(self.L.iblbm_aos_to_soa(ptr(fpost0), self.geom, ptr(self.f[0]), s), "iblbm_aos_to_soa")
+        del feq0, fpost0, fib0
+        self.uring = [U0.reshape(-1).clone(), U0.reshape(-1).clone()]
+        self.ro_out = torch.empty(N, dtype=f64, device=dev)
+        self.U_out = torch.empty(N * 2, dtype=f64, device=dev)
+        self.fstar_out = torch.empty(9 * self.qstride, dtype=f64, device=dev)
+        self.parity = 0
+        self.ttt = 1
+
+        # ---- immersed boundary -------------------------------------------------------
+        self.method = cfg.ibm_method
+        self.moving = cfg.motion_type is not None
+        parts = st.particles
+        if parts is not None:
+            lbs = [p.Lb for p in parts]
+            self.larea_h = np.array([p.Larea for p in parts])
+        else:
+            lbs = [st.Lb]
+            self.larea_h = np.array([st.Larea])
+        self.P = len(lbs)
+        self.Lb = int(sum(lbs))
+        moff = np.concatenate([[0], np.cumsum(lbs)]).astype(np.int32)
+        S = (2 * DELTA_RADIUS[cfg.delta_type] + 1) ** 2
+        self.B = B = self.Lb * S
+        t = lambda n, dt=f64: torch.zeros(max(int(n), 1), dtype=dt, device=dev)
+        self.d_moff = torch.as_tensor(moff, device=dev)
+        self.d_larea = torch.as_tensor(self.larea_h, device=dev)
+        self.d_Lx, self.d_Ly, self.d_dv = t(self.Lb), t(self.Lb), t(2 * self.Lb)
+        self._upload_markers()
+        self.d_box = t(4, i32)
+        self.d_map = torch.full((N,), -1, dtype=i32, device=dev)
+        self.d_nodes, self.d_count = t(B, i32), t(1, i32)
+        self.d_fib, self.d_df = t(2 * B), t(9 * B)
+        self.d_fib_part = t(2 * B * self.P)
+        self.d_scr = t(self.L.iblbm_ibm_scratch_doubles(self.Lb, B, self.P))
+        self.d_iscr = t(self.L.iblbm_ibm_scratch_ints(self.Lb, B, N), i32)
+        self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy = (t(self.Lb) for _ in range(4))
+        self.d_dfc_force = t(2 * self.Lb)
+        self.d_stats, self.d_dstats = t(5, i32), t(2)
+        self.d_lambda, self.d_lambda_valid = t(self.Lb), t(1, i32)
+        self.d_counter = t(1, i32)
+        self.xt = None
+        if cfg.motion_type == "oscillating":
+            table = oscillation_table(cfg.max_steps + 2, cfg.lattice_u, cfg.KC, st.r, st.lattice_r)
+            self.xt = torch.as_tensor(table, device=dev)
+            self.d_Lxc = torch.as_tensor(st.Lx, device=dev)
+            self.d_Lyc = torch.as_tensor(st.Ly, device=dev)
+            self.d_counter.fill_(1)
+        self.omega = 1.0
+        if self.method == "MDF":
+            # iblbm/ibm/strategies/mdf.py:26-38 (markers of the initial cylinder)
+            self.omega = mdf_relaxation_factor(st.Lx, st.Ly, cfg.delta_type, float(st.Larea), float(st.dx))
+            if cfg.motion_type == "sedimentation" and cfg.enable_rotation:
+                self.omega = min(float(self.omega), MOVING_ROTATION_OMEGA_MAX)
+        self.ibm_args = [self._make_ibm_args(p) for p in (0, 1)]
+        self.dense_args = [[self._make_dense_args(p, out) for out in (False, True)] for p in (0, 1)]
+        self.rebuild_next = True
+        self.graphs = {}
+        self.last_out_step = 0
+
+    # ------------------------------------------------------------------------------
+    def _collide_aos(self, fstar, feq, U, fib, out):
+        c, s, N = self.case, self.stream(), self.N
+        if c.collision == 0:
+            rc = self.L.iblbm_collision_bgk(ptr(fstar), ptr(feq), ptr(U), ptr(fib), N, c.tau, c.dt, ptr(out), s)
+        elif c.collision == 1:
+            rc = self.L.iblbm_collision_trt(ptr(fstar), ptr(feq), ptr(U), ptr(fib), N, c.tau, self.st.tau_minus,
+                                            c.dt, ptr(out), s)
+        else:
+            Sd = (ctypes.c_double * 9)(*[float(v) for v in self.st.S_diag])
+            rc = self.L.iblbm_collision_cm_mrt(ptr(fstar), ptr(U), ptr(fib), N, Sd, c.dt, ptr(out), s)
+        check(rc, "initial collision")
+
+    def _upload_markers(self):
+        st = self.st
+        if st.particles is not None:
+            Lx = np.concatenate([p.Lx for p in st.particles])
+            Ly = np.concatenate([p.Ly for p in st.particles])
+            dv = np.concatenate([p.desired_velocity for p in st.particles])
+        else:
+            Lx, Ly, dv = st.Lx, st.Ly, st.desired_velocity
+        tt = self.torch
+        self.d_Lx.copy_(tt.as_tensor(np.ascontiguousarray(Lx, dtype=np.float64)))
+        self.d_Ly.copy_(tt.as_tensor(np.ascontiguousarray(Ly, dtype=np.float64)))
+        self.d_dv.copy_(tt.as_tensor(np.ascontiguousarray(dv, dtype=np.float64).reshape(-1)))
+
+    def _make_ibm_args(self, parity):
+        cfg, a = self.cfg, IbmArgs()
+        a.g, a.c = self.geom, self.case
+        a.method = IBM_IDS[self.method]
+        a.delta_type = DELTA_IDS[cfg.delta_type]
+        a.rebuild = 1
+        a.n_particles, a.lb_total = self.P, self.Lb
+        a.moff, a.Lx, a.Ly, a.dvel, a.larea = (ptr(x) for x in (self.d_moff, self.d_Lx, self.d_Ly, self.d_dv,
+                                                                 self.d_larea))
+        a.dx, a.dy = self.st.dx, self.st.dy
+        if self.xt is not None:
+            a.Lx_c, a.Ly_c, a.xt_table, a.step_counter = ptr(self.d_Lxc), ptr(self.d_Lyc), ptr(self.xt), ptr(
+                self.d_counter)
+            a.xt_len = int(self.xt.numel())
+        a.mdf_iterations = int(cfg.mdf_iterations)
+        a.mdf_min_iterations = int(cfg.mdf_min_iterations)
+        a.mdf_coupled = int(self.P >= 2)
+        a.mdf_omega, a.mdf_tol, a.mdf_omega_max = float(self.omega), float(cfg.mdf_tolerance), MDF_COUPLED_OMEGA_MAX
+        a.lambda_, a.lambda_valid = ptr(self.d_lambda), ptr(self.d_lambda_valid)
+        a.dfc_cache_lambda = int(cfg.motion_type is None)
+        a.correction_scale = 1.0
+        a.fpost_prev, a.uring_prev = ptr(self.f[parity]), ptr(self.uring[parity])
+        a.box, a.map, a.band_nodes, a.band_count = (ptr(x) for x in (self.d_box, self.d_map, self.d_nodes,
+                                                                     self.d_count))
+        a.band_capacity, a.box_capacity = self.B, self.N
+        a.band_fib, a.band_df, a.band_fib_part = ptr(self.d_fib), ptr(self.d_df), ptr(self.d_fib_part)
+        a.scratch, a.iscratch = ptr(self.d_scr), ptr(self.d_iscr)
+        a.Lux, a.Luy, a.Lfx, a.Lfy = (ptr(x) for x in (self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy))
+        a.dfc_force = ptr(self.d_dfc_force)
+        a.stats, a.dstats = ptr(self.d_stats), ptr(self.d_dstats)
+        return a
+
+    def _make_dense_args(self, parity, outputs):
+        a = DenseArgs()
+        a.g, a.c = self.geom, self.case
+        a.ibm = IBM_IDS[self.method]
+        a.fpost_prev, a.fpost_next = ptr(self.f[parity]), ptr(self.f[1 - parity])
+        a.uring_prev, a.uring_next = ptr(self.uring[parity]), ptr(self.uring[1 - parity])
+        a.band = BandView(ptr(self.d_box), ptr(self.d_map), ptr(self.d_fib), ptr(self.d_df))
+        if outputs:
+            a.ro_out, a.U_out, a.fstar_out = ptr(self.ro_out), ptr(self.U_out), ptr(self.fstar_out)
+        return a
+
+    # ------------------------------------------------------------------------------
+    def _launch(self, outputs=False, events=None):
+        """Launch one timestep (IBM band kernel, then the dense kernel).  With
+        events=(e0, e1, e2) the three CUDA events are recorded before the IBM
+        kernel, between the two kernels and after the dense kernel."""
+        s = self.stream()
+        ia = self.ibm_args[self.parity]
+        ia.rebuild = 1 if (self.rebuild_next or self.moving) else 0
+        if events:
+            events[0].record()
+        check(self.L.iblbm_ibm_step_f64(ctypes.byref(ia), s), "iblbm_ibm_step_f64")
+        self.rebuild_next = False
+        if events:
+            events[1].record()
+        da = self.dense_args[self.parity][1 if outputs else 0]
+        check(self.L.iblbm_dense_step_f64(ctypes.byref(da), s), "iblbm_dense_step_f64")
+        if events:
+            events[2].record()
+        self.parity ^= 1
+
+    def _graph(self, length):
+        key = (self.parity, length)
+        g = self.graphs.get(key)
+        if g is None:
+            torch = self.torch
+            side = torch.cuda.Stream(self.dev)
+            side.wait_stream(torch.cuda.current_stream(self.dev))
+            g = torch.cuda.CUDAGraph()
+            p0 = self.parity
+            with torch.cuda.stream(side):
+                with torch.cuda.graph(g, stream=side):
+                    for _ in range(length):
+                        self._launch(False)
+            torch.cuda.current_stream(self.dev).wait_stream(side)
+            self.parity = p0  # capture does not execute; restore the bookkeeping
+            self.graphs[key] = g
+        return g
+
+    def advance(self, nsteps, outputs_last=True, use_graph=True):
+        """Advance nsteps timesteps; the last one writes rho/U/f* when outputs_last."""
+        if nsteps <= 0:
+            return
+        if self.st.particles is not None:
+            for k in range(nsteps):
+                self._sedimentation_step(outputs=outputs_last and k == nsteps - 1)
+            return
+        if self.rebuild_next:
+            self._launch(outputs=(outputs_last and nsteps == 1))
+            self.ttt += 1
+            nsteps -= 1
+        body = nsteps - 1 if outputs_last else nsteps
+        if body > 0:
+            if use_graph and body >= 4:
+                g = self._graph(body)
+                g.replay()
+                self.parity ^= (body & 1)
+            else:
+                for _ in range(body):
+                    self._launch(False)
+            self.ttt += body
+        if outputs_last and nsteps > 0:
+            self._launch(True)
+            self.ttt += 1
+            self.last_out_step = self.ttt - 1
+
+    # ---- multi-particle sedimentation (host Newton-Euler, as the reference) ----------
+    def _sedimentation_step(self, outputs):
+        cfg, st = self.cfg, self.st
+        for p in st.particles:  # runtime/scenarios/sedimentation_multi.py:36-80
+            F = p.force + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
+            vel_half = p.vel + 0.5 * st.dt * F / p.mass
+            hist = history_increment(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            if hist is not None:
+                vel_half = vel_half + 0.5 * hist
+            p.pos = p.pos + st.dt * vel_half * st.dx
+            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=0.0)
+            dv = np.empty((p.Lb, 2))
+            dv[:, 0] = float(vel_half[0])
+            dv[:, 1] = float(vel_half[1])
+            p.desired_velocity = dv
+            p.vel_half = vel_half
+        self._upload_markers()
+        self._launch(outputs)
+        self.ttt += 1
+        if outputs:
+            self.last_out_step = self.ttt - 1
+        forces = self.particle_forces()
+        for p, fp in zip(st.particles, forces):  # runtime/scenarios/sedimentation_multi.py:83-111
+            p.fib_force = fp
+            F = fp + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
+            vel_new = p.vel_half + 0.5 * st.dt * F / p.mass
+            hist = history_increment(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            if hist is not None:
+                vel_new = vel_new + 0.5 * hist
+            if cfg.settling_inertia_model == "feng_b2":
+                vel_new = vel_new + (1.0 / p.rho_ratio) * (p.vel - p.vel_prev)
+            p.vel_prev = p.vel.copy()
+            p.vel = vel_new
+            p.force = fp
+
+    def particle_forces(self):
+        """-sum of each particle's spread force over the lattice, summed like the
+        reference (numpy over the dense N x 2 field: iblbm/ibm/multi_particle.py:233-241)."""
+        nb = int(self.d_count.item())
+        nodes = self.d_nodes[:nb].cpu().numpy()
+        part = self.d_fib_part[: 2 * self.B * self.P].reshape(self.P, self.B, 2)[:, :nb].cpu().numpy()
+        out = []
+        for p in range(self.P):
+            dense = np.zeros((self.N, 2))
+            dense[nodes] = part[p]
+            out.append(np.array([-float(dense[:, 0].sum()), -float(dense[:, 1].sum())]))
+        return out
+
+    # ---- read-back ----------------------------------------------------------------
+    def band_fib_dense(self):
+        torch = self.torch
+        nb = int(self.d_count.item())
+        fib = torch.zeros(self.N, 2, dtype=torch.float64, device=self.dev)
+        if self.method in ("DF", "MDF") and nb > 0:
+            fib[self.d_nodes[:nb].long()] = self.d_fib[: 2 * nb].reshape(nb, 2)
+        return fib
+
+    def cd_cl(self):
+        """Cd, Cl of the last output step — iblbm/diagnostics/core.py:53-113."""
+        cfg, st = self.cfg, self.st
+        u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
+        ro_mean = float(self.ro_out.mean())
+        denom = ro_mean * u_ref ** 2 * st.lattice_r
+        if self.method == "DFC":
+            force = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).sum(0).cpu().numpy()
+            return float(abs(force[0])) / denom, float(force[1]) / denom
+        nb = int(self.d_count.item())
+        sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).sum(0).cpu())
+        return abs(sx) / denom, sy / denom
+
+    def mdf_stats(self):
+        s = self.d_stats.cpu().numpy()
+        d = self.d_dstats.cpu().numpy()
+        return {"iter_count": int(s[0]), "diverged": bool(s[1]), "converged": bool(s[2]),
+                "guard_trips": int(s[3]), "last_residual": float(d[0]), "omega_used": float(d[1])}
+
+    def status(self):
+        return int(self.d_stats[4].item())
+
+    def read_state(self):
+        """Copy the last output step's fields into host arrays on self.st (AoS, the
+        reference's layout) and return it."""
+        torch, st = self.torch, self.st
+        s = self.stream()
+        fs = torch.empty(self.N * 9, dtype=torch.float64, device=self.dev)
+        check(self.L.iblbm_soa_to_aos(ptr(self.fstar_out), self.geom, ptr(fs), s), "iblbm_soa_to_aos")
+        feq = torch.empty_like(fs)
+        check(self.L.iblbm_feq(ptr(self.ro_out), ptr(self.U_out), self.N, self.case.incompressible, ptr(feq), s),
+              "iblbm_feq")
+        st.fstar = fs.reshape(self.N, 9).cpu().numpy()
+        st.feq = feq.reshape(self.N, 9).cpu().numpy()
+        st.ro = self.ro_out.cpu().numpy()
+        st.U = self.U_out.reshape(self.N, 2).cpu().numpy()
+        st.fib = self.band_fib_dense().cpu().numpy()
+        if self.method == "DFC":
+            st.dfc_force_lagr = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).cpu().numpy()
+        if self.method == "MDF":
+            st.mdf_iter_stats = self.mdf_stats()
+        return st
+
+    def fpost_aos(self):
+        """Post-collision populations of the last completed step (AoS)."""
+        torch = self.torch
+        out = torch.empty(self.N * 9, dtype=torch.float64, device=self.dev)
+        check(self.L.iblbm_soa_to_aos(ptr(self.f[self.parity]), self.geom, ptr(out), self.stream()),
+              "iblbm_soa_to_aos")
+        return out.reshape(self.N, 9).cpu().numpy()

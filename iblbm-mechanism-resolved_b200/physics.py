@@ -1,0 +1,116 @@
+"""Host-side setup physics: marker geometry, the MDF relaxation factor, the
+oscillation table and rigid-body (Newton-Euler) helpers.
+
+These run once per run (or once per step on a few scalars) on the host in FP64
+numpy, as in the reference; the per-node and per-marker work is on the GPU.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DELTA_RADIUS = {"peskin4pt": 2, "hat": 1}
+
+
+def circle_markers(cx, cy, r_domain, lattice_r, dx, spacing_factor, retraction_dx):
+    """Equally spaced markers on a circle — iblbm/init.py:211-243 and
+    iblbm/physics/markers.py:61-85 (both use this arithmetic).
+
+    Returns (Lx, Ly, Lb, Larea); coordinates in domain units, Larea (the arc
+    length per marker) in lattice units."""
+    n_param = 2.0 * np.pi * lattice_r / spacing_factor
+    step = 1.0 / n_param
+    s = np.arange(0, 1.0 + step * 0.5, step)
+    s = s[s <= 1.0 + 1e-12]
+    if len(s) > 1 and np.abs(s[-1] - 1.0) < step * 0.5:
+        s = s[:-1]  # the last point would duplicate the first
+    theta = 2.0 * np.pi * s
+    radius = r_domain - retraction_dx * dx
+    Lx = radius * np.cos(theta) + cx
+    Ly = radius * np.sin(theta) + cy
+    Lb = len(Lx)
+    Larea = 2.0 * np.pi * (lattice_r - retraction_dx) / Lb
+    return np.ascontiguousarray(Lx), np.ascontiguousarray(Ly), Lb, Larea
+
+
+def _phi_np(delta_type, r):
+    ar = np.abs(r)
+    if delta_type == "hat":
+        return np.maximum(1.0 - ar, 0.0)
+    out = np.zeros_like(ar)
+    near = ar <= 1.0
+    far = (~near) & (ar <= 2.0)
+    a1, a2 = ar[near], ar[far]
+    out[near] = 0.125 * (3.0 - 2.0 * a1 + np.sqrt(np.maximum(1.0 + 4.0 * a1 - 4.0 * a1 ** 2, 0.0)))
+    out[far] = 0.125 * (5.0 - 2.0 * a2 - np.sqrt(np.maximum(-7.0 + 12.0 * a2 - 4.0 * a2 ** 2, 0.0)))
+    return out
+
+
+def mdf_relaxation_factor(Lx, Ly, delta_type, Larea, dx):
+    """omega = 1 / ||A||_inf of the marker coupling matrix (Zhang et al. 2020,
+    Eqs. 39 and 46) — iblbm/ibm/a_norm.py:75-266.
+
+    A_lm = (ds / dx^2) * S_x(l, m) * S_y(l, m) with separable 1-D overlaps
+    S_x = sum_i phi(i - x_l) phi(i - x_m) over the integer nodes the two stencils
+    share.  Evaluated for all l at once, accumulating over m in order so every
+    row sum is formed exactly as the reference's double loop forms it."""
+    a = DELTA_RADIUS[delta_type]
+    x = np.asarray(Lx, dtype=np.float64) / float(dx)
+    y = np.asarray(Ly, dtype=np.float64) / float(dx)
+    factor = float(Larea) / (1.0 * 1.0)
+    cutoff = 2.0 * a * 1.0
+    acc = np.zeros(len(x))
+    for m in range(len(x)):
+        sums = []
+        for pl, pm in ((x, x[m]), (y, y[m])):
+            lo = np.maximum(pl, pm) - a * 1.0
+            hi = np.minimum(pl, pm) + a * 1.0
+            i_lo = np.ceil(lo / 1.0)
+            n = np.floor(hi / 1.0) + 1 - i_lo  # node count of the shared support
+            s = np.zeros(len(x))
+            for t in range(2 * a + 1):
+                node = (i_lo + t) * 1.0
+                v = _phi_np(delta_type, (node - pl) / 1.0) * _phi_np(delta_type, (node - pm) / 1.0)
+                s = s + np.where(t < n, v, 0.0)
+            sums.append(s)
+        far = (np.abs(x - x[m]) >= cutoff) | (np.abs(y - y[m]) >= cutoff)
+        term = factor * sums[0] * sums[1]
+        acc = acc + np.where(far | (sums[0] == 0.0) | (sums[1] == 0.0), 0.0, term)
+    return 1.0 / float(np.max(acc))
+
+
+def oscillation_table(max_steps, lattice_u, KC, r_domain, lattice_r):
+    """Marker displacement used at each step of the oscillating cylinder.
+
+    iblbm/physics/motion.py:15-52 moves the markers after the collision of step
+    t to Lx_c - x(t), x(t) = A sin(2 pi f0 t), and sets the desired velocity to
+    (x(t), 0) (the reference's displacement convention); step t + 1 uses them.
+    Entry t of the table is the displacement in force during step t (entry 1
+    is 0: the initial markers).  Evaluated with the same scalar numpy calls as
+    the reference so every entry is bit-identical."""
+    f0 = lattice_u / (KC * 2.0 * lattice_r)
+    A = KC * 2.0 * r_domain / (2.0 * np.pi)
+    table = np.zeros(max_steps + 2)
+    for t in range(1, max_steps + 1):
+        table[t + 1] = A * np.sin(f0 * 2.0 * np.pi * t)
+    return table
+
+
+def net_gravity(rho_ratio, r_lattice, g_lattice, direction="down"):
+    """(rho_s/rho_f - 1) * pi r^2 * g — iblbm/physics/gravity.py:16-34."""
+    mag = (rho_ratio - 1.0) * (np.pi * r_lattice ** 2) * g_lattice
+    return np.array([mag, 0.0]) if direction == "right" else np.array([0.0, -mag])
+
+
+def history_increment(model, vel, vel_prev, mass, r_lattice):
+    """explicit_history: (m_f/m_s)(U^n - U^{n-1}) — physics/inertia/explicit_history.py:53-66."""
+    if model == "explicit_history":
+        return (np.pi * r_lattice ** 2 / mass) * (vel - vel_prev)
+    return None
+
+
+def rigid_markers(Lx_c, Ly_c, cx0, cy0, pos, angle=0.0):
+    """X = R(angle) (X_c - X_0) + x_p — iblbm/physics/markers.py:23-38."""
+    c, s = np.cos(angle), np.sin(angle)
+    rx = Lx_c - cx0
+    ry = Ly_c - cy0
+    return c * rx - s * ry + pos[0], s * rx + c * ry + pos[1]

@@ -1,0 +1,186 @@
+/*
+ * iblbm_b200.h — C ABI of the B200-native IB-LBM hot path (libiblbm_b200.so).
+ *
+ * Plain C: device pointers are `void*`/typed pointers into CUDA global memory
+ * (any allocator; the Python host uses PyTorch tensors), sizes are ints, the
+ * stream is a `cudaStream_t` passed as `void*`.  Every entry point returns 0 on
+ * success and a negative IBLBM_E_* code on a rejected argument or a CUDA launch
+ * error; kernels that can fail at run time (bounded iteration, capacity) report
+ * through a device-side status word that the caller reads.
+ *
+ * The reference (mulgae-life/iblbm-mechanism-resolved) binds its GPU path from
+ * Python through CuPy RawModule kernels wrapped in iblbm/gpu_kernels.py; the
+ * "Replaces" line of each entry point names the wrapper and its caller it
+ * stands in for.  Population arrays of the reference-shaped entry points use
+ * the reference's AoS layout f[n*9 + q], n = j*nx + i; the fused step engine
+ * uses the pitched structure-of-arrays layout described by iblbm_geom.
+ */
+#ifndef IBLBM_B200_H
+#define IBLBM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IBLBM_OK 0
+#define IBLBM_E_ARG -1      /* bad argument (null pointer, size, unknown id) */
+#define IBLBM_E_LAUNCH -2   /* CUDA launch / configuration error */
+#define IBLBM_E_CAPACITY -3 /* a size exceeds the scratch capacity the caller provided */
+
+/* collision ids */
+#define IBLBM_COLL_BGK 0
+#define IBLBM_COLL_TRT 1
+#define IBLBM_COLL_CMMRT 2
+/* boundary closure ids (iblbm/boundary/*.py) */
+#define IBLBM_BC_DIRICHLET_NEUMANN 0
+#define IBLBM_BC_OPEN 1
+#define IBLBM_BC_SETTLING 2
+#define IBLBM_BC_VELOCITY_INLET 3
+/* immersed-boundary method ids (iblbm/ibm/strategies/*.py) */
+#define IBLBM_IBM_NONE 0
+#define IBLBM_IBM_DF 1
+#define IBLBM_IBM_MDF 2
+#define IBLBM_IBM_DFC 3
+/* delta kernel ids (iblbm/ibm/common.py:52-119) */
+#define IBLBM_DELTA_PESKIN4 0
+#define IBLBM_DELTA_HAT 1
+
+/* Lattice geometry of the fused engine: population q of node (i, j) is element
+ * q*qstride + j*pitch + i of a population buffer; pitch >= nx is a multiple of 32. */
+typedef struct {
+    int nx, ny, pitch;
+    long long qstride;
+} iblbm_geom;
+
+/* Physical/numerical parameters of one lattice case (host-computed with the
+ * reference's formulas, iblbm/init.py:116-265 and lbm/collision/*.py). */
+typedef struct {
+    int collision;       /* IBLBM_COLL_* */
+    int bc;              /* IBLBM_BC_* */
+    int incompressible;  /* SimConfig.incompressible_lbgk */
+    double tau, dt;
+    double s_minus;      /* TRT: 1/tau_minus */
+    double S[9];         /* CM-MRT relaxation rates */
+    double inflow_u, dens;
+} iblbm_case;
+
+/* Band: the lattice nodes under the marker stencils.  `box` holds x0, y0, w, h
+ * of the box enclosing the band; `map` is a full-lattice int array (nx*ny) that
+ * holds the band index of band nodes and -1 elsewhere inside the box. */
+typedef struct {
+    const int *box;
+    const int *map;
+    const double *fib;  /* band x 2: IB force density (DF/MDF) */
+    const double *df;   /* band x 9: distribution correction (DFC) */
+} iblbm_band_view;
+
+/* One fused timestep over the whole lattice (FP64, the reference's arithmetic):
+ * pull-streaming from fpost_prev, boundary closure, band correction, macroscopic
+ * moments, velocity correction, equilibrium and collision into fpost_next.
+ * Optional outputs (may be NULL): ro/U (nx*ny, nx*ny*2, AoS) after the velocity
+ * correction, fstar (SoA like fpost) after streaming/closure/DFC. */
+typedef struct {
+    iblbm_geom g;
+    iblbm_case c;
+    int ibm;                    /* IBLBM_IBM_* applied on the band */
+    const double *fpost_prev;   /* SoA, 9 * qstride */
+    double *fpost_next;
+    const double *uring_prev;   /* nx*ny*2, previous step's U on rows/cols 1,2,n-3,n-2 */
+    double *uring_next;
+    iblbm_band_view band;
+    double *ro_out, *U_out, *fstar_out;
+} iblbm_dense_args;
+
+/* Replaces (fused): collision_gpu/collision_trt_gpu/collision_cm_mrt_gpu
+ * (iblbm/gpu_kernels.py:760-843), streaming_gpu (:846-875), the boundary
+ * closures (iblbm/boundary/*.py apply_bc_*), macroscopic_gpu (:878-903),
+ * velocity_correction_gpu (:930-948) and feq_gpu (:906-927), in the order of
+ * iblbm/runtime/loop.py:63-138. */
+int iblbm_dense_step_f64(const iblbm_dense_args *a, void *stream);
+
+/* Immersed-boundary band step (one CTA): rebuilds the band from the current
+ * markers (when `rebuild` or the markers move), computes the post-streaming
+ * populations and moments on the band, and runs DF / MDF / coupled MDF / DFC.
+ * Marker positions are in domain units (x / dx is the lattice coordinate). */
+typedef struct {
+    iblbm_geom g;
+    iblbm_case c;
+    int method;        /* IBLBM_IBM_DF / MDF / DFC */
+    int delta_type;    /* IBLBM_DELTA_* */
+    int rebuild;       /* 1: rebuild stencils, band and lists this step */
+    int n_particles;   /* >= 1; markers of particle p are [moff[p], moff[p+1]) */
+    int lb_total;      /* moff[n_particles] (sizes the shared-memory marker arrays) */
+    const int *moff;   /* device, n_particles + 1 */
+    const double *Lx, *Ly;   /* device, marker positions (Lb_total) */
+    const double *dvel;      /* device, desired velocity (Lb_total x 2) */
+    const double *larea;     /* device, arc length per particle */
+    double dx, dy;
+    /* motion from a table: when xt_table != NULL the markers this step are
+     * Lx = Lx_c - xt_table[*step_counter], desired velocity (xt, 0)
+     * (iblbm/physics/motion.py:15-52); step_counter is incremented. */
+    const double *Lx_c, *Ly_c, *xt_table;
+    int *step_counter;
+    int xt_len;        /* entries in xt_table; a counter past the end sets status 4 */
+    /* MDF */
+    int mdf_iterations, mdf_min_iterations, mdf_coupled;
+    double mdf_omega, mdf_tol, mdf_omega_max;
+    /* DFC */
+    double *lambda;    /* Lb_total: lambda(k) */
+    int *lambda_valid; /* device flag: lambda holds a cached value */
+    int dfc_cache_lambda; /* 1 for fixed bodies: compute lambda once, then reuse (strategies/dfc.py:32,48-49) */
+    double correction_scale;
+    /* inputs */
+    const double *fpost_prev, *uring_prev;
+    /* band state (written) */
+    int *box, *map, *band_nodes, *band_count; /* map: nx*ny ints, -1 outside the band */
+    int band_capacity, box_capacity;
+    double *band_fib, *band_df;        /* band x 2, band x 9 */
+    double *band_fib_part;             /* particles x band x 2 (per-particle totals) */
+    double *scratch;                   /* >= iblbm_ibm_scratch_doubles(...) doubles */
+    int *iscratch;                     /* >= iblbm_ibm_scratch_ints(...) ints */
+    /* per-marker outputs (Lb_total): interpolated velocity, force, DFC force */
+    double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
+    /* stats: [iter_count, diverged, converged, guard_trips, status],
+     * dstats: [last_residual, omega_used] */
+    int *stats;
+    double *dstats;
+} iblbm_ibm_args;
+
+/* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
+ * ibm/strategies/df.py:27-49, the MDF loop of iblbm/ibm/mdf.py:61-229 (and the
+ * coupled multi-particle loop of iblbm/ibm/multi_particle.py:62-316), and
+ * compute_lambda_gpu + dfc_correction_gpu (gpu_kernels.py:1091-1223) called
+ * from ibm/strategies/dfc.py:31-54. */
+int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
+int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
+int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int box_capacity);
+int iblbm_ibm_smem_bytes(int lb_total);
+
+/* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
+/* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */
+int iblbm_feq(const double *ro, const double *U, int N, int incompressible, double *feq, void *stream);
+/* Replaces macroscopic_gpu (gpu_kernels.py:878-903) <- lbm/macroscopic.py:52-59 */
+int iblbm_macroscopic(const double *fstar, int N, int incompressible, double *ro, double *U, void *stream);
+/* Replaces collision_gpu (gpu_kernels.py:760-784) <- lbm/collision/bgk.py:55-57 */
+int iblbm_collision_bgk(const double *fstar, const double *feq, const double *U, const double *fib, int N,
+                        double tau, double dt, double *f, void *stream);
+/* Replaces collision_trt_gpu (gpu_kernels.py:787-812) <- lbm/collision/trt.py:88-90 */
+int iblbm_collision_trt(const double *fstar, const double *feq, const double *U, const double *fib, int N,
+                        double tau, double tau_minus, double dt, double *f, void *stream);
+/* Replaces collision_cm_mrt_gpu (gpu_kernels.py:815-843) <- lbm/collision/cm_mrt.py:198-200 */
+int iblbm_collision_cm_mrt(const double *fstar, const double *U, const double *fib, int N,
+                           const double *S_diag_host, double dt, double *f, void *stream);
+/* Replaces streaming_gpu (gpu_kernels.py:846-875) <- lbm/streaming.py:80-84 */
+int iblbm_streaming(const double *fstar_old, const double *f, int nx, int ny, double *fstar_new, void *stream);
+/* Replaces velocity_correction_gpu (gpu_kernels.py:930-948) <- ibm/dispatch.py:18-33 */
+int iblbm_velocity_correction(double *U, const double *fib, const double *ro, int N, double dt,
+                              int incompressible, void *stream);
+
+/* ---- layout conversion between the reference AoS and the engine SoA ----- */
+int iblbm_aos_to_soa(const double *aos, iblbm_geom g, double *soa, void *stream);
+int iblbm_soa_to_aos(const double *soa, iblbm_geom g, double *aos, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IBLBM_B200_H */

@@ -1,0 +1,60 @@
+"""The C-ABI library loads, exports every entry point include/iblbm_b200.h
+declares, and the ctypes structures match the C layout (CPU only: no kernel
+is launched)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "iblbm_b200.h")
+
+
+def _declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^int\s+(iblbm_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from iblbm_b200 import _lib
+    L = _lib.lib()
+    names = _declared()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) <= set(_lib._SIGS), set(names) - set(_lib._SIGS)
+
+
+def test_struct_layout_matches_c(tmp_path):
+    from iblbm_b200 import _lib
+    probe = tmp_path / "probe.c"
+    fields = {"iblbm_ibm_args": [f for f, _ in _lib.IbmArgs._fields_],
+              "iblbm_dense_args": [f for f, _ in _lib.DenseArgs._fields_],
+              "iblbm_case": [f for f, _ in _lib.Case._fields_]}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
+    for st, fl in fields.items():
+        lines.append(f'printf("{st} %zu\\n", sizeof({st}));')
+        for f in fl:
+            cf = "lambda" if f == "lambda_" else f
+            lines.append(f'printf("{st}.{f} %zu\\n", offsetof({st}, {cf}));')
+    lines.append("return 0;}")
+    probe.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.check_call(["gcc", str(probe), "-o", str(exe)])
+    out = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().split("\n") if l)
+    for st, cls in (("iblbm_ibm_args", _lib.IbmArgs), ("iblbm_dense_args", _lib.DenseArgs),
+                    ("iblbm_case", _lib.Case)):
+        assert int(out[st]) == ctypes.sizeof(cls), st
+        for f, _ in cls._fields_:
+            assert int(out[f"{st}.{f}"]) == getattr(cls, f).offset, (st, f)
+
+
+def test_rejects_bad_arguments_without_a_gpu():
+    """Argument validation happens on the host before any launch."""
+    from iblbm_b200 import _lib
+    L = _lib.lib()
+    assert L.iblbm_dense_step_f64(None, None) == -1
+    assert L.iblbm_ibm_step_f64(None, None) == -1
+    assert L.iblbm_feq(None, None, 10, 0, None, None) == -1
