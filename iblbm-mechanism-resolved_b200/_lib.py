@@ -38,7 +38,7 @@ class BandView(ctypes.Structure):
 class DenseArgs(ctypes.Structure):
     _fields_ = [("g", Geom), ("c", Case), ("ibm", _i), ("fpost_prev", _vp), ("fpost_next", _vp),
                 ("uring_prev", _vp), ("uring_next", _vp), ("band", BandView), ("ro_out", _vp),
-                ("U_out", _vp), ("fstar_out", _vp)]
+                ("U_out", _vp), ("fstar_out", _vp), ("skip_box", _vp), ("only_box", _vp), ("box_blocks", _i)]
 
 
 class IbmArgs(ctypes.Structure):
@@ -49,7 +49,8 @@ class IbmArgs(ctypes.Structure):
                 ("mdf_min_iterations", _i), ("mdf_coupled", _i), ("mdf_omega", _d), ("mdf_tol", _d),
                 ("mdf_omega_max", _d), ("lambda_", _vp), ("lambda_valid", _vp), ("dfc_cache_lambda", _i),
                 ("correction_scale", _d), ("fpost_prev", _vp), ("uring_prev", _vp), ("box", _vp),
-                ("map", _vp), ("band_nodes", _vp), ("band_count", _vp), ("band_capacity", _i),
+                ("map", _vp), ("band_nodes", _vp), ("band_count", _vp), ("list_cache", _vp), ("excl_cur", _vp),
+                ("excl_next", _vp), ("band_capacity", _i),
                 ("box_capacity", _i), ("band_fib", _vp), ("band_df", _vp), ("band_fib_part", _vp),
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp)]
@@ -61,7 +62,8 @@ _SIGS = {
     "iblbm_ibm_step_f64": [ctypes.POINTER(IbmArgs), _vp],
     "iblbm_ibm_scratch_doubles": [_i, _i, _i],
     "iblbm_ibm_scratch_ints": [_i, _i, _i],
-    "iblbm_ibm_smem_bytes": [_i],
+    "iblbm_ibm_list_cache_ints": [_i, _i, _i],
+    "iblbm_ibm_smem_bytes": [_i, _i, _i],
     "iblbm_feq": [_vp, _vp, _i, _i, _vp, _vp],
     "iblbm_macroscopic": [_vp, _i, _i, _vp, _vp, _vp],
     "iblbm_collision_bgk": [_vp, _vp, _vp, _vp, _i, _d, _d, _vp, _vp],

@@ -1,55 +1,71 @@
 // ibm_f64.cu — immersed-boundary marker loop on the band, FP64.
 //
 // The band is the set of lattice nodes under the marker stencils (a few hundred
-// to a few thousand nodes).  One CTA of 1024 threads owns it for the whole step:
+// to a few thousand nodes).  One CTA of 512 threads owns it for the whole step:
 //
 //   rebuild (fixed bodies: once; moving bodies: every step)
-//     markers -> nearest node ix0 = floor(x/dx + 0.5), separable weights
-//     wx[5], wy[5]; bounding box; band compaction in row-major (= lattice
-//     index) order; per-node contribution lists (CSR) sorted by the
-//     reference's scatter order e = k*Lb + l (stencil slot k = (di outer,
-//     dj inner), then marker l), which is the order numpy's add.at applies.
+//     markers -> nearest node ix0 = floor(x/dx + 0.5) and separable weights
+//     wx[2a+1], wy[2a+1]; bounding box; band compaction in row-major (= lattice
+//     index) order; per-node contribution lists sorted by stencil slot k
+//     (di outer, dj inner) then marker l — the order in which numpy's add.at
+//     applies the reference's scatter.
 //   every step
-//     post-streaming populations and moments on the band (same device
-//     functions as the dense kernel), then DF, MDF (all iterations resident,
-//     residual reduced on chip, no host round trip), coupled multi-particle
-//     MDF, or DFC.
+//     post-streaming populations and moments on the band (the dense kernel's
+//     device functions), then DF, MDF (every iteration resident on chip: two
+//     barriers per iteration, residual reduced in shared memory, no host round
+//     trip), coupled multi-particle MDF, or DFC.
+//   exclusion box
+//     the band's bounding box dilated by one node is written for the next
+//     step: markers move less than one node per step, so the next band lies
+//     inside it.  The bulk collide-stream kernel of the next step skips that
+//     box and runs concurrently with this kernel; a small box kernel updates
+//     the box once this kernel has produced the band forces.
 //
-// Marker arrays live in shared memory; band arrays in global scratch (they are
-// a few tens of KB and stay in L1/L2).  Sums run in the reference's order, so
-// results are bit-identical to the reference CPU path (-fmad=false).
+// Marker data, band moments and the contribution lists live in shared memory;
+// each band node belongs to one thread, which keeps its accumulators in
+// registers.  All sums run in the reference's order, so results are
+// bit-identical to the reference CPU path (built with -fmad=false).
+#include <climits>
 #include "common.cuh"
 #include "../../include/iblbm_b200.h"
 
 namespace iblbm {
 
-constexpr int IBM_THREADS = 1024;
-constexpr int MAX_S = 25;  // (2a+1)^2 for the Peskin 4-point kernel
+constexpr int IBM_THREADS = 512;
+constexpr int NPT = 8;     // band nodes per thread: band capacity <= 4096
+constexpr int MAXP = 8;    // particles per band kernel
+constexpr int NWARP = IBM_THREADS / 32;
 
-enum IbmStatus : int { ST_OK = 0, ST_BAND_CAPACITY = 1, ST_BOX_CAPACITY = 2, ST_MARKERS = 3, ST_TABLE = 4 };
+enum IbmStatus : int { ST_OK = 0, ST_BAND_CAPACITY = 1, ST_BOX_CAPACITY = 2, ST_MARKERS = 3, ST_TABLE = 4,
+                       ST_EXCL = 5 };
 
-struct IbmShared {
-    int *ix0, *iy0, *sidx, *part;
-    double *wx, *wy, *dvx, *dvy, *R, *Lux, *Luy, *Lfx, *Lfy;
-    double* red;  // 32 doubles
-    int* ired;    // 64 ints
+template <int A>
+struct Sten {
+    static constexpr int SW = 2 * A + 1;
+    static constexpr int S = SW * SW;
 };
 
-__device__ __forceinline__ size_t align8(size_t x) { return (x + 7) & ~size_t(7); }
-
-__host__ __device__ inline size_t ibm_smem_bytes(int Lb)
+__host__ __device__ inline size_t ibm_smem_bytes_t(int Lb, int NB, int S)
 {
     size_t s = 0;
-    s += sizeof(double) * (size_t)Lb * (5 + 5 + 7);
-    s += sizeof(double) * 32;
-    s += sizeof(int) * (size_t)Lb * (2 + MAX_S + 1);
-    s += sizeof(int) * 64;
+    s += sizeof(double) * (size_t)Lb * 17;            // wx[5], wy[5], dvx, dvy, R, Lux, Luy, Lfx, Lfy
+    s += sizeof(double) * (size_t)NB * 3;             // band rho, U_work x, U_work y
+    s += sizeof(double) * 2 * MAXP * NWARP;           // warp partial maxima
+    s += sizeof(int) * (size_t)Lb * (3 + 2 * S);      // ix0, iy0, part, sidx[S], entries[S]
+    s += sizeof(int) * ((size_t)NB + 1);              // list starts
+    s += sizeof(int) * 64;                            // scan scratch
     return (s + 15) & ~size_t(15);
 }
 
-__device__ IbmShared carve(char* base, int Lb)
+struct Sm {
+    double *wx, *wy, *dvx, *dvy, *R, *Lux, *Luy, *Lfx, *Lfy, *bro, *bwx, *bwy, *wred;
+    int *ix0, *iy0, *part, *sidx, *cent, *cstart, *ired;
+};
+
+template <int S>
+__device__ Sm carve(char* base, int Lb, int NB)
 {
-    IbmShared s;
+    Sm s;
     double* d = reinterpret_cast<double*>(base);
     s.wx = d; d += 5 * Lb;
     s.wy = d; d += 5 * Lb;
@@ -60,49 +76,34 @@ __device__ IbmShared carve(char* base, int Lb)
     s.Luy = d; d += Lb;
     s.Lfx = d; d += Lb;
     s.Lfy = d; d += Lb;
-    s.red = d; d += 32;
+    s.bro = d; d += NB;
+    s.bwx = d; d += NB;
+    s.bwy = d; d += NB;
+    s.wred = d; d += 2 * MAXP * NWARP;
     int* p = reinterpret_cast<int*>(d);
     s.ix0 = p; p += Lb;
     s.iy0 = p; p += Lb;
-    s.sidx = p; p += MAX_S * Lb;
     s.part = p; p += Lb;
+    s.sidx = p; p += S * Lb;
+    s.cent = p; p += S * Lb;
+    s.cstart = p; p += NB + 1;
     s.ired = p;
     return s;
 }
 
-// Block-wide max with NaN propagation (numpy max semantics).  All threads
-// receive the result.
-__device__ double block_max_nan(double v, double* red)
+__device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+__device__ __forceinline__ double warp_nanmax(double v)
 {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double u = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (u > v || u != u) ? u : v;
-    }
-    __syncthreads();
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        double x = (lane < (blockDim.x >> 5)) ? red[lane] : -INFINITY;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double u = __shfl_xor_sync(0xffffffffu, x, o);
-            x = (u > x || u != u) ? u : x;
-        }
-        if (lane == 0) red[0] = x;
-    }
-    __syncthreads();
-    const double r = red[0];
-    __syncthreads();
-    return r;
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
-// Block-wide exclusive scan of one int per thread; returns the prefix and
-// writes the total to *total.
+// Block-wide exclusive scan of one int per thread; returns the prefix, writes the total.
 __device__ int block_exscan(int v, int* ired, int* total)
 {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -113,85 +114,78 @@ __device__ int block_exscan(int v, int* ired, int* total)
     if (lane == 31) ired[wid] = x;
     __syncthreads();
     if (wid == 0) {
-        int y = lane < nw ? ired[lane] : 0;
+        int y = lane < NWARP ? ired[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, y, o);
             if (lane >= o) y += u;
         }
-        if (lane < nw) ired[32 + lane] = y;
+        if (lane < NWARP) ired[32 + lane] = y;
     }
     __syncthreads();
     const int base = wid > 0 ? ired[32 + wid - 1] : 0;
-    *total = ired[32 + nw - 1];
+    *total = ired[32 + NWARP - 1];
     __syncthreads();
     return base + x - v;
 }
 
 template <int BC>
 __device__ void band_moments(const iblbm_ibm_args& a, const Geom& g, const BcParams& bc, int nb, const int* nodes,
-                             double* bro, double* bu0, double* bu1, double* bfs)
+                             Sm& sh, double* bfs)
 {
     const bool incomp = a.c.incompressible != 0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    for (int b = threadIdx.x; b < nb; b += IBM_THREADS) {
         const int n = nodes[b];
         const int j = n / g.nx, i = n - j * g.nx;
         double f[9];
         fstar_node<BC>(a.fpost_prev, a.uring_prev, g, bc, incomp, i, j, f);
         if (bfs) {
 #pragma unroll
-            for (int q = 0; q < 9; ++q) bfs[9 * b + q] = f[q];
+            for (int q = 0; q < 9; ++q) bfs[9 * (size_t)b + q] = f[q];
         }
         double ro, u0, u1;
         macro_seq(f, incomp, ro, u0, u1);
-        bro[b] = ro;
-        bu0[b] = u0;
-        bu1[b] = u1;
+        sh.bro[b] = ro;
+        sh.bwx[b] = u0;
+        sh.bwy[b] = u1;
     }
 }
 
-void make_params(const iblbm_case& c, CollParams& cp, BcParams& bc);
+template <int A>
+__device__ __forceinline__ double wgt(const Sm& sh, int l, int k)
+{
+    constexpr int SW = Sten<A>::SW;
+    return sh.wx[l * 5 + k / SW] * sh.wy[l * 5 + k % SW];
+}
 
+template <int A>
 __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ibm_args a, BcParams bc)
 {
+    constexpr int SW = Sten<A>::SW, S = Sten<A>::S;
     extern __shared__ __align__(16) char smem_raw[];
     const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
-    const int P = a.n_particles;
-    __shared__ int s_lb, s_nb, s_status, s_box[4], s_step;
-    if (threadIdx.x == 0) {
-        s_lb = a.lb_total;
+    const int P = a.n_particles, Lb = a.lb_total, NB = a.band_capacity;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    __shared__ int s_nb, s_status, s_box[4], s_step;
+    if (tid == 0) {
         s_status = ST_OK;
         s_step = a.step_counter ? *a.step_counter : 0;
         if (a.xt_table && (s_step < 0 || s_step >= a.xt_len)) s_status = ST_TABLE;
     }
     __syncthreads();
     if (s_status != ST_OK) {
-        if (threadIdx.x == 0) a.stats[4] = s_status;
+        if (tid == 0) a.stats[4] = s_status;
         return;
     }
-    const int Lb = s_lb;
-    IbmShared sh = carve(smem_raw, Lb);
-    const int A = (a.delta_type == 0) ? 2 : 1;
-    const int SW = 2 * A + 1, S = SW * SW;
+    Sm sh = carve<S>(smem_raw, Lb, NB);
     const double dx = a.dx, dy = a.dy, dt = a.c.dt;
-
-    // global scratch carve (matches iblbm_ibm_scratch_doubles / _ints)
-    const int B = a.band_capacity;
-    double* bro = a.scratch;
-    double* bu0 = bro + B;
-    double* bu1 = bu0 + B;
-    double* bvs = bu1 + B;
-    double* bwx = bvs + B;       // U_work x (MDF) / W_total (DFC)
-    double* bwy = bwx + B;       // U_work y (MDF)
-    double* bfs = bwy + B;       // 9 * B post-streaming populations (DFC)
-    double* dfl = bfs + 9 * (size_t)B;  // 9 * Lb distribution corrections per marker (DFC)
-    int* cstart = a.iscratch;     // B + 1
-    int* cfill = cstart + B + 1;  // B
-    int* centry = cfill + B;      // Lb * 25
+    double* bfs = a.scratch;                       // 9 * NB post-streaming populations (DFC)
+    double* dfl = a.scratch + 9 * (size_t)NB;      // 9 * Lb distribution corrections (DFC)
+    int* cfill = a.iscratch;                       // NB
     int* nodes = a.band_nodes;
 
-    // ---- markers for this step -------------------------------------------
-    for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+    // ---- markers of this step ------------------------------------------------
+    for (int l = tid; l < Lb; l += IBM_THREADS) {
         double x, y, vx, vy;
         if (a.xt_table) {
             // iblbm/physics/motion.py:44-50: Lx = Lx_c - xt, desired velocity (xt, 0)
@@ -213,73 +207,66 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
         while (p + 1 < P && l >= a.moff[p + 1]) ++p;
         sh.part[l] = p;
         // iblbm/ibm/df.py:94-114: nearest node and separable weights
-        const long long ix0 = (long long)floor(x / dx + 0.5);
-        const long long iy0 = (long long)floor(y / dy + 0.5);
+        const double fx = floor(x / dx + 0.5), fy = floor(y / dy + 0.5);
+        const long long ix0 = (long long)fmin(fmax(fx, -1.0e9), 1.0e9);
+        const long long iy0 = (long long)fmin(fmax(fy, -1.0e9), 1.0e9);
         sh.ix0[l] = (int)ix0;
         sh.iy0[l] = (int)iy0;
+#pragma unroll
         for (int d = -A; d <= A; ++d) {
-            sh.wx[l * 5 + d + A] = phi(a.delta_type, (x - (double)(ix0 + d) * dx) / dx);
-            sh.wy[l * 5 + d + A] = phi(a.delta_type, (y - (double)(iy0 + d) * dy) / dy);
+            sh.wx[l * 5 + d + A] = phi(A == 2 ? 0 : 1, (x - (double)(ix0 + d) * dx) / dx);
+            sh.wy[l * 5 + d + A] = phi(A == 2 ? 0 : 1, (y - (double)(iy0 + d) * dy) / dy);
         }
     }
     __syncthreads();
 
+    auto node_of = [&](int l, int k) -> long long {
+        const int ei = min(max(sh.ix0[l] + k / SW - A, 0), g.nx - 1);
+        const int ej = min(max(sh.iy0[l] + k % SW - A, 0), g.ny - 1);
+        return (long long)ej * g.nx + ei;
+    };
+
     int nb;
     if (a.rebuild || a.xt_table) {
-        // ---- band rebuild ----------------------------------------------------
-        if (threadIdx.x == 0) { s_box[0] = INT_MAX; s_box[1] = INT_MAX; s_box[2] = INT_MIN; s_box[3] = INT_MIN; }
-        __syncthreads();
-        for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
-            const int x0 = min(max(sh.ix0[l] - A, 0), g.nx - 1), x1 = min(max(sh.ix0[l] + A, 0), g.nx - 1);
-            const int y0 = min(max(sh.iy0[l] - A, 0), g.ny - 1), y1 = min(max(sh.iy0[l] + A, 0), g.ny - 1);
-            atomicMin(&s_box[0], x0);
-            atomicMin(&s_box[1], y0);
-            atomicMax(&s_box[2], x1);
-            atomicMax(&s_box[3], y1);
-        }
-        // clear the previous band's map entries
+        // ---- band rebuild ------------------------------------------------------
+        if (tid == 0) { s_box[0] = INT_MAX; s_box[1] = INT_MAX; s_box[2] = INT_MIN; s_box[3] = INT_MIN; }
         const int nprev = *a.band_count;
-        for (int b = threadIdx.x; b < nprev; b += blockDim.x) a.map[nodes[b]] = -1;
+        __syncthreads();
+        for (int l = tid; l < Lb; l += IBM_THREADS) {
+            atomicMin(&s_box[0], min(max(sh.ix0[l] - A, 0), g.nx - 1));
+            atomicMin(&s_box[1], min(max(sh.iy0[l] - A, 0), g.ny - 1));
+            atomicMax(&s_box[2], min(max(sh.ix0[l] + A, 0), g.nx - 1));
+            atomicMax(&s_box[3], min(max(sh.iy0[l] + A, 0), g.ny - 1));
+        }
+        for (int b = tid; b < nprev; b += IBM_THREADS) a.map[nodes[b]] = -1;  // clear the previous band
         __syncthreads();
         const int bx0 = s_box[0], by0 = s_box[1], bw = s_box[2] - s_box[0] + 1, bh = s_box[3] - s_box[1] + 1;
-        if ((long long)bw * bh > (long long)a.box_capacity) {
-            if (threadIdx.x == 0) s_status = ST_BOX_CAPACITY;
-        }
-        // mark stencil nodes
-        for (int e = threadIdx.x; e < S * Lb; e += blockDim.x) {
-            const int l = e % Lb, k = e / Lb;
-            const int di = k / SW - A, dj = k % SW - A;
-            const int ei = min(max(sh.ix0[l] + di, 0), g.nx - 1), ej = min(max(sh.iy0[l] + dj, 0), g.ny - 1);
-            a.map[(long long)ej * g.nx + ei] = -2;
-        }
+        for (int e = tid; e < S * Lb; e += IBM_THREADS) a.map[node_of(e % Lb, e / Lb)] = -2;
         __syncthreads();
-        // compaction over the box in row-major order
         const int cells = bw * bh;
-        const int chunk = (cells + blockDim.x - 1) / blockDim.x;
-        const int c0 = threadIdx.x * chunk, c1 = min(c0 + chunk, cells);
+        const int chunk = (cells + IBM_THREADS - 1) / IBM_THREADS;
+        const int c0 = tid * chunk, c1 = min(c0 + chunk, cells);
         int cnt = 0;
-        for (int c = c0; c < c1; ++c) {
-            const int n = (by0 + c / bw) * g.nx + bx0 + c % bw;
-            cnt += (a.map[n] == -2);
-        }
+        for (int c = c0; c < c1; ++c) cnt += (a.map[(long long)(by0 + c / bw) * g.nx + bx0 + c % bw] == -2);
         int total;
         int idx = block_exscan(cnt, sh.ired, &total);
-        if (total > B) {
-            if (threadIdx.x == 0) s_status = ST_BAND_CAPACITY;
-            __syncthreads();
+        if (total > NB) {
+            if (tid == 0) s_status = ST_BAND_CAPACITY;
         } else {
             for (int c = c0; c < c1; ++c) {
-                const int n = (by0 + c / bw) * g.nx + bx0 + c % bw;
+                const long long n = (long long)(by0 + c / bw) * g.nx + bx0 + c % bw;
                 if (a.map[n] == -2) {
                     a.map[n] = idx;
-                    nodes[idx] = n;
+                    nodes[idx] = (int)n;
                     ++idx;
                 }
             }
         }
         __syncthreads();
         if (s_status != ST_OK) {
-            if (threadIdx.x == 0) {
+            // leave a consistent empty band: unmark every node this step marked
+            for (int e = tid; e < S * Lb; e += IBM_THREADS) a.map[node_of(e % Lb, e / Lb)] = -1;
+            if (tid == 0) {
                 a.stats[4] = s_status;
                 *a.band_count = 0;
                 a.box[0] = 0; a.box[1] = 0; a.box[2] = 0; a.box[3] = 0;
@@ -287,89 +274,118 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
             return;
         }
         nb = total;
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             *a.band_count = nb;
             a.box[0] = bx0; a.box[1] = by0; a.box[2] = bw; a.box[3] = bh;
-            s_nb = nb;
         }
-        // stencil slot -> band index; contribution counts
-        for (int b = threadIdx.x; b <= nb; b += blockDim.x) { cstart[b] = 0; if (b < nb) cfill[b] = 0; }
+        // slot -> band index, list counts
+        for (int b = tid; b < nb; b += IBM_THREADS) cfill[b] = 0;
         __syncthreads();
-        for (int e = threadIdx.x; e < S * Lb; e += blockDim.x) {
+        for (int e = tid; e < S * Lb; e += IBM_THREADS) {
             const int l = e % Lb, k = e / Lb;
-            const int di = k / SW - A, dj = k % SW - A;
-            const int ei = min(max(sh.ix0[l] + di, 0), g.nx - 1), ej = min(max(sh.iy0[l] + dj, 0), g.ny - 1);
-            const int b = a.map[(long long)ej * g.nx + ei];
-            sh.sidx[l * MAX_S + k] = b;
+            const int b = a.map[node_of(l, k)];
+            sh.sidx[l * S + k] = b;
             atomicAdd(&cfill[b], 1);
         }
         __syncthreads();
-        // exclusive scan of counts -> cstart
         {
-            const int ch = (nb + blockDim.x - 1) / blockDim.x;
-            const int b0 = threadIdx.x * ch, b1 = min(b0 + ch, nb);
+            const int ch = (nb + IBM_THREADS - 1) / IBM_THREADS;
+            const int b0 = tid * ch, b1 = min(b0 + ch, nb);
             int c = 0;
             for (int b = b0; b < b1; ++b) c += cfill[b];
             int tot;
             int base = block_exscan(c, sh.ired, &tot);
-            for (int b = b0; b < b1; ++b) { cstart[b] = base; base += cfill[b]; cfill[b] = 0; }
-            if (threadIdx.x == 0) cstart[nb] = tot;
+            for (int b = b0; b < b1; ++b) { sh.cstart[b] = base; base += cfill[b]; cfill[b] = 0; }
+            if (tid == 0) sh.cstart[nb] = tot;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < S * Lb; e += blockDim.x) {
+        for (int e = tid; e < S * Lb; e += IBM_THREADS) {
             const int l = e % Lb, k = e / Lb;
-            const int b = sh.sidx[l * MAX_S + k];
-            const int pos = cstart[b] + atomicAdd(&cfill[b], 1);
-            centry[pos] = e;
+            const int b = sh.sidx[l * S + k];
+            sh.cent[sh.cstart[b] + atomicAdd(&cfill[b], 1)] = (l << 5) | k;
         }
         __syncthreads();
-        // sort each node's list by e (insertion sort; lists are short)
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            const int s0 = cstart[b], s1 = cstart[b + 1];
+        // order each list by (k, l): the reference's scatter order
+        for (int b = tid; b < nb; b += IBM_THREADS) {
+            const int s0 = sh.cstart[b], s1 = sh.cstart[b + 1];
             for (int u = s0 + 1; u < s1; ++u) {
-                const int v = centry[u];
+                const int v = sh.cent[u];
+                const int kv = v & 31, lv = v >> 5;
                 int w = u - 1;
-                while (w >= s0 && centry[w] > v) { centry[w + 1] = centry[w]; --w; }
-                centry[w + 1] = v;
+                while (w >= s0) {
+                    const int c = sh.cent[w];
+                    const int kc = c & 31, lc = c >> 5;
+                    if (kc < kv || (kc == kv && lc < lv)) break;
+                    sh.cent[w + 1] = c;
+                    --w;
+                }
+                sh.cent[w + 1] = v;
             }
         }
         __syncthreads();
+        for (int u = tid; u < S * Lb; u += IBM_THREADS) a.list_cache[u] = sh.cent[u];
+        for (int b = tid; b <= nb; b += IBM_THREADS) a.list_cache[S * Lb + b] = sh.cstart[b];
+        if (tid == 0) s_nb = nb;
+        __syncthreads();
     } else {
-        if (threadIdx.x == 0) s_nb = *a.band_count;
+        if (tid == 0) {
+            s_nb = *a.band_count;
+            s_box[0] = a.box[0];
+            s_box[1] = a.box[1];
+            s_box[2] = a.box[0] + a.box[2] - 1;
+            s_box[3] = a.box[1] + a.box[3] - 1;
+        }
         __syncthreads();
         nb = s_nb;
-        for (int e = threadIdx.x; e < S * Lb; e += blockDim.x) {
+        for (int e = tid; e < S * Lb; e += IBM_THREADS) {
             const int l = e % Lb, k = e / Lb;
-            const int di = k / SW - A, dj = k % SW - A;
-            const int ei = min(max(sh.ix0[l] + di, 0), g.nx - 1), ej = min(max(sh.iy0[l] + dj, 0), g.ny - 1);
-            sh.sidx[l * MAX_S + k] = a.map[(long long)ej * g.nx + ei];
+            sh.sidx[l * S + k] = a.map[node_of(l, k)];
         }
+        for (int u = tid; u < S * Lb; u += IBM_THREADS) sh.cent[u] = a.list_cache[u];
+        for (int b = tid; b <= nb; b += IBM_THREADS) sh.cstart[b] = a.list_cache[S * Lb + b];
         __syncthreads();
     }
 
-    // ---- post-streaming populations and moments on the band ----------------
+    // ---- exclusion boxes: this step's (checked) and the next step's ------------
+    if (tid == 0) {
+        const int x0 = s_box[0], y0 = s_box[1], x1 = s_box[2], y1 = s_box[3];
+        if (a.excl_cur) {
+            const int* e = a.excl_cur;
+            if (x0 < e[0] || y0 < e[1] || x1 >= e[0] + e[2] || y1 >= e[1] + e[3]) s_status = ST_EXCL;
+        }
+        if (a.excl_next) {
+            const int ex0 = max(x0 - 1, 0), ey0 = max(y0 - 1, 0);
+            const int ex1 = min(x1 + 1, g.nx - 1), ey1 = min(y1 + 1, g.ny - 1);
+            a.excl_next[0] = ex0;
+            a.excl_next[1] = ey0;
+            a.excl_next[2] = ex1 - ex0 + 1;
+            a.excl_next[3] = ey1 - ey0 + 1;
+        }
+    }
+
+    // ---- post-streaming populations and moments on the band ------------------------
     double* fs_keep = (a.method == IBM_DFC) ? bfs : nullptr;
     switch (a.c.bc) {
-    case BC_DIRICHLET_NEUMANN: band_moments<BC_DIRICHLET_NEUMANN>(a, g, bc, nb, nodes, bro, bu0, bu1, fs_keep); break;
-    case BC_OPEN: band_moments<BC_OPEN>(a, g, bc, nb, nodes, bro, bu0, bu1, fs_keep); break;
-    case BC_SETTLING: band_moments<BC_SETTLING>(a, g, bc, nb, nodes, bro, bu0, bu1, fs_keep); break;
-    default: band_moments<BC_VELOCITY_INLET>(a, g, bc, nb, nodes, bro, bu0, bu1, fs_keep); break;
+    case BC_DIRICHLET_NEUMANN: band_moments<BC_DIRICHLET_NEUMANN>(a, g, bc, nb, nodes, sh, fs_keep); break;
+    case BC_OPEN: band_moments<BC_OPEN>(a, g, bc, nb, nodes, sh, fs_keep); break;
+    case BC_SETTLING: band_moments<BC_SETTLING>(a, g, bc, nb, nodes, sh, fs_keep); break;
+    default: band_moments<BC_VELOCITY_INLET>(a, g, bc, nb, nodes, sh, fs_keep); break;
     }
     __syncthreads();
 
-    auto wgt = [&](int l, int k) -> double { return sh.wx[l * 5 + k / SW] * sh.wy[l * 5 + k % SW]; };
-
+    const size_t pstride = 2 * (size_t)NB;
     if (a.method == IBM_DF) {
-        // iblbm/ibm/df.py:93-154 (per particle: multi_particle_df sums them)
+        // iblbm/ibm/df.py:93-154, summed over particles as ibm/multi_particle.py:404-421
         const bool incomp = a.c.incompressible != 0;
-        for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+        for (int l = tid; l < Lb; l += IBM_THREADS) {
             double R = 0.0, ux = 0.0, uy = 0.0;
+#pragma unroll
             for (int k = 0; k < S; ++k) {
-                const int b = sh.sidx[l * MAX_S + k];
-                const double w = wgt(l, k);
-                R += bro[b] * w;
-                ux += bu0[b] * w;
-                uy += bu1[b] * w;
+                const int b = sh.sidx[l * S + k];
+                const double w = wgt<A>(sh, l, k);
+                R += sh.bro[b] * w;
+                ux += sh.bwx[b] * w;
+                uy += sh.bwy[b] * w;
             }
             sh.R[l] = R; sh.Lux[l] = ux; sh.Luy[l] = uy;
             if (incomp) {
@@ -381,21 +397,21 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
             }
         }
         __syncthreads();
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        for (int b = tid; b < nb; b += IBM_THREADS) {
             double tx = 0.0, ty = 0.0;
             for (int p = 0; p < P; ++p) {
                 const double La = a.larea[p];
                 double ax = 0.0, ay = 0.0;
-                for (int u = cstart[b]; u < cstart[b + 1]; ++u) {
-                    const int e = centry[u], l = e % Lb, k = e / Lb;
+                for (int u = sh.cstart[b]; u < sh.cstart[b + 1]; ++u) {
+                    const int e = sh.cent[u], l = e >> 5, k = e & 31;
                     if (sh.part[l] != p) continue;
-                    const double w = wgt(l, k) * La;
+                    const double w = wgt<A>(sh, l, k) * La;
                     ax += sh.Lfx[l] * w;
                     ay += sh.Lfy[l] * w;
                 }
                 if (a.band_fib_part) {
-                    a.band_fib_part[2 * ((size_t)p * B + b)] = ax;
-                    a.band_fib_part[2 * ((size_t)p * B + b) + 1] = ay;
+                    a.band_fib_part[p * pstride + 2 * b] = ax;
+                    a.band_fib_part[p * pstride + 2 * b + 1] = ay;
                 }
                 tx += ax;
                 ty += ay;
@@ -404,31 +420,30 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
             a.band_fib[2 * b + 1] = ty;
         }
     } else if (a.method == IBM_MDF) {
-        // iblbm/ibm/mdf.py:61-229 (P == 1 or not coupled) and
-        // iblbm/ibm/multi_particle.py:62-316 (coupled, P >= 2)
+        // iblbm/ibm/mdf.py:61-229 (one body) and iblbm/ibm/multi_particle.py:62-316 (coupled)
         const bool coupled = a.mdf_coupled != 0;
         const bool incomp = coupled && a.c.incompressible != 0;  // mdf.py always uses the compressible law
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-            bvs[b] = dt / (2.0 * bro[b]);
-            bwx[b] = bu0[b];
-            bwy[b] = bu1[b];
-            a.band_fib[2 * b] = 0.0;
-            a.band_fib[2 * b + 1] = 0.0;
-            if (a.band_fib_part)
+        double vs[NPT], ftx[NPT], fty[NPT];
+#pragma unroll
+        for (int jn = 0; jn < NPT; ++jn) {
+            const int b = tid + jn * IBM_THREADS;
+            vs[jn] = b < nb ? dt / (2.0 * sh.bro[b]) : 0.0;
+            ftx[jn] = 0.0;
+            fty[jn] = 0.0;
+            if (b < nb && coupled && a.band_fib_part)
                 for (int p = 0; p < P; ++p) {
-                    a.band_fib_part[2 * ((size_t)p * B + b)] = 0.0;
-                    a.band_fib_part[2 * ((size_t)p * B + b) + 1] = 0.0;
+                    a.band_fib_part[p * pstride + 2 * b] = 0.0;
+                    a.band_fib_part[p * pstride + 2 * b + 1] = 0.0;
                 }
         }
-        for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+        for (int l = tid; l < Lb; l += IBM_THREADS) {
             double R = 0.0;
-            for (int k = 0; k < S; ++k) R += bro[sh.sidx[l * MAX_S + k]] * wgt(l, k);
+#pragma unroll
+            for (int k = 0; k < S; ++k) R += sh.bro[sh.sidx[l * S + k]] * wgt<A>(sh, l, k);
             sh.R[l] = R;
         }
-        int min_iter = min(a.mdf_min_iterations, a.mdf_iterations);
-        min_iter = max(1, min_iter);
-        double omega = a.mdf_omega;
-        double omega_min = 0.0;
+        const int min_iter = max(1, min(a.mdf_min_iterations, a.mdf_iterations));
+        double omega = a.mdf_omega, omega_min = 0.0;
         if (coupled) {
             omega = fmin(a.mdf_omega * 0.8, a.mdf_omega_max);
             omega_min = omega * 0.125;
@@ -437,21 +452,28 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
         int iter_count = 0, diverged = 0, converged = 0, guard = 0;
         __syncthreads();
         for (int it = 0; it < a.mdf_iterations; ++it) {
-            // interpolation of the working velocity and slip residual
-            double rloc = -INFINITY;
-            for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+            double* wr = sh.wred + (it & 1) * MAXP * NWARP;
+            // phase A: interpolate the working velocity, slip residual, force
+            double rl[MAXP];
+#pragma unroll
+            for (int p = 0; p < MAXP; ++p) rl[p] = -INFINITY;
+            for (int l = tid; l < Lb; l += IBM_THREADS) {
                 double ux = 0.0, uy = 0.0;
+#pragma unroll
                 for (int k = 0; k < S; ++k) {
-                    const int b = sh.sidx[l * MAX_S + k];
-                    const double w = wgt(l, k);
-                    ux += bwx[b] * w;
-                    uy += bwy[b] * w;
+                    const int b = sh.sidx[l * S + k];
+                    const double w = wgt<A>(sh, l, k);
+                    ux += sh.bwx[b] * w;
+                    uy += sh.bwy[b] * w;
                 }
                 sh.Lux[l] = ux;
                 sh.Luy[l] = uy;
                 const double vx = sh.dvx[l] - ux, vy = sh.dvy[l] - uy;
                 const double r = sqrt(vx * vx + vy * vy);
-                if (!coupled) rloc = (r > rloc || r != r) ? r : rloc;
+                const int pl = coupled ? sh.part[l] : 0;
+#pragma unroll
+                for (int p = 0; p < MAXP; ++p)
+                    if (p == pl) rl[p] = nanmax(rl[p], r);
                 if (incomp) {
                     sh.Lfx[l] = 2.0 * (sh.dvx[l] - ux) / dt;
                     sh.Lfy[l] = 2.0 * (sh.dvy[l] - uy) / dt;
@@ -460,21 +482,23 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
                     sh.Lfy[l] = 2.0 * sh.R[l] * (sh.dvy[l] - uy) / dt;
                 }
             }
+            const int np = coupled ? P : 1;
+#pragma unroll
+            for (int p = 0; p < MAXP; ++p) {
+                if (p >= np) break;
+                const double v = warp_nanmax(rl[p]);
+                if (lane == 0) wr[p * NWARP + wid] = v;
+            }
+            __syncthreads();  // (a)
             double residual;
             if (!coupled) {
-                residual = block_max_nan(rloc, sh.red);
+                residual = -INFINITY;
+                for (int w = 0; w < NWARP; ++w) residual = nanmax(residual, wr[w]);
             } else {
-                // per-particle numpy max, folded with Python's max starting at 0.0
-                __syncthreads();
-                residual = 0.0;
+                residual = 0.0;  // Python max over the particles' numpy maxima, from 0.0
                 for (int p = 0; p < P; ++p) {
                     double rp = -INFINITY;
-                    for (int l = a.moff[p] + threadIdx.x; l < a.moff[p + 1]; l += blockDim.x) {
-                        const double vx = sh.dvx[l] - sh.Lux[l], vy = sh.dvy[l] - sh.Luy[l];
-                        const double r = sqrt(vx * vx + vy * vy);
-                        rp = (r > rp || r != r) ? r : rp;
-                    }
-                    rp = block_max_nan(rp, sh.red);
+                    for (int w = 0; w < NWARP; ++w) rp = nanmax(rp, wr[p * NWARP + w]);
                     if (rp > residual) residual = rp;
                 }
             }
@@ -495,38 +519,42 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
                 prev = residual;
                 continue;
             }
-            // spread, relax and update the working velocity (band nodes)
-            for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            // phase B: spread, relax, update the working velocity of the owned nodes
+#pragma unroll
+            for (int jn = 0; jn < NPT; ++jn) {
+                const int b = tid + jn * IBM_THREADS;
+                if (b >= nb) break;
+                const int u0 = sh.cstart[b], u1 = sh.cstart[b + 1];
                 double tx = 0.0, ty = 0.0;
                 for (int p = 0; p < P; ++p) {
                     const double La = a.larea[p];
                     double ax = 0.0, ay = 0.0;
-                    for (int u = cstart[b]; u < cstart[b + 1]; ++u) {
-                        const int e = centry[u], l = e % Lb, k = e / Lb;
-                        if (sh.part[l] != p) continue;
-                        const double w = wgt(l, k) * La;
+                    for (int u = u0; u < u1; ++u) {
+                        const int e = sh.cent[u], l = e >> 5, k = e & 31;
+                        if (P > 1 && sh.part[l] != p) continue;
+                        const double w = wgt<A>(sh, l, k) * La;
                         ax += sh.Lfx[l] * w;
                         ay += sh.Lfy[l] * w;
                     }
                     const double fx = ax * omega, fy = ay * omega;
                     if (coupled && a.band_fib_part) {
-                        a.band_fib_part[2 * ((size_t)p * B + b)] += fx;
-                        a.band_fib_part[2 * ((size_t)p * B + b) + 1] += fy;
+                        a.band_fib_part[p * pstride + 2 * b] += fx;
+                        a.band_fib_part[p * pstride + 2 * b + 1] += fy;
                     }
                     tx += fx;
                     ty += fy;
                 }
-                a.band_fib[2 * b] += tx;
-                a.band_fib[2 * b + 1] += ty;
+                ftx[jn] += tx;
+                fty[jn] += ty;
                 if (incomp) {
-                    bwx[b] += 0.5 * tx * dt;
-                    bwy[b] += 0.5 * ty * dt;
+                    sh.bwx[b] += 0.5 * tx * dt;
+                    sh.bwy[b] += 0.5 * ty * dt;
                 } else {
-                    bwx[b] += tx * bvs[b];
-                    bwy[b] += ty * bvs[b];
+                    sh.bwx[b] += tx * vs[jn];
+                    sh.bwy[b] += ty * vs[jn];
                 }
             }
-            __syncthreads();
+            __syncthreads();  // (b)
             prev = residual;
             if (coupled) iter_count += 1;
             else iter_count = it + 1;
@@ -535,14 +563,18 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
                 break;
             }
         }
-        if (!coupled && a.band_fib_part) {
-            __syncthreads();
-            for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-                a.band_fib_part[2 * (size_t)b] = a.band_fib[2 * b];
-                a.band_fib_part[2 * (size_t)b + 1] = a.band_fib[2 * b + 1];
+#pragma unroll
+        for (int jn = 0; jn < NPT; ++jn) {
+            const int b = tid + jn * IBM_THREADS;
+            if (b >= nb) break;
+            a.band_fib[2 * b] = ftx[jn];
+            a.band_fib[2 * b + 1] = fty[jn];
+            if (!coupled && a.band_fib_part) {
+                a.band_fib_part[2 * b] = ftx[jn];
+                a.band_fib_part[2 * b + 1] = fty[jn];
             }
         }
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             a.stats[0] = iter_count;
             a.stats[1] = diverged;
             a.stats[2] = converged;
@@ -557,33 +589,35 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
         const double La = a.larea[0];
         const bool have = a.dfc_cache_lambda && a.lambda_valid && *a.lambda_valid;
         if (!have) {
-            for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            for (int b = tid; b < nb; b += IBM_THREADS) {
                 double wt = 0.0;
-                for (int u = cstart[b]; u < cstart[b + 1]; ++u) {
-                    const int e = centry[u], l = e % Lb, k = e / Lb;
-                    wt += wgt(l, k);
+                for (int u = sh.cstart[b]; u < sh.cstart[b + 1]; ++u) {
+                    const int e = sh.cent[u];
+                    wt += wgt<A>(sh, e >> 5, e & 31);
                 }
-                bwx[b] = wt;
+                sh.bwx[b] = wt;  // W_total
             }
             __syncthreads();
-            for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+            for (int l = tid; l < Lb; l += IBM_THREADS) {
                 double ws = 0.0;
-                for (int k = 0; k < S; ++k) ws += bwx[sh.sidx[l * MAX_S + k]] * wgt(l, k);
+#pragma unroll
+                for (int k = 0; k < S; ++k) ws += sh.bwx[sh.sidx[l * S + k]] * wgt<A>(sh, l, k);
                 a.lambda[l] = 1.0 / (2.0 * 1.0 * La * ws);
             }
             __syncthreads();
-            if (threadIdx.x == 0 && a.dfc_cache_lambda && a.lambda_valid) *a.lambda_valid = 1;
+            if (tid == 0 && a.dfc_cache_lambda && a.lambda_valid) *a.lambda_valid = 1;
         }
         const double cs2 = 1.0 / 3.0;
-        for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+        for (int l = tid; l < Lb; l += IBM_THREADS) {
             double fi[9];
 #pragma unroll
             for (int q = 0; q < 9; ++q) fi[q] = 0.0;
-            for (int k = 0; k < S; ++k) {
-                const int b = sh.sidx[l * MAX_S + k];
-                const double w = wgt(l, k);
 #pragma unroll
-                for (int q = 0; q < 9; ++q) fi[q] += bfs[9 * b + q] * w;
+            for (int k = 0; k < S; ++k) {
+                const int b = sh.sidx[l * S + k];
+                const double w = wgt<A>(sh, l, k);
+#pragma unroll
+                for (int q = 0; q < 9; ++q) fi[q] += bfs[9 * (size_t)b + q] * w;
             }
             const double lam = a.lambda[l];
             double sx = 0.0, sy = 0.0;
@@ -592,7 +626,7 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
                 const double edu = e_dot(q, sh.dvx[l], sh.dvy[l]);
                 const double fbb = fi[opp_(q)] + 2.0 * w_(q) * 1.0 * edu / cs2;
                 const double dev = fbb - fi[q];
-                dfl[9 * l + q] = a.correction_scale * lam * dev;
+                dfl[9 * (size_t)l + q] = a.correction_scale * lam * dev;
                 const double s = -(lam * dev * La);
                 sx += s * (double)ex_(q);
                 sy += s * (double)ey_(q);
@@ -603,55 +637,69 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const iblbm_ib
             }
         }
         __syncthreads();
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        for (int b = tid; b < nb; b += IBM_THREADS) {
             double acc[9];
 #pragma unroll
             for (int q = 0; q < 9; ++q) acc[q] = 0.0;
-            for (int u = cstart[b]; u < cstart[b + 1]; ++u) {
-                const int e = centry[u], l = e % Lb, k = e / Lb;
-                const double w = wgt(l, k) * La;
+            for (int u = sh.cstart[b]; u < sh.cstart[b + 1]; ++u) {
+                const int e = sh.cent[u], l = e >> 5, k = e & 31;
+                const double w = wgt<A>(sh, l, k) * La;
 #pragma unroll
-                for (int q = 0; q < 9; ++q) acc[q] += dfl[9 * l + q] * w;
+                for (int q = 0; q < 9; ++q) acc[q] += dfl[9 * (size_t)l + q] * w;
             }
 #pragma unroll
             for (int q = 0; q < 9; ++q) a.band_df[9 * (size_t)b + q] = acc[q];
         }
     }
     __syncthreads();
-    for (int l = threadIdx.x; l < Lb; l += blockDim.x) {
+    for (int l = tid; l < Lb; l += IBM_THREADS) {
         if (a.Lux) a.Lux[l] = sh.Lux[l];
         if (a.Luy) a.Luy[l] = sh.Luy[l];
         if (a.Lfx) a.Lfx[l] = sh.Lfx[l];
         if (a.Lfy) a.Lfy[l] = sh.Lfy[l];
     }
-    if (threadIdx.x == 0) {
-        a.stats[4] = ST_OK;
+    if (tid == 0) {
+        a.stats[4] = s_status;
         if (a.step_counter) *a.step_counter = s_step + 1;
     }
 }
+
+void make_params(const iblbm_case& c, CollParams& cp, BcParams& bc);
 
 }  // namespace iblbm
 
 using namespace iblbm;
 
-extern "C" int iblbm_ibm_smem_bytes(int lb_total) { return (int)ibm_smem_bytes(lb_total); }
+extern "C" int iblbm_ibm_smem_bytes(int lb_total, int band_capacity, int delta_type)
+{
+    const int S = delta_type == 0 ? 25 : 9;
+    return (int)ibm_smem_bytes_t(lb_total, band_capacity, S);
+}
 
 extern "C" int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles)
 {
     (void)n_particles;
-    return 15 * band_capacity + 9 * lb_total;
+    return 9 * band_capacity + 9 * lb_total;
 }
 
-extern "C" int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int box_capacity)
+extern "C" int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type)
 {
-    (void)box_capacity;
-    return 2 * band_capacity + 1 + MAX_S * lb_total;
+    (void)lb_total;
+    (void)delta_type;
+    return band_capacity;
+}
+
+extern "C" int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type)
+{
+    const int S = delta_type == 0 ? 25 : 9;
+    return S * lb_total + band_capacity + 1;
 }
 
 extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 {
-    if (!a || !a->moff || a->n_particles < 1 || a->lb_total < 1 || !a->fpost_prev || !a->box || !a->map ||
-        !a->band_nodes || !a->band_count || !a->scratch || !a->iscratch || !a->stats || !a->dstats || !a->larea)
+    if (!a || !a->moff || a->n_particles < 1 || a->n_particles > MAXP || a->lb_total < 1 || !a->fpost_prev ||
+        !a->box || !a->map || !a->band_nodes || !a->band_count || !a->scratch || !a->iscratch || !a->stats ||
+        !a->dstats || !a->larea || !a->list_cache)
         return IBLBM_E_ARG;
     if (a->delta_type != 0 && a->delta_type != 1) return IBLBM_E_ARG;
     if (a->method != IBM_DF && a->method != IBM_MDF && a->method != IBM_DFC) return IBLBM_E_ARG;
@@ -660,19 +708,27 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
     if (!a->xt_table && (!a->Lx || !a->Ly || !a->dvel)) return IBLBM_E_ARG;
     if (a->xt_table && (!a->Lx_c || !a->Ly_c || !a->step_counter || a->xt_len < 1)) return IBLBM_E_ARG;
     if ((a->c.bc == BC_OPEN || a->c.bc == BC_VELOCITY_INLET) && !a->uring_prev) return IBLBM_E_ARG;
-    if (a->band_capacity < 1 || a->g.nx < 4 || a->g.ny < 4) return IBLBM_E_ARG;
-    const size_t smem = ibm_smem_bytes(a->lb_total);
+    if (a->band_capacity < 1 || a->band_capacity > NPT * IBM_THREADS || a->g.nx < 4 || a->g.ny < 4)
+        return IBLBM_E_ARG;
+    if ((long long)a->lb_total * 32 >= (1LL << 31)) return IBLBM_E_ARG;
+    const int S = a->delta_type == 0 ? 25 : 9;
+    const size_t smem = ibm_smem_bytes_t(a->lb_total, a->band_capacity, S);
     if (smem > 220 * 1024) return IBLBM_E_CAPACITY;
     static int configured = 0;
     if (!configured) {
-        if (cudaFuncSetAttribute(ibm_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024) !=
-            cudaSuccess)
+        if (cudaFuncSetAttribute(ibm_step_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(ibm_step_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024) !=
+                cudaSuccess)
             return IBLBM_E_LAUNCH;
         configured = 1;
     }
     CollParams cp;
     BcParams bc;
     make_params(a->c, cp, bc);
-    ibm_step_kernel<<<1, IBM_THREADS, smem, (cudaStream_t)stream>>>(*a, bc);
+    if (a->delta_type == 0)
+        ibm_step_kernel<2><<<1, IBM_THREADS, smem, (cudaStream_t)stream>>>(*a, bc);
+    else
+        ibm_step_kernel<1><<<1, IBM_THREADS, smem, (cudaStream_t)stream>>>(*a, bc);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

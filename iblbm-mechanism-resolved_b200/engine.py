@@ -119,7 +119,7 @@ class Engine:
         self.Lb = int(sum(lbs))
         moff = np.concatenate([[0], np.cumsum(lbs)]).astype(np.int32)
         S = (2 * DELTA_RADIUS[cfg.delta_type] + 1) ** 2
-        self.B = B = self.Lb * S
+        self.B = B = self._band_capacity(S)
         t = lambda n, dt=f64: torch.zeros(max(int(n), 1), dtype=dt, device=dev)
         self.d_moff = torch.as_tensor(moff, device=dev)
         self.d_larea = torch.as_tensor(self.larea_h, device=dev)
@@ -130,8 +130,11 @@ class Engine:
         self.d_nodes, self.d_count = t(B, i32), t(1, i32)
         self.d_fib, self.d_df = t(2 * B), t(9 * B)
         self.d_fib_part = t(2 * B * self.P)
+        delta_id = DELTA_IDS[cfg.delta_type]
         self.d_scr = t(self.L.iblbm_ibm_scratch_doubles(self.Lb, B, self.P))
-        self.d_iscr = t(self.L.iblbm_ibm_scratch_ints(self.Lb, B, N), i32)
+        self.d_iscr = t(self.L.iblbm_ibm_scratch_ints(self.Lb, B, delta_id), i32)
+        self.d_lists = t(self.L.iblbm_ibm_list_cache_ints(self.Lb, B, delta_id), i32)
+        self.d_excl = torch.zeros(2, 4, dtype=i32, device=dev)
         self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy = (t(self.Lb) for _ in range(4))
         self.d_dfc_force = t(2 * self.Lb)
         self.d_stats, self.d_dstats = t(5, i32), t(2)
@@ -151,10 +154,36 @@ class Engine:
             if cfg.motion_type == "sedimentation" and cfg.enable_rotation:
                 self.omega = min(float(self.omega), MOVING_ROTATION_OMEGA_MAX)
         self.ibm_args = [self._make_ibm_args(p) for p in (0, 1)]
-        self.dense_args = [[self._make_dense_args(p, out) for out in (False, True)] for p in (0, 1)]
+        # dense pass variants per parity and output flag: whole lattice, bulk
+        # (skips the exclusion box), box (only the exclusion box)
+        self.dense_full = [[self._make_dense_args(p, out, "full") for out in (False, True)] for p in (0, 1)]
+        self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
+        self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
+        self.side = torch.cuda.Stream(self.dev, priority=-1)
+        self.ev_bulk = torch.cuda.Event()
+        self.ev_side = torch.cuda.Event()
+        self.overlap = True
         self.rebuild_next = True
         self.graphs = {}
         self.last_out_step = 0
+
+    def _band_capacity(self, S):
+        """Band capacity from the initial markers: 1.5 x the number of distinct
+        stencil nodes plus 256, within [1, min(Lb*S, 4096)]."""
+        st, cfg = self.st, self.cfg
+        if st.particles is not None:
+            Lx = np.concatenate([p.Lx for p in st.particles])
+            Ly = np.concatenate([p.Ly for p in st.particles])
+        else:
+            Lx, Ly = st.Lx, st.Ly
+        a = DELTA_RADIUS[cfg.delta_type]
+        ix0 = np.floor(Lx / st.dx + 0.5).astype(np.int64)
+        iy0 = np.floor(Ly / st.dy + 0.5).astype(np.int64)
+        off = np.arange(-a, a + 1)
+        ii = np.clip(ix0[:, None, None] + off[None, :, None], 0, st.nx - 1)
+        jj = np.clip(iy0[:, None, None] + off[None, None, :], 0, st.ny - 1)
+        n0 = len(np.unique((jj * st.nx + ii).ravel()))
+        return int(min(max(1, int(1.5 * n0) + 256), self.Lb * S, 4096))
 
     # ------------------------------------------------------------------------------
     def _collide_aos(self, fstar, feq, U, fib, out):
@@ -206,6 +235,9 @@ class Engine:
         a.fpost_prev, a.uring_prev = ptr(self.f[parity]), ptr(self.uring[parity])
         a.box, a.map, a.band_nodes, a.band_count = (ptr(x) for x in (self.d_box, self.d_map, self.d_nodes,
                                                                      self.d_count))
+        a.list_cache = ptr(self.d_lists)
+        a.excl_cur = ptr(self.d_excl[parity])
+        a.excl_next = ptr(self.d_excl[1 - parity])
         a.band_capacity, a.box_capacity = self.B, self.N
         a.band_fib, a.band_df, a.band_fib_part = ptr(self.d_fib), ptr(self.d_df), ptr(self.d_fib_part)
         a.scratch, a.iscratch = ptr(self.d_scr), ptr(self.d_iscr)
@@ -214,51 +246,114 @@ class Engine:
         a.stats, a.dstats = ptr(self.d_stats), ptr(self.d_dstats)
         return a
 
-    def _make_dense_args(self, parity, outputs):
+    def _make_dense_args(self, parity, outputs, mode):
         a = DenseArgs()
         a.g, a.c = self.geom, self.case
-        a.ibm = IBM_IDS[self.method]
+        a.ibm = 0 if mode == "bulk" else IBM_IDS[self.method]
         a.fpost_prev, a.fpost_next = ptr(self.f[parity]), ptr(self.f[1 - parity])
         a.uring_prev, a.uring_next = ptr(self.uring[parity]), ptr(self.uring[1 - parity])
         a.band = BandView(ptr(self.d_box), ptr(self.d_map), ptr(self.d_fib), ptr(self.d_df))
         if outputs:
             a.ro_out, a.U_out, a.fstar_out = ptr(self.ro_out), ptr(self.U_out), ptr(self.fstar_out)
+        if mode == "bulk":
+            a.skip_box = ptr(self.d_excl[parity])
+        elif mode == "box":
+            a.only_box = ptr(self.d_excl[parity])
+            a.box_blocks = 2 * 148
         return a
 
     # ------------------------------------------------------------------------------
-    def _launch(self, outputs=False, events=None):
-        """Launch one timestep (IBM band kernel, then the dense kernel).  With
-        events=(e0, e1, e2) the three CUDA events are recorded before the IBM
-        kernel, between the two kernels and after the dense kernel."""
-        s = self.stream()
+    def _ibm(self, stream, excl_check):
         ia = self.ibm_args[self.parity]
         ia.rebuild = 1 if (self.rebuild_next or self.moving) else 0
+        ia.excl_cur = ptr(self.d_excl[self.parity]) if excl_check else 0
+        check(self.L.iblbm_ibm_step_f64(ctypes.byref(ia), stream), "iblbm_ibm_step_f64")
+        self.rebuild_next = False
+
+    def _dense(self, variant, outputs, stream):
+        da = variant[self.parity][1 if outputs else 0]
+        check(self.L.iblbm_dense_step_f64(ctypes.byref(da), stream), "iblbm_dense_step_f64")
+
+    def _step_serial(self, outputs=False, events=None):
+        """One timestep on the current stream: band kernel, then the whole lattice.
+        With events=(e0, e1, e2): recorded before, between and after the kernels."""
+        torch = self.torch
+        s = self.stream()
         if events:
             events[0].record()
-        check(self.L.iblbm_ibm_step_f64(ctypes.byref(ia), s), "iblbm_ibm_step_f64")
-        self.rebuild_next = False
+        self._ibm(s, excl_check=False)
         if events:
             events[1].record()
-        da = self.dense_args[self.parity][1 if outputs else 0]
-        check(self.L.iblbm_dense_step_f64(ctypes.byref(da), s), "iblbm_dense_step_f64")
+        self._dense(self.dense_full, outputs, s)
         if events:
             events[2].record()
         self.parity ^= 1
+
+    def _step_overlapped(self, outputs=False, bulk_events=None):
+        """One timestep with the band kernel and the box pass on the side stream,
+        concurrent with the bulk pass on the current stream.
+
+        Dependencies (n = this step): band(n) and box(n) wait for bulk(n-1);
+        bulk(n) waits for box(n-1).  Reads of f_post(n-1) and writes of f_post(n)
+        therefore never race, and the ping-pong buffers are safe to reuse."""
+        torch = self.torch
+        main = torch.cuda.current_stream(self.dev)
+        side = self.side
+        side.wait_event(self.ev_bulk)
+        self._ibm(side.cuda_stream, excl_check=True)
+        self._dense(self.dense_box, outputs, side.cuda_stream)
+        main.wait_event(self.ev_side)
+        self.ev_side.record(side)
+        if bulk_events:
+            bulk_events[0].record(main)
+        self._dense(self.dense_bulk, outputs, main.cuda_stream)
+        if bulk_events:
+            bulk_events[1].record(main)
+        self.ev_bulk.record(main)
+        self.parity ^= 1
+
+    def join(self):
+        """Make the current stream wait for the side stream's work."""
+        self.torch.cuda.current_stream(self.dev).wait_event(self.ev_side)
+
+    def fence(self):
+        """Order everything queued so far on the current stream before the next
+        step's work on both streams."""
+        main = self.torch.cuda.current_stream(self.dev)
+        self.ev_bulk.record(main)
+        self.ev_side.record(main)
+
+    def _launch(self, outputs=False, events=None):
+        """One timestep: serial for the first step (and when overlap is off), else overlapped."""
+        if self.rebuild_next or not self.overlap or self.st.particles is not None:
+            self._step_serial(outputs, events)
+            main = self.torch.cuda.current_stream(self.dev)
+            self.ev_bulk.record(main)
+            self.ev_side.record(main)
+        else:
+            self._step_overlapped(outputs)
+            if outputs or events is not None:
+                self.join()
 
     def _graph(self, length):
         key = (self.parity, length)
         g = self.graphs.get(key)
         if g is None:
             torch = self.torch
-            side = torch.cuda.Stream(self.dev)
-            side.wait_stream(torch.cuda.current_stream(self.dev))
+            cap = torch.cuda.Stream(self.dev)
+            cap.wait_stream(torch.cuda.current_stream(self.dev))
+            cap.wait_stream(self.side)
             g = torch.cuda.CUDAGraph()
             p0 = self.parity
-            with torch.cuda.stream(side):
-                with torch.cuda.graph(g, stream=side):
+            with torch.cuda.stream(cap):
+                with torch.cuda.graph(g, stream=cap):
+                    # fork: the side stream's first wait must be on captured work
+                    self.ev_bulk.record(cap)
+                    self.ev_side.record(cap)
                     for _ in range(length):
                         self._launch(False)
-            torch.cuda.current_stream(self.dev).wait_stream(side)
+                    self.join()
+            torch.cuda.current_stream(self.dev).wait_stream(cap)
             self.parity = p0  # capture does not execute; restore the bookkeeping
             self.graphs[key] = g
         return g
@@ -278,12 +373,17 @@ class Engine:
         body = nsteps - 1 if outputs_last else nsteps
         if body > 0:
             if use_graph and body >= 4:
+                self.join()
                 g = self._graph(body)
                 g.replay()
                 self.parity ^= (body & 1)
+                main = self.torch.cuda.current_stream(self.dev)
+                self.ev_bulk.record(main)
+                self.ev_side.record(main)
             else:
                 for _ in range(body):
                     self._launch(False)
+                self.join()
             self.ttt += body
         if outputs_last and nsteps > 0:
             self._launch(True)
@@ -367,12 +467,14 @@ class Engine:
                 "guard_trips": int(s[3]), "last_residual": float(d[0]), "omega_used": float(d[1])}
 
     def status(self):
+        self.join()
         return int(self.d_stats[4].item())
 
     def read_state(self):
         """Copy the last output step's fields into host arrays on self.st (AoS, the
         reference's layout) and return it."""
         torch, st = self.torch, self.st
+        self.join()
         s = self.stream()
         fs = torch.empty(self.N * 9, dtype=torch.float64, device=self.dev)
         check(self.L.iblbm_soa_to_aos(ptr(self.fstar_out), self.geom, ptr(fs), s), "iblbm_soa_to_aos")

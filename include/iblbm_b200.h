@@ -89,6 +89,9 @@ typedef struct {
     double *uring_next;
     iblbm_band_view band;
     double *ro_out, *U_out, *fstar_out;
+    const int *skip_box;        /* device x0, y0, w, h: nodes left to the box pass (NULL: none) */
+    const int *only_box;        /* device x0, y0, w, h: update only these nodes (box pass; NULL: all) */
+    int box_blocks;             /* grid of the box pass (blocks of 128 threads, grid-stride) */
 } iblbm_dense_args;
 
 /* Replaces (fused): collision_gpu/collision_trt_gpu/collision_cm_mrt_gpu
@@ -133,9 +136,12 @@ typedef struct {
     const double *fpost_prev, *uring_prev;
     /* band state (written) */
     int *box, *map, *band_nodes, *band_count; /* map: nx*ny ints, -1 outside the band */
+    int *list_cache;   /* iblbm_ibm_list_cache_ints(...) ints: contribution lists kept between steps */
+    const int *excl_cur;  /* optional: this step's exclusion box; the band must lie inside (status 5) */
+    int *excl_next;       /* optional: written with the band box dilated by one node */
     int band_capacity, box_capacity;
     double *band_fib, *band_df;        /* band x 2, band x 9 */
-    double *band_fib_part;             /* particles x band x 2 (per-particle totals) */
+    double *band_fib_part;             /* particles x band_capacity x 2 (per-particle totals) */
     double *scratch;                   /* >= iblbm_ibm_scratch_doubles(...) doubles */
     int *iscratch;                     /* >= iblbm_ibm_scratch_ints(...) ints */
     /* per-marker outputs (Lb_total): interpolated velocity, force, DFC force */
@@ -153,8 +159,9 @@ typedef struct {
  * from ibm/strategies/dfc.py:31-54. */
 int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
 int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
-int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int box_capacity);
-int iblbm_ibm_smem_bytes(int lb_total);
+int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
+int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type);
+int iblbm_ibm_smem_bytes(int lb_total, int band_capacity, int delta_type);
 
 /* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
 /* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */
