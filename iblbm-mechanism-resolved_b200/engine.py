@@ -101,7 +101,7 @@ class Engine:
         self.uring = [U0.reshape(-1).clone(), U0.reshape(-1).clone()]
         self.ro_out = torch.empty(N, dtype=f64, device=dev)
         self.U_out = torch.empty(N * 2, dtype=f64, device=dev)
-        self.fstar_out = torch.empty(9 * self.qstride, dtype=f64, device=dev)
+        self.fstar_out = torch.zeros(9 * self.qstride, dtype=f64, device=dev)
         self.parity = 0
         self.ttt = 1
 
