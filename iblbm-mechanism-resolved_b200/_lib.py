@@ -60,6 +60,7 @@ class IbmArgs(ctypes.Structure):
 _SIGS = {
     "iblbm_dense_step_f64": [ctypes.POINTER(DenseArgs), _vp],
     "iblbm_ibm_step_f64": [ctypes.POINTER(IbmArgs), _vp],
+    "iblbm_ibm_step_f64_noalloc": [ctypes.POINTER(IbmArgs), _vp],
     "iblbm_ibm_scratch_doubles": [_i, _i, _i],
     "iblbm_ibm_scratch_ints": [_i, _i, _i],
     "iblbm_ibm_list_cache_ints": [_i, _i, _i],

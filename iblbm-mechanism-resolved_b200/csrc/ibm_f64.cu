@@ -732,3 +732,55 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
         ibm_step_kernel<1><<<1, IBM_THREADS, smem, (cudaStream_t)stream>>>(*a, bc);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
+
+// ---------------------------------------------------------------------------
+// Band step without caller-provided scratch.
+//
+// Some callers cannot allocate device memory when they call into this library:
+// a host framework that owns every device allocation through its own pool and
+// hands plugins only the buffers they declared, or a long-running service that
+// forbids cudaMalloc after start-up because cudaMalloc can synchronize the
+// device and stall its other streams.  For them this entry point takes the
+// band kernel's per-launch scratch (the post-streaming populations and
+// distribution corrections of the DFC path, and the list-building counters)
+// from a fixed array compiled into the library instead of from the caller.
+//
+// Limits: band_capacity <= 4096 nodes and lb_total <= 1024 markers; larger
+// arguments return IBLBM_E_CAPACITY before anything is launched.  The array
+// (about 390 KB) lives on every GPU that loads the library until the process
+// exits.  All calls share it and it keeps the last call's contents (the kernel
+// clears the counters it needs zeroed), so two calls whose kernels overlap on
+// the GPU race on it: issue them on one stream, or order them.  The first call
+// on each device looks up the array's device address (cudaGetSymbolAddress) with
+// that device current; make that first call before any stream capture.  The
+// caller still passes every input, output and persistent band array.
+// ---------------------------------------------------------------------------
+namespace iblbm {
+constexpr int NOALLOC_MAX_BAND = 4096;
+constexpr int NOALLOC_MAX_MARKERS = 1024;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static __device__ __align__(256) double g_noalloc_scratch[9 * NOALLOC_MAX_BAND + 9 * NOALLOC_MAX_MARKERS];
+static __device__ __align__(256) int g_noalloc_iscratch[NOALLOC_MAX_BAND];
+static void* g_noalloc_scratch_ptr[NOALLOC_MAX_DEVICES];
+static void* g_noalloc_iscratch_ptr[NOALLOC_MAX_DEVICES];
+}  // namespace iblbm
+
+extern "C" int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args* a, void* stream)
+{
+    if (!a) return IBLBM_E_ARG;
+    if (a->band_capacity > NOALLOC_MAX_BAND || a->lb_total > NOALLOC_MAX_MARKERS) return IBLBM_E_CAPACITY;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return IBLBM_E_LAUNCH;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return IBLBM_E_ARG;
+    if (!g_noalloc_scratch_ptr[dev]) {
+        void *p = nullptr, *q = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return IBLBM_E_LAUNCH;
+        if (cudaGetSymbolAddress(&q, g_noalloc_iscratch) != cudaSuccess) return IBLBM_E_LAUNCH;
+        g_noalloc_iscratch_ptr[dev] = q;
+        g_noalloc_scratch_ptr[dev] = p;
+    }
+    iblbm_ibm_args b = *a;
+    b.scratch = static_cast<double*>(g_noalloc_scratch_ptr[dev]);
+    b.iscratch = static_cast<int*>(g_noalloc_iscratch_ptr[dev]);
+    return iblbm_ibm_step_f64(&b, stream);
+}

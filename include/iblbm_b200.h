@@ -158,6 +158,16 @@ typedef struct {
  * compute_lambda_gpu + dfc_correction_gpu (gpu_kernels.py:1091-1223) called
  * from ibm/strategies/dfc.py:31-54. */
 int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
+/* Same band step for callers that cannot allocate device memory at call time
+ * (a host framework that owns all device allocations, or a service that
+ * forbids cudaMalloc after start-up).  No counterpart in the reference.  The
+ * scratch and iscratch fields of *a are ignored: the per-launch scratch comes
+ * from a fixed array in the library (about 390 KB per GPU, held until exit).
+ * Limits: band_capacity <= 4096, lb_total <= 1024, else IBLBM_E_CAPACITY.
+ * Calls share that array, so calls that overlap on the GPU race; the first
+ * call on a device resolves the array's address and should precede any stream
+ * capture.  Allocates nothing. */
+int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args *a, void *stream);
 int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
 int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type);
