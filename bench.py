@@ -42,6 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_LU_F64 = 144
+BYTES_PER_LU_F32 = 72
 METRIC = "MLUPS and HBM GB/s (1 B200), chosen vs plain form at Cd within 0.1% of FP64"
 
 
@@ -180,30 +181,27 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def run_b200(args):
+def measure(eng, args, dist, ws):
+    """Time one engine on the workload: per-step (L2 flushed) overlapped steps,
+    the band kernel alone, graph-replayed steady state and the host-buffer e2e
+    loop.  Returns a dict of the numbers (all ranks)."""
     import torch
-    dist, rank, ws, local = _dist()
-    torch.cuda.set_device(local)
-    from iblbm_b200.engine import Engine
-    cfg = workload_config(max_steps=args.warmup + 4 * args.steps + 16)
-    eng = Engine(cfg)
     N = eng.N
     # warm-up: graph chunks and eager steps
     eng.advance(max(args.warmup, 3), outputs_last=True)
     torch.cuda.synchronize()
     flush = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    sink = torch.zeros(1, dtype=torch.float32, device="cuda")
+    sink = torch.zeros((), dtype=torch.float32, device="cuda")
     K = args.steps
     E = lambda: torch.cuda.Event(enable_timing=True)
     ev = [[E() for _ in range(4)] for _ in range(K)]
-    peak, peak_kind = _peaks()
     excl = eng.d_excl[eng.parity].tolist()
     box_nodes = excl[2] * excl[3]
     main = torch.cuda.current_stream()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with Clocks(local) as clk:
+    with Clocks(torch.cuda.current_device()) as clk:
         t_wall = time.perf_counter()
         for k in range(K):
             ev[k][0].record(main)
@@ -214,7 +212,6 @@ def run_b200(args):
             eng.fence()
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
-    clocks = clk.summary()
     step_ms = [ev[k][0].elapsed_time(ev[k][3]) for k in range(K)]
     dense_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
     tot_ms = sum(step_ms)
@@ -222,11 +219,8 @@ def run_b200(args):
         t = torch.tensor([tot_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         tot_ms = float(t.item())
-    status = eng.status()
-    stats = eng.mdf_stats()
-    value = N * K * ws / (tot_ms / 1e3) / 1e6
     dense_avg = sum(dense_ms) / K
-    achieved = BYTES_PER_LU_F64 * (N - box_nodes) / (dense_avg / 1e3) / 1e9
+    bpl = BYTES_PER_LU_F32 if eng.f32 else BYTES_PER_LU_F64
 
     # band kernel alone (serial step: band kernel then the whole lattice), for the breakdown
     sev = [[E() for _ in range(3)] for _ in range(8)]
@@ -239,7 +233,7 @@ def run_b200(args):
 
     # steady state: CUDA-graph replay, no flush (L2-warm; reported, not the headline)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0, e1 = E(), E()
     eng.advance(K, outputs_last=False)  # capture
     torch.cuda.synchronize()
     e0.record()
@@ -265,33 +259,69 @@ def run_b200(args):
         eng.d_dv.copy_(host_in[2 * Lb:], non_blocking=True)
         eng._launch(False)
         eng.join()
-        host_out.copy_(eng.d_fib[: 2 * nb].view(nb, 2).sum(0), non_blocking=True)
+        host_out.copy_(eng.d_fib[: 2 * nb].view(nb, 2).double().sum(0), non_blocking=True)
         torch.cuda.current_stream().synchronize()
     e2e_s = time.perf_counter() - t0
-    e2e = N * Ke / e2e_s / 1e6
+    # one output step so both forms can be compared at the same step
+    eng.advance(1, outputs_last=True)
+    torch.cuda.synchronize()
+    cd, cl = eng.cd_cl()
+    return {"value": N * K * ws / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "dense_ms": dense_avg,
+            "box_nodes": box_nodes, "bytes_per_lu": bpl,
+            "achieved": bpl * (N - box_nodes) / (dense_avg / 1e3) / 1e9, "band_ms": ibm_ms, "full_ms": full_ms,
+            "steady": steady, "e2e": N * Ke * ws / e2e_s / 1e6, "e2e_h2d": 4 * Lb * 8, "e2e_d2h": 16,
+            "clocks": clk.summary(), "wall_s_timed": t_wall, "status": eng.status(), "mdf": eng.mdf_stats(),
+            "cd": cd, "cl": cl, "steps_done": eng.ttt - 1}
 
+
+def run_b200(args):
+    import torch
+    dist, rank, ws, local = _dist()
+    torch.cuda.set_device(local)
+    from iblbm_b200.engine import Engine
+    cfg = workload_config(max_steps=args.warmup + 4 * args.steps + 16)
+    peak, peak_kind = _peaks()
+    plain = measure(Engine(cfg, precision="f64"), args, dist, ws)
+    chosen = measure(Engine(cfg, precision="f32"), args, dist, ws) if args.form == "chosen" else None
+    head = chosen or plain
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
+    N = 1601 * 641
     cpu = cpu_baseline(seconds=float(os.environ.get("IBLBM_CPU_SECONDS", "20"))) if ws == 1 else None
-    line = {"metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": ws, "steps": K, "warmup": args.warmup,
-            "ms_per_step": tot_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (deterministic initial state of the workload)",
-            "config": dict(WORKLOAD, parallelism=f"replicas x{ws}"),
-            "hbm_gbs_dense": achieved,
-            "band_kernel_ms": ibm_ms, "bulk_kernel_ms": dense_avg, "whole_lattice_kernel_ms_serial": full_ms,
+    form = "FP32 shifted populations (FP64 force sums, MDF residual norm)" if chosen else "FP64 plain"
+
+    def summary(m):
+        return {"mlups": m["value"], "ms_per_step": m["ms_per_step"], "bulk_kernel_ms": m["dense_ms"],
+                "hbm_gbs_bulk": m["achieved"], "bytes_per_lu": m["bytes_per_lu"], "band_kernel_ms": m["band_ms"],
+                "whole_lattice_kernel_ms_serial": m["full_ms"], "steady_state_mlups_graph_l2_warm": m["steady"],
+                "e2e_mlups": m["e2e"], "mdf_last_iterations": m["mdf"]["iter_count"], "status": m["status"],
+                "Cd": m["cd"], "Cl": m["cl"], "step": m["steps_done"]}
+
+    line = {"metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if chosen else "f64",
+            "data": "synthetic (deterministic initial state of the workload)",
+            "config": dict(WORKLOAD, form=form, parallelism=f"replicas x{ws}"),
+            "hbm_gbs_dense": head["achieved"],
             "schedule": "band kernel + box pass (side stream) concurrent with the bulk pass",
-            "mdf_last_iterations": stats["iter_count"], "status": status,
-            "steady_state_mlups_graph_l2_warm": steady,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "dense_step_kernel bulk pass (fused pull-stream+BC+macro+collide, FP64)",
-                         "bytes_per_lu": BYTES_PER_LU_F64, "lattice_updates_per_launch": N - box_nodes},
+            "roofline": {"bound": "hbm", "achieved": head["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": head["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": ("dense32_kernel" if chosen else "dense_step_kernel") +
+                                   " bulk pass (fused pull-stream+BC+macro+collide)",
+                         "bytes_per_lu": head["bytes_per_lu"], "lattice_updates_per_launch": N - head["box_nodes"]},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": 4 * Lb * 8, "d2h_bytes_per_step": 16},
-            "gpu_launches": 3 * K,
-            "clocks": clocks, "wall_s_timed": t_wall}
+            "e2e": {"value": head["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": head["e2e_h2d"],
+                    "d2h_bytes_per_step": head["e2e_d2h"]},
+            "gpu_launches": 3 * args.steps,
+            "clocks": head["clocks"], "wall_s_timed": head["wall_s_timed"],
+            "plain": summary(plain)}
+    if chosen:
+        line["chosen"] = summary(chosen)
+        line["chosen_vs_plain"] = chosen["value"] / plain["value"]
+        line["cd_rel_err_vs_f64"] = abs(chosen["cd"] - plain["cd"]) / abs(plain["cd"])
+        line["cl_err_vs_f64_rel_cd"] = abs(chosen["cl"] - plain["cl"]) / abs(plain["cd"])
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -302,7 +332,8 @@ def run_profile(args):
     (two kernel launches each), no graphs, no baseline, no clock sampling."""
     import torch
     from iblbm_b200.engine import Engine
-    eng = Engine(workload_config(collision=args.collision, max_steps=args.warmup + args.steps + 8))
+    eng = Engine(workload_config(collision=args.collision, max_steps=args.warmup + args.steps + 8),
+                 precision=args.precision)
     for _ in range(args.warmup + args.steps):
         eng._launch(False)
     eng.join()
@@ -318,6 +349,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--profile", action="store_true", help="short eager run for ncu captures")
     ap.add_argument("--collision", default="TRT", choices=["BGK", "TRT", "CM_MRT"])
+    ap.add_argument("--form", default="chosen", choices=["chosen", "plain"],
+                    help="chosen: time the FP32 shifted form and the FP64 plain form; plain: FP64 only")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="form used by --profile")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -56,6 +56,11 @@ class IbmArgs(ctypes.Structure):
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp)]
 
 
+# The FP32 argument structs (iblbm_dense32_args, iblbm_ibm32_args) have the
+# same fields in the same order as the FP64 ones; only the pointee types differ.
+Dense32Args = DenseArgs
+Ibm32Args = IbmArgs
+
 # entry point -> argtypes (all return int status)
 _SIGS = {
     "iblbm_dense_step_f64": [ctypes.POINTER(DenseArgs), _vp],
@@ -72,6 +77,12 @@ _SIGS = {
     "iblbm_collision_cm_mrt": [_vp, _vp, _vp, _i, ctypes.POINTER(_d), _d, _vp, _vp],
     "iblbm_streaming": [_vp, _vp, _i, _i, _vp, _vp],
     "iblbm_velocity_correction": [_vp, _vp, _vp, _i, _d, _i, _vp],
+    "iblbm_dense_step_f32": [ctypes.POINTER(DenseArgs), _vp],
+    "iblbm_ibm_step_f32": [ctypes.POINTER(IbmArgs), _vp],
+    "iblbm_ibm32_list_cache_ints": [_i, _i, _i],
+    "iblbm_ibm32_smem_bytes": [_i, _i, _i],
+    "iblbm_to_shifted_f32": [_vp, Geom, _vp, _vp],
+    "iblbm_from_shifted_f32": [_vp, Geom, _vp, _vp],
     "iblbm_aos_to_soa": [_vp, Geom, _vp, _vp],
     "iblbm_soa_to_aos": [_vp, Geom, _vp, _vp],
 }

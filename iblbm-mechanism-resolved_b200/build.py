@@ -25,6 +25,8 @@ UNITS = {
     "dense_f64.cu": ["-fmad=false"],
     "ibm_f64.cu": ["-fmad=false"],
     "ops_f64.cu": ["-fmad=false"],
+    "dense_f32.cu": [],
+    "ibm_f32.cu": [],
 }
 
 

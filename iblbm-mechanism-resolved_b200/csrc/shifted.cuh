@@ -1,0 +1,393 @@
+// shifted.cuh — FP32 "shifted population" form of the per-node timestep.
+//
+// Populations are stored and collided as deviations g_q = f_q - w_q in FP32.
+// The O(1) lattice weights never enter an FP32 sum, so the deviations keep
+// ~7 significant digits of the O(u) physics instead of losing 2-3 digits to
+// cancellation against w_q.  Identities used (lattice weights w_q = w_opp(q),
+// sum w = 1, sum w e = 0, sum w e_x^2 = 1/3, sum w e_x^2 e_y^2 = 1/9):
+//   rho = 1 + sum g,  rho u = sum g e;
+//   feq_q - w_q = w_q (d_rho + rho X_q)          (compressible)
+//              = w_q (d_rho + X_q)              (incompressible, He-Luo)
+//   with X_q = 3 e.u + 4.5 (e.u)^2 - 1.5 u^2 and d_rho = rho - 1;
+//   the Zou-He unknown-population formulas pair equal weights, so they hold
+//   unchanged on g, and their density sums become 1 + (sum of the g's);
+//   CM-MRT relaxes k(g) with the analytic central moments of the weights
+//   k(w) about u, and maps the post-collision difference back with the same
+//   linear transform, so g_out = T(k_post - k(w)).
+// Arithmetic is FP32 (contracted to FMA where the compiler chooses).
+#pragma once
+#include "common.cuh"
+#include "../../include/iblbm_b200.h"
+
+namespace iblbm {
+
+struct BcParams32 {
+    float inflow_u, dens;
+    float geq_in[9];  // feq(dens, (inflow_u, 0)) - w, rounded from FP64
+};
+
+struct CollParams32 {
+    float inv_tau, guo_pref, s_plus, s_minus, dt;
+    float S[9];
+};
+
+__device__ __forceinline__ float wf(int q) { return (float)w_(q); }
+
+// feq - w in shifted form
+template <bool INCOMP>
+__device__ __forceinline__ float geq_q(int q, float drho, float rho, float u0, float u1, float u2)
+{
+    const float eu = (float)ex_(q) * u0 + (float)ey_(q) * u1;
+    const float X = 3.0f * eu + 4.5f * eu * eu - 1.5f * u2;
+    return INCOMP ? wf(q) * (drho + X) : wf(q) * (drho + rho * X);
+}
+
+__device__ __forceinline__ void macro_g(const float* g, bool incomp, float& drho, float& rho, float& u0, float& u1)
+{
+    float s = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) s += g[q];
+    const float jx = ((g[1] - g[3]) + (g[5] - g[6])) + (g[8] - g[7]);
+    const float jy = ((g[2] - g[4]) + (g[5] + g[6])) - (g[7] + g[8]);
+    drho = s;
+    rho = 1.0f + s;
+    if (incomp) { u0 = jx; u1 = jy; }
+    else { const float inv = 1.0f / rho; u0 = jx * inv; u1 = jy * inv; }
+}
+
+__device__ __forceinline__ void geq_all(float dens, float u0, float u1, bool incomp, float* out)
+{
+    const float drho = dens - 1.0f, u2 = u0 * u0 + u1 * u1;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) out[q] = incomp ? geq_q<true>(q, drho, dens, u0, u1, u2) : geq_q<false>(q, drho, dens, u0, u1, u2);
+}
+
+// ---- boundary closures on g (see the formulas of common.cuh) ---------------------
+__device__ __forceinline__ float uo32_x(const float* __restrict__ ur, const Geom& g, int i, int j)
+{
+    return ur[2 * ((long long)j * g.nx + i)];
+}
+__device__ __forceinline__ float uo32_y(const float* __restrict__ ur, const Geom& g, int i, int j)
+{
+    return ur[2 * ((long long)j * g.nx + i) + 1];
+}
+
+__device__ __forceinline__ void bc32_dirichlet_neumann(const float* __restrict__ fp, const Geom& g, const BcParams32& bc,
+                                                       int i, int j, float* f)
+{
+    if (i == g.nx - 1) {
+        const int js = (j == 0) ? 1 : (j == g.ny - 1 ? g.ny - 2 : j);
+        float fi[9], fq[9], drho, rho, a, b;
+        pull(fp, g, g.nx - 2, js, fi);
+        macro_g(fi, false, drho, rho, a, b);
+        geq_all(rho, a, b, false, fq);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] = fq[q] + (fi[q] - fq[q]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] = bc.geq_in[q];
+    }
+}
+
+__device__ __forceinline__ void bc32_open(const float* __restrict__ ur, const Geom& g, const BcParams32& bc, int i,
+                                          int j, float* f)
+{
+    const int nx = g.nx, ny = g.ny;
+    const float ro = bc.dens, dr = bc.dens - 1.0f;
+    if ((i == 0 || i == nx - 1) && (j == 0 || j == ny - 1)) {
+        const int di = (i == 0) ? 1 : nx - 2, dj = (j == 0) ? 1 : ny - 2;
+        geq_all(ro, uo32_x(ur, g, di, dj), uo32_y(ur, g, di, dj), false, f);
+        return;
+    }
+    if (i == 0) {
+        const float G = f[0] + f[2] + f[4] + 2.0f * (f[3] + f[7] + f[6]);
+        const float ux = (dr - G) / ro;
+        const float uy = (4.0f * uo32_y(ur, g, 1, j) - uo32_y(ur, g, 2, j)) / 3.0f;
+        f[1] = f[3] + (2.0f / 3.0f) * ro * ux;
+        f[5] = f[7] - 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+        f[8] = f[6] + 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+    } else if (i == nx - 1) {
+        const float G = f[0] + f[2] + f[4] + 2.0f * (f[1] + f[5] + f[8]);
+        const float ux = (G - dr) / ro;
+        const float uy = (4.0f * uo32_y(ur, g, nx - 2, j) - uo32_y(ur, g, nx - 3, j)) / 3.0f;
+        f[3] = f[1] - (2.0f / 3.0f) * ro * ux;
+        f[7] = f[5] + 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+        f[6] = f[8] - 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+    } else if (j == ny - 1) {
+        const float G = f[0] + f[1] + f[3] + 2.0f * (f[2] + f[5] + f[6]);
+        const float uy = (G - dr) / ro;
+        const float ux = (4.0f * uo32_x(ur, g, i, ny - 2) - uo32_x(ur, g, i, ny - 3)) / 3.0f;
+        f[4] = f[2] - (2.0f / 3.0f) * ro * uy;
+        f[7] = f[5] + 0.5f * (f[1] - f[3]) - (1.0f / 6.0f) * ro * uy - 0.5f * ro * ux;
+        f[8] = f[6] - 0.5f * (f[1] - f[3]) - (1.0f / 6.0f) * ro * uy + 0.5f * ro * ux;
+    } else {
+        const float G = f[0] + f[1] + f[3] + 2.0f * (f[4] + f[7] + f[8]);
+        const float uy = (dr - G) / ro;
+        const float ux = (4.0f * uo32_x(ur, g, i, 1) - uo32_x(ur, g, i, 2)) / 3.0f;
+        f[2] = f[4] + (2.0f / 3.0f) * ro * uy;
+        f[5] = f[7] - 0.5f * (f[1] - f[3]) + (1.0f / 6.0f) * ro * uy + 0.5f * ro * ux;
+        f[6] = f[8] + 0.5f * (f[1] - f[3]) + (1.0f / 6.0f) * ro * uy - 0.5f * ro * ux;
+    }
+}
+
+__device__ __forceinline__ void bc32_settling(const Geom& g, const BcParams32& bc, bool incomp, int i, int j, float* f)
+{
+    const int nx = g.nx, ny = g.ny;
+    if ((i == 0 || i == nx - 1) && (j == 0 || j == ny - 1)) {
+        geq_all(bc.dens, 0.0f, 0.0f, incomp, f);
+        return;
+    }
+    if (i == 0) {
+        f[1] = f[3];
+        f[5] = f[7] - 0.5f * (f[2] - f[4]);
+        f[8] = f[6] + 0.5f * (f[2] - f[4]);
+    } else if (i == nx - 1) {
+        f[3] = f[1];
+        f[7] = f[5] + 0.5f * (f[2] - f[4]);
+        f[6] = f[8] - 0.5f * (f[2] - f[4]);
+    } else if (j == ny - 1) {
+        f[4] = f[2];
+        f[7] = f[5] + 0.5f * (f[1] - f[3]);
+        f[8] = f[6] - 0.5f * (f[1] - f[3]);
+    } else {
+        f[2] = f[4];
+        f[5] = f[7] - 0.5f * (f[1] - f[3]);
+        f[6] = f[8] + 0.5f * (f[1] - f[3]);
+    }
+}
+
+__device__ __forceinline__ void bc32_velocity_inlet(const float* __restrict__ ur, const Geom& g, const BcParams32& bc,
+                                                    int i, int j, float* f)
+{
+    const int nx = g.nx, ny = g.ny;
+    if (i == 0) {
+        if (j == 0 || j == ny - 1) {
+            geq_all(bc.dens, bc.inflow_u, 0.0f, false, f);
+            return;
+        }
+        const float ux = bc.inflow_u, uy = 0.0f;
+        const float ro = (1.0f + (f[0] + f[2] + f[4] + 2.0f * (f[3] + f[6] + f[7]))) / (1.0f - ux);
+        f[1] = f[3] + (2.0f / 3.0f) * ro * ux;
+        f[5] = f[7] - 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+        f[8] = f[6] + 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+        return;
+    }
+    if (i == nx - 1) {
+        if (j == 0 || j == ny - 1) {
+            const int r1 = (j == 0) ? 1 : ny - 2, r2 = (j == 0) ? 2 : ny - 3;
+            const float b1 = (4.0f * uo32_x(ur, g, nx - 2, r1) - uo32_x(ur, g, nx - 2, r2)) / 3.0f;
+            const float b2 = (4.0f * uo32_x(ur, g, nx - 3, r1) - uo32_x(ur, g, nx - 3, r2)) / 3.0f;
+            geq_all(bc.dens, (4.0f * b1 - b2) / 3.0f, 0.0f, false, f);
+            return;
+        }
+        const float ro = bc.dens, dr = bc.dens - 1.0f;
+        const float uy = (4.0f * uo32_y(ur, g, nx - 2, j) - uo32_y(ur, g, nx - 3, j)) / 3.0f;
+        const float ux = ((f[0] + f[2] + f[4] + 2.0f * (f[1] + f[5] + f[8])) - dr) / ro;
+        f[3] = f[1] - (2.0f / 3.0f) * ro * ux;
+        f[7] = f[5] + 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+        f[6] = f[8] - 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+        return;
+    }
+    if (j == ny - 1) {
+        const float ux = (4.0f * uo32_x(ur, g, i, ny - 2) - uo32_x(ur, g, i, ny - 3)) / 3.0f;
+        const float ro = 1.0f + (f[0] + f[1] + f[3] + 2.0f * (f[2] + f[5] + f[6]));
+        f[4] = f[2];
+        f[7] = f[5] + 0.5f * (f[1] - f[3]) - 0.5f * ro * ux;
+        f[8] = f[6] - 0.5f * (f[1] - f[3]) + 0.5f * ro * ux;
+        return;
+    }
+    const float ux = (4.0f * uo32_x(ur, g, i, 1) - uo32_x(ur, g, i, 2)) / 3.0f;
+    const float ro = 1.0f + (f[0] + f[1] + f[3] + 2.0f * (f[4] + f[7] + f[8]));
+    f[2] = f[4];
+    f[5] = f[7] - 0.5f * (f[1] - f[3]) + 0.5f * ro * ux;
+    f[6] = f[8] + 0.5f * (f[1] - f[3]) - 0.5f * ro * ux;
+}
+
+template <int BC>
+__device__ __forceinline__ void gstar_node(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
+                                           const BcParams32& bc, bool incomp, int i, int j, float* f)
+{
+    const bool boundary = (i == 0) | (j == 0) | (i == g.nx - 1) | (j == g.ny - 1);
+    if (BC == BC_DIRICHLET_NEUMANN && boundary) {
+        bc32_dirichlet_neumann(fp, g, bc, i, j, f);
+        return;
+    }
+    pull(fp, g, i, j, f);
+    if (!boundary) return;
+    if (BC == BC_OPEN) bc32_open(ur, g, bc, i, j, f);
+    else if (BC == BC_SETTLING) bc32_settling(g, bc, incomp, i, j, f);
+    else if (BC == BC_VELOCITY_INLET) bc32_velocity_inlet(ur, g, bc, i, j, f);
+}
+
+// ---- collisions on g ----------------------------------------------------------
+__device__ __forceinline__ float guo_bare(int q, float u0, float u1, float F0, float F1)
+{
+    const float ex = (float)ex_(q), ey = (float)ey_(q);
+    const float eU = ex * u0 + ey * u1;
+    return wf(q) * ((3.0f * (ex - u0) + 9.0f * eU * ex) * F0 + (3.0f * (ey - u1) + 9.0f * eU * ey) * F1);
+}
+
+template <bool INCOMP, bool FORCED>
+__device__ __forceinline__ void collide32_bgk(const float* g, float drho, float rho, float u0, float u1, float F0,
+                                              float F1, const CollParams32& cp, float* out)
+{
+    const float u2 = u0 * u0 + u1 * u1;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        float v = g[q] - cp.inv_tau * (g[q] - geq_q<INCOMP>(q, drho, rho, u0, u1, u2));
+        if (FORCED) v += cp.guo_pref * guo_bare(q, u0, u1, F0, F1) * cp.dt;
+        out[q] = v;
+    }
+}
+
+template <bool INCOMP, bool FORCED>
+__device__ __forceinline__ void collide32_trt(const float* g, float drho, float rho, float u0, float u1, float F0,
+                                              float F1, const CollParams32& cp, float* out)
+{
+    const float u2 = u0 * u0 + u1 * u1;
+    float ge[9], bare[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        ge[q] = geq_q<INCOMP>(q, drho, rho, u0, u1, u2);
+        bare[q] = FORCED ? guo_bare(q, u0, u1, F0, F1) : 0.0f;
+    }
+    const float gp = 1.0f - 0.5f * cp.s_plus, gm = 1.0f - 0.5f * cp.s_minus;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const int o = opp_(q);
+        const float fp = 0.5f * (g[q] + g[o]) - 0.5f * (ge[q] + ge[o]);
+        const float fm = 0.5f * (g[q] - g[o]) - 0.5f * (ge[q] - ge[o]);
+        float v = g[q] - (cp.s_plus * fp + cp.s_minus * fm);
+        if (FORCED) v += (gp * 0.5f * (bare[q] + bare[o]) + gm * 0.5f * (bare[q] - bare[o])) * cp.dt;
+        out[q] = v;
+    }
+}
+
+template <bool FORCED>
+__device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, float ux, float uy, float F0, float F1,
+                                                const CollParams32& cp, float* out)
+{
+    float k[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float ex = (float)ex_(q), ey = (float)ey_(q);
+        const float cx = ex - ux, cy = ey - uy, cx2 = cx * cx, cy2 = cy * cy;
+        const float v = g[q];
+        k[0] += v; k[1] += v * cx; k[2] += v * cy; k[3] += v * cx2; k[4] += v * cy2;
+        k[5] += v * cx * cy; k[6] += v * cx2 * cy; k[7] += v * cx * cy2; k[8] += v * cx2 * cy2;
+        if (FORCED) {
+            const float b = guo_bare(q, ux, uy, F0, F1);
+            F[0] += b; F[1] += b * cx; F[2] += b * cy; F[3] += b * cx2; F[4] += b * cy2;
+            F[5] += b * cx * cy; F[6] += b * cx2 * cy; F[7] += b * cx * cy2; F[8] += b * cx2 * cy2;
+        }
+    }
+    // central moments of the weights about u, and the equilibrium minus them
+    const float ax = 1.0f / 3.0f + ux * ux, ay = 1.0f / 3.0f + uy * uy;
+    const float kw[9] = {1.0f, -ux, -uy, ax, ay, ux * uy, -uy * ax, -ux * ay, ax * ay};
+    const float rho = 1.0f + drho;
+    const float keq[9] = {rho, 0.0f, 0.0f, rho / 3.0f, rho / 3.0f, 0.0f, 0.0f, 0.0f, rho / 9.0f};
+    float c[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+        // k_post - k(w) = k(g) - S (k(g) + k(w) - k_eq) + (1 - S/2) F dt
+        const float neq = (m == 0) ? 0.0f : (k[m] + (kw[m] - keq[m]));
+        c[m] = k[m] - cp.S[m] * neq;
+        if (FORCED) c[m] += (1.0f - 0.5f * cp.S[m]) * F[m] * cp.dt;
+    }
+    const float ux2 = ux * ux, uy2 = uy * uy;
+    const float k0 = c[0];
+    const float k1 = c[1] + ux * c[0];
+    const float k2 = c[2] + uy * c[0];
+    const float k3 = c[3] + 2.0f * ux * c[1] + ux2 * c[0];
+    const float k4 = c[4] + 2.0f * uy * c[2] + uy2 * c[0];
+    const float k5 = c[5] + uy * c[1] + ux * c[2] + ux * uy * c[0];
+    const float k6 = c[6] + uy * c[3] + 2.0f * ux * c[5] + 2.0f * ux * uy * c[1] + ux2 * c[2] + ux2 * uy * c[0];
+    const float k7 = c[7] + 2.0f * uy * c[5] + ux * c[4] + 2.0f * ux * uy * c[2] + uy2 * c[1] + ux * uy2 * c[0];
+    const float k8 = c[8] + 2.0f * uy * c[6] + uy2 * c[3] + 2.0f * ux * c[7] + 4.0f * ux * uy * c[5] +
+                     2.0f * ux * uy2 * c[1] + ux2 * c[4] + 2.0f * ux2 * uy * c[2] + ux2 * uy2 * c[0];
+    out[0] = k0 - k3 - k4 + k8;
+    out[1] = 0.5f * (k1 + k3 - k7 - k8);
+    out[2] = 0.5f * (k2 + k4 - k6 - k8);
+    out[3] = 0.5f * (-k1 + k3 + k7 - k8);
+    out[4] = 0.5f * (-k2 + k4 + k6 - k8);
+    out[5] = 0.25f * (k5 + k6 + k7 + k8);
+    out[6] = 0.25f * (-k5 + k6 - k7 + k8);
+    out[7] = 0.25f * (k5 - k6 - k7 + k8);
+    out[8] = 0.25f * (-k5 - k6 + k7 + k8);
+}
+
+template <int COLL, bool INCOMP, bool FORCED>
+__device__ __forceinline__ void collide32(const float* g, float drho, float rho, float u0, float u1, float F0, float F1,
+                                          const CollParams32& cp, float* out)
+{
+    if (COLL == COLL_BGK) collide32_bgk<INCOMP, FORCED>(g, drho, rho, u0, u1, F0, F1, cp, out);
+    else if (COLL == COLL_TRT) collide32_trt<INCOMP, FORCED>(g, drho, rho, u0, u1, F0, F1, cp, out);
+    else collide32_cmmrt<FORCED>(g, drho, u0, u1, F0, F1, cp, out);
+}
+
+struct BandView32 {
+    const int* box;
+    const int* map;
+    const float* fib;  // band x 2
+    const float* df;   // band x 9 (shifted distribution correction)
+};
+
+struct DenseOut32 {
+    float* fpost_next;
+    float* uring_next;
+    float* ro_out;
+    float* U_out;
+    float* fstar_out;
+};
+
+__device__ __forceinline__ int band_lookup32(const BandView32& bv, int nx, int i, int j)
+{
+    const int x0 = __ldg(bv.box + 0), y0 = __ldg(bv.box + 1), w = __ldg(bv.box + 2), h = __ldg(bv.box + 3);
+    if (i < x0 || i >= x0 + w || j < y0 || j >= y0 + h) return -1;
+    return bv.map[(long long)j * nx + i];
+}
+
+template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
+__device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
+                                             const CollParams32& cp, const BcParams32& bc, const BandView32& band,
+                                             const DenseOut32& o, int i, int j)
+{
+    float f[9];
+    gstar_node<BC>(fp, ur, g, bc, INCOMP, i, j, f);
+    int b = -1;
+    if (IBM != IBM_NONE) b = band_lookup32(band, g.nx, i, j);
+    if (IBM == IBM_DFC && b >= 0) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] += band.df[9 * (long long)b + q];
+    }
+    const long long site = (long long)j * g.pitch + i;
+    if (OUT && o.fstar_out) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) o.fstar_out[q * g.qstride + site] = f[q];
+    }
+    float drho, rho, u0, u1;
+    macro_g(f, INCOMP, drho, rho, u0, u1);
+    float out[9];
+    if ((IBM == IBM_DF || IBM == IBM_MDF) && b >= 0) {
+        const float F0 = band.fib[2 * (long long)b], F1 = band.fib[2 * (long long)b + 1];
+        if (INCOMP) { u0 += 0.5f * F0 * cp.dt; u1 += 0.5f * F1 * cp.dt; }
+        else { const float h = cp.dt / (2.0f * rho); u0 += F0 * h; u1 += F1 * h; }
+        collide32<COLL, INCOMP, true>(f, drho, rho, u0, u1, F0, F1, cp, out);
+    } else {
+        collide32<COLL, INCOMP, false>(f, drho, rho, u0, u1, 0.0f, 0.0f, cp, out);
+    }
+    if (OUT) {
+        const long long n = (long long)j * g.nx + i;
+        if (o.ro_out) o.ro_out[n] = rho;
+        if (o.U_out) { o.U_out[2 * n] = u0; o.U_out[2 * n + 1] = u1; }
+    }
+    if ((BC == BC_OPEN || BC == BC_VELOCITY_INLET) && is_ring(g, i, j)) {
+        const long long n = (long long)j * g.nx + i;
+        o.uring_next[2 * n] = u0;
+        o.uring_next[2 * n + 1] = u1;
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) o.fpost_next[q * g.qstride + site] = out[q];
+}
+
+}  // namespace iblbm

@@ -8,6 +8,10 @@ Per timestep the engine launches, on one CUDA stream:
    moments + collision over the whole lattice, ping-ponging two population
    buffers.
 
+With ``precision="f32"`` the same schedule runs on the shifted FP32 form
+(``iblbm_ibm_step_f32`` / ``iblbm_dense_step_f32``): populations are held as
+g = f - w in FP32; marker data, per-marker forces and every force sum stay FP64.
+
 Steps between diagnostics are captured once into CUDA graphs and replayed, so
 the host issues one graph launch per chunk instead of two kernel launches per
 step.  Device layout: populations are pitched structure-of-arrays planes
@@ -38,10 +42,15 @@ def _torch():
 
 
 class Engine:
-    """One lattice case on one GPU (FP64 form, the reference's arithmetic)."""
+    """One lattice case on one GPU: FP64 form (the reference's arithmetic) or
+    the shifted FP32 form (``precision="f32"``)."""
 
-    def __init__(self, cfg, device=None):
+    def __init__(self, cfg, device=None, precision="f64"):
         torch = _torch()
+        if precision not in ("f64", "f32"):
+            raise ValueError(f"precision='{precision}' (f64 or f32)")
+        self.precision = precision
+        self.f32 = precision == "f32"
         self.torch = torch
         self.cfg = cfg
         self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -72,6 +81,7 @@ class Engine:
         self.geom = Geom(nx, ny, pitch, pitch * ny)
         self.qstride = pitch * ny
         dev, f64, i32 = self.dev, torch.float64, torch.int32
+        ldt = self.ldt = torch.float32 if self.f32 else torch.float64  # lattice and band fields
         self.stream = lambda: torch.cuda.current_stream(self.dev).cuda_stream
         self.case = Case()
         c = self.case
@@ -95,13 +105,16 @@ class Engine:
         fib0 = torch.zeros(N * 2, dtype=f64, device=dev)
         fpost0 = torch.empty_like(feq0)
         self._collide_aos(feq0, feq0, U0, fib0, fpost0)
-        self.f = [torch.empty(9 * self.qstride, dtype=f64, device=dev) for _ in range(2)]
-        check(self.L.iblbm_aos_to_soa(ptr(fpost0), self.geom, ptr(self.f[0]), s), "iblbm_aos_to_soa")
+        self.f = [torch.empty(9 * self.qstride, dtype=ldt, device=dev) for _ in range(2)]
+        if self.f32:
+            check(self.L.iblbm_to_shifted_f32(ptr(fpost0), self.geom, ptr(self.f[0]), s), "iblbm_to_shifted_f32")
+        else:
+            check(self.L.iblbm_aos_to_soa(ptr(fpost0), self.geom, ptr(self.f[0]), s), "iblbm_aos_to_soa")
         del feq0, fpost0, fib0
-        self.uring = [U0.reshape(-1).clone(), U0.reshape(-1).clone()]
-        self.ro_out = torch.empty(N, dtype=f64, device=dev)
-        self.U_out = torch.empty(N * 2, dtype=f64, device=dev)
-        self.fstar_out = torch.zeros(9 * self.qstride, dtype=f64, device=dev)
+        self.uring = [U0.reshape(-1).to(ldt).clone(), U0.reshape(-1).to(ldt).clone()]
+        self.ro_out = torch.empty(N, dtype=ldt, device=dev)
+        self.U_out = torch.empty(N * 2, dtype=ldt, device=dev)
+        self.fstar_out = torch.zeros(9 * self.qstride, dtype=ldt, device=dev)
         self.parity = 0
         self.ttt = 1
 
@@ -128,12 +141,13 @@ class Engine:
         self.d_box = t(4, i32)
         self.d_map = torch.full((N,), -1, dtype=i32, device=dev)
         self.d_nodes, self.d_count = t(B, i32), t(1, i32)
-        self.d_fib, self.d_df = t(2 * B), t(9 * B)
-        self.d_fib_part = t(2 * B * self.P)
+        self.d_fib, self.d_df = t(2 * B, ldt), t(9 * B, ldt)
+        self.d_fib_part = t(2 * B * self.P, ldt)
         delta_id = DELTA_IDS[cfg.delta_type]
-        self.d_scr = t(self.L.iblbm_ibm_scratch_doubles(self.Lb, B, self.P))
+        self.d_scr = t(self.L.iblbm_ibm_scratch_doubles(self.Lb, B, self.P), ldt)
         self.d_iscr = t(self.L.iblbm_ibm_scratch_ints(self.Lb, B, delta_id), i32)
-        self.d_lists = t(self.L.iblbm_ibm_list_cache_ints(self.Lb, B, delta_id), i32)
+        cache_ints = self.L.iblbm_ibm32_list_cache_ints if self.f32 else self.L.iblbm_ibm_list_cache_ints
+        self.d_lists = t(cache_ints(self.Lb, B, delta_id), i32)
         self.d_excl = torch.zeros(2, 4, dtype=i32, device=dev)
         self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy = (t(self.Lb) for _ in range(4))
         self.d_dfc_force = t(2 * self.Lb)
@@ -267,12 +281,18 @@ class Engine:
         ia = self.ibm_args[self.parity]
         ia.rebuild = 1 if (self.rebuild_next or self.moving) else 0
         ia.excl_cur = ptr(self.d_excl[self.parity]) if excl_check else 0
-        check(self.L.iblbm_ibm_step_f64(ctypes.byref(ia), stream), "iblbm_ibm_step_f64")
+        if self.f32:
+            check(self.L.iblbm_ibm_step_f32(ctypes.byref(ia), stream), "iblbm_ibm_step_f32")
+        else:
+            check(self.L.iblbm_ibm_step_f64(ctypes.byref(ia), stream), "iblbm_ibm_step_f64")
         self.rebuild_next = False
 
     def _dense(self, variant, outputs, stream):
         da = variant[self.parity][1 if outputs else 0]
-        check(self.L.iblbm_dense_step_f64(ctypes.byref(da), stream), "iblbm_dense_step_f64")
+        if self.f32:
+            check(self.L.iblbm_dense_step_f32(ctypes.byref(da), stream), "iblbm_dense_step_f32")
+        else:
+            check(self.L.iblbm_dense_step_f64(ctypes.byref(da), stream), "iblbm_dense_step_f64")
 
     def _step_serial(self, outputs=False, events=None):
         """One timestep on the current stream: band kernel, then the whole lattice.
@@ -431,6 +451,7 @@ class Engine:
         nb = int(self.d_count.item())
         nodes = self.d_nodes[:nb].cpu().numpy()
         part = self.d_fib_part[: 2 * self.B * self.P].reshape(self.P, self.B, 2)[:, :nb].cpu().numpy()
+        part = part.astype(np.float64)
         out = []
         for p in range(self.P):
             dense = np.zeros((self.N, 2))
@@ -444,20 +465,20 @@ class Engine:
         nb = int(self.d_count.item())
         fib = torch.zeros(self.N, 2, dtype=torch.float64, device=self.dev)
         if self.method in ("DF", "MDF") and nb > 0:
-            fib[self.d_nodes[:nb].long()] = self.d_fib[: 2 * nb].reshape(nb, 2)
+            fib[self.d_nodes[:nb].long()] = self.d_fib[: 2 * nb].reshape(nb, 2).double()
         return fib
 
     def cd_cl(self):
         """Cd, Cl of the last output step — iblbm/diagnostics/core.py:53-113."""
         cfg, st = self.cfg, self.st
         u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
-        ro_mean = float(self.ro_out.mean())
+        ro_mean = float(self.ro_out.double().mean())
         denom = ro_mean * u_ref ** 2 * st.lattice_r
         if self.method == "DFC":
             force = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).sum(0).cpu().numpy()
             return float(abs(force[0])) / denom, float(force[1]) / denom
         nb = int(self.d_count.item())
-        sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).sum(0).cpu())
+        sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).double().sum(0).cpu())
         return abs(sx) / denom, sy / denom
 
     def mdf_stats(self):
@@ -477,14 +498,14 @@ class Engine:
         self.join()
         s = self.stream()
         fs = torch.empty(self.N * 9, dtype=torch.float64, device=self.dev)
-        check(self.L.iblbm_soa_to_aos(ptr(self.fstar_out), self.geom, ptr(fs), s), "iblbm_soa_to_aos")
+        self._to_aos(self.fstar_out, fs)
         feq = torch.empty_like(fs)
-        check(self.L.iblbm_feq(ptr(self.ro_out), ptr(self.U_out), self.N, self.case.incompressible, ptr(feq), s),
-              "iblbm_feq")
+        ro, U = self.ro_out.double().contiguous(), self.U_out.double().contiguous()
+        check(self.L.iblbm_feq(ptr(ro), ptr(U), self.N, self.case.incompressible, ptr(feq), s), "iblbm_feq")
         st.fstar = fs.reshape(self.N, 9).cpu().numpy()
         st.feq = feq.reshape(self.N, 9).cpu().numpy()
-        st.ro = self.ro_out.cpu().numpy()
-        st.U = self.U_out.reshape(self.N, 2).cpu().numpy()
+        st.ro = ro.cpu().numpy()
+        st.U = U.reshape(self.N, 2).cpu().numpy()
         st.fib = self.band_fib_dense().cpu().numpy()
         if self.method == "DFC":
             st.dfc_force_lagr = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).cpu().numpy()
@@ -496,6 +517,13 @@ class Engine:
         """Post-collision populations of the last completed step (AoS)."""
         torch = self.torch
         out = torch.empty(self.N * 9, dtype=torch.float64, device=self.dev)
-        check(self.L.iblbm_soa_to_aos(ptr(self.f[self.parity]), self.geom, ptr(out), self.stream()),
-              "iblbm_soa_to_aos")
+        self._to_aos(self.f[self.parity], out)
         return out.reshape(self.N, 9).cpu().numpy()
+
+    def _to_aos(self, soa, out):
+        """Lattice SoA buffer -> FP64 AoS f[N, 9] (adds the weights back in the FP32 form)."""
+        if self.f32:
+            check(self.L.iblbm_from_shifted_f32(ptr(soa), self.geom, ptr(out), self.stream()),
+                  "iblbm_from_shifted_f32")
+        else:
+            check(self.L.iblbm_soa_to_aos(ptr(soa), self.geom, ptr(out), self.stream()), "iblbm_soa_to_aos")

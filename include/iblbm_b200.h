@@ -173,6 +173,82 @@ int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm_smem_bytes(int lb_total, int band_capacity, int delta_type);
 
+/* ---- FP32 shifted-population form ----------------------------------------
+ * Populations are held as deviations g = f - w from the lattice weights, in
+ * FP32 (72 bytes per lattice update instead of 144).  Equilibria, closures and
+ * collisions are rewritten on g (rho = 1 + sum g); marker positions, desired
+ * velocities, per-marker forces, the MDF residual norm and everything downstream
+ * of the marker forces (force sums, Newton-Euler) stay FP64.  Same layout and
+ * schedule as the FP64 entries; no reference counterpart (the reference is
+ * FP64 throughout), the FP64 entries are its drop-in. */
+typedef struct {
+    const int *box;
+    const int *map;
+    const float *fib;   /* band x 2 */
+    const float *df;    /* band x 9 */
+} iblbm_band_view32;
+
+typedef struct {
+    iblbm_geom g;
+    iblbm_case c;               /* FP64 parameters, rounded to FP32 at launch */
+    int ibm;
+    const float *fpost_prev;    /* SoA deviations g = f - w */
+    float *fpost_next;
+    const float *uring_prev;
+    float *uring_next;
+    iblbm_band_view32 band;
+    float *ro_out, *U_out, *fstar_out;  /* ro is rho (not rho - 1); fstar is shifted */
+    const int *skip_box;
+    const int *only_box;
+    int box_blocks;
+} iblbm_dense32_args;
+
+/* Fused timestep on the shifted FP32 form (see iblbm_dense_step_f64). */
+int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
+/* f (FP64 AoS, the reference's f[N, 9]) -> g = f - w (FP32 SoA), and back. */
+int iblbm_to_shifted_f32(const double *aos, iblbm_geom g, float *soa, void *stream);
+int iblbm_from_shifted_f32(const float *soa, iblbm_geom g, double *aos, void *stream);
+
+/* Band step on the shifted FP32 lattice.  Fields as iblbm_ibm_args; the
+ * lattice inputs, band forces/corrections and scratch are FP32, the marker
+ * arrays and per-marker outputs FP64. */
+typedef struct {
+    iblbm_geom g;
+    iblbm_case c;
+    int method, delta_type, rebuild, n_particles, lb_total;
+    const int *moff;
+    const double *Lx, *Ly;
+    const double *dvel;
+    const double *larea;
+    double dx, dy;
+    const double *Lx_c, *Ly_c, *xt_table;
+    int *step_counter;
+    int xt_len;
+    int mdf_iterations, mdf_min_iterations, mdf_coupled;
+    double mdf_omega, mdf_tol, mdf_omega_max;
+    double *lambda;
+    int *lambda_valid;
+    int dfc_cache_lambda;
+    double correction_scale;
+    const float *fpost_prev, *uring_prev;
+    int *box, *map, *band_nodes, *band_count;
+    int *list_cache;   /* iblbm_ibm32_list_cache_ints(...) ints */
+    const int *excl_cur;
+    int *excl_next;
+    int band_capacity, box_capacity;
+    float *band_fib, *band_df;
+    float *band_fib_part;
+    float *scratch;    /* >= iblbm_ibm_scratch_doubles(...) floats */
+    int *iscratch;
+    double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
+    int *stats;
+    double *dstats;
+} iblbm_ibm32_args;
+
+int iblbm_ibm_step_f32(const iblbm_ibm32_args *a, void *stream);
+int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int delta_type);
+int iblbm_ibm32_smem_bytes(int lb_total, int band_capacity, int delta_type);
+
 /* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
 /* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */
 int iblbm_feq(const double *ro, const double *U, int N, int incompressible, double *feq, void *stream);

@@ -32,6 +32,8 @@ def test_struct_layout_matches_c(tmp_path):
     probe = tmp_path / "probe.c"
     fields = {"iblbm_ibm_args": [f for f, _ in _lib.IbmArgs._fields_],
               "iblbm_dense_args": [f for f, _ in _lib.DenseArgs._fields_],
+              "iblbm_ibm32_args": [f for f, _ in _lib.Ibm32Args._fields_],
+              "iblbm_dense32_args": [f for f, _ in _lib.Dense32Args._fields_],
               "iblbm_case": [f for f, _ in _lib.Case._fields_]}
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
     for st, fl in fields.items():
@@ -45,6 +47,7 @@ def test_struct_layout_matches_c(tmp_path):
     subprocess.check_call(["gcc", str(probe), "-o", str(exe)])
     out = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().split("\n") if l)
     for st, cls in (("iblbm_ibm_args", _lib.IbmArgs), ("iblbm_dense_args", _lib.DenseArgs),
+                    ("iblbm_ibm32_args", _lib.Ibm32Args), ("iblbm_dense32_args", _lib.Dense32Args),
                     ("iblbm_case", _lib.Case)):
         assert int(out[st]) == ctypes.sizeof(cls), st
         for f, _ in cls._fields_:
@@ -57,4 +60,6 @@ def test_rejects_bad_arguments_without_a_gpu():
     L = _lib.lib()
     assert L.iblbm_dense_step_f64(None, None) == -1
     assert L.iblbm_ibm_step_f64(None, None) == -1
+    assert L.iblbm_dense_step_f32(None, None) == -1
+    assert L.iblbm_ibm_step_f32(None, None) == -1
     assert L.iblbm_feq(None, None, 10, 0, None, None) == -1

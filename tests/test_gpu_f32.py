@@ -1,0 +1,159 @@
+"""GPU: the shifted FP32 form against the FP64 plain form on the same inputs.
+
+The FP32 form stores populations as g = f - w in FP32 and keeps FP64 for the
+force sums, so it is not bit-exact; it is held to the accuracy the FP32 form
+promises for the quantities that leave the solver:
+  Cd within 0.1 % (relative), Cl within 0.1 % of Cd,
+  |rho_32 - rho_64| <= 1e-5 and |u_32 - u_64| <= 1e-4 U (L-infinity over the lattice),
+  interpolated marker velocities (the slip) within 1e-4 U.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CD_RTOL = 1e-3
+RHO_ATOL = 1e-5
+U_REL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _cfg(kw):
+    from iblbm_b200.config import SimConfig
+    kw = dict(kw)
+    kw["cylinder_center"] = tuple(kw["cylinder_center"])
+    if kw.get("particles_config"):
+        kw["particles_config"] = [dict(p, center=tuple(p["center"])) for p in kw["particles_config"]]
+    return SimConfig(**kw)
+
+
+def _pair(cfg):
+    from iblbm_b200 import run
+    from iblbm_b200.engine import Engine
+    r64 = run(cfg, verbose=False, engine=Engine(cfg, precision="f64"))
+    r32 = run(cfg, verbose=False, engine=Engine(cfg, precision="f32"))
+    assert r64["engine"].status() == 0 and r32["engine"].status() == 0
+    return r64, r32
+
+
+def _u_ref(cfg):
+    return float(cfg.lattice_u if cfg.motion_type == "oscillating" else cfg.inflow_u)
+
+
+def _check_fields(cfg, r64, r32):
+    s64, s32 = r64["state"], r32["state"]
+    U = _u_ref(cfg)
+    assert np.all(np.isfinite(s32.U))
+    np.testing.assert_allclose(s32.ro, s64.ro, rtol=0, atol=RHO_ATOL)
+    np.testing.assert_allclose(s32.U, s64.U, rtol=0, atol=U_REL * U)
+
+
+def _check_forces(r64, r32):
+    cd64, cd32 = np.asarray(r64["Cd_history"]), np.asarray(r32["Cd_history"])
+    cl64, cl32 = np.asarray(r64["Cl_history"]), np.asarray(r32["Cl_history"])
+    assert cd64.shape == cd32.shape and cd64.size > 0
+    scale = np.maximum(np.abs(cd64), 1e-12)
+    assert np.max(np.abs(cd32 - cd64) / scale) <= CD_RTOL
+    assert np.max(np.abs(cl32 - cl64) / scale) <= CD_RTOL
+
+
+def test_shifted_roundtrip(torch):
+    """f -> g = f - w (FP32 SoA) -> f: error of one FP32 rounding of the deviation."""
+    from iblbm_b200._lib import Geom, lib, ptr
+    L = lib()
+    nx, ny = 37, 11
+    pitch = 64
+    g = Geom(nx, ny, pitch, pitch * ny)
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    rng = np.random.default_rng(5)
+    f = w[None, :] * (1.0 + 0.05 * rng.standard_normal((nx * ny, 9)))
+    d = torch.as_tensor(f.reshape(-1), device="cuda")
+    soa = torch.zeros(9 * pitch * ny, dtype=torch.float32, device="cuda")
+    back = torch.empty_like(d)
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.iblbm_to_shifted_f32(ptr(d), g, ptr(soa), s) == 0
+    assert L.iblbm_from_shifted_f32(ptr(soa), g, ptr(back), s) == 0
+    fb = back.cpu().numpy().reshape(-1, 9)
+    dev = f - w[None, :]
+    assert np.max(np.abs(fb - f) / np.maximum(np.abs(dev), 1e-30)) <= 2 ** -24 * 1.01
+
+
+def test_rest_state_is_exact(torch):
+    """A fluid at rest with no body stays exactly at g = 0 in the shifted form
+    (every equilibrium deviation is 0), with no drift from the weights."""
+    from iblbm_b200.engine import Engine
+    kw = dict(Re=20, NN=41, xmax=2, ymax=1, cylinder_center=(1.0, 0.5), cylinder_D_ratio=0.25, lattice_u=0.05,
+              inflow_u=0.0, bc_type="settling_channel", delta_type="hat", ibm_method="DF",
+              collision_model="BGK", marker_spacing_factor=1.0, max_steps=50, use_convergence=False,
+              check_interval=50)
+    e = Engine(_cfg(kw), precision="f32")
+    e.advance(50, outputs_last=True)
+    torch.cuda.synchronize()
+    st = e.read_state()
+    assert np.all(st.U == 0.0)
+    assert np.all(st.ro == 1.0)
+
+
+from tests.golden.make_golden import RUN_CASES  # noqa: E402
+
+F32_CASES = ["c1_df_bgk_hat", "c2_mdf_trt_p4", "c2_mdf_cmmrt_p4", "c3_dfc_bgk_p4_osc", "vin_df_bgk_p4",
+             "dfc_trt_hat_fixed", "inc_df_bgk_hat"]
+
+
+@pytest.mark.parametrize("name", F32_CASES)
+def test_f32_matches_f64(torch, name):
+    cfg = _cfg(RUN_CASES[name])
+    r64, r32 = _pair(cfg)
+    _check_fields(cfg, r64, r32)
+    _check_forces(r64, r32)
+    e64, e32 = r64["engine"], r32["engine"]
+    if cfg.ibm_method in ("DF", "MDF"):
+        U = _u_ref(cfg)
+        for k in ("d_Lux", "d_Luy"):
+            a64 = getattr(e64, k)[: e64.Lb].cpu().numpy()
+            a32 = getattr(e32, k)[: e32.Lb].cpu().numpy()
+            np.testing.assert_allclose(a32, a64, rtol=0, atol=U_REL * U, err_msg=k)
+
+
+@pytest.mark.parametrize("collision", ["BGK", "TRT", "CM_MRT"])
+@pytest.mark.parametrize("method,delta", [("DF", "hat"), ("MDF", "peskin4pt"), ("DFC", "peskin4pt")])
+def test_f32_method_matrix(torch, collision, method, delta):
+    kw = dict(Re=40, NN=49, xmax=2, ymax=1, cylinder_center=(0.45, 0.5), cylinder_D_ratio=0.25, lattice_u=0.05,
+              inflow_u=0.05, bc_type="dirichlet_neumann", delta_type=delta, ibm_method=method,
+              collision_model=collision, trt_magic_param=0.1875, mdf_iterations=20, mdf_min_iterations=5,
+              mdf_tolerance=1e-6, marker_spacing_factor=1.0, max_steps=400, use_convergence=False,
+              check_interval=100)
+    cfg = _cfg(kw)
+    r64, r32 = _pair(cfg)
+    _check_fields(cfg, r64, r32)
+    _check_forces(r64, r32)
+
+
+def test_f32_sedimentation_trajectories(torch):
+    """Two settling discs: FP64 Newton-Euler on FP32-form forces; positions
+    within 1e-4 lattice units of the FP64 form after the golden run."""
+    name = "c5_sed2_mdf_cmmrt_p4"
+    cfg = _cfg(RUN_CASES[name])
+    r64, r32 = _pair(cfg)
+    for p, q in zip(r32["state"].particles, r64["state"].particles):
+        dxl = (np.asarray(p.pos) - np.asarray(q.pos)) / r64["state"].dx
+        assert np.max(np.abs(dxl)) <= 1e-4
+        np.testing.assert_allclose(p.vel, q.vel, rtol=0, atol=1e-4 * max(1e-3, float(np.max(np.abs(q.vel)))))
+
+
+def test_f32_config1_geometry_long(torch):
+    """Config-1 geometry (401 x 161, D = 20, DF + BGK + hat) for 3000 steps:
+    Cd/Cl of the FP32 form within 0.1 % of the FP64 form throughout."""
+    kw = dict(RUN_CASES["c1_df_bgk_hat"], max_steps=3000, check_interval=250)
+    cfg = _cfg(kw)
+    r64, r32 = _pair(cfg)
+    _check_fields(cfg, r64, r32)
+    _check_forces(r64, r32)
