@@ -187,8 +187,12 @@ def measure(eng, args, dist, ws):
     loop.  Returns a dict of the numbers (all ranks)."""
     import torch
     N = eng.N
-    # warm-up: graph chunks and eager steps
+    # warm-up: graph chunks and eager steps; tile choice of the FP32 pass
     eng.advance(max(args.warmup, 3), outputs_last=True)
+    torch.cuda.synchronize()
+    from iblbm_b200.autotune import tune_dense
+    tile_ms, tile = tune_dense(eng)
+    eng.advance(3, outputs_last=True)
     torch.cuda.synchronize()
     flush = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     sink = torch.zeros((), dtype=torch.float32, device="cuda")
@@ -271,7 +275,8 @@ def measure(eng, args, dist, ws):
             "achieved": bpl * (N - box_nodes) / (dense_avg / 1e3) / 1e9, "band_ms": ibm_ms, "full_ms": full_ms,
             "steady": steady, "e2e": N * Ke * ws / e2e_s / 1e6, "e2e_h2d": 4 * Lb * 8, "e2e_d2h": 16,
             "clocks": clk.summary(), "wall_s_timed": t_wall, "status": eng.status(), "mdf": eng.mdf_stats(),
-            "cd": cd, "cl": cl, "steps_done": eng.ttt - 1}
+            "cd": cd, "cl": cl, "steps_done": eng.ttt - 1,
+            "tile": list(tile) if tile else None, "tile_ms": {f"{k[0]}x{k[1]}": v for k, v in tile_ms.items()}}
 
 
 def run_b200(args):
@@ -297,7 +302,8 @@ def run_b200(args):
                 "hbm_gbs_bulk": m["achieved"], "bytes_per_lu": m["bytes_per_lu"], "band_kernel_ms": m["band_ms"],
                 "whole_lattice_kernel_ms_serial": m["full_ms"], "steady_state_mlups_graph_l2_warm": m["steady"],
                 "e2e_mlups": m["e2e"], "mdf_last_iterations": m["mdf"]["iter_count"], "status": m["status"],
-                "Cd": m["cd"], "Cl": m["cl"], "step": m["steps_done"]}
+                "Cd": m["cd"], "Cl": m["cl"], "step": m["steps_done"], "tile": m["tile"],
+                "tile_ms_whole_lattice": m["tile_ms"]}
 
     line = {"metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,

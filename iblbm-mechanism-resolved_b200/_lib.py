@@ -56,10 +56,14 @@ class IbmArgs(ctypes.Structure):
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp)]
 
 
-# The FP32 argument structs (iblbm_dense32_args, iblbm_ibm32_args) have the
-# same fields in the same order as the FP64 ones; only the pointee types differ.
-Dense32Args = DenseArgs
+# The FP32 band-step struct (iblbm_ibm32_args) has the same fields in the same
+# order as the FP64 one; only the pointee types differ.  The FP32 dense struct
+# adds the tile choice at the end.
 Ibm32Args = IbmArgs
+
+
+class Dense32Args(ctypes.Structure):
+    _fields_ = DenseArgs._fields_ + [("tile_nodes", _i), ("tile_rows", _i)]
 
 # entry point -> argtypes (all return int status)
 _SIGS = {
@@ -77,7 +81,7 @@ _SIGS = {
     "iblbm_collision_cm_mrt": [_vp, _vp, _vp, _i, ctypes.POINTER(_d), _d, _vp, _vp],
     "iblbm_streaming": [_vp, _vp, _i, _i, _vp, _vp],
     "iblbm_velocity_correction": [_vp, _vp, _vp, _i, _d, _i, _vp],
-    "iblbm_dense_step_f32": [ctypes.POINTER(DenseArgs), _vp],
+    "iblbm_dense_step_f32": [ctypes.POINTER(Dense32Args), _vp],
     "iblbm_ibm_step_f32": [ctypes.POINTER(IbmArgs), _vp],
     "iblbm_ibm32_list_cache_ints": [_i, _i, _i],
     "iblbm_ibm32_smem_bytes": [_i, _i, _i],

@@ -4,6 +4,7 @@
 // moments, velocity correction, equilibrium, collision, store) on deviations
 // g = f - w held in FP32: 72 bytes per lattice update.  Compiled with the
 // default multiply-add contraction.
+#include <cstdint>
 #include "shifted.cuh"
 
 namespace iblbm {
@@ -44,6 +45,79 @@ __global__ void __launch_bounds__(256) dense32_kernel(const iblbm_dense32_args a
     dense_node32<COLL, BC, INCOMP, IBM, OUT>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
 }
 
+// Four consecutive nodes per thread, one warp per 128-node row segment,
+// blockDim.y rows per CTA.  Each population plane is read with one aligned
+// 16-byte load per thread; the x-shifted pull sources come from the neighbouring
+// lane's load (warp shuffle) or, at the warp's two ends, from one scalar load.
+// Groups that touch the lattice boundary or the skipped box take the per-node
+// path (closures, exact skip test).
+__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
+__global__ void __launch_bounds__(256) dense32_vec4_kernel(const iblbm_dense32_args a, CollParams32 cp, BcParams32 bc)
+{
+    const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
+    const int lane = threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= g.ny) return;  // uniform over the warp
+    const int i0 = (blockIdx.x * 32 + lane) * 4;
+    int sx0 = 0, sy0 = 0, sx1 = -1, sy1 = -1;
+    if (a.skip_box) {
+        sx0 = __ldg(a.skip_box + 0);
+        sy0 = __ldg(a.skip_box + 1);
+        sx1 = sx0 + __ldg(a.skip_box + 2) - 1;
+        sy1 = sy0 + __ldg(a.skip_box + 3) - 1;
+    }
+    const bool row_skip = j >= sy0 && j <= sy1;
+    const bool interior_row = j >= 1 && j <= g.ny - 2;
+    const bool fast = interior_row && i0 >= 4 && i0 + 3 <= g.nx - 2 && !(row_skip && i0 <= sx1 && i0 + 3 >= sx0);
+    const BandView32 bv{a.band.box, a.band.map, a.band.fib, a.band.df};
+    const DenseOut32 o{a.fpost_next, a.uring_next, OUT ? a.ro_out : nullptr, OUT ? a.U_out : nullptr,
+                       OUT ? a.fstar_out : nullptr};
+    float v[9][4];
+    if (interior_row) {  // uniform over the warp: every lane takes part in the shuffles
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const float* p = a.fpost_prev + q * g.qstride + (long long)(j - ey_(q)) * g.pitch;
+            const float4 c = i0 < g.nx ? ld4(p + i0) : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ex_(q) == 0) {
+                v[q][0] = c.x; v[q][1] = c.y; v[q][2] = c.z; v[q][3] = c.w;
+            } else if (ex_(q) == 1) {  // source i - 1
+                float left = __shfl_up_sync(0xffffffffu, c.w, 1);
+                if (lane == 0) left = (i0 >= 1 && i0 <= g.nx) ? __ldg(p + i0 - 1) : 0.f;
+                v[q][0] = left; v[q][1] = c.x; v[q][2] = c.y; v[q][3] = c.z;
+            } else {  // source i + 1
+                float right = __shfl_down_sync(0xffffffffu, c.x, 1);
+                if (lane == 31) right = (i0 + 4 < g.nx) ? __ldg(p + i0 + 4) : 0.f;
+                v[q][0] = c.y; v[q][1] = c.z; v[q][2] = c.w; v[q][3] = right;
+            }
+        }
+    }
+    if (fast) {
+        float w[9][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float f[9], out[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q) f[q] = v[q][k];
+            node_core32<COLL, BC, INCOMP, IBM, OUT>(f, g, cp, bv, o, i0 + k, j, out);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) w[q][k] = out[q];
+        }
+        float* dst = a.fpost_next + (long long)j * g.pitch + i0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            *reinterpret_cast<float4*>(dst + q * g.qstride) = make_float4(w[q][0], w[q][1], w[q][2], w[q][3]);
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < 4; ++k) {
+            const int i = i0 + k;
+            if (i >= g.nx || (row_skip && i >= sx0 && i <= sx1)) continue;
+            dense_node32<COLL, BC, INCOMP, IBM, OUT>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+        }
+    }
+}
+
 template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
 __global__ void __launch_bounds__(128) dense32_box_kernel(const iblbm_dense32_args a, CollParams32 cp, BcParams32 bc)
 {
@@ -70,9 +144,16 @@ static cudaError_t launch32_ibm(const iblbm_dense32_args& a, const CollParams32&
         else dense32_box_kernel<COLL, BC, INCOMP, IBM, false><<<nblk, 128, 0, s>>>(a, cp, bc);
         return cudaGetLastError();
     }
-    dim3 block(256, 1), grid((a.g.nx + 255) / 256, a.g.ny);
-    if (out) dense32_kernel<COLL, BC, INCOMP, IBM, true><<<grid, block, 0, s>>>(a, cp, bc);
-    else dense32_kernel<COLL, BC, INCOMP, IBM, false><<<grid, block, 0, s>>>(a, cp, bc);
+    if (a.tile_nodes == 1) {
+        dim3 block(256, 1), grid((a.g.nx + 255) / 256, a.g.ny);
+        if (out) dense32_kernel<COLL, BC, INCOMP, IBM, true><<<grid, block, 0, s>>>(a, cp, bc);
+        else dense32_kernel<COLL, BC, INCOMP, IBM, false><<<grid, block, 0, s>>>(a, cp, bc);
+        return cudaGetLastError();
+    }
+    const int rows = a.tile_rows > 0 ? a.tile_rows : 4;
+    dim3 block(32, rows), grid((a.g.nx + 127) / 128, (a.g.ny + rows - 1) / rows);
+    if (out) dense32_vec4_kernel<COLL, BC, INCOMP, IBM, true><<<grid, block, 0, s>>>(a, cp, bc);
+    else dense32_vec4_kernel<COLL, BC, INCOMP, IBM, false><<<grid, block, 0, s>>>(a, cp, bc);
     return cudaGetLastError();
 }
 
@@ -139,6 +220,11 @@ extern "C" int iblbm_dense_step_f32(const iblbm_dense32_args* a, void* stream)
     if ((a->ibm == IBM_DF || a->ibm == IBM_MDF) && !a->band.fib) return IBLBM_E_ARG;
     if (a->ibm == IBM_DFC && !a->band.df) return IBLBM_E_ARG;
     if (a->skip_box && a->only_box) return IBLBM_E_ARG;
+    if (a->tile_nodes != 0 && a->tile_nodes != 1 && a->tile_nodes != 4) return IBLBM_E_ARG;
+    if (a->tile_rows < 0 || a->tile_rows > 8 || (a->tile_rows & (a->tile_rows - 1)) != 0) return IBLBM_E_ARG;
+    if ((reinterpret_cast<uintptr_t>(a->fpost_prev) & 15) || (reinterpret_cast<uintptr_t>(a->fpost_next) & 15) ||
+        (a->g.pitch & 3))
+        return IBLBM_E_ARG;
     CollParams32 cp;
     BcParams32 bc;
     make_params32(a->c, cp, bc);

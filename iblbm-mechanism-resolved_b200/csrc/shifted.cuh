@@ -347,13 +347,14 @@ __device__ __forceinline__ int band_lookup32(const BandView32& bv, int nx, int i
     return bv.map[(long long)j * nx + i];
 }
 
+// Everything after streaming and closure for node (i, j): band correction,
+// optional f* output, moments, velocity correction, collision, ro/U outputs and
+// the velocity ring.  f holds the post-streaming populations; out receives the
+// post-collision populations (stored by the caller).
 template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
-__device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
-                                             const CollParams32& cp, const BcParams32& bc, const BandView32& band,
-                                             const DenseOut32& o, int i, int j)
+__device__ __forceinline__ void node_core32(float* f, const Geom& g, const CollParams32& cp,
+                                            const BandView32& band, const DenseOut32& o, int i, int j, float* out)
 {
-    float f[9];
-    gstar_node<BC>(fp, ur, g, bc, INCOMP, i, j, f);
     int b = -1;
     if (IBM != IBM_NONE) b = band_lookup32(band, g.nx, i, j);
     if (IBM == IBM_DFC && b >= 0) {
@@ -367,7 +368,6 @@ __device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const
     }
     float drho, rho, u0, u1;
     macro_g(f, INCOMP, drho, rho, u0, u1);
-    float out[9];
     if ((IBM == IBM_DF || IBM == IBM_MDF) && b >= 0) {
         const float F0 = band.fib[2 * (long long)b], F1 = band.fib[2 * (long long)b + 1];
         if (INCOMP) { u0 += 0.5f * F0 * cp.dt; u1 += 0.5f * F1 * cp.dt; }
@@ -386,6 +386,17 @@ __device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const
         o.uring_next[2 * n] = u0;
         o.uring_next[2 * n + 1] = u1;
     }
+}
+
+template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
+__device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
+                                             const CollParams32& cp, const BcParams32& bc, const BandView32& band,
+                                             const DenseOut32& o, int i, int j)
+{
+    float f[9], out[9];
+    gstar_node<BC>(fp, ur, g, bc, INCOMP, i, j, f);
+    node_core32<COLL, BC, INCOMP, IBM, OUT>(f, g, cp, band, o, i, j, out);
+    const long long site = (long long)j * g.pitch + i;
 #pragma unroll
     for (int q = 0; q < 9; ++q) o.fpost_next[q * g.qstride + site] = out[q];
 }

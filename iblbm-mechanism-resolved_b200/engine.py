@@ -24,8 +24,8 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView, Case, DenseArgs, Geom,
-                   IbmArgs, check, lib, ptr)
+from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView, Case, Dense32Args, DenseArgs,
+                   Geom, IbmArgs, check, lib, ptr)
 from .physics import (history_increment, mdf_relaxation_factor, net_gravity, oscillation_table,
                       rigid_markers)
 from .state import initial_velocity, initialize
@@ -168,17 +168,14 @@ class Engine:
             if cfg.motion_type == "sedimentation" and cfg.enable_rotation:
                 self.omega = min(float(self.omega), MOVING_ROTATION_OMEGA_MAX)
         self.ibm_args = [self._make_ibm_args(p) for p in (0, 1)]
-        # dense pass variants per parity and output flag: whole lattice, bulk
-        # (skips the exclusion box), box (only the exclusion box)
-        self.dense_full = [[self._make_dense_args(p, out, "full") for out in (False, True)] for p in (0, 1)]
-        self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
-        self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
+        self.tile = (4, 4)  # FP32 pass: nodes per thread, rows per CTA
+        self.graphs = {}
+        self._make_dense_variants()
         self.side = torch.cuda.Stream(self.dev, priority=-1)
         self.ev_bulk = torch.cuda.Event()
         self.ev_side = torch.cuda.Event()
         self.overlap = True
         self.rebuild_next = True
-        self.graphs = {}
         self.last_out_step = 0
 
     def _band_capacity(self, S):
@@ -260,8 +257,26 @@ class Engine:
         a.stats, a.dstats = ptr(self.d_stats), ptr(self.d_dstats)
         return a
 
+    def _make_dense_variants(self):
+        """Dense pass variants per parity and output flag: whole lattice, bulk
+        (skips the exclusion box), box (only the exclusion box)."""
+        self.dense_full = [[self._make_dense_args(p, out, "full") for out in (False, True)] for p in (0, 1)]
+        self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
+        self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
+
+    def set_tile(self, nodes, rows):
+        """Tile of the FP32 whole-lattice/bulk pass (nodes per thread 1 or 4,
+        rows per CTA 1/2/4/8).  Drops captured graphs."""
+        if nodes not in (1, 4) or rows not in (1, 2, 4, 8):
+            raise ValueError(f"tile ({nodes}, {rows})")
+        self.tile = (nodes, rows)
+        self._make_dense_variants()
+        self.graphs = {}
+
     def _make_dense_args(self, parity, outputs, mode):
-        a = DenseArgs()
+        a = Dense32Args() if self.f32 else DenseArgs()
+        if self.f32:
+            a.tile_nodes, a.tile_rows = self.tile
         a.g, a.c = self.geom, self.case
         a.ibm = 0 if mode == "bulk" else IBM_IDS[self.method]
         a.fpost_prev, a.fpost_next = ptr(self.f[parity]), ptr(self.f[1 - parity])

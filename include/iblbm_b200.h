@@ -201,6 +201,11 @@ typedef struct {
     const int *skip_box;
     const int *only_box;
     int box_blocks;
+    /* tile of the whole-lattice/bulk pass: nodes per thread (4: one 16-byte
+     * load per population plane; 1: one node per thread; 0: 4) and rows per CTA
+     * (1, 2, 4 or 8; 0: 4).  Population buffers must be 16-byte aligned and the
+     * pitch a multiple of 4. */
+    int tile_nodes, tile_rows;
 } iblbm_dense32_args;
 
 /* Fused timestep on the shifted FP32 form (see iblbm_dense_step_f64). */
