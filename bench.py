@@ -276,7 +276,7 @@ def measure(eng, args, dist, ws):
             "steady": steady, "e2e": N * Ke * ws / e2e_s / 1e6, "e2e_h2d": 4 * Lb * 8, "e2e_d2h": 16,
             "clocks": clk.summary(), "wall_s_timed": t_wall, "status": eng.status(), "mdf": eng.mdf_stats(),
             "cd": cd, "cl": cl, "steps_done": eng.ttt - 1,
-            "tile": list(tile) if tile else None, "tile_ms": {f"{k[0]}x{k[1]}": v for k, v in tile_ms.items()}}
+            "tile": tile, "tile_ms": tile_ms}
 
 
 def run_b200(args):

@@ -63,7 +63,10 @@ Ibm32Args = IbmArgs
 
 
 class Dense32Args(ctypes.Structure):
-    _fields_ = DenseArgs._fields_ + [("tile_nodes", _i), ("tile_rows", _i)]
+    _fields_ = DenseArgs._fields_ + [("tile", _i), ("status", _vp)]
+
+
+TILES = {"pipe4x2": 0, "node": 1, "pipe8x2": 2, "rows2": 3, "rows4": 4}
 
 # entry point -> argtypes (all return int status)
 _SIGS = {

@@ -6,6 +6,7 @@
 // default multiply-add contraction.
 #include <cstdint>
 #include "shifted.cuh"
+#include "tma.cuh"
 
 namespace iblbm {
 
@@ -45,22 +46,17 @@ __global__ void __launch_bounds__(256) dense32_kernel(const iblbm_dense32_args a
     dense_node32<COLL, BC, INCOMP, IBM, OUT>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
 }
 
-// Four consecutive nodes per thread, one warp per 128-node row segment,
-// blockDim.y rows per CTA.  Each population plane is read with one aligned
-// 16-byte load per thread; the x-shifted pull sources come from the neighbouring
-// lane's load (warp shuffle) or, at the warp's two ends, from one scalar load.
-// Groups that touch the lattice boundary or the skipped box take the per-node
-// path (closures, exact skip test).
-__device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-
-template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
-__global__ void __launch_bounds__(256) dense32_vec4_kernel(const iblbm_dense32_args a, CollParams32 cp, BcParams32 bc)
+// NR nodes per thread, stacked in y: the 9 * NR pull loads of all of them are
+// issued before the first collision, so each thread keeps NR times the bytes in
+// flight of the one-node form (the pass is bound by outstanding loads, not by
+// arithmetic).  128 threads per CTA along x, NR rows per CTA.
+template <int COLL, int BC, bool INCOMP, int IBM, int NR>
+__global__ void __launch_bounds__(128) dense32_rows_kernel(const iblbm_dense32_args a, CollParams32 cp, BcParams32 bc)
 {
     const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
-    const int lane = threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (j >= g.ny) return;  // uniform over the warp
-    const int i0 = (blockIdx.x * 32 + lane) * 4;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j0 = blockIdx.y * NR;
+    if (i >= g.nx) return;
     int sx0 = 0, sy0 = 0, sx1 = -1, sy1 = -1;
     if (a.skip_box) {
         sx0 = __ldg(a.skip_box + 0);
@@ -68,54 +64,189 @@ __global__ void __launch_bounds__(256) dense32_vec4_kernel(const iblbm_dense32_a
         sx1 = sx0 + __ldg(a.skip_box + 2) - 1;
         sy1 = sy0 + __ldg(a.skip_box + 3) - 1;
     }
-    const bool row_skip = j >= sy0 && j <= sy1;
-    const bool interior_row = j >= 1 && j <= g.ny - 2;
-    const bool fast = interior_row && i0 >= 4 && i0 + 3 <= g.nx - 2 && !(row_skip && i0 <= sx1 && i0 + 3 >= sx0);
-    const BandView32 bv{a.band.box, a.band.map, a.band.fib, a.band.df};
-    const DenseOut32 o{a.fpost_next, a.uring_next, OUT ? a.ro_out : nullptr, OUT ? a.U_out : nullptr,
-                       OUT ? a.fstar_out : nullptr};
-    float v[9][4];
-    if (interior_row) {  // uniform over the warp: every lane takes part in the shuffles
+    const bool col_skip = i >= sx0 && i <= sx1;
+    float f[NR][9];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) {
-            const float* p = a.fpost_prev + q * g.qstride + (long long)(j - ey_(q)) * g.pitch;
-            const float4 c = i0 < g.nx ? ld4(p + i0) : make_float4(0.f, 0.f, 0.f, 0.f);
-            if (ex_(q) == 0) {
-                v[q][0] = c.x; v[q][1] = c.y; v[q][2] = c.z; v[q][3] = c.w;
-            } else if (ex_(q) == 1) {  // source i - 1
-                float left = __shfl_up_sync(0xffffffffu, c.w, 1);
-                if (lane == 0) left = (i0 >= 1 && i0 <= g.nx) ? __ldg(p + i0 - 1) : 0.f;
-                v[q][0] = left; v[q][1] = c.x; v[q][2] = c.y; v[q][3] = c.z;
-            } else {  // source i + 1
-                float right = __shfl_down_sync(0xffffffffu, c.x, 1);
-                if (lane == 31) right = (i0 + 4 < g.nx) ? __ldg(p + i0 + 4) : 0.f;
-                v[q][0] = c.y; v[q][1] = c.z; v[q][2] = c.w; v[q][3] = right;
+    for (int n = 0; n < NR; ++n)
+        if (j0 + n < g.ny) pull(a.fpost_prev, g, i, j0 + n, f[n]);
+    const BandView32 bv{a.band.box, a.band.map, a.band.fib, a.band.df};
+    const DenseOut32 o{a.fpost_next, a.uring_next, nullptr, nullptr, nullptr};
+#pragma unroll
+    for (int n = 0; n < NR; ++n) {
+        const int j = j0 + n;
+        if (j >= g.ny || (col_skip && j >= sy0 && j <= sy1)) continue;
+        closure_node<BC>(a.fpost_prev, a.uring_prev, g, bc, INCOMP, i, j, f[n]);
+        float out[9];
+        node_core32<COLL, has_ring<BC>(), INCOMP, IBM, false>(f[n], g, cp, bv, o, i, j, out);
+        float* dst = a.fpost_next + (long long)j * g.pitch + i;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dst[q * g.qstride] = out[q];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined pass: persistent CTAs, one producer warp staging each tile's
+// population rows into shared memory with bulk copies (cp.async.bulk, completing
+// on an mbarrier), ROWS consumer warps computing from shared memory and storing
+// straight to global memory.  A tile is ROWS lattice rows x PIPE_W columns; the
+// stage buffer holds, for every population plane q, the rows y0 + r - ey(q)
+// (r < ROWS) over columns x0 - 4 .. x0 + PIPE_W + 3, so every pull source of
+// the tile's interior nodes is on chip.  STAGES buffers rotate: while the
+// consumers work on one tile the copies of the next STAGES - 1 are in flight.
+// Edge nodes of the lattice take the per-node path (closures read global
+// memory); nodes in the skip box are left to the box pass.
+// ---------------------------------------------------------------------------
+constexpr int PIPE_W = 128;
+constexpr int PIPE_SW = PIPE_W + 8;
+constexpr long long PIPE_WAIT_LIMIT = 1LL << 24;
+constexpr int PIPE_TIMEOUT = 1;  // status code: a pipeline wait ran out
+
+template <int ROWS, int STAGES>
+constexpr size_t pipe_smem_bytes() { return sizeof(float) * (size_t)STAGES * 9 * ROWS * PIPE_SW; }
+
+template <int COLL, bool INCOMP, int IBM>
+__device__ __forceinline__ void node_generic32(const iblbm_dense32_args& a, const Geom& g, const CollParams32& cp,
+                                               const BcParams32& bc, const BandView32& bv, const DenseOut32& o,
+                                               int i, int j)
+{
+    switch (a.c.bc) {
+    case BC_DIRICHLET_NEUMANN:
+        dense_node32<COLL, BC_DIRICHLET_NEUMANN, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+        break;
+    case BC_OPEN:
+        dense_node32<COLL, BC_OPEN, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+        break;
+    case BC_SETTLING:
+        dense_node32<COLL, BC_SETTLING, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+        break;
+    default:
+        dense_node32<COLL, BC_VELOCITY_INLET, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i,
+                                                                   j);
+        break;
+    }
+}
+
+template <int COLL, bool RING, bool INCOMP, int IBM, int ROWS, int STAGES, int MINB>
+__global__ void __launch_bounds__(32 * (ROWS + 1), MINB) dense32_pipe_kernel(const iblbm_dense32_args a, CollParams32 cp,
+                                                                     BcParams32 bc)
+{
+    extern __shared__ __align__(128) float psm[];
+    __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+    const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ntx = (g.nx + PIPE_W - 1) / PIPE_W, nty = (g.ny + ROWS - 1) / ROWS;
+    const int ntiles = ntx * nty;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], ROWS);
+        }
+    }
+    __syncthreads();
+    int sx0 = 0, sy0 = 0, sx1 = -1, sy1 = -1;
+    if (a.skip_box) {
+        sx0 = __ldg(a.skip_box + 0);
+        sy0 = __ldg(a.skip_box + 1);
+        sx1 = sx0 + __ldg(a.skip_box + 2) - 1;
+        sy1 = sy0 + __ldg(a.skip_box + 3) - 1;
+    }
+    constexpr int STAGE_F = 9 * ROWS * PIPE_SW;
+    if (warp == ROWS) {
+        // producer
+        int k = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+            const int s = k % STAGES;
+            if (k >= STAGES && !mbar_wait_bounded(&empty[s], ((k / STAGES) & 1) ^ 1, PIPE_WAIT_LIMIT)) {
+                if (lane == 0 && a.status) atomicExch(a.status, PIPE_TIMEOUT);
+                break;
+            }
+            const int x0 = (t % ntx) * PIPE_W, y0 = (t / ntx) * ROWS;
+            const int c0 = max(x0 - 4, 0), c1 = min(x0 + PIPE_W + 4, g.pitch);
+            const uint32_t row_bytes = (uint32_t)(c1 - c0) * 4u;
+            if (lane == 0) {
+                uint32_t total = 0;
+                for (int c = 0; c < 9 * ROWS; ++c) {
+                    const int row = y0 + c % ROWS - ey_(c / ROWS);
+                    if (row >= 0 && row < g.ny) total += row_bytes;
+                }
+                mbar_expect(&full[s], total);
+            }
+            __syncwarp();
+            float* st = psm + (size_t)s * STAGE_F;
+            for (int c = lane; c < 9 * ROWS; c += 32) {
+                const int q = c / ROWS, r = c % ROWS;
+                const int row = y0 + r - ey_(q);
+                if (row < 0 || row >= g.ny) continue;
+                bulk_copy(st + (q * ROWS + r) * PIPE_SW + (c0 - (x0 - 4)),
+                          a.fpost_prev + q * g.qstride + (long long)row * g.pitch + c0, row_bytes, &full[s]);
             }
         }
+        return;
     }
-    if (fast) {
-        float w[9][4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            float f[9], out[9];
-#pragma unroll
-            for (int q = 0; q < 9; ++q) f[q] = v[q][k];
-            node_core32<COLL, BC, INCOMP, IBM, OUT>(f, g, cp, bv, o, i0 + k, j, out);
-#pragma unroll
-            for (int q = 0; q < 9; ++q) w[q][k] = out[q];
+    // consumers: warp r computes row y0 + r of each tile
+    const BandView32 bv{a.band.box, a.band.map, a.band.fib, a.band.df};
+    const DenseOut32 o{a.fpost_next, a.uring_next, nullptr, nullptr, nullptr};
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        const int s = k % STAGES;
+        if (!mbar_wait_bounded(&full[s], (k / STAGES) & 1, PIPE_WAIT_LIMIT)) {
+            if (lane == 0 && a.status) atomicExch(a.status, PIPE_TIMEOUT);
+            break;
         }
-        float* dst = a.fpost_next + (long long)j * g.pitch + i0;
-#pragma unroll
-        for (int q = 0; q < 9; ++q)
-            *reinterpret_cast<float4*>(dst + q * g.qstride) = make_float4(w[q][0], w[q][1], w[q][2], w[q][3]);
-    } else {
+        const int x0 = (t % ntx) * PIPE_W, y0 = (t / ntx) * ROWS;
+        const int j = y0 + warp;
+        const float* st = psm + (size_t)s * STAGE_F + warp * PIPE_SW;
+        if (j < g.ny) {
+            const bool row_in = j >= 1 && j <= g.ny - 2;
+            const bool row_skip = j >= sy0 && j <= sy1;
 #pragma unroll 1
-        for (int k = 0; k < 4; ++k) {
-            const int i = i0 + k;
-            if (i >= g.nx || (row_skip && i >= sx0 && i <= sx1)) continue;
-            dense_node32<COLL, BC, INCOMP, IBM, OUT>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+            for (int ii = 0; ii < PIPE_W / 32; ++ii) {
+                const int i = x0 + ii * 32 + lane;
+                if (i >= g.nx || (row_skip && i >= sx0 && i <= sx1)) continue;
+                if (row_in && i >= 1 && i <= g.nx - 2) {
+                    float f[9], out[9];
+                    const int c = i - x0 + 4;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) f[q] = st[q * ROWS * PIPE_SW + c - ex_(q)];
+                    node_core32<COLL, RING, INCOMP, IBM, false>(f, g, cp, bv, o, i, j, out);
+                    float* dst = a.fpost_next + (long long)j * g.pitch + i;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) dst[q * g.qstride] = out[q];
+                } else {
+                    node_generic32<COLL, INCOMP, IBM>(a, g, cp, bc, bv, o, i, j);
+                }
+            }
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
     }
+}
+
+// Persistent grid of one pipelined instantiation: resident CTAs per SM x SMs,
+// at most one CTA per tile.  The first launch of each sets its shared-memory
+// limit and reads the occupancy (for the device current at that call).
+template <int COLL, bool RING, bool INCOMP, int IBM, int ROWS, int STAGES, int MINB>
+static cudaError_t launch_pipe(const iblbm_dense32_args& a, const CollParams32& cp, const BcParams32& bc, cudaStream_t s)
+{
+    auto K = dense32_pipe_kernel<COLL, RING, INCOMP, IBM, ROWS, STAGES, MINB>;
+    constexpr size_t smem = pipe_smem_bytes<ROWS, STAGES>();
+    constexpr int threads = 32 * (ROWS + 1);
+    static int per_sm = 0, sms = 0;
+    if (per_sm == 0) {
+        cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0, n = 0, occ = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, K, threads, smem)) != cudaSuccess) return e;
+        if (occ < 1) return cudaErrorInvalidConfiguration;
+        sms = n;
+        per_sm = occ;
+    }
+    const int ntiles = ((a.g.nx + PIPE_W - 1) / PIPE_W) * ((a.g.ny + ROWS - 1) / ROWS);
+    const int grid = min(ntiles, per_sm * sms);
+    K<<<grid, threads, smem, s>>>(a, cp, bc);
+    return cudaGetLastError();
 }
 
 template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
@@ -144,17 +275,24 @@ static cudaError_t launch32_ibm(const iblbm_dense32_args& a, const CollParams32&
         else dense32_box_kernel<COLL, BC, INCOMP, IBM, false><<<nblk, 128, 0, s>>>(a, cp, bc);
         return cudaGetLastError();
     }
-    if (a.tile_nodes == 1) {
+    if (out || a.tile == IBLBM_TILE_NODE) {
         dim3 block(256, 1), grid((a.g.nx + 255) / 256, a.g.ny);
         if (out) dense32_kernel<COLL, BC, INCOMP, IBM, true><<<grid, block, 0, s>>>(a, cp, bc);
         else dense32_kernel<COLL, BC, INCOMP, IBM, false><<<grid, block, 0, s>>>(a, cp, bc);
         return cudaGetLastError();
     }
-    const int rows = a.tile_rows > 0 ? a.tile_rows : 4;
-    dim3 block(32, rows), grid((a.g.nx + 127) / 128, (a.g.ny + rows - 1) / rows);
-    if (out) dense32_vec4_kernel<COLL, BC, INCOMP, IBM, true><<<grid, block, 0, s>>>(a, cp, bc);
-    else dense32_vec4_kernel<COLL, BC, INCOMP, IBM, false><<<grid, block, 0, s>>>(a, cp, bc);
-    return cudaGetLastError();
+    // the pipelined pass dispatches the closures at run time: its instantiations
+    // depend on the boundary only through the velocity ring
+    constexpr bool RING = has_ring<BC>();
+    if (a.tile == IBLBM_TILE_ROWS2 || a.tile == IBLBM_TILE_ROWS4) {
+        const int nr = a.tile == IBLBM_TILE_ROWS2 ? 2 : 4;
+        dim3 grid((a.g.nx + 127) / 128, (a.g.ny + nr - 1) / nr);
+        if (nr == 2) dense32_rows_kernel<COLL, BC, INCOMP, IBM, 2><<<grid, 128, 0, s>>>(a, cp, bc);
+        else dense32_rows_kernel<COLL, BC, INCOMP, IBM, 4><<<grid, 128, 0, s>>>(a, cp, bc);
+        return cudaGetLastError();
+    }
+    if (a.tile == IBLBM_TILE_PIPE_8x2) return launch_pipe<COLL, RING, INCOMP, IBM, 8, 2, 2>(a, cp, bc, s);
+    return launch_pipe<COLL, RING, INCOMP, IBM, 4, 2, 5>(a, cp, bc, s);
 }
 
 template <int COLL, int BC, bool INCOMP>
@@ -220,8 +358,7 @@ extern "C" int iblbm_dense_step_f32(const iblbm_dense32_args* a, void* stream)
     if ((a->ibm == IBM_DF || a->ibm == IBM_MDF) && !a->band.fib) return IBLBM_E_ARG;
     if (a->ibm == IBM_DFC && !a->band.df) return IBLBM_E_ARG;
     if (a->skip_box && a->only_box) return IBLBM_E_ARG;
-    if (a->tile_nodes != 0 && a->tile_nodes != 1 && a->tile_nodes != 4) return IBLBM_E_ARG;
-    if (a->tile_rows < 0 || a->tile_rows > 8 || (a->tile_rows & (a->tile_rows - 1)) != 0) return IBLBM_E_ARG;
+    if (a->tile < IBLBM_TILE_PIPE_4x2 || a->tile > IBLBM_TILE_ROWS4) return IBLBM_E_ARG;
     if ((reinterpret_cast<uintptr_t>(a->fpost_prev) & 15) || (reinterpret_cast<uintptr_t>(a->fpost_next) & 15) ||
         (a->g.pitch & 3))
         return IBLBM_E_ARG;

@@ -219,6 +219,21 @@ __device__ __forceinline__ void gstar_node(const float* __restrict__ fp, const f
     else if (BC == BC_VELOCITY_INLET) bc32_velocity_inlet(ur, g, bc, i, j, f);
 }
 
+// Closure of a node whose pulled populations are already in f (the Dirichlet /
+// Neumann edge recomputes them from its neighbour column instead).
+template <int BC>
+__device__ __forceinline__ void closure_node(const float* __restrict__ fp, const float* __restrict__ ur,
+                                             const Geom& g, const BcParams32& bc, bool incomp, int i, int j,
+                                             float* f)
+{
+    const bool boundary = (i == 0) | (j == 0) | (i == g.nx - 1) | (j == g.ny - 1);
+    if (!boundary) return;
+    if (BC == BC_DIRICHLET_NEUMANN) bc32_dirichlet_neumann(fp, g, bc, i, j, f);
+    else if (BC == BC_OPEN) bc32_open(ur, g, bc, i, j, f);
+    else if (BC == BC_SETTLING) bc32_settling(g, bc, incomp, i, j, f);
+    else bc32_velocity_inlet(ur, g, bc, i, j, f);
+}
+
 // ---- collisions on g ----------------------------------------------------------
 __device__ __forceinline__ float guo_bare(int q, float u0, float u1, float F0, float F1)
 {
@@ -351,7 +366,7 @@ __device__ __forceinline__ int band_lookup32(const BandView32& bv, int nx, int i
 // optional f* output, moments, velocity correction, collision, ro/U outputs and
 // the velocity ring.  f holds the post-streaming populations; out receives the
 // post-collision populations (stored by the caller).
-template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
+template <int COLL, bool RING, bool INCOMP, int IBM, bool OUT>
 __device__ __forceinline__ void node_core32(float* f, const Geom& g, const CollParams32& cp,
                                             const BandView32& band, const DenseOut32& o, int i, int j, float* out)
 {
@@ -381,12 +396,16 @@ __device__ __forceinline__ void node_core32(float* f, const Geom& g, const CollP
         if (o.ro_out) o.ro_out[n] = rho;
         if (o.U_out) { o.U_out[2 * n] = u0; o.U_out[2 * n + 1] = u1; }
     }
-    if ((BC == BC_OPEN || BC == BC_VELOCITY_INLET) && is_ring(g, i, j)) {
+    if (RING && is_ring(g, i, j)) {
         const long long n = (long long)j * g.nx + i;
         o.uring_next[2 * n] = u0;
         o.uring_next[2 * n + 1] = u1;
     }
 }
+
+// closures that extrapolate from the previous step's velocity ring
+template <int BC>
+__host__ __device__ constexpr bool has_ring() { return BC == BC_OPEN || BC == BC_VELOCITY_INLET; }
 
 template <int COLL, int BC, bool INCOMP, int IBM, bool OUT>
 __device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
@@ -395,7 +414,7 @@ __device__ __forceinline__ void dense_node32(const float* __restrict__ fp, const
 {
     float f[9], out[9];
     gstar_node<BC>(fp, ur, g, bc, INCOMP, i, j, f);
-    node_core32<COLL, BC, INCOMP, IBM, OUT>(f, g, cp, band, o, i, j, out);
+    node_core32<COLL, has_ring<BC>(), INCOMP, IBM, OUT>(f, g, cp, band, o, i, j, out);
     const long long site = (long long)j * g.pitch + i;
 #pragma unroll
     for (int q = 0; q < 9; ++q) o.fpost_next[q * g.qstride + site] = out[q];

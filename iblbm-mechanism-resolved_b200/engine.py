@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView, Case, Dense32Args, DenseArgs,
-                   Geom, IbmArgs, check, lib, ptr)
+                   Geom, IbmArgs, TILES, check, lib, ptr)
 from .physics import (history_increment, mdf_relaxation_factor, net_gravity, oscillation_table,
                       rigid_markers)
 from .state import initial_velocity, initialize
@@ -168,7 +168,8 @@ class Engine:
             if cfg.motion_type == "sedimentation" and cfg.enable_rotation:
                 self.omega = min(float(self.omega), MOVING_ROTATION_OMEGA_MAX)
         self.ibm_args = [self._make_ibm_args(p) for p in (0, 1)]
-        self.tile = (4, 4)  # FP32 pass: nodes per thread, rows per CTA
+        self.tile = "rows2"  # FP32 pass tile shape (iblbm_b200._lib.TILES)
+        self.d_pipe_status = torch.zeros(1, dtype=i32, device=dev)
         self.graphs = {}
         self._make_dense_variants()
         self.side = torch.cuda.Stream(self.dev, priority=-1)
@@ -264,19 +265,20 @@ class Engine:
         self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
         self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
 
-    def set_tile(self, nodes, rows):
-        """Tile of the FP32 whole-lattice/bulk pass (nodes per thread 1 or 4,
-        rows per CTA 1/2/4/8).  Drops captured graphs."""
-        if nodes not in (1, 4) or rows not in (1, 2, 4, 8):
-            raise ValueError(f"tile ({nodes}, {rows})")
-        self.tile = (nodes, rows)
+    def set_tile(self, tile):
+        """Tile shape of the FP32 whole-lattice/bulk pass (a key of
+        iblbm_b200._lib.TILES).  Drops captured graphs."""
+        if tile not in TILES:
+            raise ValueError(f"tile {tile!r} (one of {sorted(TILES)})")
+        self.tile = tile
         self._make_dense_variants()
         self.graphs = {}
 
     def _make_dense_args(self, parity, outputs, mode):
         a = Dense32Args() if self.f32 else DenseArgs()
         if self.f32:
-            a.tile_nodes, a.tile_rows = self.tile
+            a.tile = TILES[self.tile]
+            a.status = ptr(self.d_pipe_status)
         a.g, a.c = self.geom, self.case
         a.ibm = 0 if mode == "bulk" else IBM_IDS[self.method]
         a.fpost_prev, a.fpost_next = ptr(self.f[parity]), ptr(self.f[1 - parity])
@@ -503,8 +505,15 @@ class Engine:
                 "guard_trips": int(s[3]), "last_residual": float(d[0]), "omega_used": float(d[1])}
 
     def status(self):
+        """Band-kernel status word (0 = ok); a pipeline timeout of the FP32 pass
+        reads as 100 + its code."""
         self.join()
-        return int(self.d_stats[4].item())
+        st = int(self.d_stats[4].item())
+        if st == 0 and self.f32:
+            p = int(self.d_pipe_status.item())
+            if p:
+                return 100 + p
+        return st
 
     def read_state(self):
         """Copy the last output step's fields into host arrays on self.st (AoS, the

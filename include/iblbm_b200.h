@@ -201,12 +201,21 @@ typedef struct {
     const int *skip_box;
     const int *only_box;
     int box_blocks;
-    /* tile of the whole-lattice/bulk pass: nodes per thread (4: one 16-byte
-     * load per population plane; 1: one node per thread; 0: 4) and rows per CTA
-     * (1, 2, 4 or 8; 0: 4).  Population buffers must be 16-byte aligned and the
-     * pitch a multiple of 4. */
-    int tile_nodes, tile_rows;
+    int tile;      /* IBLBM_TILE_*: shape of the whole-lattice / bulk pass */
+    int *status;   /* optional device int: set to 1 if a pipeline wait ran out */
 } iblbm_dense32_args;
+
+/* Tile shapes of the FP32 pass.  PIPE_RxS: persistent CTAs of R consumer warps
+ * (R lattice rows x 128 columns per tile) and one producer warp staging S tiles
+ * ahead in shared memory with bulk copies; NODE: one thread per node; ROWSn:
+ * one thread per n nodes stacked in y, all their loads issued first.  Population
+ * buffers must be 16-byte aligned (pitch a multiple of 32 as everywhere).
+ * Output steps (ro/U/fstar requested) use NODE. */
+#define IBLBM_TILE_PIPE_4x2 0
+#define IBLBM_TILE_NODE 1
+#define IBLBM_TILE_PIPE_8x2 2
+#define IBLBM_TILE_ROWS2 3
+#define IBLBM_TILE_ROWS4 4
 
 /* Fused timestep on the shifted FP32 form (see iblbm_dense_step_f64). */
 int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
