@@ -86,6 +86,8 @@ _SIGS = {
     "iblbm_velocity_correction": [_vp, _vp, _vp, _i, _d, _i, _vp],
     "iblbm_dense_step_f32": [ctypes.POINTER(Dense32Args), _vp],
     "iblbm_ibm_step_f32": [ctypes.POINTER(IbmArgs), _vp],
+    "iblbm_ibm_step_f32_batch": [ctypes.POINTER(IbmArgs), _vp, _i, _vp],
+    "iblbm_dense_step_f32_batch": [ctypes.POINTER(Dense32Args), _i, _vp],
     "iblbm_ibm32_list_cache_ints": [_i, _i, _i],
     "iblbm_ibm32_smem_bytes": [_i, _i, _i],
     "iblbm_to_shifted_f32": [_vp, Geom, _vp, _vp],

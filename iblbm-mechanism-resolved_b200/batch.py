@@ -1,0 +1,224 @@
+"""Many independent cases advancing together on one GPU (shifted FP32 form).
+
+A parameter sweep (Reynolds number x band method x delta kernel x collision
+model, lattices of uneven size) is a set of independent cases.  Run one at a
+time, each timestep of a small case is two short launches whose fixed costs
+dominate, and the band kernel (one CTA, latency-bound) leaves most of the GPU
+idle.  ``Batch`` advances all cases in lockstep with, per timestep:
+
+* one launch of the batched band kernel (``iblbm_ibm_step_f32_batch``): one CTA
+  per case, every case's DF / MDF / DFC on the GPU at once;
+* per kind of case (collision, closure, compressibility, band method) one
+  launch of the batched collide-stream pass (``iblbm_dense_step_f32_batch``)
+  over the lattices of all cases of that kind.
+
+From the second step on the schedule is the single-case overlapped one: the
+band kernels and the box passes run on a high-priority side stream while the
+bulk passes of all cases stream the lattices; steps between outputs are
+captured once into a CUDA graph and replayed.  Each case keeps its own
+``Engine`` (device buffers, host-side state, diagnostics); the batch only
+drives their kernels together.  Output steps (rho, u, Cd, Cl) run through each
+case's own engine.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._lib import IBM_IDS, TILES, Dense32Args, IbmArgs, check
+from .engine import Engine
+
+MAX_KIND = 72  # cases per batched collide-stream launch (iblbm_dense_step_f32_batch)
+
+
+def _copy(struct):
+    return type(struct).from_buffer_copy(bytes(struct))
+
+
+class Batch:
+    """Independent cases on one GPU, stepped together (FP32 shifted form)."""
+
+    def __init__(self, cfgs, device=None, tile="rows2"):
+        if not cfgs:
+            raise ValueError("empty batch")
+        self.engines = [Engine(cfg, device, precision="f32") for cfg in cfgs]
+        for e in self.engines:
+            if e.st.particles is not None:
+                raise NotImplementedError("free particles (host Newton-Euler) are stepped one case at a time")
+        e0 = self.engines[0]
+        self.torch, self.dev, self.L = e0.torch, e0.dev, e0.L
+        torch = self.torch
+        self.C = len(self.engines)
+        self.N = sum(e.N for e in self.engines)
+        self.parity = 0
+        self.started = False
+        kinds = {}
+        for k, e in enumerate(self.engines):
+            c = e.case
+            key = (c.collision, c.bc, c.incompressible, IBM_IDS[e.method])
+            kinds.setdefault(key, []).append(k)
+        self.kinds = []
+        for key, idx in sorted(kinds.items()):
+            for s in range(0, len(idx), MAX_KIND):
+                self.kinds.append(idx[s:s + MAX_KIND])
+        self.tiles = [tile] * len(self.kinds)
+        # band argument blocks: [first step | later steps][parity], host and device copies
+        self.ibm_host = {}
+        self.ibm_dev = {}
+        for first in (True, False):
+            for p in (0, 1):
+                arr = (IbmArgs * self.C)()
+                for k, e in enumerate(self.engines):
+                    a = _copy(e.ibm_args[p])
+                    a.rebuild = 1 if (first or e.moving) else 0
+                    a.excl_cur = 0 if first else int(e.d_excl[p].data_ptr())
+                    arr[k] = a
+                self.ibm_host[first, p] = arr
+                raw = bytearray(bytes(arr))
+                self.ibm_dev[first, p] = torch.frombuffer(raw, dtype=torch.uint8).to(self.dev)
+        self._make_dense_arrays()
+        self.side = torch.cuda.Stream(self.dev, priority=-1)
+        self.ev_bulk = torch.cuda.Event()
+        self.ev_side = torch.cuda.Event()
+        self.graphs = {}
+
+    def _make_dense_arrays(self):
+        """Per kind and parity, the argument arrays of the whole-lattice, bulk
+        and box passes (tile of the kind set on every entry)."""
+        self.dense = {}
+        for g, idx in enumerate(self.kinds):
+            for p in (0, 1):
+                for mode in ("full", "bulk", "box"):
+                    arr = (Dense32Args * len(idx))()
+                    for n, k in enumerate(idx):
+                        e = self.engines[k]
+                        src = {"full": e.dense_full, "bulk": e.dense_bulk, "box": e.dense_box}[mode][p][0]
+                        a = _copy(src)
+                        a.tile = TILES[self.tiles[g]]
+                        a.box_blocks = 8
+                        arr[n] = a
+                    self.dense[g, p, mode] = arr
+
+    def set_tile(self, kind, tile):
+        if tile not in ("node", "rows2", "rows4"):
+            raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
+        self.tiles[kind] = tile
+        self._make_dense_arrays()
+        self.graphs = {}
+
+    # ---------------------------------------------------------------------------------
+    def _band(self, first, stream):
+        p = self.parity
+        check(self.L.iblbm_ibm_step_f32_batch(self.ibm_host[first, p], self.ibm_dev[first, p].data_ptr(), self.C,
+                                              stream), "iblbm_ibm_step_f32_batch")
+
+    def _dense(self, g, mode, stream):
+        arr = self.dense[g, self.parity, mode]
+        check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
+
+    def _sync_engines(self):
+        for e in self.engines:
+            e.parity = self.parity
+            e.rebuild_next = False
+
+    def _step_first(self):
+        """Serial step with band rebuild: band kernels, then every whole lattice."""
+        torch = self.torch
+        main = torch.cuda.current_stream(self.dev)
+        s = main.cuda_stream
+        self._band(True, s)
+        for g in range(len(self.kinds)):
+            self._dense(g, "full", s)
+        self.parity ^= 1
+        self.ev_bulk.record(main)
+        self.ev_side.record(main)
+        self.started = True
+
+    def _step(self):
+        """Overlapped step: band kernels and box passes on the side stream,
+        bulk passes of every kind on the current stream."""
+        torch = self.torch
+        main = torch.cuda.current_stream(self.dev)
+        side = self.side
+        side.wait_event(self.ev_bulk)
+        self._band(False, side.cuda_stream)
+        for g in range(len(self.kinds)):
+            self._dense(g, "box", side.cuda_stream)
+        main.wait_event(self.ev_side)
+        self.ev_side.record(side)
+        for g in range(len(self.kinds)):
+            self._dense(g, "bulk", main.cuda_stream)
+        self.ev_bulk.record(main)
+        self.parity ^= 1
+
+    def join(self):
+        self.torch.cuda.current_stream(self.dev).wait_event(self.ev_side)
+
+    def fence(self):
+        main = self.torch.cuda.current_stream(self.dev)
+        self.ev_bulk.record(main)
+        self.ev_side.record(main)
+
+    def _graph(self, length):
+        key = (self.parity, length)
+        g = self.graphs.get(key)
+        if g is None:
+            torch = self.torch
+            cap = torch.cuda.Stream(self.dev)
+            cap.wait_stream(torch.cuda.current_stream(self.dev))
+            cap.wait_stream(self.side)
+            g = torch.cuda.CUDAGraph()
+            p0 = self.parity
+            with torch.cuda.stream(cap):
+                with torch.cuda.graph(g, stream=cap):
+                    self.ev_bulk.record(cap)
+                    self.ev_side.record(cap)
+                    for _ in range(length):
+                        self._step()
+                    self.join()
+            torch.cuda.current_stream(self.dev).wait_stream(cap)
+            self.parity = p0
+            self.graphs[key] = g
+        return g
+
+    def advance(self, nsteps, outputs_last=True, use_graph=True):
+        """Advance every case nsteps timesteps; with outputs_last the last step
+        writes each case's rho / u / f* (read with its engine's cd_cl, read_state)."""
+        if nsteps <= 0:
+            return
+        if not self.started:
+            self._step_first()
+            nsteps -= 1
+            self._bump(1)
+        body = nsteps - 1 if (outputs_last and nsteps > 0) else nsteps
+        if body > 0:
+            if use_graph and body >= 4:
+                self.join()
+                self._graph(body).replay()
+                self.parity ^= (body & 1)
+                self.fence()
+            else:
+                for _ in range(body):
+                    self._step()
+                self.join()
+            self._bump(body)
+        if outputs_last and nsteps > 0:
+            self.join()
+            self._sync_engines()
+            for e in self.engines:
+                e._step_serial(outputs=True)
+            self.parity ^= 1
+            self.fence()
+            self._bump(1)
+            for e in self.engines:
+                e.last_out_step = e.ttt - 1
+        self._sync_engines()
+
+    def _bump(self, n):
+        for e in self.engines:
+            e.ttt += n
+
+    def status(self):
+        return [e.status() for e in self.engines]
+
+    def cd_cl(self):
+        return [e.cd_cl() for e in self.engines]

@@ -285,8 +285,9 @@ __device__ __forceinline__ void spread2(const Sm<R>& sh, const R* gx, const R* g
 template <bool SHIFTED>
 using BcOf = typename std::conditional<SHIFTED, BcParams32, BcParams>::type;
 
+// The band step of one case, run by one CTA of IBM_THREADS threads.
 template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED>
-__global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const ARGS a, BcOf<SHIFTED> bc)
+__device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>& bc)
 {
     constexpr int SW = Sten<A>::SW, S = Sten<A>::S;
     extern __shared__ __align__(16) char smem_raw[];
@@ -843,6 +844,42 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const ARGS a, 
     if (tid == 0) {
         a.stats[4] = s_status;
         if (a.step_counter) *a.step_counter = s_step + 1;
+    }
+}
+
+template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED>
+__global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const ARGS a, BcOf<SHIFTED> bc)
+{
+    ibm_step_body<ARGS, R, SHIFTED, A, METHOD, COUPLED>(a, bc);
+}
+
+// Many independent cases in one launch: CTA b runs the band step of case b,
+// whose argument block it copies from global into shared memory first.  The
+// stencil radius, method and coupling are per case (uniform over the CTA).
+template <class ARGS, typename R, bool SHIFTED>
+__global__ void __launch_bounds__(IBM_THREADS, 1) ibm_batch_kernel(const ARGS* __restrict__ args)
+{
+    __shared__ __align__(16) ARGS sa;
+    __shared__ BcOf<SHIFTED> sbc;
+    {
+        const int* src = reinterpret_cast<const int*>(args + blockIdx.x);
+        int* dst = reinterpret_cast<int*>(&sa);
+        for (int k = threadIdx.x; k < (int)(sizeof(ARGS) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) make_bc(sa.c, sbc);
+    __syncthreads();
+    const bool coupled = sa.method == IBM_MDF && sa.mdf_coupled;
+    if (sa.delta_type == 0) {
+        if (sa.method == IBM_DF) ibm_step_body<ARGS, R, SHIFTED, 2, IBM_DF, false>(sa, sbc);
+        else if (sa.method == IBM_DFC) ibm_step_body<ARGS, R, SHIFTED, 2, IBM_DFC, false>(sa, sbc);
+        else if (coupled) ibm_step_body<ARGS, R, SHIFTED, 2, IBM_MDF, true>(sa, sbc);
+        else ibm_step_body<ARGS, R, SHIFTED, 2, IBM_MDF, false>(sa, sbc);
+    } else {
+        if (sa.method == IBM_DF) ibm_step_body<ARGS, R, SHIFTED, 1, IBM_DF, false>(sa, sbc);
+        else if (sa.method == IBM_DFC) ibm_step_body<ARGS, R, SHIFTED, 1, IBM_DFC, false>(sa, sbc);
+        else if (coupled) ibm_step_body<ARGS, R, SHIFTED, 1, IBM_MDF, true>(sa, sbc);
+        else ibm_step_body<ARGS, R, SHIFTED, 1, IBM_MDF, false>(sa, sbc);
     }
 }
 

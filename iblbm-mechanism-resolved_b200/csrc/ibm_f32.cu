@@ -3,6 +3,7 @@
 // band_kernel.cuh instantiated with R = float: band moments from g = f - w
 // (rho = 1 + sum g), interpolation, spreading and MDF relaxation in FP32, the
 // MDF residual norm in FP64; per-marker outputs are written as FP64.
+#include <algorithm>
 #include "band_kernel.cuh"
 
 namespace iblbm {
@@ -31,4 +32,26 @@ extern "C" int iblbm_ibm_step_f32(const iblbm_ibm32_args* a, void* stream)
     BcParams32 bc;
     make_params32(a->c, cp, bc);
     return dispatch_ibm<iblbm_ibm32_args, float, true>(a, bc, stream);
+}
+
+extern "C" int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args* host_args, const iblbm_ibm32_args* dev_args, int n,
+                                        void* stream)
+{
+    if (!host_args || !dev_args || n < 1 || n > 65535) return IBLBM_E_ARG;
+    size_t smem = 0;
+    for (int b = 0; b < n; ++b) {
+        const int chk = check_ibm_args<float>(&host_args[b]);
+        if (chk != IBLBM_OK) return chk;
+        const int S = host_args[b].delta_type == 0 ? 25 : 9;
+        smem = std::max(smem, make_layout<float>(host_args[b].lb_total, host_args[b].band_capacity, S).total);
+    }
+    auto K = ibm_batch_kernel<iblbm_ibm32_args, float, true>;
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT) != cudaSuccess)
+            return IBLBM_E_LAUNCH;
+        configured = true;
+    }
+    K<<<n, IBM_THREADS, smem, (cudaStream_t)stream>>>(dev_args);
+    return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

@@ -31,6 +31,19 @@ struct CollParams32 {
     float S[9];
 };
 
+// Closure constants of a case, rounded from its FP64 parameters.
+__host__ __device__ inline void make_bc(const iblbm_case& c, BcParams32& bc)
+{
+    bc.inflow_u = (float)c.inflow_u;
+    bc.dens = (float)c.dens;
+    const double u0 = c.inflow_u, u2 = u0 * u0;
+    for (int q = 0; q < 9; ++q) {
+        const double eU = (double)ex_(q) * u0;
+        const double feq = c.dens * w_(q) * (1.0 + 3.0 * eU + 4.5 * eU * eU - 1.5 * u2);
+        bc.geq_in[q] = (float)(feq - w_(q));
+    }
+}
+
 __device__ __forceinline__ float wf(int q) { return (float)w_(q); }
 
 // feq - w in shifted form

@@ -219,6 +219,12 @@ typedef struct {
 
 /* Fused timestep on the shifted FP32 form (see iblbm_dense_step_f64). */
 int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
+/* The pass of n <= 72 independent cases of one kind (same collision, closure,
+ * compressibility, band method, and all bulk/whole-lattice or all box passes)
+ * in one launch; lattices may differ in size.  Tile NODE, ROWS2 or ROWS4 (taken
+ * from a[0]); no ro/U/fstar outputs.  Calls must not run concurrently on the
+ * host (the parameter block is staged in one static buffer). */
+int iblbm_dense_step_f32_batch(const iblbm_dense32_args *a, int n, void *stream);
 /* f (FP64 AoS, the reference's f[N, 9]) -> g = f - w (FP32 SoA), and back. */
 int iblbm_to_shifted_f32(const double *aos, iblbm_geom g, float *soa, void *stream);
 int iblbm_from_shifted_f32(const float *soa, iblbm_geom g, double *aos, void *stream);
@@ -260,6 +266,12 @@ typedef struct {
 } iblbm_ibm32_args;
 
 int iblbm_ibm_step_f32(const iblbm_ibm32_args *a, void *stream);
+/* Band steps of n independent cases in one launch (one CTA per case; stencil,
+ * method and coupling may differ between cases).  host_args and dev_args hold
+ * the same n argument blocks, on the host (checked here, sizes the shared
+ * memory) and in device memory (read by the kernel). */
+int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args *host_args, const iblbm_ibm32_args *dev_args, int n,
+                             void *stream);
 int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm32_smem_bytes(int lb_total, int band_capacity, int delta_type);
 
