@@ -1,32 +1,42 @@
 #!/usr/bin/env python
 """Benchmark of the IB-LBM per-timestep hot path on B200.
 
-Workload (the reference's config-2 case, the largest single-case benchmark
-configuration): fixed cylinder at Re = 100 on a 1601 x 641 D2Q9 lattice,
-D = 40, 126 Lagrangian markers, inflow u = 0.04, TRT collision (magic
-Lambda = 3/16), multi-direct forcing with the Peskin 4-point kernel (5 to 20
-iterations until the slip residual < 1e-6), Dirichlet/Neumann channel
-boundaries.  Inputs are the deterministic initial state of that case (no
-dataset).  One "step" is one full lattice timestep: the IBM band kernel (all MDF
-iterations) plus the fused collide-stream kernel.
+Two forms of the hot path are timed on one GPU:
+
+plain   the FP64 form (the reference's arithmetic, bit for bit) on the
+        reference's single-case benchmark: fixed cylinder at Re = 100 on a
+        1601 x 641 D2Q9 lattice, D = 40, 126 Lagrangian markers, inflow
+        u = 0.04, TRT (magic Lambda = 3/16), multi-direct forcing with the
+        Peskin 4-point kernel (5 to 20 iterations until the slip residual
+        < 1e-6), Dirichlet/Neumann channel.  One step = the band kernel (all MDF
+        iterations) and the fused collide-stream pass; L2 flushed between steps.
+chosen  the FP32 shifted-population form (FP64 force sums and MDF residual
+        norm) run batched: the 72-case sweep Re {20, 40, 100, 200} x
+        {DF, MDF, DFC} x {hat, Peskin-4} x {BGK, TRT, CM-MRT} of fixed cylinders
+        on 401x161 to 1921x961 lattices, all cases stepped together (one
+        batched band launch, one collide-stream launch per kind of case).  The
+        same workload as the plain form is also timed in the FP32 form, one
+        case alone (chosen_single_case).
 
 Reported (one JSON line on rank 0):
-  value       MLUPS of whole timesteps, inputs resident in HBM, L2 flushed
-              between timed steps (the 150 MB population working set is close
-              to the 126 MB L2, so each step is timed cold), CUDA events.
-  e2e         MLUPS through the public engine with host buffers: every step
-              uploads the marker positions / desired velocities from pinned
-              host memory and reads the drag/lift force sums back.
-  roofline    the fused collide-stream kernel against the measured HBM copy
-              bandwidth: 144 algorithmic bytes per lattice update (9 FP64
-              populations read + 9 written).
+  value       aggregate MLUPS of the chosen form (device time, CUDA events);
+              plain.mlups is the plain form's.
+  e2e         the same through the public API with host buffers: every step
+              uploads all cases' markers from pinned host memory and reads all
+              marker forces back.
+  roofline    the collide-stream launches of a step against the measured HBM
+              copy bandwidth: 72 algorithmic bytes per lattice update in FP32
+              (9 populations read + 9 written), 144 in FP64.
+  sweep       Cd/Cl of every batched case against the FP64 plain form of the
+              same case after the same steps (target: within 0.1 %).
   cpu_baseline  the CPU oracle (a C + OpenMP restatement of the reference's
-              CPU path) on a bounded sample of the same workload.
+              CPU path) on a bounded sample of the single-case workload.
 
---impl reference times that CPU restatement of the reference's own path (the
-reference is a Python package whose CPU path cannot travel to the GPU box).
-Multi-GPU: a single case does not shard; N ranks run N independent replicas
-(weak scaling), timed as the max over ranks.
+Inputs are deterministic initial states (no dataset).  --form plain times the
+plain form alone.  --impl reference times the CPU restatement of the
+reference's own path (the reference is a Python package whose CPU path cannot
+travel to the GPU box).  Multi-GPU: cases do not shard; N ranks run N
+independent replicas (weak scaling), timed as the max over ranks.
 """
 from __future__ import annotations
 
@@ -279,23 +289,161 @@ def measure(eng, args, dist, ws):
             "tile": tile, "tile_ms": tile_ms}
 
 
+# Batched sweep: fixed cylinders, Re x band method x delta kernel x collision
+# model on uneven lattices (Re -> NN, xmax, D/(NN-1), inflow u).
+SWEEP_SIZES = {20: (161, 2.5, 0.125, 0.05), 40: (321, 2.5, 0.1, 0.05), 100: (641, 2.5, 0.0625, 0.04),
+               200: (961, 2.0, 0.05, 0.04)}
+
+
+def sweep_configs(max_steps):
+    from iblbm_b200 import SimConfig
+    out = []
+    for Re, (NN, xmax, Dr, u) in SWEEP_SIZES.items():
+        for method in ("DF", "MDF", "DFC"):
+            for delta in ("hat", "peskin4pt"):
+                for coll in ("BGK", "TRT", "CM_MRT"):
+                    out.append(SimConfig(Re=Re, NN=NN, xmax=xmax, ymax=1, cylinder_center=(0.5, 0.5),
+                                         cylinder_D_ratio=Dr, lattice_u=u, inflow_u=u, bc_type="dirichlet_neumann",
+                                         delta_type=delta, ibm_method=method, collision_model=coll,
+                                         trt_magic_param=0.1875, mdf_iterations=20, mdf_min_iterations=5,
+                                         mdf_tolerance=1e-6, marker_spacing_factor=1.0, max_steps=max_steps,
+                                         use_convergence=False, check_interval=100))
+    return out
+
+
+def measure_batch(b, K, W, dist, ws):
+    """Time the batched sweep: per-kind tile tuning, K overlapped steps (every
+    step streams the whole sweep, ~4 GB, far above L2), graph-replayed steady
+    state, and the host-buffer loop (all markers in, all marker forces out)."""
+    import torch
+    E = lambda: torch.cuda.Event(enable_timing=True)
+    b.advance(max(W, 3), outputs_last=False)
+    torch.cuda.synchronize()
+    # per-kind tile choice: the bulk pass is side-effect free when repeated without a parity flip
+    tiles = {}
+    main = torch.cuda.current_stream()
+    for g in range(len(b.kinds)):
+        best = None
+        for tile in ("node", "rows2", "rows4"):
+            b.set_tile(g, tile)
+            b._dense(g, "bulk", main.cuda_stream)
+            ev = [(E(), E()) for _ in range(3)]
+            for e0, e1 in ev:
+                e0.record()
+                b._dense(g, "bulk", main.cuda_stream)
+                e1.record()
+            torch.cuda.synchronize()
+            ms = min(e0.elapsed_time(e1) for e0, e1 in ev)
+            if best is None or ms < best[1]:
+                best = (tile, ms)
+        b.set_tile(g, best[0])
+        tiles[g] = best
+    b.fence()
+    ev = [[E() for _ in range(4)] for _ in range(K)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(torch.cuda.current_device()) as clk:
+        t_wall = time.perf_counter()
+        for k in range(K):
+            ev[k][0].record(main)
+            b._step(bulk_events=(ev[k][1], ev[k][2]))
+            b.join()
+            ev[k][3].record(main)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    b._bump(K)
+    tot_ms = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(K))
+    bulk_ms = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(K)) / K
+    if dist:
+        t = torch.tensor([tot_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    box_nodes = sum(int(x[2]) * int(x[3]) for e in b.engines for x in [e.d_excl[b.parity].tolist()])
+    achieved = BYTES_PER_LU_F32 * (b.N - box_nodes) / (bulk_ms / 1e3) / 1e9
+    # steady state through one captured graph
+    e0, e1 = E(), E()
+    b.advance(K, outputs_last=False)
+    torch.cuda.synchronize()
+    e0.record()
+    b.advance(K, outputs_last=False)
+    e1.record()
+    torch.cuda.synchronize()
+    steady = b.N * K / (e0.elapsed_time(e1) / 1e3) / 1e6
+    # host buffers: every step uploads all cases' markers and reads all marker forces back
+    nin = b.marker_in.numel()
+    host_in = torch.empty(nin, dtype=torch.float64).pin_memory()
+    host_in.copy_(b.marker_in.cpu())
+    host_out = torch.empty(b.marker_out.numel(), dtype=torch.float64).pin_memory()
+    Ke = max(10, K // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        b.marker_in.copy_(host_in, non_blocking=True)
+        b._step()
+        b.join()
+        host_out.copy_(b.marker_out, non_blocking=True)
+        main.synchronize()
+    e2e_s = time.perf_counter() - t0
+    b._bump(Ke)
+    b.fence()
+    b.advance(1, outputs_last=True)
+    torch.cuda.synchronize()
+    return {"value": b.N * K * ws / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "bulk_ms": bulk_ms,
+            "achieved": achieved, "box_nodes": box_nodes, "steady": steady,
+            "e2e": b.N * Ke * ws / e2e_s / 1e6, "h2d": nin * 8, "d2h": host_out.numel() * 8,
+            "clocks": clk.summary(), "wall_s_timed": t_wall, "status": b.status(),
+            "tiles": {str(g): {"tile": t, "bulk_ms": ms, "cases": len(b.kinds[g])} for g, (t, ms) in tiles.items()},
+            "launches_per_step": 1 + 2 * len(b.kinds), "steps_done": b.engines[0].ttt - 1}
+
+
+def sweep_cd_check(cfgs, batch, steps):
+    """Cd/Cl of every batched case against the FP64 plain form of the same case
+    after the same number of steps (one case at a time)."""
+    import torch
+    from iblbm_b200.engine import Engine
+    worst_cd, worst_cl, rows = 0.0, 0.0, []
+    for cfg, eb in zip(cfgs, batch.engines):
+        e = Engine(cfg, precision="f64")
+        e.advance(steps, outputs_last=True)
+        torch.cuda.synchronize()
+        cd64, cl64 = e.cd_cl()
+        cd32, cl32 = eb.cd_cl()
+        rc = abs(cd32 - cd64) / abs(cd64)
+        rl = abs(cl32 - cl64) / abs(cd64)
+        worst_cd, worst_cl = max(worst_cd, rc), max(worst_cl, rl)
+        rows.append((cfg.Re, cfg.ibm_method, cfg.delta_type, cfg.collision_model, cd64, rc))
+        del e
+    torch.cuda.empty_cache()
+    return worst_cd, worst_cl, rows
+
+
 def run_b200(args):
     import torch
     dist, rank, ws, local = _dist()
     torch.cuda.set_device(local)
+    from iblbm_b200.batch import Batch
     from iblbm_b200.engine import Engine
     cfg = workload_config(max_steps=args.warmup + 4 * args.steps + 16)
     peak, peak_kind = _peaks()
     plain = measure(Engine(cfg, precision="f64"), args, dist, ws)
-    chosen = measure(Engine(cfg, precision="f32"), args, dist, ws) if args.form == "chosen" else None
-    head = chosen or plain
+    single = measure(Engine(cfg, precision="f32"), args, dist, ws)
+    bres, sweep = None, None
+    if args.form == "chosen":
+        Kb = max(20, args.steps // 8)
+        cfgs = sweep_configs(max_steps=args.warmup + 4 * Kb + 16)
+        batch = Batch(cfgs)
+        bres = measure_batch(batch, Kb, args.warmup, dist, ws)
+        worst_cd, worst_cl, rows = sweep_cd_check(cfgs, batch, bres["steps_done"])
+        sweep = {"cases": len(cfgs), "lattice_nodes": batch.N, "max_cd_rel_err_vs_f64": worst_cd,
+                 "max_cl_err_vs_f64_rel_cd": worst_cl, "worst_case": max(rows, key=lambda r: r[5])[:4]}
+        del batch
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     N = 1601 * 641
     cpu = cpu_baseline(seconds=float(os.environ.get("IBLBM_CPU_SECONDS", "20"))) if ws == 1 else None
-    form = "FP32 shifted populations (FP64 force sums, MDF residual norm)" if chosen else "FP64 plain"
 
     def summary(m):
         return {"mlups": m["value"], "ms_per_step": m["ms_per_step"], "bulk_kernel_ms": m["dense_ms"],
@@ -305,29 +453,53 @@ def run_b200(args):
                 "Cd": m["cd"], "Cl": m["cl"], "step": m["steps_done"], "tile": m["tile"],
                 "tile_ms_whole_lattice": m["tile_ms"]}
 
-    line = {"metric": METRIC, "value": head["value"], "unit": "MLUPS", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if chosen else "f64",
-            "data": "synthetic (deterministic initial state of the workload)",
-            "config": dict(WORKLOAD, form=form, parallelism=f"replicas x{ws}"),
-            "hbm_gbs_dense": head["achieved"],
-            "schedule": "band kernel + box pass (side stream) concurrent with the bulk pass",
-            "roofline": {"bound": "hbm", "achieved": head["achieved"], "peak": peak, "unit": "GB/s",
-                         "frac": head["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": ("dense32_kernel" if chosen else "dense_step_kernel") +
-                                   " bulk pass (fused pull-stream+BC+macro+collide)",
-                         "bytes_per_lu": head["bytes_per_lu"], "lattice_updates_per_launch": N - head["box_nodes"]},
-            "cpu_baseline": cpu,
-            "e2e": {"value": head["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": head["e2e_h2d"],
-                    "d2h_bytes_per_step": head["e2e_d2h"]},
-            "gpu_launches": 3 * args.steps,
-            "clocks": head["clocks"], "wall_s_timed": head["wall_s_timed"],
-            "plain": summary(plain)}
-    if chosen:
-        line["chosen"] = summary(chosen)
-        line["chosen_vs_plain"] = chosen["value"] / plain["value"]
-        line["cd_rel_err_vs_f64"] = abs(chosen["cd"] - plain["cd"]) / abs(plain["cd"])
-        line["cl_err_vs_f64_rel_cd"] = abs(chosen["cl"] - plain["cl"]) / abs(plain["cd"])
+    line = {"metric": METRIC, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic (deterministic initial states of the workloads)"}
+    single_s = summary(single)
+    single_s["cd_rel_err_vs_f64"] = abs(single["cd"] - plain["cd"]) / abs(plain["cd"])
+    single_s["cl_err_vs_f64_rel_cd"] = abs(single["cl"] - plain["cl"]) / abs(plain["cd"])
+    if bres:
+        line.update({
+            "value": bres["value"], "ms_per_step": bres["ms_per_step"], "dtype": "f32",
+            "config": {"workload": "chosen form: batched sweep of 72 fixed-cylinder cases, Re {20,40,100,200} x "
+                                   "{DF,MDF,DFC} x {hat,P4} x {BGK,TRT,CM-MRT} on 401x161 (D=20), 801x321 (D=32), "
+                                   "1601x641 (D=40), 1921x961 (D=48) lattices, FP32 shifted populations with FP64 "
+                                   "force sums; plain form: " + WORKLOAD["workload"] + ", FP64",
+                       "cases": sweep["cases"], "lattice_nodes_per_step": bres and sweep["lattice_nodes"],
+                       "l2": "per-step traffic ~4 GB (inputs far larger than L2), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "steps_batch": max(20, args.steps // 8),
+            "schedule": "one batched band launch + box passes (side stream) concurrent with one bulk launch per "
+                        "kind of case; CUDA graph between outputs",
+            "roofline": {"bound": "hbm", "achieved": bres["achieved"], "peak": peak, "unit": "GB/s",
+                         "frac": bres["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "dense32_batch_kernel bulk passes of all kinds (fused pull-stream+BC+macro+"
+                                   "collide, FP32 shifted)", "bytes_per_lu": BYTES_PER_LU_F32,
+                         "lattice_updates_per_step": bres and (sweep["lattice_nodes"] - bres["box_nodes"])},
+            "e2e": {"value": bres["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": bres["h2d"],
+                    "d2h_bytes_per_step": bres["d2h"]},
+            "gpu_launches": bres["launches_per_step"] * max(20, args.steps // 8),
+            "clocks": bres["clocks"], "wall_s_timed": bres["wall_s_timed"],
+            "chosen_vs_plain": bres["value"] / plain["value"],
+            "sweep": dict(sweep, steady_state_mlups_graph=bres["steady"], status_nonzero=[
+                k for k, st in enumerate(bres["status"]) if st], tiles=bres["tiles"],
+                bulk_ms_per_step=bres["bulk_ms"])})
+    else:
+        line.update({"value": plain["value"], "ms_per_step": plain["ms_per_step"], "dtype": "f64",
+                     "config": dict(WORKLOAD, form="FP64 plain", parallelism=f"replicas x{ws}"),
+                     "roofline": {"bound": "hbm", "achieved": plain["achieved"], "peak": peak, "unit": "GB/s",
+                                  "frac": plain["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
+                                  "kernel": "dense_step_kernel bulk pass (FP64)", "bytes_per_lu": BYTES_PER_LU_F64,
+                                  "lattice_updates_per_launch": N - plain["box_nodes"]},
+                     "e2e": {"value": plain["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": plain["e2e_h2d"],
+                             "d2h_bytes_per_step": plain["e2e_d2h"]},
+                     "gpu_launches": 3 * args.steps, "clocks": plain["clocks"],
+                     "wall_s_timed": plain["wall_s_timed"]})
+    line["cpu_baseline"] = cpu
+    line["plain"] = summary(plain)
+    line["plain"]["roofline_frac_bulk"] = plain["achieved"] / peak
+    line["chosen_single_case"] = single_s
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
@@ -347,6 +519,22 @@ def run_profile(args):
     print(json.dumps({"profile_steps": args.steps, "status": eng.status(), "mdf": eng.mdf_stats()}))
 
 
+def run_profile_batch(args):
+    """A short eager batched run for ncu captures: the Re 20 and 40 part of the
+    sweep (36 cases, ~1.5 GB on the device), warm-up steps then args.steps."""
+    import torch
+    from iblbm_b200.batch import Batch
+    cfgs = [c for c in sweep_configs(max_steps=args.warmup + args.steps + 8) if c.Re in (20, 40)]
+    b = Batch(cfgs)
+    b.advance(1, outputs_last=False)
+    for _ in range(args.warmup + args.steps):
+        b._step()
+    b.join()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_batch_steps": args.steps, "cases": len(cfgs), "nodes": b.N,
+                      "status_nonzero": [k for k, st in enumerate(b.status()) if st]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,6 +542,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--profile", action="store_true", help="short eager run for ncu captures")
+    ap.add_argument("--profile-batch", action="store_true", help="short eager batched run for ncu captures")
     ap.add_argument("--collision", default="TRT", choices=["BGK", "TRT", "CM_MRT"])
     ap.add_argument("--form", default="chosen", choices=["chosen", "plain"],
                     help="chosen: time the FP32 shifted form and the FP64 plain form; plain: FP64 only")
@@ -361,7 +550,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile:
+    if args.profile_batch:
+        run_profile_batch(args)
+    elif args.profile:
         run_profile(args)
     elif args.impl == "reference":
         run_reference(args)

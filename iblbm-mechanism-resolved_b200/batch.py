@@ -47,6 +47,7 @@ class Batch:
         e0 = self.engines[0]
         self.torch, self.dev, self.L = e0.torch, e0.dev, e0.L
         torch = self.torch
+        self._pool_marker_arrays()
         self.C = len(self.engines)
         self.N = sum(e.N for e in self.engines)
         self.parity = 0
@@ -80,6 +81,30 @@ class Batch:
         self.ev_bulk = torch.cuda.Event()
         self.ev_side = torch.cuda.Event()
         self.graphs = {}
+
+    def _pool_marker_arrays(self):
+        """Place every case's marker inputs (x, y, desired velocity) in one device
+        array and its per-marker outputs (IB force, DFC force) in another, so a
+        host program moves all cases' markers with one copy each way."""
+        torch = self.torch
+        tot = sum(e.Lb for e in self.engines)
+        self.marker_in = torch.zeros(4 * tot, dtype=torch.float64, device=self.dev)
+        self.marker_out = torch.zeros(4 * tot, dtype=torch.float64, device=self.dev)
+        o = 0
+        self.marker_slices = []
+        for e in self.engines:
+            Lb = e.Lb
+            xin, yin = self.marker_in[o:o + Lb], self.marker_in[tot + o:tot + o + Lb]
+            dvin = self.marker_in[2 * tot + 2 * o:2 * tot + 2 * o + 2 * Lb]
+            xin.copy_(e.d_Lx[:Lb]); yin.copy_(e.d_Ly[:Lb]); dvin.copy_(e.d_dv[:2 * Lb])
+            e.d_Lx, e.d_Ly, e.d_dv = xin, yin, dvin
+            e.d_Lfx = self.marker_out[o:o + Lb]
+            e.d_Lfy = self.marker_out[tot + o:tot + o + Lb]
+            e.d_dfc_force = self.marker_out[2 * tot + 2 * o:2 * tot + 2 * o + 2 * Lb]
+            e.ibm_args = [e._make_ibm_args(p) for p in (0, 1)]
+            self.marker_slices.append((o, Lb))
+            o += Lb
+        self.markers_total = tot
 
     def _make_dense_arrays(self):
         """Per kind and parity, the argument arrays of the whole-lattice, bulk
@@ -133,9 +158,10 @@ class Batch:
         self.ev_side.record(main)
         self.started = True
 
-    def _step(self):
+    def _step(self, bulk_events=None):
         """Overlapped step: band kernels and box passes on the side stream,
-        bulk passes of every kind on the current stream."""
+        bulk passes of every kind on the current stream (bulk_events: two
+        events recorded around the bulk passes)."""
         torch = self.torch
         main = torch.cuda.current_stream(self.dev)
         side = self.side
@@ -145,8 +171,12 @@ class Batch:
             self._dense(g, "box", side.cuda_stream)
         main.wait_event(self.ev_side)
         self.ev_side.record(side)
+        if bulk_events:
+            bulk_events[0].record(main)
         for g in range(len(self.kinds)):
             self._dense(g, "bulk", main.cuda_stream)
+        if bulk_events:
+            bulk_events[1].record(main)
         self.ev_bulk.record(main)
         self.parity ^= 1
 

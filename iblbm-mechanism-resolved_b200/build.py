@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -26,6 +27,8 @@ UNITS = {
     "ibm_f64.cu": ["-fmad=false"],
     "ops_f64.cu": ["-fmad=false"],
     "dense_f32.cu": [],
+    "pipe_f32.cu": [],
+    "batch_f32.cu": [],
     "ibm_f32.cu": [],
 }
 
@@ -50,7 +53,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
     headers.append(os.path.join(INCLUDE, "iblbm_b200.h"))
-    objs = []
+    objs, cmds = [], []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
@@ -60,7 +63,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.check_call(cmd)
+            cmds.append(cmd)
+    # the units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for _ in pool.map(subprocess.check_call, cmds):
+            pass
     if force or _stale(LIB, objs):
         subprocess.check_call([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
     return LIB

@@ -232,6 +232,29 @@ __device__ __forceinline__ void gstar_node(const float* __restrict__ fp, const f
     else if (BC == BC_VELOCITY_INLET) bc32_velocity_inlet(ur, g, bc, i, j, f);
 }
 
+// Pull offsets of an interior node relative to its own site: population q
+// comes from q*qstride - ey(q)*pitch - ex(q) (fits an int: the host checks
+// 9 * qstride < 2^31).
+__device__ __forceinline__ void pull_offsets(const Geom& g, int* off)
+{
+#pragma unroll
+    for (int q = 0; q < 9; ++q) off[q] = q * (int)g.qstride - ey_(q) * g.pitch - ex_(q);
+}
+
+// Pull of node (i, j): interior nodes read through the precomputed offsets,
+// edge nodes through the bounds-checked pull.
+__device__ __forceinline__ void pull_node(const float* __restrict__ fp, const Geom& g, const int* off, int i, int j,
+                                          float* f)
+{
+    if (i >= 1 && i <= g.nx - 2 && j >= 1 && j <= g.ny - 2) {
+        const float* site = fp + (long long)j * g.pitch + i;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) f[q] = __ldg(site + off[q]);
+    } else {
+        pull(fp, g, i, j, f);
+    }
+}
+
 // Closure of a node whose pulled populations are already in f (the Dirichlet /
 // Neumann edge recomputes them from its neighbour column instead).
 template <int BC>
@@ -255,63 +278,124 @@ __device__ __forceinline__ float guo_bare(int q, float u0, float u1, float F0, f
     return wf(q) * ((3.0f * (ex - u0) + 9.0f * eU * ex) * F0 + (3.0f * (ey - u1) + 9.0f * eU * ey) * F1);
 }
 
+// The four opposite pairs (q, opp q) with e_q = (+1, 0), (0, +1), (+1, +1), (-1, +1).
+__device__ __forceinline__ constexpr int pair_q(int p) { return p == 0 ? 1 : (p == 1 ? 2 : (p == 2 ? 5 : 6)); }
+
+// Equilibrium deviation of a pair, split into its even part (same for q and
+// opp q) and odd part (sign flips): geq_q = even + odd, geq_opp = even - odd.
+template <bool INCOMP>
+__device__ __forceinline__ void geq_pair(int q, float drho, float rho, float u0, float u1, float u2, float& even,
+                                         float& odd)
+{
+    const float eu = (float)ex_(q) * u0 + (float)ey_(q) * u1;
+    const float r = INCOMP ? 1.0f : rho;
+    even = wf(q) * (drho + r * (4.5f * eu * eu - 1.5f * u2));
+    odd = wf(q) * r * 3.0f * eu;
+}
+
 template <bool INCOMP, bool FORCED>
 __device__ __forceinline__ void collide32_bgk(const float* g, float drho, float rho, float u0, float u1, float F0,
                                               float F1, const CollParams32& cp, float* out)
 {
     const float u2 = u0 * u0 + u1 * u1;
+    const float fp = cp.guo_pref * cp.dt;
+    {
+        const float ge = wf(0) * (drho + (INCOMP ? 1.0f : rho) * (-1.5f * u2));
+        float v = g[0] - cp.inv_tau * (g[0] - ge);
+        if (FORCED) v += fp * guo_bare(0, u0, u1, F0, F1);
+        out[0] = v;
+    }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        float v = g[q] - cp.inv_tau * (g[q] - geq_q<INCOMP>(q, drho, rho, u0, u1, u2));
-        if (FORCED) v += cp.guo_pref * guo_bare(q, u0, u1, F0, F1) * cp.dt;
-        out[q] = v;
+    for (int p = 0; p < 4; ++p) {
+        const int q = pair_q(p), o = opp_(q);
+        float even, odd;
+        geq_pair<INCOMP>(q, drho, rho, u0, u1, u2, even, odd);
+        float vq = g[q] - cp.inv_tau * (g[q] - (even + odd));
+        float vo = g[o] - cp.inv_tau * (g[o] - (even - odd));
+        if (FORCED) {
+            vq += fp * guo_bare(q, u0, u1, F0, F1);
+            vo += fp * guo_bare(o, u0, u1, F0, F1);
+        }
+        out[q] = vq;
+        out[o] = vo;
     }
 }
 
+// TRT on pairs: the even part relaxes with s+, the odd part with s-.
 template <bool INCOMP, bool FORCED>
 __device__ __forceinline__ void collide32_trt(const float* g, float drho, float rho, float u0, float u1, float F0,
                                               float F1, const CollParams32& cp, float* out)
 {
     const float u2 = u0 * u0 + u1 * u1;
-    float ge[9], bare[9];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        ge[q] = geq_q<INCOMP>(q, drho, rho, u0, u1, u2);
-        bare[q] = FORCED ? guo_bare(q, u0, u1, F0, F1) : 0.0f;
-    }
     const float gp = 1.0f - 0.5f * cp.s_plus, gm = 1.0f - 0.5f * cp.s_minus;
+    {
+        const float ge = wf(0) * (drho + (INCOMP ? 1.0f : rho) * (-1.5f * u2));
+        float v = g[0] - cp.s_plus * (g[0] - ge);
+        if (FORCED) v += gp * guo_bare(0, u0, u1, F0, F1) * cp.dt;
+        out[0] = v;
+    }
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const int o = opp_(q);
-        const float fp = 0.5f * (g[q] + g[o]) - 0.5f * (ge[q] + ge[o]);
-        const float fm = 0.5f * (g[q] - g[o]) - 0.5f * (ge[q] - ge[o]);
-        float v = g[q] - (cp.s_plus * fp + cp.s_minus * fm);
-        if (FORCED) v += (gp * 0.5f * (bare[q] + bare[o]) + gm * 0.5f * (bare[q] - bare[o])) * cp.dt;
-        out[q] = v;
+    for (int p = 0; p < 4; ++p) {
+        const int q = pair_q(p), o = opp_(q);
+        float even, odd;
+        geq_pair<INCOMP>(q, drho, rho, u0, u1, u2, even, odd);
+        const float ne = 0.5f * (g[q] + g[o]) - even;  // non-equilibrium, even part
+        const float no = 0.5f * (g[q] - g[o]) - odd;   // non-equilibrium, odd part
+        float vq = g[q] - (cp.s_plus * ne + cp.s_minus * no);
+        float vo = g[o] - (cp.s_plus * ne - cp.s_minus * no);
+        if (FORCED) {
+            const float bq = guo_bare(q, u0, u1, F0, F1), bo = guo_bare(o, u0, u1, F0, F1);
+            const float be = 0.5f * (bq + bo), bd = 0.5f * (bq - bo);
+            vq += (gp * be + gm * bd) * cp.dt;
+            vo += (gp * be - gm * bd) * cp.dt;
+        }
+        out[q] = vq;
+        out[o] = vo;
     }
 }
 
+// CM-MRT: raw moments of g (sums and differences of populations, e in {0, +-1}),
+// shifted to central moments about u by the binomial formulas.
 template <bool FORCED>
 __device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, float ux, float uy, float F0, float F1,
                                                 const CollParams32& cp, float* out)
 {
-    float k[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const float s57 = g[5] + g[7], s68 = g[6] + g[8], d57 = g[5] - g[7], d68 = g[6] - g[8];
+    const float m00 = (g[0] + (g[1] + g[3])) + ((g[2] + g[4]) + (s57 + s68));
+    const float m10 = (g[1] - g[3]) + (d57 - d68);
+    const float m01 = (g[2] - g[4]) + (d57 + d68);
+    const float m20 = (g[1] + g[3]) + (s57 + s68);
+    const float m02 = (g[2] + g[4]) + (s57 + s68);
+    const float m11 = s57 - s68;
+    const float m21 = d57 + d68;
+    const float m12 = d57 - d68;
+    const float m22 = s57 + s68;
+    const float ux2 = ux * ux, uy2 = uy * uy, uxy = ux * uy;
+    float k[9];
+    k[0] = m00;
+    k[1] = m10 - ux * m00;
+    k[2] = m01 - uy * m00;
+    k[3] = m20 - 2.0f * ux * m10 + ux2 * m00;
+    k[4] = m02 - 2.0f * uy * m01 + uy2 * m00;
+    k[5] = m11 - ux * m01 - uy * m10 + uxy * m00;
+    k[6] = m21 - 2.0f * ux * m11 - uy * m20 + ux2 * m01 + 2.0f * uxy * m10 - ux2 * uy * m00;
+    k[7] = m12 - 2.0f * uy * m11 - ux * m02 + uy2 * m10 + 2.0f * uxy * m01 - ux * uy2 * m00;
+    k[8] = m22 - 2.0f * ux * m12 - 2.0f * uy * m21 + ux2 * m02 + uy2 * m20 + 4.0f * uxy * m11 -
+           2.0f * ux * uy2 * m10 - 2.0f * ux2 * uy * m01 + ux2 * uy2 * m00;
+    float F[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (FORCED) {
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const float ex = (float)ex_(q), ey = (float)ey_(q);
-        const float cx = ex - ux, cy = ey - uy, cx2 = cx * cx, cy2 = cy * cy;
-        const float v = g[q];
-        k[0] += v; k[1] += v * cx; k[2] += v * cy; k[3] += v * cx2; k[4] += v * cy2;
-        k[5] += v * cx * cy; k[6] += v * cx2 * cy; k[7] += v * cx * cy2; k[8] += v * cx2 * cy2;
-        if (FORCED) {
+        for (int q = 0; q < 9; ++q) {
+            const float ex = (float)ex_(q), ey = (float)ey_(q);
+            const float cx = ex - ux, cy = ey - uy, cx2 = cx * cx, cy2 = cy * cy;
             const float b = guo_bare(q, ux, uy, F0, F1);
             F[0] += b; F[1] += b * cx; F[2] += b * cy; F[3] += b * cx2; F[4] += b * cy2;
             F[5] += b * cx * cy; F[6] += b * cx2 * cy; F[7] += b * cx * cy2; F[8] += b * cx2 * cy2;
         }
     }
     // central moments of the weights about u, and the equilibrium minus them
-    const float ax = 1.0f / 3.0f + ux * ux, ay = 1.0f / 3.0f + uy * uy;
-    const float kw[9] = {1.0f, -ux, -uy, ax, ay, ux * uy, -uy * ax, -ux * ay, ax * ay};
+    const float ax = 1.0f / 3.0f + ux2, ay = 1.0f / 3.0f + uy2;
+    const float kw[9] = {1.0f, -ux, -uy, ax, ay, uxy, -uy * ax, -ux * ay, ax * ay};
     const float rho = 1.0f + drho;
     const float keq[9] = {rho, 0.0f, 0.0f, rho / 3.0f, rho / 3.0f, 0.0f, 0.0f, 0.0f, rho / 9.0f};
     float c[9];
@@ -322,16 +406,15 @@ __device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, floa
         c[m] = k[m] - cp.S[m] * neq;
         if (FORCED) c[m] += (1.0f - 0.5f * cp.S[m]) * F[m] * cp.dt;
     }
-    const float ux2 = ux * ux, uy2 = uy * uy;
     const float k0 = c[0];
     const float k1 = c[1] + ux * c[0];
     const float k2 = c[2] + uy * c[0];
     const float k3 = c[3] + 2.0f * ux * c[1] + ux2 * c[0];
     const float k4 = c[4] + 2.0f * uy * c[2] + uy2 * c[0];
-    const float k5 = c[5] + uy * c[1] + ux * c[2] + ux * uy * c[0];
-    const float k6 = c[6] + uy * c[3] + 2.0f * ux * c[5] + 2.0f * ux * uy * c[1] + ux2 * c[2] + ux2 * uy * c[0];
-    const float k7 = c[7] + 2.0f * uy * c[5] + ux * c[4] + 2.0f * ux * uy * c[2] + uy2 * c[1] + ux * uy2 * c[0];
-    const float k8 = c[8] + 2.0f * uy * c[6] + uy2 * c[3] + 2.0f * ux * c[7] + 4.0f * ux * uy * c[5] +
+    const float k5 = c[5] + uy * c[1] + ux * c[2] + uxy * c[0];
+    const float k6 = c[6] + uy * c[3] + 2.0f * ux * c[5] + 2.0f * uxy * c[1] + ux2 * c[2] + ux2 * uy * c[0];
+    const float k7 = c[7] + 2.0f * uy * c[5] + ux * c[4] + 2.0f * uxy * c[2] + uy2 * c[1] + ux * uy2 * c[0];
+    const float k8 = c[8] + 2.0f * uy * c[6] + uy2 * c[3] + 2.0f * ux * c[7] + 4.0f * uxy * c[5] +
                      2.0f * ux * uy2 * c[1] + ux2 * c[4] + 2.0f * ux2 * uy * c[2] + ux2 * uy2 * c[0];
     out[0] = k0 - k3 - k4 + k8;
     out[1] = 0.5f * (k1 + k3 - k7 - k8);
