@@ -56,10 +56,12 @@ class IbmArgs(ctypes.Structure):
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp)]
 
 
-# The FP32 band-step struct (iblbm_ibm32_args) has the same fields in the same
-# order as the FP64 one; only the pointee types differ.  The FP32 dense struct
-# adds the tile choice at the end.
-Ibm32Args = IbmArgs
+# The FP32 structs have the FP64 ones' fields in the same order (only pointee
+# types differ) and add their own at the end: the learned warm start for the
+# band step, the tile choice for the dense pass.
+class Ibm32Args(ctypes.Structure):
+    _fields_ = IbmArgs._fields_ + [("mlp_mode", _i), ("mlp_uref", ctypes.c_float), ("mlp_re", ctypes.c_float),
+                                   ("mlp_params", _vp), ("mlp_features", _vp), ("mlp_targets", _vp)]
 
 
 class Dense32Args(ctypes.Structure):
@@ -85,8 +87,11 @@ _SIGS = {
     "iblbm_streaming": [_vp, _vp, _i, _i, _vp, _vp],
     "iblbm_velocity_correction": [_vp, _vp, _vp, _i, _d, _i, _vp],
     "iblbm_dense_step_f32": [ctypes.POINTER(Dense32Args), _vp],
-    "iblbm_ibm_step_f32": [ctypes.POINTER(IbmArgs), _vp],
-    "iblbm_ibm_step_f32_batch": [ctypes.POINTER(IbmArgs), _vp, _i, _vp],
+    "iblbm_ibm_step_f32": [ctypes.POINTER(Ibm32Args), _vp],
+    "iblbm_ibm_step_f32_batch": [ctypes.POINTER(Ibm32Args), _vp, _i, _vp],
+    "iblbm_mlp_param_count": [],
+    "iblbm_mlp_infer": [_vp, _vp, _i, _vp, _vp],
+    "iblbm_mlp_train_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_float, _i, _vp, _i, _vp],
     "iblbm_dense_step_f32_batch": [ctypes.POINTER(Dense32Args), _i, _vp],
     "iblbm_ibm32_list_cache_ints": [_i, _i, _i],
     "iblbm_ibm32_smem_bytes": [_i, _i, _i],

@@ -24,7 +24,7 @@ from __future__ import annotations
 
 import ctypes
 
-from ._lib import IBM_IDS, TILES, Dense32Args, IbmArgs, check
+from ._lib import IBM_IDS, TILES, Dense32Args, Ibm32Args, check
 from .engine import Engine
 
 MAX_KIND = 72  # cases per batched collide-stream launch (iblbm_dense_step_f32_batch)
@@ -67,7 +67,7 @@ class Batch:
         self.ibm_dev = {}
         for first in (True, False):
             for p in (0, 1):
-                arr = (IbmArgs * self.C)()
+                arr = (Ibm32Args * self.C)()
                 for k, e in enumerate(self.engines):
                     a = _copy(e.ibm_args[p])
                     a.rebuild = 1 if (first or e.moving) else 0

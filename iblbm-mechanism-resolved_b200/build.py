@@ -30,6 +30,7 @@ UNITS = {
     "pipe_f32.cu": [],
     "batch_f32.cu": [],
     "ibm_f32.cu": [],
+    "mlp_f32.cu": [],
 }
 
 

@@ -40,6 +40,7 @@
 #include "common.cuh"
 #include "shifted.cuh"
 #include "tma.cuh"
+#include "mlp.cuh"
 #include "../../include/iblbm_b200.h"
 
 namespace iblbm {
@@ -51,7 +52,6 @@ constexpr int MAXP = 8;    // particles per band kernel
 constexpr int NWARP = IBM_THREADS / 32;
 constexpr long long TMA_WAIT_LIMIT = 1LL << 22;
 constexpr int IBM_SMEM_LIMIT = 220 * 1024;
-
 enum IbmStatus : int { ST_OK = 0, ST_BAND_CAPACITY = 1, ST_BOX_CAPACITY = 2, ST_MARKERS = 3, ST_TABLE = 4,
                        ST_EXCL = 5, ST_COPY_TIMEOUT = 6 };
 
@@ -62,6 +62,21 @@ struct Sten {
 };
 
 __host__ __device__ inline size_t up16(size_t x) { return (x + 15) & ~size_t(15); }
+
+constexpr int MLP_CHUNK = MLP_RPT * IBM_THREADS / 64;  // markers per network tile (128)
+
+// Shared memory of the learned warm start, placed after the band layout: two
+// activation tiles, the outputs of a tile, and the predicted force per marker.
+__host__ __device__ inline size_t mlp_smem_bytes(int Lb)
+{
+    return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * 64 + 2 * MLP_CHUNK + 2 * (size_t)Lb));
+}
+inline bool mlp_on(const iblbm_ibm_args&) { return false; }
+inline bool mlp_on(const iblbm_ibm32_args& a)
+{
+    return a.mlp_mode != 0 && a.method == IBM_MDF && !a.mdf_coupled;
+}
+
 
 // Shared-memory layout.  The "static" block (everything a fixed body keeps
 // between steps) is contiguous so that one bulk copy restores it.
@@ -610,6 +625,92 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             for (int k = 0; k < S; ++k) Rl += sh.bro[hb[k]] * (hwx[k / SW] * hwy[k % SW]);
             sh.R_[lo] = Rl;
         }
+        // ---- learned warm start (FP32 form, one body) ---------------------------------
+        // Features of each marker before any correction; with bit 2 of mlp_mode the
+        // network predicts the marker's converged force sum_it omega Lf, which is
+        // spread and applied before the first iteration; with bit 1 the features
+        // and the force actually accumulated are written out as training pairs.
+        R mlp_gx = 0, mlp_gy = 0;
+        bool mlp_rec = false;
+        if constexpr (SHIFTED && !COUPLED) {
+            const int mode = a.mlp_mode;
+            mlp_rec = (mode & 1) != 0;
+            const bool warm = (mode & 2) != 0;
+            if (mode) {
+                float* mA = reinterpret_cast<float*>(smem_raw + Lay.total);
+                float* mB = mA + MLP_CHUNK * 64;
+                float* mY = mB + MLP_CHUNK * 64;
+                float* mGx = mY + MLP_CHUNK * 2;
+                float* mGy = mGx + Lb;
+                const float* Pm = a.mlp_params;
+                const float inv_u = 1.0f / a.mlp_uref;
+                for (int c0 = 0; c0 < Lb; c0 += MLP_CHUNK) {
+                    const int rows = min(MLP_CHUNK, Lb - c0);
+                    if (own && lo >= c0 && lo < c0 + rows) {
+                        float* row = mA + (lo - c0) * 64;
+                        float* grow = mlp_rec ? a.mlp_features + (size_t)lo * 64 : nullptr;
+                        auto put = [&](int i, float v) {
+                            if (grow) grow[i] = v;
+                            if (warm) row[i] = (v - __ldg(Pm + i)) * __ldg(Pm + 64 + i);
+                        };
+                        R ux = 0, uy = 0;
+#pragma unroll
+                        for (int k = 0; k < S; ++k) {
+                            const R w = hwx[k / SW] * hwy[k % SW];
+                            const R bx = sh.bwx[hb[k]], by = sh.bwy[hb[k]];
+                            ux += bx * w;
+                            uy += by * w;
+                            put(2 + 2 * k, bx * inv_u);
+                            put(3 + 2 * k, by * inv_u);
+                        }
+                        for (int k = S; k < 25; ++k) { put(2 + 2 * k, 0.0f); put(3 + 2 * k, 0.0f); }
+                        put(0, (dvx - ux) * inv_u);
+                        put(1, (dvy - uy) * inv_u);
+                        double x, y;
+                        if (a.xt_table) { x = a.Lx_c[lo] - a.xt_table[s_step]; y = a.Ly_c[lo]; }
+                        else { x = a.Lx[lo]; y = a.Ly[lo]; }
+                        put(52, (float)(x / dx - floor(x / dx + 0.5)));
+                        put(53, (float)(y / dy - floor(y / dy + 0.5)));
+                        const int p = sh.part[lo], m0 = a.moff[p], m1 = a.moff[p + 1];
+                        float sn, cs;
+                        sincosf(6.283185307179586f * (float)(lo - m0) / (float)max(m1 - m0, 1), &sn, &cs);
+                        put(54, cs);
+                        put(55, sn);
+                        put(56, A == 2 ? 1.0f : 0.0f);
+                        put(57, a.mlp_re * 0.01f);
+                        put(58, (Rl - 1.0f) * 100.0f);
+                        for (int i = 59; i < 64; ++i) put(i, 0.0f);
+                    }
+                    __syncthreads();
+                    if (warm) {
+                        mlp_forward_tile(Pm, mA, mB, mY, rows);
+                        if (own && lo >= c0 && lo < c0 + rows) {
+                            mGx[lo] = mY[(lo - c0) * 2] / __ldg(Pm + 128);
+                            mGy[lo] = mY[(lo - c0) * 2 + 1] / __ldg(Pm + 129);
+                        }
+                        __syncthreads();
+                    }
+                }
+                if (warm) {
+                    // spread the predicted forces and correct the working velocity
+#pragma unroll
+                    for (int jn = 0; jn < NPT; ++jn) {
+                        const int b = tid + jn * IBM_THREADS;
+                        if (b < nb) {
+                            R tx, ty;
+                            spread2(sh, mGx, mGy, sh.cstart[b], sh.cstart[b + 1], tx, ty);
+                            ftx[jn] += tx;
+                            fty[jn] += ty;
+                            sh.bwx[b] += tx * vs[jn];
+                            sh.bwy[b] += ty * vs[jn];
+                        }
+                    }
+                    if (own) { mlp_gx = mGx[lo]; mlp_gy = mGy[lo]; }
+                    __syncthreads();
+                }
+            }
+        }
+        R lfx = 0, lfy = 0;
         const int min_iter = max(1, min(a.mdf_min_iterations, a.mdf_iterations));
         double omega_d = a.mdf_omega, omega_min = 0.0;
         if (COUPLED) {
@@ -649,8 +750,10 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 R fx, fy;
                 if (incomp) { fx = (R)2 * (dvx - ux); fy = (R)2 * (dvy - uy); }
                 else { fx = (R)2 * Rl * (dvx - ux); fy = (R)2 * Rl * (dvy - uy); }
-                sh.Lfx[lo] = unit_dt ? fx : fx / dt;
-                sh.Lfy[lo] = unit_dt ? fy : fy / dt;
+                lfx = unit_dt ? fx : fx / dt;
+                lfy = unit_dt ? fy : fy / dt;
+                sh.Lfx[lo] = lfx;
+                sh.Lfy[lo] = lfy;
             }
             if (!COUPLED) {
                 const double v = warp_nanmax(rl);
@@ -692,6 +795,10 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 }
                 prev = residual;
                 continue;
+            }
+            if (mlp_rec && own) {
+                mlp_gx += omega * lfx;
+                mlp_gy += omega * lfy;
             }
             // phase B: spread, relax, update the working velocity of the owned nodes
 #pragma unroll
@@ -764,6 +871,12 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             a.stats[3] = guard;
             a.dstats[0] = last;
             a.dstats[1] = omega_d;
+        }
+        if constexpr (SHIFTED && !COUPLED) {
+            if (mlp_rec && own) {
+                a.mlp_targets[2 * lo] = mlp_gx;
+                a.mlp_targets[2 * lo + 1] = mlp_gy;
+            }
         }
     } else if (METHOD == IBM_DFC) {
         // iblbm/ibm/dfc.py: compute_lambda (126-186) unless cached, interpolate_f
@@ -897,6 +1010,26 @@ static cudaError_t launch_ibm(const ARGS& a, const BCP& bc, size_t smem, void* s
     return cudaGetLastError();
 }
 
+// Dynamic shared memory of one band step.
+template <typename R, class ARGS>
+static size_t ibm_smem(const ARGS& a)
+{
+    const int S = a.delta_type == 0 ? 25 : 9;
+    size_t t = make_layout<R>(a.lb_total, a.band_capacity, S).total;
+    if (mlp_on(a)) t += mlp_smem_bytes(a.lb_total);
+    return t;
+}
+
+inline bool mlp_args_ok(const iblbm_ibm_args&) { return true; }
+inline bool mlp_args_ok(const iblbm_ibm32_args& a)
+{
+    if (!mlp_on(a)) return true;
+    if (a.mlp_mode & ~3) return false;
+    if ((a.mlp_mode & 2) && !a.mlp_params) return false;
+    if ((a.mlp_mode & 1) && (!a.mlp_features || !a.mlp_targets)) return false;
+    return a.mlp_uref > 0.0f;
+}
+
 // Argument checks shared by both forms; returns IBLBM_OK or an error code.
 template <typename R, class ARGS>
 static int check_ibm_args(const ARGS* a)
@@ -916,8 +1049,8 @@ static int check_ibm_args(const ARGS* a)
         return IBLBM_E_ARG;
     if ((long long)a->lb_total * 32 >= (1LL << 31)) return IBLBM_E_ARG;
     if ((reinterpret_cast<uintptr_t>(a->list_cache) & 15) != 0) return IBLBM_E_ARG;  // bulk-copy source
-    const int S = a->delta_type == 0 ? 25 : 9;
-    if (make_layout<R>(a->lb_total, a->band_capacity, S).total > (size_t)IBM_SMEM_LIMIT) return IBLBM_E_CAPACITY;
+    if (ibm_smem<R>(*a) > (size_t)IBM_SMEM_LIMIT) return IBLBM_E_CAPACITY;
+    if (!mlp_args_ok(*a)) return IBLBM_E_ARG;
     if (a->method == IBM_MDF && a->lb_total > IBM_THREADS) return IBLBM_E_CAPACITY;
     return IBLBM_OK;
 }
@@ -927,8 +1060,7 @@ template <class ARGS, typename R, bool SHIFTED>
 static int dispatch_ibm(const ARGS* a, const BcOf<SHIFTED>& bc, void* stream)
 {
     using BCP = BcOf<SHIFTED>;
-    const int S = a->delta_type == 0 ? 25 : 9;
-    const size_t smem = make_layout<R>(a->lb_total, a->band_capacity, S).total;
+    const size_t smem = ibm_smem<R>(*a);
     const bool coupled = a->method == IBM_MDF && a->mdf_coupled;
     cudaError_t e = cudaErrorInvalidValue;
 #define IBLBM_LAUNCH(AR, M, C) e = launch_ibm<ARGS, BCP, ibm_step_kernel<ARGS, R, SHIFTED, AR, M, C>>(*a, bc, smem, stream)

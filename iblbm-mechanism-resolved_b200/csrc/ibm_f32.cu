@@ -42,8 +42,7 @@ extern "C" int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args* host_args, const
     for (int b = 0; b < n; ++b) {
         const int chk = check_ibm_args<float>(&host_args[b]);
         if (chk != IBLBM_OK) return chk;
-        const int S = host_args[b].delta_type == 0 ? 25 : 9;
-        smem = std::max(smem, make_layout<float>(host_args[b].lb_total, host_args[b].band_capacity, S).total);
+        smem = std::max(smem, ibm_smem<float>(host_args[b]));
     }
     auto K = ibm_batch_kernel<iblbm_ibm32_args, float, true>;
     static bool configured = false;

@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView, Case, Dense32Args, DenseArgs,
-                   Geom, IbmArgs, TILES, check, lib, ptr)
+                   Geom, Ibm32Args, IbmArgs, TILES, check, lib, ptr)
 from .physics import (history_increment, mdf_relaxation_factor, net_gravity, oscillation_table,
                       rigid_markers)
 from .state import initial_velocity, initialize
@@ -224,7 +224,7 @@ class Engine:
         self.d_dv.copy_(tt.as_tensor(np.ascontiguousarray(dv, dtype=np.float64).reshape(-1)))
 
     def _make_ibm_args(self, parity):
-        cfg, a = self.cfg, IbmArgs()
+        cfg, a = self.cfg, (Ibm32Args if self.f32 else IbmArgs)()
         a.g, a.c = self.geom, self.case
         a.method = IBM_IDS[self.method]
         a.delta_type = DELTA_IDS[cfg.delta_type]
@@ -264,6 +264,33 @@ class Engine:
         self.dense_full = [[self._make_dense_args(p, out, "full") for out in (False, True)] for p in (0, 1)]
         self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
         self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
+
+    def set_mlp(self, mode, net=None):
+        """Learned MDF warm start of the FP32 form (single-body MDF): mode bit 1
+        records each step's marker features and accumulated forces into
+        d_mlp_feat (Lb x 64) / d_mlp_targ (Lb x 2); bit 2 starts every MDF loop
+        from the forces that `net` (an iblbm_b200.learned.MdfNet) predicts."""
+        if not self.f32:
+            raise NotImplementedError("the learned warm start belongs to the FP32 form")
+        if mode and (self.method != "MDF" or self.P != 1):
+            raise NotImplementedError("the learned warm start covers single-body MDF")
+        if (mode & 2) and net is None:
+            raise ValueError("mode 2 needs a network")
+        torch = self.torch
+        if mode & 1 and not hasattr(self, "d_mlp_feat"):
+            self.d_mlp_feat = torch.zeros(self.Lb, 64, dtype=torch.float32, device=self.dev)
+            self.d_mlp_targ = torch.zeros(self.Lb, 2, dtype=torch.float32, device=self.dev)
+        self.mlp_net = net
+        cfg = self.cfg
+        uref = cfg.lattice_u if cfg.motion_type == "oscillating" else self.st.in_u
+        for a in self.ibm_args:
+            a.mlp_mode = int(mode)
+            a.mlp_uref = float(uref) if uref else 1.0
+            a.mlp_re = float(cfg.Re)
+            a.mlp_params = ptr(net.params) if (net is not None and mode & 2) else 0
+            a.mlp_features = ptr(self.d_mlp_feat) if mode & 1 else 0
+            a.mlp_targets = ptr(self.d_mlp_targ) if mode & 1 else 0
+        self.graphs = {}
 
     def set_tile(self, tile):
         """Tile shape of the FP32 whole-lattice/bulk pass (a key of

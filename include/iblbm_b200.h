@@ -263,6 +263,16 @@ typedef struct {
     double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
     int *stats;
     double *dstats;
+    /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
+     * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
+     * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,
+     * lb_total x 2); bit 2 predicts that force with the network in mlp_params
+     * (iblbm_mlp_param_count() floats) and starts the loop from it.  mlp_uref
+     * scales velocities (the inflow speed), mlp_re is the Reynolds number. */
+    int mlp_mode;
+    float mlp_uref, mlp_re;
+    const float *mlp_params;
+    float *mlp_features, *mlp_targets;
 } iblbm_ibm32_args;
 
 int iblbm_ibm_step_f32(const iblbm_ibm32_args *a, void *stream);
@@ -274,6 +284,23 @@ int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args *host_args, const iblbm_ibm3
                              void *stream);
 int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm32_smem_bytes(int lb_total, int band_capacity, int delta_type);
+
+/* ---- learned MDF warm start: the network's training and inference ---------
+ * A 64 -> 64 -> 64 -> 64 -> 2 ReLU MLP in FP32 whose parameter block holds the
+ * feature normalisation (mean, inverse scale), the target scales and the
+ * weights (layout in csrc/mlp.cuh).  No reference counterpart: the reference
+ * has no learned component. */
+int iblbm_mlp_param_count(void);
+/* y[n x 2] = network(x[n x 64]) in the targets' units. */
+int iblbm_mlp_infer(const float *params, const float *x, int n, float *y, void *stream);
+/* One training step on n samples (x[n x 64], t[n x 2]), mean squared error on
+ * the scaled targets.  grad (param_count floats) and *ticket must be zero on
+ * entry.  apply = 1: the last CTA applies Adam (step >= 1, learning rate lr;
+ * adam_m / adam_v: param_count floats each) and re-zeroes grad and ticket;
+ * apply = 0: the summed gradient is left in grad.  loss (optional, zeroed by
+ * the caller) receives the batch loss. */
+int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *grad, unsigned *ticket, const float *x,
+                         const float *t, int n, float lr, int step, float *loss, int apply, void *stream);
 
 /* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
 /* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */
