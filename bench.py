@@ -397,6 +397,76 @@ def measure_batch(b, K, W, dist, ws):
             "launches_per_step": 1 + 2 * len(b.kinds), "steps_done": b.engines[0].ttt - 1}
 
 
+def measure_learned(args, n_train=200, K=200):
+    """The learned MDF warm start on the single-case workload (FP32 form).
+
+    Plain MDF (the workload's 20 iterations per step) records n_train steps of
+    (features, accumulated force) pairs and its final slip residual; the
+    network is trained on them (GPU kernels); then two copies of that state
+    continue K steps, warm-started and plain, both iterating until the slip residual is
+    below the level plain MDF reached in 20 iterations (median over the last
+    50 training steps).  Reports both forms' step rate, mean iterations and
+    residual, and Cd against the FP64 form at the same step."""
+    import statistics
+    import torch
+    from iblbm_b200.autotune import tune_dense
+    from iblbm_b200.engine import Engine
+    from iblbm_b200.learned import MdfNet, collect
+    total = n_train + K + 8
+    cfg = workload_config(max_steps=total + 8)
+    cfg.mdf_min_iterations = 20
+    engs = {}
+    for name in ("warm", "plain"):
+        e = Engine(cfg, precision="f32")
+        tune_dense(e)
+        engs[name] = e
+    X, T, _ = collect(engs["warm"], n_train)
+    res = []
+    for _ in range(n_train):
+        engs["plain"].advance(1, outputs_last=False, use_graph=False)
+        res.append(float(engs["plain"].d_dstats[0].item()))
+    tol = statistics.median(res[-50:])
+    net = MdfNet(seed=0)
+    hist = net.fit(X, T, epochs=80, batch=512, lr=2e-3)
+    engs["warm"].set_mlp(mode=2, net=net)
+    out = {"train_pairs": int(X.shape[0]), "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
+           "tolerance": tol}
+    E = lambda: torch.cuda.Event(enable_timing=True)
+    for name, e in engs.items():
+        for a in e.ibm_args:
+            a.mdf_min_iterations = 1
+            a.mdf_tol = tol
+        e.graphs = {}
+        its, resid = [], []
+        ev = [(E(), E()) for _ in range(K)]
+        for k in range(K):
+            ev[k][0].record()
+            e._launch(False)
+            e.join()
+            ev[k][1].record()
+            its.append(e.d_stats[0].clone())
+            resid.append(e.d_dstats[0].clone())
+        torch.cuda.synchronize()
+        e.ttt += K
+        ms = sum(a.elapsed_time(b) for a, b in ev) / K
+        e.advance(1, outputs_last=True, use_graph=False)
+        torch.cuda.synchronize()
+        its = [int(x.item()) for x in its]
+        resid = [float(x.item()) for x in resid]
+        out[name] = {"mlups": e.N / (ms / 1e3) / 1e6, "ms_per_step": ms, "mean_iterations": statistics.mean(its),
+                     "max_residual": max(resid), "steps_at_tolerance": sum(r < tol for r in resid),
+                     "Cd": e.cd_cl()[0], "step": e.ttt - 1}
+    ref = Engine(cfg, precision="f64")
+    ref.advance(engs["warm"].ttt - 1, outputs_last=True)
+    torch.cuda.synchronize()
+    cd64 = ref.cd_cl()[0]
+    for name in ("warm", "plain"):
+        out[name]["cd_rel_err_vs_f64"] = abs(out[name]["Cd"] - cd64) / abs(cd64)
+    out["iterations_saved"] = out["plain"]["mean_iterations"] - out["warm"]["mean_iterations"]
+    out["speedup_vs_plain_fp32"] = out["warm"]["mlups"] / out["plain"]["mlups"]
+    return out
+
+
 def sweep_cd_check(cfgs, batch, steps):
     """Cd/Cl of every batched case against the FP64 plain form of the same case
     after the same number of steps (one case at a time)."""
@@ -438,6 +508,7 @@ def run_b200(args):
         sweep = {"cases": len(cfgs), "lattice_nodes": batch.N, "max_cd_rel_err_vs_f64": worst_cd,
                  "max_cl_err_vs_f64_rel_cd": worst_cl, "worst_case": max(rows, key=lambda r: r[5])[:4]}
         del batch
+    learned = measure_learned(args) if args.form == "chosen" else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -500,6 +571,8 @@ def run_b200(args):
     line["plain"] = summary(plain)
     line["plain"]["roofline_frac_bulk"] = plain["achieved"] / peak
     line["chosen_single_case"] = single_s
+    if learned:
+        line["learned_mdf_single_case"] = learned
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

@@ -53,7 +53,8 @@ class IbmArgs(ctypes.Structure):
                 ("excl_next", _vp), ("band_capacity", _i),
                 ("box_capacity", _i), ("band_fib", _vp), ("band_df", _vp), ("band_fib_part", _vp),
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
-                ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp)]
+                ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
+                ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee

@@ -63,14 +63,16 @@ struct Sten {
 
 __host__ __device__ inline size_t up16(size_t x) { return (x + 15) & ~size_t(15); }
 
-constexpr int MLP_CHUNK = MLP_RPT * IBM_THREADS / 64;  // markers per network tile (128)
+constexpr int MLP_CHUNK = IBM_THREADS / 4;  // markers per network tile (128)
 
 // Shared memory of the learned warm start, placed after the band layout: two
-// activation tiles, the outputs of a tile, and the predicted force per marker.
-__host__ __device__ inline size_t mlp_smem_bytes(int Lb)
+// activation tiles, the outputs of a tile, the predicted force per marker, and
+// the network's parameter block (restored by one bulk copy at kernel start).
+__host__ __device__ inline size_t mlp_act_bytes(int Lb)
 {
-    return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * 64 + 2 * MLP_CHUNK + 2 * (size_t)Lb));
+    return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * MLP_LD + 2 * MLP_CHUNK + 4 * (size_t)Lb));
 }
+__host__ __device__ inline size_t mlp_smem_bytes(int Lb) { return mlp_act_bytes(Lb) + sizeof(float) * MLP_NP; }
 inline bool mlp_on(const iblbm_ibm_args&) { return false; }
 inline bool mlp_on(const iblbm_ibm32_args& a)
 {
@@ -241,6 +243,25 @@ __device__ void band_moments(const ARGS& a, const Geom& g, const BCP& bc, int nb
     }
 }
 
+// Band moments of a reference-shaped call: density and velocity, or the
+// post-streaming populations, read from the caller's fields.
+template <class ARGS, typename R>
+__device__ void field_moments(const ARGS& a, int nb, Sm<R>& sh, R* bfs)
+{
+    const int s = a.field_ustride > 0 ? a.field_ustride : 1;
+    for (int b = threadIdx.x; b < nb; b += IBM_THREADS) {
+        const long long n = sh.nodes[b];
+        if (bfs) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) bfs[9 * (size_t)b + q] = a.field_fstar[9 * n + q];
+        } else {
+            sh.bro[b] = a.field_ro[n];
+            sh.bwx[b] = a.field_ux[n * s];
+            sh.bwy[b] = a.field_uy[n * s];
+        }
+    }
+}
+
 template <int A, typename R>
 __device__ __forceinline__ R wgt(const Sm<R>& sh, int l, int k)
 {
@@ -312,8 +333,24 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     const Layout Lay = make_layout<R>(Lb, NB, S);
     Sm<R> sh = carve<R>(smem_raw, Lay);
     __shared__ int s_nb, s_status, s_box[4], s_step;
-    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ __align__(8) uint64_t s_bar, s_wbar;
     const bool rebuild = a.rebuild || a.xt_table;
+    // an early return first waits (bounded) for the network copy in flight
+    auto drain_weights = [&]() {
+        if constexpr (SHIFTED && METHOD == IBM_MDF && !COUPLED) {
+            if (a.mlp_mode & 2) mbar_wait_bounded(&s_wbar, 0, TMA_WAIT_LIMIT);
+        }
+    };
+    if constexpr (SHIFTED && METHOD == IBM_MDF && !COUPLED) {
+        // the warm start's network: one bulk copy into shared memory, waited for
+        // just before its first use
+        if (tid == 0 && (a.mlp_mode & 2)) {
+            mbar_init(&s_wbar);
+            mbar_expect(&s_wbar, (uint32_t)(sizeof(float) * MLP_NP));
+            bulk_copy(smem_raw + Lay.total + mlp_act_bytes(Lb), a.mlp_params, (uint32_t)(sizeof(float) * MLP_NP),
+                      &s_wbar);
+        }
+    }
     if (tid == 0) {
         s_status = ST_OK;
         s_step = a.step_counter ? *a.step_counter : 0;
@@ -338,6 +375,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     __syncthreads();
     if (s_status != ST_OK) {
         if (tid == 0) a.stats[4] = s_status;
+        drain_weights();
         return;
     }
     const double dx = a.dx, dy = a.dy;
@@ -436,6 +474,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 *a.band_count = 0;
                 a.box[0] = 0; a.box[1] = 0; a.box[2] = 0; a.box[3] = 0;
             }
+            drain_weights();
             return;
         }
         nb = total;
@@ -512,6 +551,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         __syncthreads();
         if (s_status != ST_OK) {
             if (tid == 0) a.stats[4] = s_status;
+            drain_weights();
             return;
         }
         nb = s_nb;
@@ -536,7 +576,9 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
 
     // ---- post-streaming populations and moments on the band ------------------------
     R* fs_keep = (METHOD == IBM_DFC) ? bfs : nullptr;
-    switch (a.c.bc) {
+    if (a.field_ro || a.field_fstar) {
+        field_moments(a, nb, sh, fs_keep);
+    } else switch (a.c.bc) {
     case BC_DIRICHLET_NEUMANN: band_moments<SHIFTED, BC_DIRICHLET_NEUMANN>(a, g, bc, nb, sh, fs_keep); break;
     case BC_OPEN: band_moments<SHIFTED, BC_OPEN>(a, g, bc, nb, sh, fs_keep); break;
     case BC_SETTLING: band_moments<SHIFTED, BC_SETTLING>(a, g, bc, nb, sh, fs_keep); break;
@@ -638,40 +680,58 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             const bool warm = (mode & 2) != 0;
             if (mode) {
                 float* mA = reinterpret_cast<float*>(smem_raw + Lay.total);
-                float* mB = mA + MLP_CHUNK * 64;
-                float* mY = mB + MLP_CHUNK * 64;
+                float* mB = mA + MLP_CHUNK * MLP_LD;
+                float* mY = mB + MLP_CHUNK * MLP_LD;
                 float* mGx = mY + MLP_CHUNK * 2;
                 float* mGy = mGx + Lb;
-                const float* Pm = a.mlp_params;
+                const float* Pm = reinterpret_cast<const float*>(smem_raw + Lay.total + mlp_act_bytes(Lb));
+                bool use_net = false;
+                if (warm) {
+                    // a copy that does not land leaves this step on plain MDF
+                    const bool ok = mbar_wait_bounded(&s_wbar, 0, TMA_WAIT_LIMIT);
+                    use_net = __syncthreads_and(ok) != 0;
+                }
                 const float inv_u = 1.0f / a.mlp_uref;
+                // every marker's slip first: the features include the neighbours' slips
+                float* mSx = mGy + Lb;
+                float* mSy = mSx + Lb;
+                if (own) {
+                    R ux = 0, uy = 0;
+#pragma unroll
+                    for (int k = 0; k < S; ++k) {
+                        const R w = hwx[k / SW] * hwy[k % SW];
+                        ux += sh.bwx[hb[k]] * w;
+                        uy += sh.bwy[hb[k]] * w;
+                    }
+                    mSx[lo] = (dvx - ux) * inv_u;
+                    mSy[lo] = (dvy - uy) * inv_u;
+                }
+                __syncthreads();
                 for (int c0 = 0; c0 < Lb; c0 += MLP_CHUNK) {
                     const int rows = min(MLP_CHUNK, Lb - c0);
                     if (own && lo >= c0 && lo < c0 + rows) {
-                        float* row = mA + (lo - c0) * 64;
+                        float* row = mA + (lo - c0) * MLP_LD;
                         float* grow = mlp_rec ? a.mlp_features + (size_t)lo * 64 : nullptr;
                         auto put = [&](int i, float v) {
                             if (grow) grow[i] = v;
-                            if (warm) row[i] = (v - __ldg(Pm + i)) * __ldg(Pm + 64 + i);
+                            if (use_net) row[i] = (v - Pm[i]) * Pm[64 + i];
                         };
-                        R ux = 0, uy = 0;
 #pragma unroll
                         for (int k = 0; k < S; ++k) {
-                            const R w = hwx[k / SW] * hwy[k % SW];
-                            const R bx = sh.bwx[hb[k]], by = sh.bwy[hb[k]];
-                            ux += bx * w;
-                            uy += by * w;
-                            put(2 + 2 * k, bx * inv_u);
-                            put(3 + 2 * k, by * inv_u);
+                            put(2 + 2 * k, sh.bwx[hb[k]] * inv_u);
+                            put(3 + 2 * k, sh.bwy[hb[k]] * inv_u);
                         }
                         for (int k = S; k < 25; ++k) { put(2 + 2 * k, 0.0f); put(3 + 2 * k, 0.0f); }
-                        put(0, (dvx - ux) * inv_u);
-                        put(1, (dvy - uy) * inv_u);
+                        put(0, mSx[lo]);
+                        put(1, mSy[lo]);
                         double x, y;
                         if (a.xt_table) { x = a.Lx_c[lo] - a.xt_table[s_step]; y = a.Ly_c[lo]; }
                         else { x = a.Lx[lo]; y = a.Ly[lo]; }
                         put(52, (float)(x / dx - floor(x / dx + 0.5)));
                         put(53, (float)(y / dy - floor(y / dy + 0.5)));
                         const int p = sh.part[lo], m0 = a.moff[p], m1 = a.moff[p + 1];
+                        const int nm = max(m1 - m0, 1);
+                        const int lp = m0 + (lo - m0 + 1) % nm, lm = m0 + (lo - m0 + nm - 1) % nm;
                         float sn, cs;
                         sincosf(6.283185307179586f * (float)(lo - m0) / (float)max(m1 - m0, 1), &sn, &cs);
                         put(54, cs);
@@ -679,19 +739,24 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                         put(56, A == 2 ? 1.0f : 0.0f);
                         put(57, a.mlp_re * 0.01f);
                         put(58, (Rl - 1.0f) * 100.0f);
-                        for (int i = 59; i < 64; ++i) put(i, 0.0f);
+                        // slips of the two neighbouring markers on the body
+                        put(59, mSx[lp]);
+                        put(60, mSy[lp]);
+                        put(61, mSx[lm]);
+                        put(62, mSy[lm]);
+                        put(63, 0.0f);
                     }
                     __syncthreads();
-                    if (warm) {
-                        mlp_forward_tile(Pm, mA, mB, mY, rows);
+                    if (use_net) {
+                        mlp_forward_tile<IBM_THREADS>(Pm, mA, mB, mY, rows);
                         if (own && lo >= c0 && lo < c0 + rows) {
-                            mGx[lo] = mY[(lo - c0) * 2] / __ldg(Pm + 128);
-                            mGy[lo] = mY[(lo - c0) * 2 + 1] / __ldg(Pm + 129);
+                            mGx[lo] = mY[(lo - c0) * 2] / Pm[128];
+                            mGy[lo] = mY[(lo - c0) * 2 + 1] / Pm[129];
                         }
                         __syncthreads();
                     }
                 }
-                if (warm) {
+                if (use_net) {
                     // spread the predicted forces and correct the working velocity
 #pragma unroll
                     for (int jn = 0; jn < NPT; ++jn) {
@@ -1025,7 +1090,7 @@ inline bool mlp_args_ok(const iblbm_ibm32_args& a)
 {
     if (!mlp_on(a)) return true;
     if (a.mlp_mode & ~3) return false;
-    if ((a.mlp_mode & 2) && !a.mlp_params) return false;
+    if ((a.mlp_mode & 2) && (!a.mlp_params || (reinterpret_cast<uintptr_t>(a.mlp_params) & 15))) return false;
     if ((a.mlp_mode & 1) && (!a.mlp_features || !a.mlp_targets)) return false;
     return a.mlp_uref > 0.0f;
 }
@@ -1034,7 +1099,11 @@ inline bool mlp_args_ok(const iblbm_ibm32_args& a)
 template <typename R, class ARGS>
 static int check_ibm_args(const ARGS* a)
 {
-    if (!a || !a->moff || a->n_particles < 1 || a->n_particles > MAXP || a->lb_total < 1 || !a->fpost_prev ||
+    if (!a) return IBLBM_E_ARG;
+    const bool fields = a->field_ro || a->field_fstar;
+    if (fields && (a->method == IBM_DFC ? !a->field_fstar : (!a->field_ro || !a->field_ux || !a->field_uy)))
+        return IBLBM_E_ARG;
+    if (!a->moff || a->n_particles < 1 || a->n_particles > MAXP || a->lb_total < 1 || (!a->fpost_prev && !fields) ||
         !a->box || !a->map || !a->band_nodes || !a->band_count || !a->scratch || !a->iscratch || !a->stats ||
         !a->dstats || !a->larea || !a->list_cache)
         return IBLBM_E_ARG;
@@ -1044,7 +1113,7 @@ static int check_ibm_args(const ARGS* a)
     if (a->method == IBM_DFC && (!a->band_df || !a->lambda || a->n_particles != 1)) return IBLBM_E_ARG;
     if (!a->xt_table && (!a->Lx || !a->Ly || !a->dvel)) return IBLBM_E_ARG;
     if (a->xt_table && (!a->Lx_c || !a->Ly_c || !a->step_counter || a->xt_len < 1)) return IBLBM_E_ARG;
-    if ((a->c.bc == BC_OPEN || a->c.bc == BC_VELOCITY_INLET) && !a->uring_prev) return IBLBM_E_ARG;
+    if (!fields && (a->c.bc == BC_OPEN || a->c.bc == BC_VELOCITY_INLET) && !a->uring_prev) return IBLBM_E_ARG;
     if (a->band_capacity < 1 || a->band_capacity > MAX_BAND || a->g.nx < 4 || a->g.ny < 4)
         return IBLBM_E_ARG;
     if ((long long)a->lb_total * 32 >= (1LL << 31)) return IBLBM_E_ARG;

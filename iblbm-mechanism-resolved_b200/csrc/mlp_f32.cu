@@ -15,12 +15,13 @@ namespace iblbm {
 constexpr int TRAIN_ROWS = 64;
 constexpr int TRAIN_THREADS = 256;
 constexpr int INFER_THREADS = 512;
-constexpr int INFER_ROWS = MLP_RPT * INFER_THREADS / 64;  // 128
+constexpr int INFER_ROWS = INFER_THREADS / 4;  // 128
 constexpr float ADAM_B1 = 0.9f, ADAM_B2 = 0.999f, ADAM_EPS = 1e-8f;
 
 // Smem layout of the training kernel (floats): A0..A3 activations, two delta
 // buffers, the staged weight matrix (row stride 65), outputs and output deltas.
-constexpr int TR_A = TRAIN_ROWS * 64;
+static_assert(TRAIN_ROWS == TRAIN_THREADS / 4, "one layer tile per CTA");
+constexpr int TR_A = TRAIN_ROWS * MLP_LD;
 constexpr size_t TRAIN_SMEM = sizeof(float) * (size_t)(4 * TR_A + 2 * TR_A + 64 * 65 + 2 * TRAIN_ROWS * 2);
 
 // Normalised input tile: rows beyond n are zero.
@@ -29,7 +30,7 @@ __device__ __forceinline__ void load_inputs(const float* __restrict__ P, const f
 {
     for (int e = threadIdx.x; e < nrows_tile * 64; e += blockDim.x) {
         const int m = e >> 6, i = e & 63;
-        a[e] = m < rows ? (X[(size_t)(r0 + m) * 64 + i] - __ldg(P + i)) * __ldg(P + 64 + i) : 0.0f;
+        a[m * MLP_LD + i] = m < rows ? (X[(size_t)(r0 + m) * 64 + i] - __ldg(P + i)) * __ldg(P + 64 + i) : 0.0f;
     }
 }
 
@@ -41,15 +42,15 @@ __device__ __forceinline__ void grad_w64(const float* A, const float* D, float* 
 #pragma unroll
     for (int k = 0; k < 16; ++k) acc[k] = 0.0f;
     for (int m = 0; m < TRAIN_ROWS; ++m) {
-        const float d = D[m * 64 + o];
+        const float d = D[m * MLP_LD + o];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) acc[k] += A[m * 64 + g + k * G] * d;
+        for (int k = 0; k < 16; ++k) acc[k] += A[m * MLP_LD + g + k * G] * d;
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) atomicAdd(gW + (g + k * G) * 64 + o, acc[k]);
     if (threadIdx.x < 64) {
         float s = 0.0f;
-        for (int m = 0; m < TRAIN_ROWS; ++m) s += D[m * 64 + threadIdx.x];
+        for (int m = 0; m < TRAIN_ROWS; ++m) s += D[m * MLP_LD + threadIdx.x];
         atomicAdd(gb + threadIdx.x, s);
     }
 }
@@ -67,12 +68,12 @@ __device__ __forceinline__ void backprop64(const float* __restrict__ W, float* s
     for (int o = 0; o < 64; ++o) {
         const float w = sW[i * 65 + o];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) acc[k] += Dout[(g + k * G) * 64 + o] * w;
+        for (int k = 0; k < 16; ++k) acc[k] += Dout[(g + k * G) * MLP_LD + o] * w;
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         const int m = g + k * G;
-        Din[m * 64 + i] = A[m * 64 + i] > 0.0f ? acc[k] : 0.0f;
+        Din[m * MLP_LD + i] = A[m * MLP_LD + i] > 0.0f ? acc[k] : 0.0f;
     }
     __syncthreads();
 }
@@ -99,11 +100,11 @@ __global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restr
     const int r0 = blockIdx.x * TRAIN_ROWS, rows = min(TRAIN_ROWS, n - r0);
     load_inputs(P, X, r0, rows, TRAIN_ROWS, A0);
     __syncthreads();
-    mlp_layer64(P + MLP_W1, P + MLP_B1, A0, A1, TRAIN_ROWS, true);
+    mlp_layer64<TRAIN_THREADS>(P + MLP_W1, P + MLP_B1, A0, A1, true);
     __syncthreads();
-    mlp_layer64(P + MLP_W2, P + MLP_B2, A1, A2, TRAIN_ROWS, true);
+    mlp_layer64<TRAIN_THREADS>(P + MLP_W2, P + MLP_B2, A1, A2, true);
     __syncthreads();
-    mlp_layer64(P + MLP_W3, P + MLP_B3, A2, A3, TRAIN_ROWS, true);
+    mlp_layer64<TRAIN_THREADS>(P + MLP_W3, P + MLP_B3, A2, A3, true);
     __syncthreads();
     mlp_layer_out(P, A3, Y, TRAIN_ROWS);
     __syncthreads();
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restr
     for (int e = threadIdx.x; e < 64 * 2; e += blockDim.x) {
         const int i = e >> 1, o = e & 1;
         float s = 0.0f;
-        for (int m = 0; m < TRAIN_ROWS; ++m) s += A3[m * 64 + i] * D4[m * 2 + o];
+        for (int m = 0; m < TRAIN_ROWS; ++m) s += A3[m * MLP_LD + i] * D4[m * 2 + o];
         atomicAdd(grad + MLP_W4 + e, s);
     }
     if (threadIdx.x < 2) {
@@ -137,10 +138,10 @@ __global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restr
         for (int m = 0; m < TRAIN_ROWS; ++m) s += D4[m * 2 + threadIdx.x];
         atomicAdd(grad + MLP_B4 + threadIdx.x, s);
     }
-    for (int e = threadIdx.x; e < TR_A; e += blockDim.x) {
+    for (int e = threadIdx.x; e < TRAIN_ROWS * 64; e += blockDim.x) {
         const int m = e >> 6, i = e & 63;
         const float s = __ldg(P + MLP_W4 + i * 2) * D4[m * 2] + __ldg(P + MLP_W4 + i * 2 + 1) * D4[m * 2 + 1];
-        Da[e] = A3[e] > 0.0f ? s : 0.0f;
+        Da[m * MLP_LD + i] = A3[m * MLP_LD + i] > 0.0f ? s : 0.0f;
     }
     __syncthreads();
     grad_w64(A2, Da, grad + MLP_W3, grad + MLP_B3);
@@ -176,12 +177,12 @@ __global__ void __launch_bounds__(INFER_THREADS) mlp_infer_kernel(const float* _
 {
     extern __shared__ __align__(16) float sm[];
     float* a = sm;
-    float* b = a + INFER_ROWS * 64;
-    float* y = b + INFER_ROWS * 64;
+    float* b = a + INFER_ROWS * MLP_LD;
+    float* y = b + INFER_ROWS * MLP_LD;
     const int r0 = blockIdx.x * INFER_ROWS, rows = min(INFER_ROWS, n - r0);
     load_inputs(P, X, r0, rows, INFER_ROWS, a);
     __syncthreads();
-    mlp_forward_tile(P, a, b, y, rows);
+    mlp_forward_tile<INFER_THREADS>(P, a, b, y, rows);
     for (int e = threadIdx.x; e < rows * 2; e += blockDim.x) Yout[(size_t)r0 * 2 + e] = y[e] / __ldg(P + 128 + (e & 1));
 }
 
@@ -195,7 +196,7 @@ extern "C" int iblbm_mlp_infer(const float* params, const float* x, int n, float
 {
     if (!params || !x || !y || n < 0) return IBLBM_E_ARG;
     if (n == 0) return IBLBM_OK;
-    const size_t smem = sizeof(float) * (size_t)(2 * INFER_ROWS * 64 + INFER_ROWS * 2);
+    const size_t smem = sizeof(float) * (size_t)(2 * INFER_ROWS * MLP_LD + INFER_ROWS * 2);
     static bool configured = false;
     if (!configured) {
         if (cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=

@@ -41,6 +41,22 @@ def _torch():
     return torch
 
 
+def band_capacity(Lx, Ly, dx, dy, nx, ny, delta_type):
+    """Band capacity for markers (Lx, Ly) in domain units: 1.5 x the number of
+    distinct stencil nodes plus 256, within [1, min(Lb * S, 2048)] (S stencil
+    slots per marker; 2048 is the band kernel's limit)."""
+    a = DELTA_RADIUS[delta_type]
+    S = (2 * a + 1) ** 2
+    Lx, Ly = np.asarray(Lx, dtype=np.float64), np.asarray(Ly, dtype=np.float64)
+    ix0 = np.floor(Lx / dx + 0.5).astype(np.int64)
+    iy0 = np.floor(Ly / dy + 0.5).astype(np.int64)
+    off = np.arange(-a, a + 1)
+    ii = np.clip(ix0[:, None, None] + off[None, :, None], 0, nx - 1)
+    jj = np.clip(iy0[:, None, None] + off[None, None, :], 0, ny - 1)
+    n0 = len(np.unique((jj * nx + ii).ravel()))
+    return int(min(max(1, int(1.5 * n0) + 256), len(Lx) * S, 2048))
+
+
 class Engine:
     """One lattice case on one GPU: FP64 form (the reference's arithmetic) or
     the shifted FP32 form (``precision="f32"``)."""
@@ -180,22 +196,13 @@ class Engine:
         self.last_out_step = 0
 
     def _band_capacity(self, S):
-        """Band capacity from the initial markers: 1.5 x the number of distinct
-        stencil nodes plus 256, within [1, min(Lb*S, 4096)]."""
-        st, cfg = self.st, self.cfg
+        st = self.st
         if st.particles is not None:
             Lx = np.concatenate([p.Lx for p in st.particles])
             Ly = np.concatenate([p.Ly for p in st.particles])
         else:
             Lx, Ly = st.Lx, st.Ly
-        a = DELTA_RADIUS[cfg.delta_type]
-        ix0 = np.floor(Lx / st.dx + 0.5).astype(np.int64)
-        iy0 = np.floor(Ly / st.dy + 0.5).astype(np.int64)
-        off = np.arange(-a, a + 1)
-        ii = np.clip(ix0[:, None, None] + off[None, :, None], 0, st.nx - 1)
-        jj = np.clip(iy0[:, None, None] + off[None, None, :], 0, st.ny - 1)
-        n0 = len(np.unique((jj * st.nx + ii).ravel()))
-        return int(min(max(1, int(1.5 * n0) + 256), self.Lb * S, 4096))
+        return band_capacity(Lx, Ly, st.dx, st.dy, st.nx, st.ny, self.cfg.delta_type)
 
     # ------------------------------------------------------------------------------
     def _collide_aos(self, fstar, feq, U, fib, out):

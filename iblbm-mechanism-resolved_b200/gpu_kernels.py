@@ -95,3 +95,124 @@ def velocity_correction_gpu(U, fib, ro, dt, incompressible=False):
     fib, ro = _dev(fib, "fib"), _dev(ro, "ro")
     check(lib().iblbm_velocity_correction(ptr(U), ptr(fib), ptr(ro), U.shape[0], float(dt),
                                           int(bool(incompressible)), _stream(U)), "velocity_correction_gpu")
+
+
+# ---- immersed boundary: reference-shaped wrappers over the band kernel ---------
+_DELTA_TYPE_IDS = {"peskin4pt": 0, "hat": 1}
+_DELTA_STENCIL_A = {"peskin4pt": 2, "hat": 1}
+
+
+def _band_call(method, Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_type, incompressible,
+               ro=None, ux=None, uy=None, ustride=1, fstar=None, lambda_k=None):
+    """One band-kernel launch on caller-given fields (iblbm_ibm_step_f64 with
+    field_*): returns the band's node list and outputs."""
+    import numpy as np
+    from ._lib import DELTA_IDS, IBM_IDS, Case, Geom, IbmArgs
+    from .engine import band_capacity
+    torch = _t()
+    L = lib()
+    Lx, Ly = _dev(Lx, "Lx"), _dev(Ly, "Ly")
+    dev = Lx.device
+    Lb = int(Lx.numel())
+    N = nx * ny
+    B = band_capacity(Lx.cpu().numpy(), Ly.cpu().numpy(), dx, dy, nx, ny, delta_type)
+    i32, f64 = torch.int32, torch.float64
+    z = lambda n, dt=f64: torch.zeros(max(int(n), 1), dtype=dt, device=dev)
+    dv = _dev(desired_vel, "desired_vel").reshape(-1) if desired_vel is not None else z(2 * Lb)
+    delta = DELTA_IDS[delta_type]
+    c = Case()
+    c.collision, c.bc, c.incompressible, c.tau, c.dt, c.dens = 0, 0, int(bool(incompressible)), 1.0, float(dt), 1.0
+    a = IbmArgs()
+    a.g = Geom(nx, ny, (nx + 31) // 32 * 32, ((nx + 31) // 32 * 32) * ny)
+    a.c = c
+    a.method, a.delta_type, a.rebuild, a.n_particles, a.lb_total = IBM_IDS[method], delta, 1, 1, Lb
+    keep = {}
+    keep["moff"] = torch.tensor([0, Lb], dtype=i32, device=dev)
+    keep["larea"] = torch.tensor([float(Larea)], dtype=f64, device=dev)
+    keep["map"] = torch.full((N,), -1, dtype=i32, device=dev)
+    for k, n, dt_ in (("box", 4, i32), ("nodes", B, i32), ("count", 1, i32), ("stats", 5, i32), ("dstats", 2, f64),
+                      ("fib", 2 * B, f64), ("df", 9 * B, f64), ("Lux", Lb, f64), ("Luy", Lb, f64),
+                      ("Lfx", Lb, f64), ("Lfy", Lb, f64), ("force", 2 * Lb, f64), ("valid", 1, i32)):
+        keep[k] = z(n, dt_)
+    keep["lam"] = _dev(lambda_k, "lambda_k").clone() if lambda_k is not None else z(Lb)
+    keep["scr"] = z(L.iblbm_ibm_scratch_doubles(Lb, B, 1))
+    keep["iscr"] = z(L.iblbm_ibm_scratch_ints(Lb, B, delta), i32)
+    keep["lists"] = z(L.iblbm_ibm_list_cache_ints(Lb, B, delta), i32)
+    a.moff, a.Lx, a.Ly, a.dvel, a.larea = (ptr(x) for x in (keep["moff"], Lx, Ly, dv, keep["larea"]))
+    a.dx, a.dy = float(dx), float(dy)
+    a.lambda_, a.lambda_valid = ptr(keep["lam"]), ptr(keep["valid"])
+    if lambda_k is not None:
+        keep["valid"].fill_(1)
+        a.dfc_cache_lambda = 1
+    a.correction_scale = 1.0
+    a.box, a.map, a.band_nodes, a.band_count = (ptr(keep[k]) for k in ("box", "map", "nodes", "count"))
+    a.list_cache = ptr(keep["lists"])
+    a.band_capacity, a.box_capacity = B, N
+    a.band_fib, a.band_df, a.scratch, a.iscratch = (ptr(keep[k]) for k in ("fib", "df", "scr", "iscr"))
+    a.Lux, a.Luy, a.Lfx, a.Lfy, a.dfc_force = (ptr(keep[k]) for k in ("Lux", "Luy", "Lfx", "Lfy", "force"))
+    a.stats, a.dstats = ptr(keep["stats"]), ptr(keep["dstats"])
+    if fstar is not None:
+        keep["fstar"] = _dev(fstar, "fstar")
+        a.field_fstar = ptr(keep["fstar"])
+    else:
+        keep["ro"], keep["ux"], keep["uy"] = ro, ux, uy
+        a.field_ro, a.field_ux, a.field_uy, a.field_ustride = ptr(ro), ptr(ux), ptr(uy), int(ustride)
+    check(L.iblbm_ibm_step_f64(ctypes.byref(a), _stream(Lx)), "iblbm_ibm_step_f64")
+    st = int(keep["stats"][4].item())
+    if st != 0:
+        raise RuntimeError(f"band kernel status {st}")
+    nb = int(keep["count"].item())
+    keep["nb"] = nb
+    keep["nodes_l"] = keep["nodes"][:nb].long()
+    return keep
+
+
+def ibm_direct_forcing_gpu(Lx, Ly, desired_vel, Eux, Euy, Ro, dx, dy, dt, Larea, ny, nx, delta_type="peskin4pt",
+                           return_interp_vel=False, incompressible=False):
+    """Direct forcing — replaces gpu_kernels.py:956-1042 (<- ibm/df.py:37-154).
+    Eux, Euy, Ro: (ny, nx) or (N,); returns fib (N, 2) [, Lux, Luy].  Sums run
+    in the reference CPU path's order, so results are bit-identical to it."""
+    Eux, Euy, Ro = (_dev(x, n).reshape(-1) for x, n in ((Eux, "Eux"), (Euy, "Euy"), (Ro, "Ro")))
+    k = _band_call("DF", Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_type, incompressible,
+                   ro=Ro, ux=Eux, uy=Euy)
+    torch = _t()
+    fib = torch.zeros(ny * nx, 2, dtype=torch.float64, device=Eux.device)
+    nb = k["nb"]
+    fib[k["nodes_l"]] = k["fib"][: 2 * nb].reshape(nb, 2)
+    if return_interp_vel:
+        return fib, k["Lux"], k["Luy"]
+    return fib
+
+
+def ibm_direct_forcing_fields_gpu(Lx, Ly, desired_vel, Eux, Euy, Ro, dx, dy, dt, Larea, ny, nx,
+                                  delta_type="peskin4pt", incompressible=False):
+    """Direct forcing returning the unpacked force fields — replaces
+    gpu_kernels.py:1045-1088: (Efx, Efy) as (ny, nx), Lux, Luy."""
+    fib, Lux, Luy = ibm_direct_forcing_gpu(Lx, Ly, desired_vel, Eux, Euy, Ro, dx, dy, dt, Larea, ny, nx, delta_type,
+                                           True, incompressible)
+    return fib[:, 0].reshape(ny, nx).contiguous(), fib[:, 1].reshape(ny, nx).contiguous(), Lux, Luy
+
+
+def compute_lambda_gpu(Lx, Ly, rho_f, Larea, dx, dy, ny, nx, delta_type):
+    """DFC lambda(k) = 1 / (2 rho_f ds W_sum(k)) — replaces gpu_kernels.py:1091-1141
+    (<- ibm/dfc.py:126-186).  Bit-identical to the reference for rho_f = 1 (the
+    solver's value); other rho_f divide the rho_f = 1 result."""
+    torch = _t()
+    fz = torch.zeros(ny * nx * 9, dtype=torch.float64, device=_dev(Lx, "Lx").device)
+    k = _band_call("DFC", Lx, Ly, None, dx, dy, 1.0, Larea, ny, nx, delta_type, False, fstar=fz)
+    lam = k["lam"][: Lx.numel()].clone()
+    return lam if float(rho_f) == 1.0 else lam / float(rho_f)
+
+
+def dfc_correction_gpu(Lx, Ly, desired_vel, fstar, lambda_k, dx, dy, Larea, ny, nx, delta_type, lattice=None):
+    """DFC distribution correction — replaces gpu_kernels.py:1144-1223
+    (<- ibm/dfc.py:55-253): returns (Ef_corr (N, 9), dfc_force (Lb, 2))."""
+    torch = _t()
+    fstar = _dev(fstar, "fstar")
+    k = _band_call("DFC", Lx, Ly, desired_vel, dx, dy, 1.0, Larea, ny, nx, delta_type, False,
+                   fstar=fstar.reshape(-1), lambda_k=lambda_k)
+    nb = k["nb"]
+    corr = torch.zeros(ny * nx, 9, dtype=torch.float64, device=fstar.device)
+    corr[k["nodes_l"]] = k["df"][: 9 * nb].reshape(nb, 9)
+    Lb = int(Lx.numel())
+    return corr, k["force"][: 2 * Lb].reshape(Lb, 2).clone()

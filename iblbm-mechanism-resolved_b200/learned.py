@@ -4,8 +4,10 @@ multi-direct-forcing force from its state before the first iteration.
 Per marker the band kernel forms 64 features (csrc/band_kernel.cuh): the slip
 velocity before any correction, the working velocities at its stencil nodes,
 its sub-node offset, its angular position on the body, the delta kernel, the
-Reynolds number and the interpolated density.  The target is the force the
-plain MDF loop applies to it in total, sum over iterations of omega * Lf.
+Reynolds number, the interpolated density and the slips of its two
+neighbouring markers.  The target is the force the plain MDF loop applies to
+it in total, sum over iterations of omega * Lf (``collect`` can run the loop
+past its usual limit to record forces closer to convergence).
 Training pairs come from plain MDF runs (``collect``); training and inference
 run on the GPU in this library's own kernels (``iblbm_mlp_train_step``: fused
 forward, backward and Adam in one launch; ``iblbm_mlp_infer``).  With the warm
@@ -42,7 +44,7 @@ class MdfNet:
             n = fan_in * fan_out
             p[off:off + n] = rng.standard_normal(n).astype(np.float32) * np.float32(np.sqrt(2.0 / fan_in))
             off += n + fan_out  # biases start at zero
-        assert off == self.NP
+        assert off <= self.NP  # the block is padded to a multiple of 4 floats
         self.params = torch.as_tensor(p, device=self.dev)
         self.m = torch.zeros(self.NP, dtype=torch.float32, device=self.dev)
         self.v = torch.zeros_like(self.m)
@@ -103,11 +105,18 @@ class MdfNet:
         return Y
 
 
-def collect(engine, steps):
+def collect(engine, steps, iterations=None):
     """Run `steps` timesteps of an FP32 MDF engine in plain MDF, recording each
-    marker's features and accumulated force every step.  Returns (X, T) as
-    device tensors of (steps * markers) rows and the MDF iteration counts."""
+    marker's features and accumulated force every step.  With `iterations` the
+    MDF loop runs exactly that many iterations during collection (far past the
+    usual limit, so the targets are the converged forces) and the engine's own
+    limits are restored afterwards.  Returns (X, T) as device tensors of
+    (steps * markers) rows and the MDF iteration counts."""
     torch = engine.torch
+    saved = [(a.mdf_iterations, a.mdf_min_iterations) for a in engine.ibm_args]
+    if iterations:
+        for a in engine.ibm_args:
+            a.mdf_iterations = a.mdf_min_iterations = int(iterations)
     engine.set_mlp(mode=1)
     X, T, its = [], [], []
     for _ in range(steps):
@@ -116,4 +125,6 @@ def collect(engine, steps):
         T.append(engine.d_mlp_targ.clone())
         its.append(int(engine.d_stats[0].item()))
     engine.set_mlp(mode=0)
+    for a, (n, m) in zip(engine.ibm_args, saved):
+        a.mdf_iterations, a.mdf_min_iterations = n, m
     return torch.cat(X), torch.cat(T), its

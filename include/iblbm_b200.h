@@ -150,6 +150,13 @@ typedef struct {
      * dstats: [last_residual, omega_used] */
     int *stats;
     double *dstats;
+    /* reference-shaped calls (iblbm/gpu_kernels.py:956-1223): the band takes
+     * its moments from the given fields instead of the lattice (fpost_prev and
+     * uring_prev unused).  DF / MDF read density field_ro[n] and velocity
+     * (field_ux[n * s], field_uy[n * s]), s = field_ustride, n = j*nx + i;
+     * DFC reads the post-streaming populations field_fstar[9n + q].  NULL: off. */
+    const double *field_ro, *field_ux, *field_uy, *field_fstar;
+    int field_ustride;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -263,6 +270,8 @@ typedef struct {
     double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
     int *stats;
     double *dstats;
+    const float *field_ro, *field_ux, *field_uy, *field_fstar;
+    int field_ustride;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,

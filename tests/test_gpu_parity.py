@@ -51,6 +51,33 @@ def test_reference_shaped_kernels(torch, units):
     np.testing.assert_array_equal(h(U2), Uo)
 
 
+@pytest.mark.parametrize("delta", ["hat", "peskin4pt"])
+def test_reference_shaped_ibm_wrappers(torch, units, delta):
+    """ibm_direct_forcing_gpu / compute_lambda_gpu / dfc_correction_gpu against
+    the reference's own outputs on its inputs (bit for bit)."""
+    from iblbm_b200 import gpu_kernels as gk
+    u = units
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    nx, ny, dx = int(u["i_nx"][0]), int(u["i_ny"][0]), float(u["i_dx"][0])
+    Lx, Ly, dv, La = d(u["i_Lx"]), d(u["i_Ly"]), d(u["i_dv"]), float(u["i_Larea"][0])
+    Eux, Euy, Ro = (d(u[k].ravel()) for k in ("i_Eux", "i_Euy", "i_Ro"))
+    for inc in (0, 1):
+        fib, Lux, Luy = gk.ibm_direct_forcing_gpu(Lx, Ly, dv, Eux, Euy, Ro, dx, dx, 1.0, La, ny, nx, delta, True,
+                                                  bool(inc))
+        k = f"df_{delta}_{inc}"
+        np.testing.assert_array_equal(fib.cpu().numpy(), u[k + "_fib"])
+        np.testing.assert_array_equal(Lux.cpu().numpy(), u[k + "_Lux"])
+        np.testing.assert_array_equal(Luy.cpu().numpy(), u[k + "_Luy"])
+    Efx, Efy, _, _ = gk.ibm_direct_forcing_fields_gpu(Lx, Ly, dv, Eux, Euy, Ro, dx, dx, 1.0, La, ny, nx, delta)
+    np.testing.assert_array_equal(Efx.cpu().numpy().ravel(), u[f"df_{delta}_0_fib"][:, 0])
+    lam = gk.compute_lambda_gpu(Lx, Ly, 1.0, La, dx, dx, ny, nx, delta)
+    np.testing.assert_array_equal(lam.cpu().numpy(), u[f"lam_{delta}"])
+    fstar = d(u[f"dfc_{delta}_fstar"])
+    corr, force = gk.dfc_correction_gpu(Lx, Ly, dv, fstar, lam, dx, dx, La, ny, nx, delta)
+    np.testing.assert_array_equal((fstar + corr).cpu().numpy(), u[f"dfc_{delta}_fc"])
+    np.testing.assert_allclose(force.cpu().numpy(), u[f"dfc_{delta}_force"], rtol=1e-13, atol=1e-18)
+
+
 def _cfg(kw):
     from iblbm_b200.config import SimConfig
     kw = dict(kw)
