@@ -53,6 +53,14 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_LU_F64 = 144
 BYTES_PER_LU_F32 = 72
+# DRAM bytes per updated node measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum within the kernel window, caches flushed before the
+# launch): FP32 batched bulk pass on the Re 20/40 part of the sweep (23.77 MB
+# read + 0.05 MB written for 642 962 nodes), FP64 single-case bulk pass (73.81
+# MB read + 25.93 MB written for 1 023 949 nodes).  Most population writes stay
+# in L2 until after the kernel, so the write share is a lower bound.
+TRAFFIC_PER_NODE_F32 = (23.77e6 + 0.05e6) / 642962
+TRAFFIC_PER_NODE_F64 = (73.81e6 + 25.93e6) / 1023949
 METRIC = "MLUPS and HBM GB/s (1 B200), chosen vs plain form at Cd within 0.1% of FP64"
 
 
@@ -544,7 +552,10 @@ def run_b200(args):
             "schedule": "one batched band launch + box passes (side stream) concurrent with one bulk launch per "
                         "kind of case; CUDA graph between outputs",
             "roofline": {"bound": "hbm", "achieved": bres["achieved"], "peak": peak, "unit": "GB/s",
-                         "frac": bres["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
+                         "frac": bres["achieved"] / peak,
+                         "traffic": TRAFFIC_PER_NODE_F32 * (sweep["lattice_nodes"] - bres["box_nodes"]),
+                         "traffic_unit": "bytes per step (all bulk launches), scaled from an ncu capture of the "
+                                         "36-case part of the sweep", "peak_kind": peak_kind,
                          "kernel": "dense32_batch_kernel bulk passes of all kinds (fused pull-stream+BC+macro+"
                                    "collide, FP32 shifted)", "bytes_per_lu": BYTES_PER_LU_F32,
                          "lattice_updates_per_step": bres and (sweep["lattice_nodes"] - bres["box_nodes"])},
@@ -560,7 +571,9 @@ def run_b200(args):
         line.update({"value": plain["value"], "ms_per_step": plain["ms_per_step"], "dtype": "f64",
                      "config": dict(WORKLOAD, form="FP64 plain", parallelism=f"replicas x{ws}"),
                      "roofline": {"bound": "hbm", "achieved": plain["achieved"], "peak": peak, "unit": "GB/s",
-                                  "frac": plain["achieved"] / peak, "traffic": None, "peak_kind": peak_kind,
+                                  "frac": plain["achieved"] / peak,
+                                  "traffic": TRAFFIC_PER_NODE_F64 * (N - plain["box_nodes"]),
+                                  "peak_kind": peak_kind,
                                   "kernel": "dense_step_kernel bulk pass (FP64)", "bytes_per_lu": BYTES_PER_LU_F64,
                                   "lattice_updates_per_launch": N - plain["box_nodes"]},
                      "e2e": {"value": plain["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": plain["e2e_h2d"],
