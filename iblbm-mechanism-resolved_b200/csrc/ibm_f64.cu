@@ -58,9 +58,9 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 // distribution corrections of the DFC path, and the list-building counters)
 // from a fixed array compiled into the library instead of from the caller.
 //
-// Limits: band_capacity <= 4096 nodes and lb_total <= 1024 markers; larger
+// Limits: band_capacity <= 2048 nodes and lb_total <= 1024 markers; larger
 // arguments return IBLBM_E_CAPACITY before anything is launched.  The array
-// (about 390 KB) lives on every GPU that loads the library until the process
+// (about 230 KB) lives on every GPU that loads the library until the process
 // exits.  All calls share it and it keeps the last call's contents (the kernel
 // clears the counters it needs zeroed), so two calls whose kernels overlap on
 // the GPU race on it: issue them on one stream, or order them.  The first call
@@ -69,7 +69,7 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 // caller still passes every input, output and persistent band array.
 // ---------------------------------------------------------------------------
 namespace iblbm {
-constexpr int NOALLOC_MAX_BAND = 4096;
+constexpr int NOALLOC_MAX_BAND = MAX_BAND;  // the band kernel's own limit (2048)
 constexpr int NOALLOC_MAX_MARKERS = 1024;
 constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_scratch[9 * NOALLOC_MAX_BAND + 9 * NOALLOC_MAX_MARKERS];

@@ -169,8 +169,8 @@ int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
  * (a host framework that owns all device allocations, or a service that
  * forbids cudaMalloc after start-up).  No counterpart in the reference.  The
  * scratch and iscratch fields of *a are ignored: the per-launch scratch comes
- * from a fixed array in the library (about 390 KB per GPU, held until exit).
- * Limits: band_capacity <= 4096, lb_total <= 1024, else IBLBM_E_CAPACITY.
+ * from a fixed array in the library (about 230 KB per GPU, held until exit).
+ * Limits: band_capacity <= 2048, lb_total <= 1024, else IBLBM_E_CAPACITY.
  * Calls share that array, so calls that overlap on the GPU race; the first
  * call on a device resolves the array's address and should precede any stream
  * capture.  Allocates nothing. */

@@ -37,6 +37,8 @@ def test_noalloc_rejects_sizes_beyond_its_capacity():
     a.lb_total = 10
     a.band_capacity = 4097
     assert L.iblbm_ibm_step_f64_noalloc(ctypes.byref(a), None) == -3
+    a.band_capacity = 2049  # above the band kernel's own limit
+    assert L.iblbm_ibm_step_f64_noalloc(ctypes.byref(a), None) == -3
     assert L.iblbm_ibm_step_f64_noalloc(None, None) == -1
 
 
