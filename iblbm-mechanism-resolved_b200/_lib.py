@@ -71,6 +71,15 @@ class Dense32Args(ctypes.Structure):
 
 TILES = {"pipe4x2": 0, "node": 1, "pipe8x2": 2, "rows2": 3, "rows4": 4}
 
+class ParticlesArgs(ctypes.Structure):
+    _fields_ = [("n_particles", _i), ("phase", _i), ("model", _i), ("fib_f32", _i), ("moff", _vp), ("Lx_c", _vp),
+                ("Ly_c", _vp), ("Lx", _vp), ("Ly", _vp), ("dvel", _vp), ("state", _vp), ("consts", _vp),
+                ("dt", _d), ("dx", _d), ("band_fib_part", _vp), ("band_count", _vp), ("band_capacity", _i),
+                ("forces_out", _vp)]
+
+
+INERTIA_IDS = {"none": 0, "explicit_history": 1, "feng_b2": 2}
+
 # entry point -> argtypes (all return int status)
 _SIGS = {
     "iblbm_dense_step_f64": [ctypes.POINTER(DenseArgs), _vp],
@@ -98,6 +107,7 @@ _SIGS = {
     "iblbm_ibm32_smem_bytes": [_i, _i, _i],
     "iblbm_to_shifted_f32": [_vp, Geom, _vp, _vp],
     "iblbm_from_shifted_f32": [_vp, Geom, _vp, _vp],
+    "iblbm_particles_step_f64": [ctypes.POINTER(ParticlesArgs), _vp],
     "iblbm_aos_to_soa": [_vp, Geom, _vp, _vp],
     "iblbm_soa_to_aos": [_vp, Geom, _vp, _vp],
 }

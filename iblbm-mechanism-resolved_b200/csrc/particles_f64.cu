@@ -1,0 +1,135 @@
+// particles_f64.cu — rigid-particle update of sedimentation runs on the device.
+//
+// The Velocity-Verlet Newton-Euler step of runtime/scenarios/sedimentation_multi.py
+// (:36-80 half step, :83-111 full step) for up to 8 discs, in FP64 without
+// multiply-add contraction, with the same scalar expressions as the host step:
+//   half  F = F_h + G;  v_half = v + (0.5 dt) F / m [+ 0.5 c (v - v_prev)];
+//         x_next = x + (dt v_half) dx;  markers X = R(0) (X_c - X_0) + x_next;
+//         desired velocity v_half
+//   full  F_h = -sum over the band of the particle's spread force;
+//         v_new = v_half + (0.5 dt) (F_h + G) / m [+ 0.5 c (v - v_prev)]
+//         [+ (1 / rho_ratio) (v - v_prev)];  v_prev = v;  v = v_new;  x = x_next
+// (c = pi r^2 / m for the explicit-history inertia model, physics/inertia/
+// explicit_history.py:53-66; the rho-ratio term for feng_b2, feng_b2.py:33-48).
+// One launch after the band kernel does the full step of this timestep and the
+// half step of the next, so the whole step stays on the device and can be
+// captured in a CUDA graph.  The force sum runs in a fixed order (per-thread
+// strided partial sums, then a fixed tree), so it is deterministic but not in
+// numpy's pairwise order: trajectories agree with the host step to round-off.
+#include <cstdint>
+#include "common.cuh"
+#include "../../include/iblbm_b200.h"
+
+namespace iblbm {
+
+constexpr int PART_THREADS = 256;
+constexpr int PART_MAXP = 8;
+
+template <typename F>
+__device__ void particle_forces(const iblbm_particles_args& a, const F* fib, double* s_force)
+{
+    __shared__ double red[2][PART_THREADS];
+    const int nb = *a.band_count;
+    const size_t pstride = 2 * (size_t)a.band_capacity;
+    for (int p = 0; p < a.n_particles; ++p) {
+        double sx = 0.0, sy = 0.0;
+        for (int b = threadIdx.x; b < nb; b += PART_THREADS) {
+            sx += (double)fib[p * pstride + 2 * b];
+            sy += (double)fib[p * pstride + 2 * b + 1];
+        }
+        red[0][threadIdx.x] = sx;
+        red[1][threadIdx.x] = sy;
+        __syncthreads();
+        for (int w = PART_THREADS / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) {
+                red[0][threadIdx.x] += red[0][threadIdx.x + w];
+                red[1][threadIdx.x] += red[1][threadIdx.x + w];
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            s_force[2 * p] = -red[0][0];
+            s_force[2 * p + 1] = -red[1][0];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_particles_args a)
+{
+    __shared__ double s_force[2 * PART_MAXP];
+    __shared__ double s_next[2 * PART_MAXP], s_vh[2 * PART_MAXP];
+    const int P = a.n_particles;
+    const double dt = a.dt, dx = a.dx;
+    if (a.phase & IBLBM_PARTICLES_FULL) {
+        if (a.fib_f32) particle_forces(a, static_cast<const float*>(a.band_fib_part), s_force);
+        else particle_forces(a, static_cast<const double*>(a.band_fib_part), s_force);
+        if (threadIdx.x < P) {
+            const int p = threadIdx.x;
+            double* s = a.state + IBLBM_PARTICLE_STATE * p;
+            const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
+            const double m = c[0], inv_rho = c[1], hc = c[2];
+            for (int d = 0; d < 2; ++d) {
+                const double F = s_force[2 * p + d] + c[3 + d];
+                double vn = s[6 + d] + ((0.5 * dt) * F) / m;
+                if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vn = vn + 0.5 * (hc * (s[2 + d] - s[4 + d]));
+                if (a.model == IBLBM_INERTIA_FENG_B2) vn = vn + inv_rho * (s[2 + d] - s[4 + d]);
+                s[4 + d] = s[2 + d];      // v_prev = v
+                s[2 + d] = vn;            // v
+                s[8 + d] = s_force[2 * p + d];
+                s[d] = s[10 + d];         // x = x_next
+                if (a.forces_out) a.forces_out[2 * p + d] = s_force[2 * p + d];
+            }
+        }
+        __syncthreads();
+    }
+    if (a.phase & IBLBM_PARTICLES_HALF) {
+        if (threadIdx.x < P) {
+            const int p = threadIdx.x;
+            double* s = a.state + IBLBM_PARTICLE_STATE * p;
+            const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
+            const double m = c[0], hc = c[2];
+            for (int d = 0; d < 2; ++d) {
+                const double F = s[8 + d] + c[3 + d];
+                double vh = s[2 + d] + ((0.5 * dt) * F) / m;
+                if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vh = vh + 0.5 * (hc * (s[2 + d] - s[4 + d]));
+                const double xn = s[d] + (dt * vh) * dx;
+                s[6 + d] = vh;
+                s[10 + d] = xn;
+                s_vh[2 * p + d] = vh;
+                s_next[2 * p + d] = xn;
+            }
+        }
+        __syncthreads();
+        const int Lb = a.moff[P];
+        for (int l = threadIdx.x; l < Lb; l += PART_THREADS) {
+            int p = 0;
+            while (p + 1 < P && l >= a.moff[p + 1]) ++p;
+            const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
+            const double rx = a.Lx_c[l] - c[5], ry = a.Ly_c[l] - c[6];
+            // R(0) = [[cos 0, -sin 0], [sin 0, cos 0]] = [[1, -0], [0, 1]]
+            a.Lx[l] = (1.0 * rx - 0.0 * ry) + s_next[2 * p];
+            a.Ly[l] = (0.0 * rx + 1.0 * ry) + s_next[2 * p + 1];
+            a.dvel[2 * l] = s_vh[2 * p];
+            a.dvel[2 * l + 1] = s_vh[2 * p + 1];
+        }
+    }
+}
+
+}  // namespace iblbm
+
+using namespace iblbm;
+
+extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* stream)
+{
+    if (!a || a->n_particles < 1 || a->n_particles > PART_MAXP || !a->moff || !a->state || !a->consts)
+        return IBLBM_E_ARG;
+    if ((a->phase & ~(IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_HALF)) || !a->phase) return IBLBM_E_ARG;
+    if ((a->phase & IBLBM_PARTICLES_FULL) && (!a->band_fib_part || !a->band_count || a->band_capacity < 1))
+        return IBLBM_E_ARG;
+    if ((a->phase & IBLBM_PARTICLES_HALF) && (!a->Lx_c || !a->Ly_c || !a->Lx || !a->Ly || !a->dvel))
+        return IBLBM_E_ARG;
+    if (a->model < IBLBM_INERTIA_NONE || a->model > IBLBM_INERTIA_FENG_B2) return IBLBM_E_ARG;
+    particles_kernel<<<1, PART_THREADS, 0, (cudaStream_t)stream>>>(*a);
+    return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
+}

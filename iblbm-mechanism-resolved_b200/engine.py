@@ -61,7 +61,7 @@ class Engine:
     """One lattice case on one GPU: FP64 form (the reference's arithmetic) or
     the shifted FP32 form (``precision="f32"``)."""
 
-    def __init__(self, cfg, device=None, precision="f64"):
+    def __init__(self, cfg, device=None, precision="f64", device_particles=None):
         torch = _torch()
         if precision not in ("f64", "f32"):
             raise ValueError(f"precision='{precision}' (f64 or f32)")
@@ -188,12 +188,74 @@ class Engine:
         self.d_pipe_status = torch.zeros(1, dtype=i32, device=dev)
         self.graphs = {}
         self._make_dense_variants()
+        # free particles: their Verlet step on the device (default in the FP32
+        # form; the FP64 form keeps the host step, whose force sums follow numpy's
+        # pairwise order bit for bit)
+        self.dev_particles = False
+        if st.particles is not None:
+            self.dev_particles = self.f32 if device_particles is None else bool(device_particles)
+            if self.dev_particles:
+                self._setup_device_particles()
         self.side = torch.cuda.Stream(self.dev, priority=-1)
         self.ev_bulk = torch.cuda.Event()
         self.ev_side = torch.cuda.Event()
         self.overlap = True
         self.rebuild_next = True
         self.last_out_step = 0
+
+    def _setup_device_particles(self):
+        from ._lib import INERTIA_IDS, ParticlesArgs
+        torch, st, cfg = self.torch, self.st, self.cfg
+        if cfg.settling_inertia_model not in INERTIA_IDS:
+            raise NotImplementedError(f"inertia model '{cfg.settling_inertia_model}' on the device")
+        ps = st.particles
+        state = np.zeros((len(ps), 12))
+        consts = np.zeros((len(ps), 8))
+        for k, p in enumerate(ps):
+            state[k, 0:2] = p.pos
+            state[k, 2:4] = p.vel
+            state[k, 4:6] = p.vel_prev
+            state[k, 6:8] = p.vel_half
+            state[k, 8:10] = p.force
+            state[k, 10:12] = p.pos
+            g = net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
+            consts[k] = [p.mass, 1.0 / p.rho_ratio, np.pi * p.lattice_r ** 2 / p.mass, g[0], g[1], p.cx_init,
+                         p.cy_init, 0.0]
+        self.d_pstate = torch.as_tensor(state.reshape(-1), device=self.dev)
+        self.d_pconsts = torch.as_tensor(consts.reshape(-1), device=self.dev)
+        self.d_Lxc_all = torch.as_tensor(np.concatenate([p.Lx_c for p in ps]), device=self.dev)
+        self.d_Lyc_all = torch.as_tensor(np.concatenate([p.Ly_c for p in ps]), device=self.dev)
+        self.d_pforces = torch.zeros(2 * len(ps), dtype=torch.float64, device=self.dev)
+        a = ParticlesArgs()
+        a.n_particles, a.model, a.fib_f32 = len(ps), INERTIA_IDS[cfg.settling_inertia_model], int(self.f32)
+        a.moff, a.Lx_c, a.Ly_c = ptr(self.d_moff), ptr(self.d_Lxc_all), ptr(self.d_Lyc_all)
+        a.Lx, a.Ly, a.dvel = ptr(self.d_Lx), ptr(self.d_Ly), ptr(self.d_dv)
+        a.state, a.consts = ptr(self.d_pstate), ptr(self.d_pconsts)
+        a.dt, a.dx = float(st.dt), float(st.dx)
+        a.band_fib_part, a.band_count, a.band_capacity = ptr(self.d_fib_part), ptr(self.d_count), self.B
+        a.forces_out = ptr(self.d_pforces)
+        self.part_args = a
+        self.part_started = False
+
+    def _particles(self, stream, phase):
+        a = self.part_args
+        a.phase = phase
+        check(self.L.iblbm_particles_step_f64(ctypes.byref(a), stream), "iblbm_particles_step_f64")
+
+    def pull_particles(self):
+        """Copy the device particle state (position, velocity, force of the last
+        completed step) into the host Particle objects."""
+        if not self.dev_particles:
+            return
+        self.join()
+        s = self.d_pstate.reshape(-1, 12).cpu().numpy()
+        for k, p in enumerate(self.st.particles):
+            p.pos = s[k, 0:2].copy()
+            p.vel = s[k, 2:4].copy()
+            p.vel_prev = s[k, 4:6].copy()
+            p.vel_half = s[k, 6:8].copy()
+            p.force = s[k, 8:10].copy()
+            p.fib_force = p.force.copy()
 
     def _band_capacity(self, S):
         st = self.st
@@ -352,7 +414,12 @@ class Engine:
         s = self.stream()
         if events:
             events[0].record()
+        if self.dev_particles and not self.part_started:
+            self._particles(s, 2)  # half step of the first timestep
+            self.part_started = True
         self._ibm(s, excl_check=False)
+        if self.dev_particles:
+            self._particles(s, 3)  # full step of this timestep, half step of the next
         if events:
             events[1].record()
         self._dense(self.dense_full, outputs, s)
@@ -372,6 +439,8 @@ class Engine:
         side = self.side
         side.wait_event(self.ev_bulk)
         self._ibm(side.cuda_stream, excl_check=True)
+        if self.dev_particles:
+            self._particles(side.cuda_stream, 3)
         self._dense(self.dense_box, outputs, side.cuda_stream)
         main.wait_event(self.ev_side)
         self.ev_side.record(side)
@@ -396,7 +465,7 @@ class Engine:
 
     def _launch(self, outputs=False, events=None):
         """One timestep: serial for the first step (and when overlap is off), else overlapped."""
-        if self.rebuild_next or not self.overlap or self.st.particles is not None:
+        if self.rebuild_next or not self.overlap or (self.st.particles is not None and not self.dev_particles):
             self._step_serial(outputs, events)
             main = self.torch.cuda.current_stream(self.dev)
             self.ev_bulk.record(main)
@@ -433,7 +502,7 @@ class Engine:
         """Advance nsteps timesteps; the last one writes rho/U/f* when outputs_last."""
         if nsteps <= 0:
             return
-        if self.st.particles is not None:
+        if self.st.particles is not None and not self.dev_particles:
             for k in range(nsteps):
                 self._sedimentation_step(outputs=outputs_last and k == nsteps - 1)
             return
@@ -460,6 +529,8 @@ class Engine:
             self._launch(True)
             self.ttt += 1
             self.last_out_step = self.ttt - 1
+        if self.dev_particles and outputs_last:
+            self.pull_particles()
 
     # ---- multi-particle sedimentation (host Newton-Euler, as the reference) ----------
     def _sedimentation_step(self, outputs):

@@ -311,6 +311,39 @@ int iblbm_mlp_infer(const float *params, const float *x, int n, float *y, void *
 int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *grad, unsigned *ticket, const float *x,
                          const float *t, int n, float lr, int step, float *loss, int apply, void *stream);
 
+/* ---- rigid particles of sedimentation runs on the device -------------------
+ * Replaces the host Velocity-Verlet step of runtime/scenarios/
+ * sedimentation_multi.py:36-111 (inertia models none / explicit_history /
+ * feng_b2, no rotation).  Per particle, state holds IBLBM_PARTICLE_STATE
+ * doubles: pos(2), vel(2), vel_prev(2), vel_half(2), force(2), pos_next(2);
+ * consts holds IBLBM_PARTICLE_CONSTS doubles: mass, 1/rho_ratio, pi r^2/mass,
+ * net gravity (2), initial centre (2), unused.  phase FULL finishes the current
+ * step from the band kernel's per-particle forces (band_fib_part, particles x
+ * band_capacity x 2, FP32 when fib_f32); phase HALF starts the next one: new
+ * marker positions Lx, Ly and desired velocities dvel. */
+#define IBLBM_PARTICLE_STATE 12
+#define IBLBM_PARTICLE_CONSTS 8
+#define IBLBM_PARTICLES_FULL 1
+#define IBLBM_PARTICLES_HALF 2
+#define IBLBM_INERTIA_NONE 0
+#define IBLBM_INERTIA_EXPLICIT_HISTORY 1
+#define IBLBM_INERTIA_FENG_B2 2
+typedef struct {
+    int n_particles, phase, model, fib_f32;
+    const int *moff;
+    const double *Lx_c, *Ly_c;
+    double *Lx, *Ly, *dvel;
+    double *state;
+    const double *consts;
+    double dt, dx;
+    const void *band_fib_part;
+    const int *band_count;
+    int band_capacity;
+    double *forces_out;   /* optional: particles x 2, the forces of the full step */
+} iblbm_particles_args;
+
+int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);
+
 /* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
 /* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */
 int iblbm_feq(const double *ro, const double *U, int N, int incompressible, double *feq, void *stream);

@@ -177,3 +177,20 @@ def test_f32_config1_geometry_long(torch):
     r64, r32 = _pair(cfg)
     _check_fields(cfg, r64, r32)
     _check_forces(r64, r32)
+
+
+def test_device_particles_match_host_step(torch):
+    """The FP64 form with the Verlet step on the device against the host step
+    (bit-exact to the reference): trajectories agree to round-off (the device
+    sums the band forces in its own fixed order)."""
+    from iblbm_b200 import run
+    from iblbm_b200.engine import Engine
+    cfg = _cfg(RUN_CASES["c5_sed2_mdf_cmmrt_p4"])
+    host = run(cfg, verbose=False, engine=Engine(cfg, precision="f64", device_particles=False))
+    dev = run(cfg, verbose=False, engine=Engine(cfg, precision="f64", device_particles=True))
+    assert dev["engine"].status() == 0
+    for p, q in zip(dev["state"].particles, host["state"].particles):
+        np.testing.assert_allclose(p.pos, q.pos, rtol=1e-9, atol=0)
+        np.testing.assert_allclose(p.vel, q.vel, rtol=1e-9, atol=1e-9 * float(np.max(np.abs(q.vel))))
+    for hd, hh in zip(dev["sedimentation_history"], host["sedimentation_history"]):
+        assert hd["step"] == hh["step"]
