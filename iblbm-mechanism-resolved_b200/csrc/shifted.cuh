@@ -355,7 +355,10 @@ __device__ __forceinline__ void collide32_trt(const float* g, float drho, float 
 }
 
 // CM-MRT: raw moments of g (sums and differences of populations, e in {0, +-1}),
-// shifted to central moments about u by the binomial formulas.
+// shifted to central moments about u by the binomial formulas.  Only the change
+// of the central moments, dc = c_post - k(g), is mapped back (the map is
+// linear): g_out = g + T(dc), where the conserved moments (m < 3, rate 0) change
+// only by the forcing.
 template <bool FORCED>
 __device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, float ux, float uy, float F0, float F1,
                                                 const CollParams32& cp, float* out)
@@ -372,9 +375,6 @@ __device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, floa
     const float m22 = s57 + s68;
     const float ux2 = ux * ux, uy2 = uy * uy, uxy = ux * uy;
     float k[9];
-    k[0] = m00;
-    k[1] = m10 - ux * m00;
-    k[2] = m01 - uy * m00;
     k[3] = m20 - 2.0f * ux * m10 + ux2 * m00;
     k[4] = m02 - 2.0f * uy * m01 + uy2 * m00;
     k[5] = m11 - ux * m01 - uy * m10 + uxy * m00;
@@ -395,36 +395,42 @@ __device__ __forceinline__ void collide32_cmmrt(const float* g, float drho, floa
     }
     // central moments of the weights about u, and the equilibrium minus them
     const float ax = 1.0f / 3.0f + ux2, ay = 1.0f / 3.0f + uy2;
-    const float kw[9] = {1.0f, -ux, -uy, ax, ay, uxy, -uy * ax, -ux * ay, ax * ay};
     const float rho = 1.0f + drho;
-    const float keq[9] = {rho, 0.0f, 0.0f, rho / 3.0f, rho / 3.0f, 0.0f, 0.0f, 0.0f, rho / 9.0f};
-    float c[9];
+    const float keq3 = rho * (1.0f / 3.0f), keq8 = rho * (1.0f / 9.0f);
+    // dc = -S (k(g) + k(w) - k_eq) [+ (1 - S/2) F dt]
+    float dc[9];
+    dc[3] = -cp.S[3] * (k[3] + (ax - keq3));
+    dc[4] = -cp.S[4] * (k[4] + (ay - keq3));
+    dc[5] = -cp.S[5] * (k[5] + uxy);
+    dc[6] = -cp.S[6] * (k[6] - uy * ax);
+    dc[7] = -cp.S[7] * (k[7] - ux * ay);
+    dc[8] = -cp.S[8] * (k[8] + (ax * ay - keq8));
+    dc[0] = dc[1] = dc[2] = 0.0f;
+    if (FORCED) {
 #pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        // k_post - k(w) = k(g) - S (k(g) + k(w) - k_eq) + (1 - S/2) F dt
-        const float neq = (m == 0) ? 0.0f : (k[m] + (kw[m] - keq[m]));
-        c[m] = k[m] - cp.S[m] * neq;
-        if (FORCED) c[m] += (1.0f - 0.5f * cp.S[m]) * F[m] * cp.dt;
+        for (int m = 0; m < 9; ++m) dc[m] += (1.0f - 0.5f * cp.S[m]) * F[m] * cp.dt;
     }
-    const float k0 = c[0];
-    const float k1 = c[1] + ux * c[0];
-    const float k2 = c[2] + uy * c[0];
-    const float k3 = c[3] + 2.0f * ux * c[1] + ux2 * c[0];
-    const float k4 = c[4] + 2.0f * uy * c[2] + uy2 * c[0];
-    const float k5 = c[5] + uy * c[1] + ux * c[2] + uxy * c[0];
-    const float k6 = c[6] + uy * c[3] + 2.0f * ux * c[5] + 2.0f * uxy * c[1] + ux2 * c[2] + ux2 * uy * c[0];
-    const float k7 = c[7] + 2.0f * uy * c[5] + ux * c[4] + 2.0f * uxy * c[2] + uy2 * c[1] + ux * uy2 * c[0];
-    const float k8 = c[8] + 2.0f * uy * c[6] + uy2 * c[3] + 2.0f * ux * c[7] + 4.0f * uxy * c[5] +
-                     2.0f * ux * uy2 * c[1] + ux2 * c[4] + 2.0f * ux2 * uy * c[2] + ux2 * uy2 * c[0];
-    out[0] = k0 - k3 - k4 + k8;
-    out[1] = 0.5f * (k1 + k3 - k7 - k8);
-    out[2] = 0.5f * (k2 + k4 - k6 - k8);
-    out[3] = 0.5f * (-k1 + k3 + k7 - k8);
-    out[4] = 0.5f * (-k2 + k4 + k6 - k8);
-    out[5] = 0.25f * (k5 + k6 + k7 + k8);
-    out[6] = 0.25f * (-k5 + k6 - k7 + k8);
-    out[7] = 0.25f * (k5 - k6 - k7 + k8);
-    out[8] = 0.25f * (-k5 - k6 + k7 + k8);
+    // central -> raw moments of the change
+    const float K0 = dc[0];
+    const float K1 = dc[1] + ux * dc[0];
+    const float K2 = dc[2] + uy * dc[0];
+    const float K3 = dc[3] + 2.0f * ux * dc[1] + ux2 * dc[0];
+    const float K4 = dc[4] + 2.0f * uy * dc[2] + uy2 * dc[0];
+    const float K5 = dc[5] + uy * dc[1] + ux * dc[2] + uxy * dc[0];
+    const float K6 = dc[6] + uy * dc[3] + 2.0f * ux * dc[5] + 2.0f * uxy * dc[1] + ux2 * dc[2] + ux2 * uy * dc[0];
+    const float K7 = dc[7] + 2.0f * uy * dc[5] + ux * dc[4] + 2.0f * uxy * dc[2] + uy2 * dc[1] + ux * uy2 * dc[0];
+    const float K8 = dc[8] + 2.0f * uy * dc[6] + uy2 * dc[3] + 2.0f * ux * dc[7] + 4.0f * uxy * dc[5] +
+                     2.0f * ux * uy2 * dc[1] + ux2 * dc[4] + 2.0f * ux2 * uy * dc[2] + ux2 * uy2 * dc[0];
+    // raw moments -> populations
+    out[0] = g[0] + (K0 - K3 - K4 + K8);
+    out[1] = g[1] + 0.5f * (K1 + K3 - K7 - K8);
+    out[2] = g[2] + 0.5f * (K2 + K4 - K6 - K8);
+    out[3] = g[3] + 0.5f * (-K1 + K3 + K7 - K8);
+    out[4] = g[4] + 0.5f * (-K2 + K4 + K6 - K8);
+    out[5] = g[5] + 0.25f * (K5 + K6 + K7 + K8);
+    out[6] = g[6] + 0.25f * (-K5 + K6 - K7 + K8);
+    out[7] = g[7] + 0.25f * (K5 - K6 - K7 + K8);
+    out[8] = g[8] + 0.25f * (-K5 - K6 + K7 + K8);
 }
 
 template <int COLL, bool INCOMP, bool FORCED>
