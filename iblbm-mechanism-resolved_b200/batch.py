@@ -62,6 +62,10 @@ class Batch:
             for s in range(0, len(idx), MAX_KIND):
                 self.kinds.append(idx[s:s + MAX_KIND])
         self.tiles = [tile] * len(self.kinds)
+        # bulk passes: one launch per kind, or one launch over every case
+        # (CTAs dispatch on their case's kind) when `merged`
+        self.merged = False
+        self.tile_all = tile
         # band argument blocks: [first step | later steps][parity], host and device copies
         self.ibm_host = {}
         self.ibm_dev = {}
@@ -122,6 +126,24 @@ class Batch:
                         a.box_blocks = 8
                         arr[n] = a
                     self.dense[g, p, mode] = arr
+        if self.C <= MAX_KIND:
+            order = [k for idx in self.kinds for k in idx]
+            for p in (0, 1):
+                arr = (Dense32Args * len(order))()
+                for n, k in enumerate(order):
+                    a = _copy(self.engines[k].dense_bulk[p][0])
+                    a.tile = TILES[self.tile_all]
+                    arr[n] = a
+                self.dense["all", p, "bulk"] = arr
+
+    def set_tile_all(self, tile, merged=True):
+        """Tile of the single bulk launch over all cases (and whether to use it)."""
+        if tile not in ("node", "rows2", "rows4"):
+            raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
+        self.tile_all = tile
+        self.merged = bool(merged) and self.C <= MAX_KIND
+        self._make_dense_arrays()
+        self.graphs = {}
 
     def set_tile(self, kind, tile):
         if tile not in ("node", "rows2", "rows4"):
@@ -173,8 +195,11 @@ class Batch:
         self.ev_side.record(side)
         if bulk_events:
             bulk_events[0].record(main)
-        for g in range(len(self.kinds)):
-            self._dense(g, "bulk", main.cuda_stream)
+        if self.merged:
+            self._dense("all", "bulk", main.cuda_stream)
+        else:
+            for g in range(len(self.kinds)):
+                self._dense(g, "bulk", main.cuda_stream)
         if bulk_events:
             bulk_events[1].record(main)
         self.ev_bulk.record(main)

@@ -20,6 +20,7 @@ constexpr int BATCH_MAX = 72;
 
 struct BatchCase {
     int nx, ny, pitch, bx;   // bx: 128-node column blocks
+    int kind;                // collision * 8 + closure * 2 + incompressible (mixed bulk launches)
     long long qstride;
     const float* fp;
     float* fn;
@@ -52,12 +53,10 @@ __device__ __forceinline__ int batch_case(const BatchTable& t, int blk)
     return lo;
 }
 
+// NR nodes per thread stacked in y on block `local` of case c.
 template <int COLL, int BC, bool INCOMP, int IBM, int NR>
-__global__ void __launch_bounds__(128) dense32_batch_kernel(const __grid_constant__ BatchTable t)
+__device__ __forceinline__ void batch_rows(const BatchCase& c, int local)
 {
-    const int ci = batch_case(t, blockIdx.x);
-    const BatchCase& c = t.c[ci];
-    const int local = blockIdx.x - t.off[ci];
     const Geom g{c.nx, c.ny, c.pitch, c.qstride};
     const int i = (local % c.bx) * 128 + threadIdx.x;
     const int j0 = (local / c.bx) * NR;
@@ -89,6 +88,52 @@ __global__ void __launch_bounds__(128) dense32_batch_kernel(const __grid_constan
 #pragma unroll
         for (int q = 0; q < 9; ++q) dst[q * g.qstride] = out[q];
     }
+}
+
+template <int COLL, int BC, bool INCOMP, int IBM, int NR>
+__global__ void __launch_bounds__(128) dense32_batch_kernel(const __grid_constant__ BatchTable t)
+{
+    const int ci = batch_case(t, blockIdx.x);
+    batch_rows<COLL, BC, INCOMP, IBM, NR>(t.c[ci], blockIdx.x - t.off[ci]);
+}
+
+// Bulk passes (no band) of cases of different kinds in one launch: each CTA
+// dispatches on its case's kind, so the launch has one tail instead of one per
+// kind.
+template <int COLL, int NR>
+__device__ __forceinline__ void batch_rows_bc(const BatchCase& c, int local, int bcv, bool inc)
+{
+    switch (bcv) {
+    case BC_DIRICHLET_NEUMANN:
+        if (inc) batch_rows<COLL, BC_DIRICHLET_NEUMANN, true, IBM_NONE, NR>(c, local);
+        else batch_rows<COLL, BC_DIRICHLET_NEUMANN, false, IBM_NONE, NR>(c, local);
+        break;
+    case BC_OPEN:
+        if (inc) batch_rows<COLL, BC_OPEN, true, IBM_NONE, NR>(c, local);
+        else batch_rows<COLL, BC_OPEN, false, IBM_NONE, NR>(c, local);
+        break;
+    case BC_SETTLING:
+        if (inc) batch_rows<COLL, BC_SETTLING, true, IBM_NONE, NR>(c, local);
+        else batch_rows<COLL, BC_SETTLING, false, IBM_NONE, NR>(c, local);
+        break;
+    default:
+        if (inc) batch_rows<COLL, BC_VELOCITY_INLET, true, IBM_NONE, NR>(c, local);
+        else batch_rows<COLL, BC_VELOCITY_INLET, false, IBM_NONE, NR>(c, local);
+        break;
+    }
+}
+
+template <int NR>
+__global__ void __launch_bounds__(128) dense32_batch_mixed_kernel(const __grid_constant__ BatchTable t)
+{
+    const int ci = batch_case(t, blockIdx.x);
+    const BatchCase& c = t.c[ci];
+    const int local = blockIdx.x - t.off[ci];
+    const int coll = c.kind >> 3, bcv = (c.kind >> 1) & 3;
+    const bool inc = (c.kind & 1) != 0;
+    if (coll == COLL_BGK) batch_rows_bc<COLL_BGK, NR>(c, local, bcv, inc);
+    else if (coll == COLL_TRT) batch_rows_bc<COLL_TRT, NR>(c, local, bcv, inc);
+    else batch_rows_bc<COLL_CMMRT, NR>(c, local, bcv, inc);
 }
 
 // Box passes of a batch: blockIdx.y is the case, grid-stride over its box.
@@ -172,10 +217,14 @@ extern "C" int iblbm_dense_step_f32_batch(const iblbm_dense32_args* a, int n, vo
     static BatchTable t;  // host staging of the parameter block (calls are serialised by the caller)
     t.n = n;
     t.off[0] = 0;
+    bool mixed = false;
     for (int b = 0; b < n; ++b) {
         const iblbm_dense32_args& x = a[b];
-        if (x.c.collision != a0.c.collision || x.c.bc != a0.c.bc || x.c.incompressible != a0.c.incompressible ||
-            x.ibm != a0.ibm || (x.only_box != nullptr) != box || (box && x.skip_box) || x.tile != a0.tile)
+        if (x.c.collision != a0.c.collision || x.c.bc != a0.c.bc || x.c.incompressible != a0.c.incompressible)
+            mixed = true;
+        if (x.ibm != a0.ibm || (x.only_box != nullptr) != box || (box && x.skip_box) || x.tile != a0.tile)
+            return IBLBM_E_ARG;
+        if (x.c.collision < COLL_BGK || x.c.collision > COLL_CMMRT || x.c.bc < 0 || x.c.bc > 3)
             return IBLBM_E_ARG;
         if (x.ro_out || x.U_out || x.fstar_out) return IBLBM_E_ARG;
         if (!x.fpost_prev || !x.fpost_next || x.g.nx < 4 || x.g.ny < 4 || x.g.pitch < x.g.nx) return IBLBM_E_ARG;
@@ -191,6 +240,7 @@ extern "C" int iblbm_dense_step_f32_batch(const iblbm_dense32_args* a, int n, vo
         c.pitch = x.g.pitch;
         c.qstride = x.g.qstride;
         c.bx = (x.g.nx + 127) / 128;
+        c.kind = x.c.collision * 8 + x.c.bc * 2 + (x.c.incompressible ? 1 : 0);
         c.fp = x.fpost_prev;
         c.fn = x.fpost_next;
         c.urp = x.uring_prev;
@@ -209,6 +259,15 @@ extern "C" int iblbm_dense_step_f32_batch(const iblbm_dense32_args* a, int n, vo
     const int bb = a0.box_blocks > 0 ? a0.box_blocks : 16;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e;
+    if (mixed) {
+        // cases of several kinds: only bulk passes without a band
+        if (box || a0.ibm != IBM_NONE) return IBLBM_E_ARG;
+        if (nr == 1) dense32_batch_mixed_kernel<1><<<t.off[n], 128, 0, s>>>(t);
+        else if (nr == 2) dense32_batch_mixed_kernel<2><<<t.off[n], 128, 0, s>>>(t);
+        else dense32_batch_mixed_kernel<4><<<t.off[n], 128, 0, s>>>(t);
+        e = cudaGetLastError();
+        return e == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
+    }
     switch (a0.c.collision) {
     case COLL_BGK: e = launch_batch_coll<COLL_BGK>(t, a0.c.bc, a0.c.incompressible != 0, a0.ibm, nr, box, bb, s); break;
     case COLL_TRT: e = launch_batch_coll<COLL_TRT>(t, a0.c.bc, a0.c.incompressible != 0, a0.ibm, nr, box, bb, s); break;

@@ -228,7 +228,9 @@ typedef struct {
 int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
 /* The pass of n <= 72 independent cases of one kind (same collision, closure,
  * compressibility, band method, and all bulk/whole-lattice or all box passes)
- * in one launch; lattices may differ in size.  Tile NODE, ROWS2 or ROWS4 (taken
+ * in one launch; lattices may differ in size.  Bulk passes without a band
+ * (ibm = IBLBM_IBM_NONE, no only_box) may mix kinds: each CTA then dispatches
+ * on its case's collision, closure and compressibility.  Tile NODE, ROWS2 or ROWS4 (taken
  * from a[0]); no ro/U/fstar outputs.  Calls must not run concurrently on the
  * host (the parameter block is staged in one static buffer). */
 int iblbm_dense_step_f32_batch(const iblbm_dense32_args *a, int n, void *stream);

@@ -40,12 +40,13 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("tile", ["rows2", "node"])
-def test_batch_matches_single_cases(torch, tile):
+@pytest.mark.parametrize("tile,merged", [("rows2", False), ("node", False), ("rows2", True), ("rows4", True)])
+def test_batch_matches_single_cases(torch, tile, merged):
     from iblbm_b200.batch import Batch
     from iblbm_b200.engine import Engine
     cfgs = [_cfg(**kw) for kw in CASES]
     b = Batch(cfgs, tile=tile)
+    b.set_tile_all(tile, merged=merged)
     b.advance(61, outputs_last=True)
     torch.cuda.synchronize()
     assert b.status() == [0] * len(cfgs)
