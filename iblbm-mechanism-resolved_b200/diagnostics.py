@@ -1,0 +1,98 @@
+"""Diagnostics of the reference's result analysis, on this package's arrays.
+
+``compute_strouhal`` restates iblbm/diagnostics/core.py:138-214 (Strouhal
+number from a Cl history: second half, detrended, peak of the rfft power
+spectrum without the DC term, with the reference's handling of rectified |Cl|
+series).  ``compute_slip_error`` restates iblbm/diagnostics/ibm_quality.py:
+132-188 (boundary slip of a velocity field on a diagnostic marker ring);
+its interpolation runs on the GPU through the band kernel (field-input mode),
+in the reference's summation order.  ``engine_slip`` evaluates the same on the
+engine's own markers and last output velocity.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def compute_strouhal(Cl_history, steps, D_lattice, u_ref, check_interval):
+    """St = f_shed D / U from the second half of a Cl series sampled every
+    check_interval steps (signed Cl, or |Cl| whose peak sits at 2 f_shed)."""
+    cl = np.asarray(Cl_history, dtype=float)
+    half = cl[len(cl) // 2:]
+    rectified = bool(np.all(cl >= -1e-10))
+    power = np.abs(np.fft.rfft(half - np.mean(half))) ** 2
+    power[0] = 0
+    f_peak = int(np.argmax(power)) / (len(half) * check_interval)
+    if not rectified:
+        f_shed = f_peak
+    else:
+        fs = 1.0 / check_interval
+        direct = (f_peak / 2) * D_lattice / u_ref
+        # |Cl| peaks at 2 f_shed, or at its alias fs - 2 f_shed above Nyquist;
+        # a direct reading inside the shedding range (>= 0.1) is taken as is
+        f_shed = f_peak / 2 if direct >= 0.1 else (fs - f_peak) / 2
+    return f_shed * D_lattice / u_ref
+
+
+def diagnostic_markers(cx, cy, r, NN, marker_spacing_factor=0.5):
+    """Marker ring on the body surface (no retraction), the reference's spacing
+    rule: 2 pi r_lattice / spacing points, the closing duplicate dropped."""
+    n_param = 2.0 * np.pi * (r * (NN - 1)) / marker_spacing_factor
+    step = 1.0 / n_param
+    s = np.arange(0, 1.0 + step * 0.5, step)
+    s = s[s <= 1.0 + 1e-12]
+    if len(s) > 1 and np.abs(s[-1] - 1.0) < step * 0.5:
+        s = s[:-1]
+    theta = 2.0 * np.pi * s
+    return r * np.cos(theta) + cx, r * np.sin(theta) + cy, theta
+
+
+def _interp_gpu(Eux, Euy, Lx, Ly, dx, dy, delta_type):
+    import torch
+    from . import gpu_kernels as gk
+    ny, nx = Eux.shape
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+    ex, ey = d(Eux).reshape(-1), d(Euy).reshape(-1)
+    ro = torch.ones_like(ex)
+    Lb = len(Lx)
+    _, Lux, Luy = gk.ibm_direct_forcing_gpu(d(Lx), d(Ly), torch.zeros(Lb, 2, dtype=torch.float64, device="cuda"),
+                                            ex, ey, ro, dx, dy, 1.0, 1.0, ny, nx, delta_type, True, False)
+    return Lux.cpu().numpy(), Luy.cpu().numpy()
+
+
+def compute_slip_error(Eux, Euy, dx, dy, cx, cy, D, NN, delta_type, u_target_x=None, u_target_y=None, u_ref=0.1):
+    """Slip |u(X_m) - u_target| / U_ref on a diagnostic ring: mean, max, RMS and
+    per marker.  Eux, Euy: (ny, nx) host or device arrays."""
+    Eux = np.asarray(Eux.cpu() if hasattr(Eux, "cpu") else Eux, dtype=np.float64)
+    Euy = np.asarray(Euy.cpu() if hasattr(Euy, "cpu") else Euy, dtype=np.float64)
+    Lx, Ly, theta = diagnostic_markers(cx, cy, D / 2.0, NN)
+    Lux, Luy = _interp_gpu(Eux, Euy, Lx, Ly, dx, dy, delta_type)
+    tx = np.zeros(len(Lx)) if u_target_x is None else u_target_x
+    ty = np.zeros(len(Lx)) if u_target_y is None else u_target_y
+    mag = np.sqrt((Lux - tx) ** 2 + (Luy - ty) ** 2)
+    return {"mean": float(np.mean(mag) / u_ref), "max": float(np.max(mag) / u_ref),
+            "rms": float(np.sqrt(np.mean(mag ** 2)) / u_ref), "per_marker": mag / u_ref, "theta": theta}
+
+
+def engine_slip(engine, u_ref=None):
+    """Slip of the engine's last output velocity on its own markers (the
+    simulation's ring, desired velocities as targets): mean, max and RMS over
+    U_ref (the inflow speed, or the oscillation speed scale)."""
+    st, cfg = engine.st, engine.cfg
+    if u_ref is None:
+        u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
+    U = engine.U_out.double().reshape(st.ny, st.nx, 2)
+    Lx = engine.d_Lx[: engine.Lb].cpu().numpy()
+    Ly = engine.d_Ly[: engine.Lb].cpu().numpy()
+    if engine.xt is not None:
+        # markers in force during the last output step
+        xt = float(engine.xt[engine.last_out_step].item())
+        Lx = engine.d_Lxc.cpu().numpy() - xt
+        Ly = engine.d_Lyc.cpu().numpy()
+        dv = np.stack([np.full(engine.Lb, xt), np.zeros(engine.Lb)], axis=1)
+    else:
+        dv = engine.d_dv[: 2 * engine.Lb].reshape(engine.Lb, 2).cpu().numpy()
+    Lux, Luy = _interp_gpu(U[..., 0].cpu().numpy(), U[..., 1].cpu().numpy(), Lx, Ly, st.dx, st.dy, cfg.delta_type)
+    mag = np.sqrt((Lux - dv[:, 0]) ** 2 + (Luy - dv[:, 1]) ** 2)
+    return {"mean": float(np.mean(mag) / u_ref), "max": float(np.max(mag) / u_ref),
+            "rms": float(np.sqrt(np.mean(mag ** 2)) / u_ref)}

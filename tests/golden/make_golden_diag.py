@@ -1,0 +1,58 @@
+"""Fixtures for the diagnostics (tests/test_diagnostics.py), made by running the
+reference's own functions: iblbm.diagnostics.compute_strouhal on seeded
+synthetic Cl series (signed, and rectified |Cl| on both sides of the aliasing
+threshold) and iblbm.diagnostics.compute_slip_error on a seeded velocity field.
+
+Usage:  python tests/golden/make_golden_diag.py --reference /path/to/reference
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True)
+    args = ap.parse_args()
+    os.environ["IBLBM_GPU"] = "0"
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/iblbm_numba_cache")
+    sys.path.insert(0, args.reference)
+    from iblbm.diagnostics import compute_slip_error, compute_strouhal
+    rng = np.random.default_rng(11)
+    out = {}
+    ci, D, u = 50, 20.0, 0.05
+    n = 400
+    steps = np.arange(1, n + 1) * ci
+    series = {
+        "signed": 0.3 * np.sin(2 * np.pi * 0.17 * u / D * steps) + 1e-3 * rng.standard_normal(n),
+        "rect_low": np.abs(0.3 * np.sin(2 * np.pi * 0.15 * u / D * steps)) + 1e-4 * rng.random(n),
+        "rect_high": np.abs(0.3 * np.sin(2 * np.pi * 0.2 * (u * 8) / D * steps)) + 1e-4 * rng.random(n),
+    }
+    for k, cl in series.items():
+        out[f"st_{k}_cl"] = cl
+        out[f"st_{k}"] = np.array([compute_strouhal(cl, steps, D, u * (8 if k == "rect_high" else 1), ci)])
+    out["st_ci"] = np.array([ci])
+    out["st_D"] = np.array([D])
+    out["st_u"] = np.array([u])
+    ny, nx, NN = 81, 161, 81
+    dx = dy = 1.0 / (NN - 1)
+    Eux = 0.05 + 0.01 * rng.standard_normal((ny, nx))
+    Euy = 0.01 * rng.standard_normal((ny, nx))
+    for delta in ("hat", "peskin4pt"):
+        r = compute_slip_error(Eux, Euy, dx, dy, 0.5, 0.5, 0.25, NN, delta, u_ref=0.05)
+        out[f"slip_{delta}_mean"] = np.array([r["mean"]])
+        out[f"slip_{delta}_max"] = np.array([r["max"]])
+        out[f"slip_{delta}_per_marker"] = r["per_marker"]
+    out["slip_Eux"], out["slip_Euy"] = Eux, Euy
+    np.savez_compressed(os.path.join(HERE, "diag.npz"), **out)
+    print("wrote", os.path.join(HERE, "diag.npz"))
+
+
+if __name__ == "__main__":
+    main()

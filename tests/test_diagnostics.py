@@ -1,0 +1,63 @@
+"""Diagnostics against the reference's own functions (fixtures made by
+tests/golden/make_golden_diag.py from iblbm.diagnostics)."""
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "diag.npz")
+
+
+@pytest.fixture(scope="module")
+def diag():
+    return dict(np.load(GOLD))
+
+
+@pytest.mark.parametrize("name", ["signed", "rect_low", "rect_high"])
+def test_strouhal_matches_reference(diag, name):
+    from iblbm_b200.diagnostics import compute_strouhal
+    ci, D, u = int(diag["st_ci"][0]), float(diag["st_D"][0]), float(diag["st_u"][0])
+    cl = diag[f"st_{name}_cl"]
+    steps = np.arange(1, len(cl) + 1) * ci
+    uref = u * (8 if name == "rect_high" else 1)
+    assert compute_strouhal(cl, steps, D, uref, ci) == float(diag[f"st_{name}"][0])
+
+
+def test_diagnostic_markers_count():
+    from iblbm_b200.diagnostics import diagnostic_markers
+    Lx, Ly, th = diagnostic_markers(0.5, 0.5, 0.125, 81)
+    assert len(Lx) == 126 and th[0] == 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("delta", ["hat", "peskin4pt"])
+def test_slip_error_matches_reference(diag, delta):
+    from iblbm_b200.diagnostics import compute_slip_error
+    NN = 81
+    dx = 1.0 / (NN - 1)
+    r = compute_slip_error(diag["slip_Eux"], diag["slip_Euy"], dx, dx, 0.5, 0.5, 0.25, NN, delta, u_ref=0.05)
+    np.testing.assert_allclose(r["per_marker"], diag[f"slip_{delta}_per_marker"], rtol=1e-13, atol=0)
+    assert abs(r["mean"] - float(diag[f"slip_{delta}_mean"][0])) <= 1e-13 * abs(r["mean"])
+    assert abs(r["max"] - float(diag[f"slip_{delta}_max"][0])) <= 1e-13 * abs(r["max"])
+
+
+@pytest.mark.gpu
+def test_run_reports_marker_slip():
+    """run() adds the marker slip of the last output step (mean, max, RMS over
+    U_ref), interpolated in the reference's order: equal to the oracle's
+    interpolation of the same velocity field."""
+    from iblbm_b200 import SimConfig, run
+    from oracle import harness as H
+    cfg = SimConfig(Re=20, NN=41, xmax=2.5, ymax=1, cylinder_center=(0.625, 0.5), cylinder_D_ratio=0.25,
+                    lattice_u=0.05, inflow_u=0.05, bc_type="dirichlet_neumann", delta_type="hat", ibm_method="DF",
+                    collision_model="BGK", marker_spacing_factor=1.0, max_steps=60, use_convergence=False,
+                    check_interval=20)
+    res = run(cfg, verbose=False)
+    st = res["state"]
+    Lux, Luy = H.ibm_df(st.Lx, st.Ly, np.zeros((st.Lb, 2)), np.ascontiguousarray(st.U[:, 0]),
+                        np.ascontiguousarray(st.U[:, 1]), np.ones(st.nx * st.ny), st.dx, st.dy, 1.0, st.Larea,
+                        st.ny, st.nx, "hat")[1:3]
+    mag = np.sqrt(Lux ** 2 + Luy ** 2)
+    assert res["slip"]["max"] == float(np.max(mag) / st.in_u)
+    assert res["slip"]["mean"] == float(np.mean(mag) / st.in_u)
+    assert res["slip"]["rms"] == float(np.sqrt(np.mean(mag ** 2)) / st.in_u)
