@@ -194,3 +194,38 @@ def test_device_particles_match_host_step(torch):
         np.testing.assert_allclose(p.vel, q.vel, rtol=1e-9, atol=1e-9 * float(np.max(np.abs(q.vel))))
     for hd, hh in zip(dev["sedimentation_history"], host["sedimentation_history"]):
         assert hd["step"] == hh["step"]
+
+
+@pytest.mark.parametrize("tile", ["node", "rows4", "pipe4x2", "pipe8x2"])
+def test_f32_tile_shapes_agree(torch, tile):
+    """Every tile shape of the FP32 pass computes the same lattice as the
+    default 2-row shape (same per-node arithmetic; only the load path and the
+    thread mapping differ), on a lattice whose width is not a multiple of the
+    128-node tile and with an open boundary (velocity ring)."""
+    from iblbm_b200.engine import Engine
+    for name in ("c2_mdf_trt_p4", "c3_dfc_bgk_p4_osc"):
+        kw = dict(RUN_CASES[name], max_steps=40)
+        cfg = _cfg(kw)
+        ref = Engine(cfg, precision="f32")
+        e = Engine(cfg, precision="f32")
+        e.set_tile(tile)
+        ref.advance(40, outputs_last=True)
+        e.advance(40, outputs_last=True)
+        torch.cuda.synchronize()
+        assert e.status() == 0 and ref.status() == 0
+        np.testing.assert_array_equal(e.fpost_aos(), ref.fpost_aos(), err_msg=f"{name} {tile}")
+
+
+def test_band_capacity_overflow_reports_status(torch):
+    """A band larger than the capacity given to the band kernel is reported in
+    its status word (1) with an empty band left behind, not written out of
+    bounds."""
+    from iblbm_b200.engine import Engine
+    cfg = _cfg(dict(RUN_CASES["c1_df_bgk_hat"], max_steps=5))
+    e = Engine(cfg, precision="f32")
+    for a in e.ibm_args:
+        a.band_capacity = 16
+    e.advance(1, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    assert int(e.d_stats[4].item()) == 1
+    assert int(e.d_count.item()) == 0
