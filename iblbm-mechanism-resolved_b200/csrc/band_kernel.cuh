@@ -12,12 +12,14 @@
 //     (wx*wy)*ds precomputed.
 //   every step
 //     for fixed bodies the per-step-constant block (slot -> band index, lists,
-//     weights, node list) is restored into shared memory from its global cache
+//     weights, node list, stencil origins) is restored into shared memory from its global cache
 //     with one TMA bulk copy (cp.async.bulk + mbarrier) while the marker data
 //     loads; then post-streaming populations and moments on the band (the
 //     dense kernel's device functions), and DF, MDF (every iteration resident
 //     on chip: two barriers per iteration, residual reduced in shared memory,
-//     no host round trip), coupled multi-particle MDF, or DFC.
+//     no host round trip; the FP32 form iterates a single body on its markers
+//     through a banded marker coupling matrix, one barrier per iteration),
+//     coupled multi-particle MDF, or DFC.
 //   exclusion box
 //     the band's bounding box dilated by one node is written for the next
 //     step: markers move less than one node per step, so the next band lies
@@ -73,7 +75,30 @@ __host__ __device__ inline size_t mlp_act_bytes(int Lb)
     return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * MLP_LD + 2 * MLP_CHUNK + 4 * (size_t)Lb));
 }
 __host__ __device__ inline size_t mlp_smem_bytes(int Lb) { return mlp_act_bytes(Lb) + sizeof(float) * MLP_NP; }
+
+// Marker-space MDF of the FP32 form: row l of the marker coupling matrix keeps
+// the markers l - MS_D .. l + MS_D (neighbours along the body).
+constexpr int MS_D = 8;
+constexpr int MS_W = 2 * MS_D + 1;
+// The matrix, then per stencil slot W_lk vs(b_k) while it is built, whose room
+// the two force buffers of the iterations take over.
+__host__ __device__ inline size_t ms_smem_bytes(int Lb, int S)
+{
+    return up16(sizeof(float) * ((size_t)Lb * MS_W + (size_t)Lb * (S > 4 ? S : 4)));
+}
+// Whether the marker-space loop runs: a ring of at least MS_W markers (so the
+// MS_W neighbours of a marker are distinct) whose matrix fits beside the band
+// layout (`base` bytes).  Host sizing and kernel use the same test.
+__host__ __device__ inline bool ms_fits(size_t base, int Lb, int S)
+{
+    return Lb >= MS_W && base + ms_smem_bytes(Lb, S) <= (size_t)IBM_SMEM_LIMIT;
+}
+__device__ __forceinline__ int ms_ring(int m, int Lb) { return m + (m < 0 ? Lb : 0) - (m >= Lb ? Lb : 0); }
+// Barrier `id` over the first n threads of the block (n a multiple of 32).
+__device__ __forceinline__ void bar_sync_n(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 inline bool mlp_on(const iblbm_ibm_args&) { return false; }
+inline bool ms_on(const iblbm_ibm_args&) { return false; }
+inline bool ms_on(const iblbm_ibm32_args& a) { return a.method == IBM_MDF && !a.mdf_coupled; }
 inline bool mlp_on(const iblbm_ibm32_args& a)
 {
     return a.mlp_mode != 0 && a.method == IBM_MDF && !a.mdf_coupled;
@@ -83,8 +108,8 @@ inline bool mlp_on(const iblbm_ibm32_args& a)
 // Shared-memory layout.  The "static" block (everything a fixed body keeps
 // between steps) is contiguous so that one bulk copy restores it.
 struct Layout {
-    size_t o_sidx, o_ent, o_cstart, o_nodes, o_part, o_wx, o_wy, o_entw, static_bytes;
-    size_t o_dvx, o_dvy, o_R, o_Lux, o_Luy, o_Lfx, o_Lfy, o_bro, o_bwx, o_bwy, o_wred, o_ix0, o_iy0, o_ired, total;
+    size_t o_sidx, o_ent, o_cstart, o_nodes, o_part, o_wx, o_wy, o_entw, o_ix0, o_iy0, static_bytes;
+    size_t o_dvx, o_dvy, o_R, o_Lux, o_Luy, o_Lfx, o_Lfy, o_bro, o_bwx, o_bwy, o_wred, o_ired, total;
 };
 
 template <typename R>
@@ -100,6 +125,8 @@ __host__ __device__ inline Layout make_layout(int Lb, int NB, int S)
     L.o_wx = o; o = up16(o + sizeof(R) * (size_t)Lb * 5);
     L.o_wy = o; o = up16(o + sizeof(R) * (size_t)Lb * 5);
     L.o_entw = o; o = up16(o + sizeof(R) * (size_t)Lb * S);
+    L.o_ix0 = o; o = up16(o + sizeof(int) * (size_t)Lb);
+    L.o_iy0 = o; o = up16(o + sizeof(int) * (size_t)Lb);
     L.static_bytes = o;
     L.o_dvx = o; o = up16(o + sizeof(R) * (size_t)Lb);
     L.o_dvy = o; o = up16(o + sizeof(R) * (size_t)Lb);
@@ -112,8 +139,6 @@ __host__ __device__ inline Layout make_layout(int Lb, int NB, int S)
     L.o_bwx = o; o = up16(o + sizeof(R) * (size_t)NB);
     L.o_bwy = o; o = up16(o + sizeof(R) * (size_t)NB);
     L.o_wred = o; o = up16(o + sizeof(double) * 2 * MAXP * NWARP);
-    L.o_ix0 = o; o = up16(o + sizeof(int) * (size_t)Lb);
-    L.o_iy0 = o; o = up16(o + sizeof(int) * (size_t)Lb);
     L.o_ired = o; o = up16(o + sizeof(int) * 64);
     L.total = o;
     return L;
@@ -332,7 +357,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const Layout Lay = make_layout<R>(Lb, NB, S);
     Sm<R> sh = carve<R>(smem_raw, Lay);
-    __shared__ int s_nb, s_status, s_box[4], s_step;
+    __shared__ int s_nb, s_status, s_box[4], s_step, s_cur;
     __shared__ __align__(8) uint64_t s_bar, s_wbar;
     const bool rebuild = a.rebuild || a.xt_table;
     // an early return first waits (bounded) for the network copy in flight
@@ -785,7 +810,161 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         double prev = INFINITY, last = INFINITY;
         int iter_count = 0, diverged = 0, converged = 0, guard = 0;
         __syncthreads();
-        for (int it = 0; it < a.mdf_iterations; ++it) {
+        bool node_loop = true;
+        if constexpr (SHIFTED && !COUPLED) {
+            // ---- marker-space iterations (FP32 form, one body) ---------------------
+            // An iteration changes the working velocity at the band nodes by
+            // vs * spread(omega Lf), so marker l's interpolated velocity is
+            // u_l = u0_l + sum_m A_lm G_m, with G_m the force marker m has
+            // accumulated (sum of omega Lf) and
+            // A_lm = sum over the nodes both stencils cover of W_l vs W_m ds_m.
+            // A is built once per step (banded: markers couple only to their
+            // neighbours on the body), the iterations run on the markers alone
+            // (one barrier of the marker-owning warps each), and the accumulated
+            // forces are spread to the nodes once.  The operator is the node-space
+            // loop's; that loop stays for coupled bodies, for marker sets that do
+            // not fit, and wherever the overlaps do not account for every entry of
+            // the node lists.
+            const size_t off = Lay.total + (a.mlp_mode ? mlp_smem_bytes(Lb) : 0);
+            if (ms_fits(off, Lb, S)) {
+                float* msA = reinterpret_cast<float*>(smem_raw + off);
+                float* msP = msA + (size_t)Lb * MS_W;  // W_lk vs(b_k) per stencil slot, while A is built
+                float* msG = msP;                      // then [2 buffers][x, y][Lb] of accumulated force
+                for (int e = tid; e < Lb * S; e += IBM_THREADS) {
+                    const int l = e / S, k = e - l * S;
+                    msP[e] = wgt<A>(sh, l, k) * (dt / ((R)2 * sh.bro[sh.sidx[e]]));
+                }
+                __syncthreads();
+                // slot i of marker m covers the lattice column of slot i + ox of
+                // marker l, ox = ix0_m - ix0_l (rows alike): A_lm sums W_l vs over
+                // the overlap of the two stencils times m's entry weight wx wy ds
+                for (int e = tid; e < Lb * MS_W; e += IBM_THREADS) {
+                    const int l = e / MS_W, j = e - l * MS_W;
+                    const int m = ms_ring(l + j - MS_D, Lb);
+                    const int ox = sh.ix0[m] - sh.ix0[l], oy = sh.iy0[m] - sh.iy0[l];
+                    R acc = 0;
+                    if (ox > -SW && ox < SW && oy > -SW && oy < SW) {
+                        const R La = (R)a.larea[sh.part[m]];
+                        const float* pl = msP + (size_t)l * S;
+                        const int i0 = max(0, ox), i1 = min(SW, SW + ox);
+                        const int j0 = max(0, oy), j1 = min(SW, SW + oy);
+                        for (int i = i0; i < i1; ++i) {
+                            const R wxm = sh.wx[m * 5 + i - ox];
+                            for (int jj = j0; jj < j1; ++jj)
+                                acc += pl[i * SW + jj] * ((wxm * sh.wy[m * 5 + jj - oy]) * La);
+                        }
+                    }
+                    msA[e] = acc;
+                }
+                // the overlaps must account for every entry of the lists at marker
+                // l's nodes (a marker further along the body, or stencil slots
+                // clamped onto one edge node, are not covered by A)
+                R u0x = 0, u0y = 0;
+                int over = 0;
+                if (own) {
+                    int n_list = 0, n_geo = 0;
+#pragma unroll 5
+                    for (int k = 0; k < S; ++k) {
+                        const int b = sh.sidx[lo * S + k];
+                        const R w = wgt<A>(sh, lo, k);
+                        u0x += sh.bwx[b] * w;
+                        u0y += sh.bwy[b] * w;
+                        n_list += sh.cstart[b + 1] - sh.cstart[b];
+                    }
+#pragma unroll
+                    for (int j = 0; j < MS_W; ++j) {
+                        const int m = ms_ring(lo + j - MS_D, Lb);
+                        const int ox = abs(sh.ix0[m] - sh.ix0[lo]), oy = abs(sh.iy0[m] - sh.iy0[lo]);
+                        if (ox < SW && oy < SW) n_geo += (SW - ox) * (SW - oy);
+                    }
+                    over = n_list != n_geo;
+                }
+                if (!__syncthreads_or(over)) {
+                    node_loop = false;
+                    for (int e = tid; e < 4 * Lb; e += IBM_THREADS) msG[e] = 0.0f;
+                    __syncthreads();
+                    const int nthr = (Lb + 31) & ~31;  // the warps that own markers
+                    if (tid < nthr) {
+                        const int nw = nthr >> 5;
+                        int cur = 0;
+                        R ux = 0, uy = 0;
+                        for (int it = 0; it < a.mdf_iterations; ++it) {
+                            double* wr = sh.wred + (it & 1) * MAXP * NWARP;
+                            const R omega = (R)omega_d;
+                            double rl = -INFINITY;
+                            const float* Gx = msG + cur * 2 * Lb;
+                            const float* Gy = Gx + Lb;
+                            float* Nx = msG + (cur ^ 1) * 2 * Lb;
+                            float* Ny = Nx + Lb;
+                            if (own) {
+                                R sx = 0, sy = 0;
+#pragma unroll
+                                for (int j = 0; j < MS_W; ++j) {
+                                    const int m = ms_ring(lo + j - MS_D, Lb);
+                                    const R aw = msA[lo * MS_W + j];
+                                    sx += aw * Gx[m];
+                                    sy += aw * Gy[m];
+                                }
+                                ux = u0x + sx;
+                                uy = u0y + sy;
+                                const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
+                                rl = sqrt(ex * ex + ey * ey);
+                                const R fx = (R)2 * Rl * (dvx - ux), fy = (R)2 * Rl * (dvy - uy);
+                                lfx = unit_dt ? fx : fx / dt;
+                                lfy = unit_dt ? fy : fy / dt;
+                                // next forces, kept only if this iteration is accepted
+                                Nx[lo] = Gx[lo] + omega * lfx;
+                                Ny[lo] = Gy[lo] + omega * lfy;
+                            }
+                            const double v = warp_nanmax(rl);
+                            if (lane == 0) wr[wid] = v;
+                            bar_sync_n(1, nthr);
+                            double residual = -INFINITY;
+                            for (int w = 0; w < nw; ++w) residual = nanmax(residual, wr[w]);
+                            last = residual;
+                            if (it > 0 && residual > prev * 1.5) {
+                                diverged = 1;
+                                iter_count = it + 1;
+                                break;
+                            }
+                            if (mlp_rec && own) {
+                                mlp_gx += omega * lfx;
+                                mlp_gy += omega * lfy;
+                            }
+                            cur ^= 1;
+                            prev = residual;
+                            iter_count = it + 1;
+                            if ((it + 1) >= min_iter && residual < a.mdf_tol) {
+                                converged = 1;
+                                break;
+                            }
+                        }
+                        if (own) {
+                            sh.Lux[lo] = ux;
+                            sh.Luy[lo] = uy;
+                            sh.Lfx[lo] = lfx;
+                            sh.Lfy[lo] = lfy;
+                        }
+                        if (tid == 0) s_cur = cur;
+                    }
+                    __syncthreads();
+                    guard = -1;  // reported in stats[3]: the iterations ran in marker space
+                    const float* Gx = msG + s_cur * 2 * Lb;
+                    const float* Gy = Gx + Lb;
+#pragma unroll
+                    for (int jn = 0; jn < NPT; ++jn) {
+                        const int b = tid + jn * IBM_THREADS;
+                        if (b < nb) {
+                            R tx, ty;
+                            spread2(sh, Gx, Gy, sh.cstart[b], sh.cstart[b + 1], tx, ty);
+                            ftx[jn] += tx;
+                            fty[jn] += ty;
+                        }
+                    }
+                }
+            }
+        }
+        for (int it = 0; node_loop && it < a.mdf_iterations; ++it) {
             double* wr = sh.wred + (it & 1) * MAXP * NWARP;
             const R omega = (R)omega_d;
             // phase A: interpolate the working velocity, slip residual, force
@@ -1082,6 +1261,7 @@ static size_t ibm_smem(const ARGS& a)
     const int S = a.delta_type == 0 ? 25 : 9;
     size_t t = make_layout<R>(a.lb_total, a.band_capacity, S).total;
     if (mlp_on(a)) t += mlp_smem_bytes(a.lb_total);
+    if (ms_on(a) && ms_fits(t, a.lb_total, S)) t += ms_smem_bytes(a.lb_total, S);
     return t;
 }
 

@@ -607,7 +607,8 @@ class Engine:
         s = self.d_stats.cpu().numpy()
         d = self.d_dstats.cpu().numpy()
         return {"iter_count": int(s[0]), "diverged": bool(s[1]), "converged": bool(s[2]),
-                "guard_trips": int(s[3]), "last_residual": float(d[0]), "omega_used": float(d[1])}
+                "guard_trips": max(int(s[3]), 0), "marker_space": int(s[3]) == -1,
+                "last_residual": float(d[0]), "omega_used": float(d[1])}
 
     def status(self):
         """Band-kernel status word (0 = ok); a pipeline timeout of the FP32 pass

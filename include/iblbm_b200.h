@@ -146,8 +146,9 @@ typedef struct {
     int *iscratch;                     /* >= iblbm_ibm_scratch_ints(...) ints */
     /* per-marker outputs (Lb_total): interpolated velocity, force, DFC force */
     double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
-    /* stats: [iter_count, diverged, converged, guard_trips, status],
-     * dstats: [last_residual, omega_used] */
+    /* stats: [iter_count, diverged, converged, guard_trips, status]
+     * (guard_trips: coupled MDF; -1 when the FP32 band step ran a single
+     * body's MDF iterations in marker space), dstats: [last_residual, omega_used] */
     int *stats;
     double *dstats;
     /* reference-shaped calls (iblbm/gpu_kernels.py:956-1223): the band takes

@@ -229,3 +229,21 @@ def test_band_capacity_overflow_reports_status(torch):
     torch.cuda.synchronize()
     assert int(e.d_stats[4].item()) == 1
     assert int(e.d_count.item()) == 0
+
+
+def test_marker_space_mdf_and_fallback(torch):
+    """A single body's MDF iterations run in marker space (stats[3] = -1) when
+    the overlaps of neighbouring markers' stencils account for every entry of
+    the node lists; a body whose stencils are clamped onto the wall nodes takes
+    the node-space loop instead.  Both agree with the FP64 form."""
+    base = dict(Re=40, NN=49, xmax=2, ymax=1, cylinder_D_ratio=0.25, lattice_u=0.05, inflow_u=0.05,
+                bc_type="dirichlet_neumann", delta_type="peskin4pt", ibm_method="MDF", collision_model="TRT",
+                trt_magic_param=0.1875, mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                marker_spacing_factor=1.0, max_steps=200, use_convergence=False, check_interval=50)
+    for center, marker_space in (((0.45, 0.5), True), ((0.45, 0.15), False)):
+        cfg = _cfg(dict(base, cylinder_center=center))
+        r64, r32 = _pair(cfg)
+        assert r32["engine"].mdf_stats()["marker_space"] is marker_space, center
+        assert not r64["engine"].mdf_stats()["marker_space"]
+        _check_fields(cfg, r64, r32)
+        _check_forces(r64, r32)
