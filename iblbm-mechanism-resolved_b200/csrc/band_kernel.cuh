@@ -830,6 +830,8 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 float* msA = reinterpret_cast<float*>(smem_raw + off);
                 float* msP = msA + (size_t)Lb * MS_W;  // W_lk vs(b_k) per stencil slot, while A is built
                 float* msG = msP;                      // then [2 buffers][x, y][Lb] of accumulated force
+                __shared__ R s_la[MAXP];
+                if (tid < P) s_la[tid] = (R)a.larea[tid];
                 for (int e = tid; e < Lb * S; e += IBM_THREADS) {
                     const int l = e / S, k = e - l * S;
                     msP[e] = wgt<A>(sh, l, k) * (dt / ((R)2 * sh.bro[sh.sidx[e]]));
@@ -837,24 +839,38 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 __syncthreads();
                 // slot i of marker m covers the lattice column of slot i + ox of
                 // marker l, ox = ix0_m - ix0_l (rows alike): A_lm sums W_l vs over
-                // the overlap of the two stencils times m's entry weight wx wy ds
+                // the overlap of the two stencils times m's entry weight (wx wy) ds.
+                // Entries in j-major order (a warp shares the neighbour offset),
+                // each over the full SW x SW slot grid with slots outside the
+                // overlap weighted 0 (loads clamped in bounds).
                 for (int e = tid; e < Lb * MS_W; e += IBM_THREADS) {
-                    const int l = e / MS_W, j = e - l * MS_W;
+                    const int j = e / Lb, l = e - j * Lb;
                     const int m = ms_ring(l + j - MS_D, Lb);
                     const int ox = sh.ix0[m] - sh.ix0[l], oy = sh.iy0[m] - sh.iy0[l];
                     R acc = 0;
                     if (ox > -SW && ox < SW && oy > -SW && oy < SW) {
-                        const R La = (R)a.larea[sh.part[m]];
+                        const R La = s_la[sh.part[m]];
                         const float* pl = msP + (size_t)l * S;
-                        const int i0 = max(0, ox), i1 = min(SW, SW + ox);
-                        const int j0 = max(0, oy), j1 = min(SW, SW + oy);
-                        for (int i = i0; i < i1; ++i) {
-                            const R wxm = sh.wx[m * 5 + i - ox];
-                            for (int jj = j0; jj < j1; ++jj)
-                                acc += pl[i * SW + jj] * ((wxm * sh.wy[m * 5 + jj - oy]) * La);
+                        R wym[SW];
+#pragma unroll
+                        for (int jj = 0; jj < SW; ++jj) {
+                            const int t = jj - oy;
+                            const R w = sh.wy[m * 5 + min(max(t, 0), SW - 1)];
+                            wym[jj] = (t >= 0 && t < SW) ? w : (R)0;
+                        }
+#pragma unroll 1
+                        for (int i = 0; i < SW; ++i) {
+                            const int t = i - ox;
+                            const R wxm = sh.wx[m * 5 + min(max(t, 0), SW - 1)];
+                            const bool in = t >= 0 && t < SW;
+#pragma unroll
+                            for (int jj = 0; jj < SW; ++jj) {
+                                const R ew = in ? (wxm * wym[jj]) * La : (R)0;
+                                acc += pl[i * SW + jj] * ew;
+                            }
                         }
                     }
-                    msA[e] = acc;
+                    msA[l * MS_W + j] = acc;
                 }
                 // the overlaps must account for every entry of the lists at marker
                 // l's nodes (a marker further along the body, or stencil slots
@@ -863,7 +879,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 int over = 0;
                 if (own) {
                     int n_list = 0, n_geo = 0;
-#pragma unroll 5
+#pragma unroll SW
                     for (int k = 0; k < S; ++k) {
                         const int b = sh.sidx[lo * S + k];
                         const R w = wgt<A>(sh, lo, k);
@@ -871,10 +887,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                         u0y += sh.bwy[b] * w;
                         n_list += sh.cstart[b + 1] - sh.cstart[b];
                     }
+                    const int x0 = sh.ix0[lo], y0 = sh.iy0[lo];
 #pragma unroll
                     for (int j = 0; j < MS_W; ++j) {
                         const int m = ms_ring(lo + j - MS_D, Lb);
-                        const int ox = abs(sh.ix0[m] - sh.ix0[lo]), oy = abs(sh.iy0[m] - sh.iy0[lo]);
+                        const int ox = abs(sh.ix0[m] - x0), oy = abs(sh.iy0[m] - y0);
                         if (ox < SW && oy < SW) n_geo += (SW - ox) * (SW - oy);
                     }
                     over = n_list != n_geo;
