@@ -84,7 +84,8 @@ constexpr int MS_W = 2 * MS_D + 1;
 // the two force buffers of the iterations take over.
 __host__ __device__ inline size_t ms_smem_bytes(int Lb, int S)
 {
-    return up16(sizeof(float) * ((size_t)Lb * MS_W + (size_t)Lb * (S > 4 ? S : 4)));
+    const size_t build = (size_t)Lb * S, iterate = 4 * ((size_t)Lb + 2 * MS_D);
+    return up16(sizeof(float) * ((size_t)Lb * MS_W + (build > iterate ? build : iterate)));
 }
 // Whether the marker-space loop runs: a ring of at least MS_W markers (so the
 // MS_W neighbours of a marker are distinct) whose matrix fits beside the band
@@ -181,6 +182,17 @@ __device__ inline Sm<R> carve(char* base, const Layout& L)
 }
 
 __device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
+
+// Warp maximum of 64-bit patterns of non-negative doubles or NaNs: for those
+// the unsigned order of the patterns is the numeric order, with every NaN above
+// every number (as nanmax keeps a NaN).
+__device__ __forceinline__ unsigned long long warp_max_bits(unsigned long long v)
+{
+    const unsigned hi = (unsigned)(v >> 32);
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? (unsigned)v : 0u);
+    return ((unsigned long long)mh << 32) | ml;
+}
 
 __device__ __forceinline__ double warp_nanmax(double v)
 {
@@ -810,7 +822,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         double prev = INFINITY, last = INFINITY;
         int iter_count = 0, diverged = 0, converged = 0, guard = 0;
         __syncthreads();
-        bool node_loop = true;
+        // marker space (FP32 form, one body): set once the coupling matrix is built
+        bool marker_space = false;
+        float* msA = nullptr;
+        float* msG = nullptr;
+        R u0x = 0, u0y = 0;
         if constexpr (SHIFTED && !COUPLED) {
             // ---- marker-space iterations (FP32 form, one body) ---------------------
             // An iteration changes the working velocity at the band nodes by
@@ -827,9 +843,9 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             // the node lists.
             const size_t off = Lay.total + (a.mlp_mode ? mlp_smem_bytes(Lb) : 0);
             if (ms_fits(off, Lb, S)) {
-                float* msA = reinterpret_cast<float*>(smem_raw + off);
+                msA = reinterpret_cast<float*>(smem_raw + off);
                 float* msP = msA + (size_t)Lb * MS_W;  // W_lk vs(b_k) per stencil slot, while A is built
-                float* msG = msP;                      // then [2 buffers][x, y][Lb] of accumulated force
+                msG = msP;  // then [2 buffers][x, y][MS_D + Lb + MS_D]: accumulated force with ring halos
                 __shared__ R s_la[MAXP];
                 if (tid < P) s_la[tid] = (R)a.larea[tid];
                 for (int e = tid; e < Lb * S; e += IBM_THREADS) {
@@ -875,7 +891,6 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 // the overlaps must account for every entry of the lists at marker
                 // l's nodes (a marker further along the body, or stencil slots
                 // clamped onto one edge node, are not covered by A)
-                R u0x = 0, u0y = 0;
                 int over = 0;
                 if (own) {
                     int n_list = 0, n_geo = 0;
@@ -896,221 +911,238 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                     }
                     over = n_list != n_geo;
                 }
-                if (!__syncthreads_or(over)) {
-                    node_loop = false;
-                    for (int e = tid; e < 4 * Lb; e += IBM_THREADS) msG[e] = 0.0f;
-                    __syncthreads();
-                    const int nthr = (Lb + 31) & ~31;  // the warps that own markers
-                    if (tid < nthr) {
-                        const int nw = nthr >> 5;
-                        int cur = 0;
-                        R ux = 0, uy = 0;
-                        for (int it = 0; it < a.mdf_iterations; ++it) {
-                            double* wr = sh.wred + (it & 1) * MAXP * NWARP;
-                            const R omega = (R)omega_d;
-                            double rl = -INFINITY;
-                            const float* Gx = msG + cur * 2 * Lb;
-                            const float* Gy = Gx + Lb;
-                            float* Nx = msG + (cur ^ 1) * 2 * Lb;
-                            float* Ny = Nx + Lb;
-                            if (own) {
-                                R sx = 0, sy = 0;
-#pragma unroll
-                                for (int j = 0; j < MS_W; ++j) {
-                                    const int m = ms_ring(lo + j - MS_D, Lb);
-                                    const R aw = msA[lo * MS_W + j];
-                                    sx += aw * Gx[m];
-                                    sy += aw * Gy[m];
-                                }
-                                ux = u0x + sx;
-                                uy = u0y + sy;
-                                const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
-                                rl = sqrt(ex * ex + ey * ey);
-                                const R fx = (R)2 * Rl * (dvx - ux), fy = (R)2 * Rl * (dvy - uy);
-                                lfx = unit_dt ? fx : fx / dt;
-                                lfy = unit_dt ? fy : fy / dt;
-                                // next forces, kept only if this iteration is accepted
-                                Nx[lo] = Gx[lo] + omega * lfx;
-                                Ny[lo] = Gy[lo] + omega * lfy;
-                            }
-                            const double v = warp_nanmax(rl);
-                            if (lane == 0) wr[wid] = v;
-                            bar_sync_n(1, nthr);
-                            double residual = -INFINITY;
-                            for (int w = 0; w < nw; ++w) residual = nanmax(residual, wr[w]);
-                            last = residual;
-                            if (it > 0 && residual > prev * 1.5) {
-                                diverged = 1;
-                                iter_count = it + 1;
-                                break;
-                            }
-                            if (mlp_rec && own) {
-                                mlp_gx += omega * lfx;
-                                mlp_gy += omega * lfy;
-                            }
-                            cur ^= 1;
-                            prev = residual;
-                            iter_count = it + 1;
-                            if ((it + 1) >= min_iter && residual < a.mdf_tol) {
-                                converged = 1;
-                                break;
-                            }
-                        }
-                        if (own) {
-                            sh.Lux[lo] = ux;
-                            sh.Luy[lo] = uy;
-                            sh.Lfx[lo] = lfx;
-                            sh.Lfy[lo] = lfy;
-                        }
-                        if (tid == 0) s_cur = cur;
-                    }
-                    __syncthreads();
-                    guard = -1;  // reported in stats[3]: the iterations ran in marker space
-                    const float* Gx = msG + s_cur * 2 * Lb;
-                    const float* Gy = Gx + Lb;
-#pragma unroll
-                    for (int jn = 0; jn < NPT; ++jn) {
-                        const int b = tid + jn * IBM_THREADS;
-                        if (b < nb) {
-                            R tx, ty;
-                            spread2(sh, Gx, Gy, sh.cstart[b], sh.cstart[b + 1], tx, ty);
-                            ftx[jn] += tx;
-                            fty[jn] += ty;
-                        }
-                    }
-                }
+                marker_space = !__syncthreads_or(over);
             }
         }
-        for (int it = 0; node_loop && it < a.mdf_iterations; ++it) {
-            double* wr = sh.wred + (it & 1) * MAXP * NWARP;
-            const R omega = (R)omega_d;
-            // phase A: interpolate the working velocity, slip residual, force
-            double rl = -INFINITY;
-            if (own) {
-                R ux = 0, uy = 0;
+        if (marker_space) {
+            if constexpr (SHIFTED && !COUPLED) {
+                // MDF iterations on the markers: u_l = u0_l + sum_j A_l,j G_(l+j-MS_D)
+                const int LH = Lb + 2 * MS_D;
+                for (int e = tid; e < 4 * LH; e += IBM_THREADS) msG[e] = 0.0f;
+                R arow[MS_W];
 #pragma unroll
-                for (int gi = 0; gi < SW; ++gi) {  // one stencil row (di) at a time, slots in order
-                    R vx[SW], vy[SW];
+                for (int j = 0; j < MS_W; ++j) arow[j] = own ? msA[lo * MS_W + j] : (R)0;
+                __syncthreads();
+                const int nthr = (Lb + 31) & ~31;  // the warps that own markers
+                if (tid < nthr) {
+                    const int nw = nthr >> 5;
+                    int cur = 0;
+                    R ux = 0, uy = 0;
+                    for (int it = 0; it < a.mdf_iterations; ++it) {
+                        const R omega = (R)omega_d;
+                        const float* Gx = msG + cur * 2 * LH;  // marker m at Gx[m + MS_D]
+                        const float* Gy = Gx + LH;
+                        float* Nx = msG + (cur ^ 1) * 2 * LH;
+                        float* Ny = Nx + LH;
+                        // squared slip as its FP64 bit pattern (0 for lanes without a marker)
+                        unsigned long long key = 0;
+                        if (own) {
+                            R sx = 0, sy = 0;
 #pragma unroll
-                    for (int gj = 0; gj < SW; ++gj) {
-                        vx[gj] = sh.bwx[hb[gi * SW + gj]];
-                        vy[gj] = sh.bwy[hb[gi * SW + gj]];
-                    }
-#pragma unroll
-                    for (int gj = 0; gj < SW; ++gj) {
-                        const R w = hwx[gi] * hwy[gj];
-                        ux += vx[gj] * w;
-                        uy += vy[gj] * w;
-                    }
-                }
-                sh.Lux[lo] = ux;
-                sh.Luy[lo] = uy;
-                // slip norm in FP64 (exact differences of the R values)
-                const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
-                rl = sqrt(ex * ex + ey * ey);
-                R fx, fy;
-                if (incomp) { fx = (R)2 * (dvx - ux); fy = (R)2 * (dvy - uy); }
-                else { fx = (R)2 * Rl * (dvx - ux); fy = (R)2 * Rl * (dvy - uy); }
-                lfx = unit_dt ? fx : fx / dt;
-                lfy = unit_dt ? fy : fy / dt;
-                sh.Lfx[lo] = lfx;
-                sh.Lfy[lo] = lfy;
-            }
-            if (!COUPLED) {
-                const double v = warp_nanmax(rl);
-                if (lane == 0) wr[wid] = v;
-            } else {
-                for (int p = 0; p < P; ++p) {
-                    const double v = warp_nanmax((own && pl == p) ? rl : -INFINITY);
-                    if (lane == 0) wr[p * NWARP + wid] = v;
-                }
-            }
-            __syncthreads();  // (a)
-            double residual;
-            if (!COUPLED) {
-                residual = -INFINITY;
-#pragma unroll
-                for (int w = 0; w < NWARP; ++w) residual = nanmax(residual, wr[w]);
-            } else {
-                residual = 0.0;  // Python max over the particles' numpy maxima, from 0.0
-                for (int p = 0; p < P; ++p) {
-                    double rp = -INFINITY;
-#pragma unroll
-                    for (int w = 0; w < NWARP; ++w) rp = nanmax(rp, wr[p * NWARP + w]);
-                    if (rp > residual) residual = rp;
-                }
-            }
-            last = residual;
-            if (!COUPLED) {
-                if (it > 0 && residual > prev * 1.5) {
-                    diverged = 1;
-                    iter_count = it + 1;
-                    break;
-                }
-            } else if (it > 0 && residual > prev * 1.2) {
-                guard += 1;
-                omega_d = fmax(omega_d * 0.5, omega_min);
-                if (omega_d <= omega_min) {
-                    diverged = 1;
-                    break;
-                }
-                prev = residual;
-                continue;
-            }
-            if (mlp_rec && own) {
-                mlp_gx += omega * lfx;
-                mlp_gy += omega * lfy;
-            }
-            // phase B: spread, relax, update the working velocity of the owned nodes
-#pragma unroll
-            for (int jn = 0; jn < NPT; ++jn) {
-                const int b = tid + jn * IBM_THREADS;
-                if (b < nb) {
-                    const int u0 = sh.cstart[b], u1 = sh.cstart[b + 1];
-                    R tx, ty;
-                    if (!COUPLED) {
-                        R ax, ay;
-                        spread2(sh, sh.Lfx, sh.Lfy, u0, u1, ax, ay);
-                        tx = ax * omega;
-                        ty = ay * omega;
-                    } else {
-                        tx = 0;
-                        ty = 0;
-                        for (int p = 0; p < P; ++p) {
-                            R ax = 0, ay = 0;
-                            for (int u = u0; u < u1; ++u) {
-                                const int l = sh.ent[u] >> 5;
-                                if (sh.part[l] != p) continue;
-                                ax += sh.Lfx[l] * sh.entw[u];
-                                ay += sh.Lfy[l] * sh.entw[u];
+                            for (int j = 0; j < MS_W; ++j) {
+                                sx += arow[j] * Gx[lo + j];
+                                sy += arow[j] * Gy[lo + j];
                             }
-                            const R fx = ax * omega, fy = ay * omega;
-                            if (a.band_fib_part) {
-                                a.band_fib_part[p * pstride + 2 * b] += fx;
-                                a.band_fib_part[p * pstride + 2 * b + 1] += fy;
-                            }
-                            tx += fx;
-                            ty += fy;
+                            ux = u0x + sx;
+                            uy = u0y + sy;
+                            const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
+                            key = (unsigned long long)__double_as_longlong(ex * ex + ey * ey);
+                            const R fx = (R)2 * Rl * (dvx - ux), fy = (R)2 * Rl * (dvy - uy);
+                            lfx = unit_dt ? fx : fx / dt;
+                            lfy = unit_dt ? fy : fy / dt;
+                            // next forces, kept only if this iteration is accepted
+                            const R nx = Gx[lo + MS_D] + omega * lfx, ny = Gy[lo + MS_D] + omega * lfy;
+                            Nx[lo + MS_D] = nx;
+                            Ny[lo + MS_D] = ny;
+                            if (lo < MS_D) { Nx[lo + Lb + MS_D] = nx; Ny[lo + Lb + MS_D] = ny; }
+                            if (lo >= Lb - MS_D) { Nx[lo - Lb + MS_D] = nx; Ny[lo - Lb + MS_D] = ny; }
+                        }
+                        // residual = max_l sqrt(slip^2) = sqrt(max_l slip^2) (sqrt is monotone
+                        // and correctly rounded); the max runs on the bit patterns
+                        unsigned long long* wk = reinterpret_cast<unsigned long long*>(sh.wred) + (it & 1) * NWARP;
+                        const unsigned long long wmax = warp_max_bits(key);
+                        if (lane == 0) wk[wid] = wmax;
+                        bar_sync_n(1, nthr);
+                        unsigned long long mk = 0;
+#pragma unroll
+                        for (int w = 0; w < NWARP; ++w) {
+                            const unsigned long long v = w < nw ? wk[w] : 0ull;
+                            mk = v > mk ? v : mk;
+                        }
+                        const double residual = sqrt(__longlong_as_double((long long)mk));
+                        last = residual;
+                        if (it > 0 && residual > prev * 1.5) {
+                            diverged = 1;
+                            iter_count = it + 1;
+                            break;
+                        }
+                        if (mlp_rec && own) {
+                            mlp_gx += omega * lfx;
+                            mlp_gy += omega * lfy;
+                        }
+                        cur ^= 1;
+                        prev = residual;
+                        iter_count = it + 1;
+                        if ((it + 1) >= min_iter && residual < a.mdf_tol) {
+                            converged = 1;
+                            break;
                         }
                     }
-                    ftx[jn] += tx;
-                    fty[jn] += ty;
-                    if (incomp) {
-                        sh.bwx[b] += (R)0.5 * tx * dt;
-                        sh.bwy[b] += (R)0.5 * ty * dt;
-                    } else {
-                        sh.bwx[b] += tx * vs[jn];
-                        sh.bwy[b] += ty * vs[jn];
+                    if (own) {
+                        sh.Lux[lo] = ux;
+                        sh.Luy[lo] = uy;
+                        sh.Lfx[lo] = lfx;
+                        sh.Lfy[lo] = lfy;
+                    }
+                    if (tid == 0) s_cur = cur;
+                }
+                __syncthreads();
+                guard = -1;  // reported in stats[3]: the iterations ran in marker space
+                const float* Gx = msG + s_cur * 2 * LH + MS_D;
+                const float* Gy = Gx + LH;
+#pragma unroll
+                for (int jn = 0; jn < NPT; ++jn) {
+                    const int b = tid + jn * IBM_THREADS;
+                    if (b < nb) {
+                        R tx, ty;
+                        spread2(sh, Gx, Gy, sh.cstart[b], sh.cstart[b + 1], tx, ty);
+                        ftx[jn] += tx;
+                        fty[jn] += ty;
                     }
                 }
             }
-            __syncthreads();  // (b)
-            prev = residual;
-            if (COUPLED) iter_count += 1;
-            else iter_count = it + 1;
-            if ((it + 1) >= min_iter && residual < a.mdf_tol) {
-                converged = 1;
-                break;
+        } else {
+            for (int it = 0; it < a.mdf_iterations; ++it) {
+                double* wr = sh.wred + (it & 1) * MAXP * NWARP;
+                const R omega = (R)omega_d;
+                // phase A: interpolate the working velocity, slip residual, force
+                double rl = -INFINITY;
+                if (own) {
+                    R ux = 0, uy = 0;
+#pragma unroll
+                    for (int gi = 0; gi < SW; ++gi) {  // one stencil row (di) at a time, slots in order
+                        R vx[SW], vy[SW];
+#pragma unroll
+                        for (int gj = 0; gj < SW; ++gj) {
+                            vx[gj] = sh.bwx[hb[gi * SW + gj]];
+                            vy[gj] = sh.bwy[hb[gi * SW + gj]];
+                        }
+#pragma unroll
+                        for (int gj = 0; gj < SW; ++gj) {
+                            const R w = hwx[gi] * hwy[gj];
+                            ux += vx[gj] * w;
+                            uy += vy[gj] * w;
+                        }
+                    }
+                    sh.Lux[lo] = ux;
+                    sh.Luy[lo] = uy;
+                    // slip norm in FP64 (exact differences of the R values)
+                    const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
+                    rl = sqrt(ex * ex + ey * ey);
+                    R fx, fy;
+                    if (incomp) { fx = (R)2 * (dvx - ux); fy = (R)2 * (dvy - uy); }
+                    else { fx = (R)2 * Rl * (dvx - ux); fy = (R)2 * Rl * (dvy - uy); }
+                    lfx = unit_dt ? fx : fx / dt;
+                    lfy = unit_dt ? fy : fy / dt;
+                    sh.Lfx[lo] = lfx;
+                    sh.Lfy[lo] = lfy;
+                }
+                if (!COUPLED) {
+                    const double v = warp_nanmax(rl);
+                    if (lane == 0) wr[wid] = v;
+                } else {
+                    for (int p = 0; p < P; ++p) {
+                        const double v = warp_nanmax((own && pl == p) ? rl : -INFINITY);
+                        if (lane == 0) wr[p * NWARP + wid] = v;
+                    }
+                }
+                __syncthreads();  // (a)
+                double residual;
+                if (!COUPLED) {
+                    residual = -INFINITY;
+#pragma unroll
+                    for (int w = 0; w < NWARP; ++w) residual = nanmax(residual, wr[w]);
+                } else {
+                    residual = 0.0;  // Python max over the particles' numpy maxima, from 0.0
+                    for (int p = 0; p < P; ++p) {
+                        double rp = -INFINITY;
+#pragma unroll
+                        for (int w = 0; w < NWARP; ++w) rp = nanmax(rp, wr[p * NWARP + w]);
+                        if (rp > residual) residual = rp;
+                    }
+                }
+                last = residual;
+                if (!COUPLED) {
+                    if (it > 0 && residual > prev * 1.5) {
+                        diverged = 1;
+                        iter_count = it + 1;
+                        break;
+                    }
+                } else if (it > 0 && residual > prev * 1.2) {
+                    guard += 1;
+                    omega_d = fmax(omega_d * 0.5, omega_min);
+                    if (omega_d <= omega_min) {
+                        diverged = 1;
+                        break;
+                    }
+                    prev = residual;
+                    continue;
+                }
+                if (mlp_rec && own) {
+                    mlp_gx += omega * lfx;
+                    mlp_gy += omega * lfy;
+                }
+                // phase B: spread, relax, update the working velocity of the owned nodes
+#pragma unroll
+                for (int jn = 0; jn < NPT; ++jn) {
+                    const int b = tid + jn * IBM_THREADS;
+                    if (b < nb) {
+                        const int u0 = sh.cstart[b], u1 = sh.cstart[b + 1];
+                        R tx, ty;
+                        if (!COUPLED) {
+                            R ax, ay;
+                            spread2(sh, sh.Lfx, sh.Lfy, u0, u1, ax, ay);
+                            tx = ax * omega;
+                            ty = ay * omega;
+                        } else {
+                            tx = 0;
+                            ty = 0;
+                            for (int p = 0; p < P; ++p) {
+                                R ax = 0, ay = 0;
+                                for (int u = u0; u < u1; ++u) {
+                                    const int l = sh.ent[u] >> 5;
+                                    if (sh.part[l] != p) continue;
+                                    ax += sh.Lfx[l] * sh.entw[u];
+                                    ay += sh.Lfy[l] * sh.entw[u];
+                                }
+                                const R fx = ax * omega, fy = ay * omega;
+                                if (a.band_fib_part) {
+                                    a.band_fib_part[p * pstride + 2 * b] += fx;
+                                    a.band_fib_part[p * pstride + 2 * b + 1] += fy;
+                                }
+                                tx += fx;
+                                ty += fy;
+                            }
+                        }
+                        ftx[jn] += tx;
+                        fty[jn] += ty;
+                        if (incomp) {
+                            sh.bwx[b] += (R)0.5 * tx * dt;
+                            sh.bwy[b] += (R)0.5 * ty * dt;
+                        } else {
+                            sh.bwx[b] += tx * vs[jn];
+                            sh.bwy[b] += ty * vs[jn];
+                        }
+                    }
+                }
+                __syncthreads();  // (b)
+                prev = residual;
+                if (COUPLED) iter_count += 1;
+                else iter_count = it + 1;
+                if ((it + 1) >= min_iter && residual < a.mdf_tol) {
+                    converged = 1;
+                    break;
+                }
             }
         }
 #pragma unroll
