@@ -937,14 +937,18 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                         // squared slip as its FP64 bit pattern (0 for lanes without a marker)
                         unsigned long long key = 0;
                         if (own) {
-                            R sx = 0, sy = 0;
+                            R sx0 = 0, sy0 = 0, sx1 = 0, sy1 = 0;  // two chains: even and odd j
 #pragma unroll
-                            for (int j = 0; j < MS_W; ++j) {
-                                sx += arow[j] * Gx[lo + j];
-                                sy += arow[j] * Gy[lo + j];
+                            for (int j = 0; j < MS_W; j += 2) {
+                                sx0 += arow[j] * Gx[lo + j];
+                                sy0 += arow[j] * Gy[lo + j];
+                                if (j + 1 < MS_W) {
+                                    sx1 += arow[j + 1] * Gx[lo + j + 1];
+                                    sy1 += arow[j + 1] * Gy[lo + j + 1];
+                                }
                             }
-                            ux = u0x + sx;
-                            uy = u0y + sy;
+                            ux = u0x + (sx0 + sx1);
+                            uy = u0y + (sy0 + sy1);
                             const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
                             key = (unsigned long long)__double_as_longlong(ex * ex + ey * ey);
                             const R fx = (R)2 * Rl * (dvx - ux), fy = (R)2 * Rl * (dvy - uy);
@@ -963,12 +967,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                         const unsigned long long wmax = warp_max_bits(key);
                         if (lane == 0) wk[wid] = wmax;
                         bar_sync_n(1, nthr);
-                        unsigned long long mk = 0;
-#pragma unroll
-                        for (int w = 0; w < NWARP; ++w) {
-                            const unsigned long long v = w < nw ? wk[w] : 0ull;
-                            mk = v > mk ? v : mk;
-                        }
+                        const unsigned long long mk = warp_max_bits(lane < nw ? wk[lane] : 0ull);
                         const double residual = sqrt(__longlong_as_double((long long)mk));
                         last = residual;
                         if (it > 0 && residual > prev * 1.5) {
