@@ -231,19 +231,26 @@ def test_band_capacity_overflow_reports_status(torch):
     assert int(e.d_count.item()) == 0
 
 
-def test_marker_space_mdf_and_fallback(torch):
+@pytest.mark.parametrize("delta,center,d_ratio,marker_space", [
+    ("peskin4pt", (0.45, 0.5), 0.25, True),    # 38 markers, 5x5 stencils in the interior
+    ("hat", (0.45, 0.5), 0.25, True),          # 3x3 stencils
+    ("peskin4pt", (0.45, 0.15), 0.25, False),  # stencils clamped onto the wall nodes
+    ("peskin4pt", (0.45, 0.5), 0.1, False),    # 15 markers: fewer than the 17 neighbours of a row
+])
+def test_marker_space_mdf_and_fallback(torch, delta, center, d_ratio, marker_space):
     """A single body's MDF iterations run in marker space (stats[3] = -1) when
     the overlaps of neighbouring markers' stencils account for every entry of
-    the node lists; a body whose stencils are clamped onto the wall nodes takes
-    the node-space loop instead.  Both agree with the FP64 form."""
-    base = dict(Re=40, NN=49, xmax=2, ymax=1, cylinder_D_ratio=0.25, lattice_u=0.05, inflow_u=0.05,
-                bc_type="dirichlet_neumann", delta_type="peskin4pt", ibm_method="MDF", collision_model="TRT",
-                trt_magic_param=0.1875, mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
-                marker_spacing_factor=1.0, max_steps=200, use_convergence=False, check_interval=50)
-    for center, marker_space in (((0.45, 0.5), True), ((0.45, 0.15), False)):
-        cfg = _cfg(dict(base, cylinder_center=center))
-        r64, r32 = _pair(cfg)
-        assert r32["engine"].mdf_stats()["marker_space"] is marker_space, center
-        assert not r64["engine"].mdf_stats()["marker_space"]
-        _check_fields(cfg, r64, r32)
-        _check_forces(r64, r32)
+    the node lists; otherwise (stencils clamped onto the wall nodes, a ring too
+    small for the banded coupling matrix) the node-space loop runs.  Both agree
+    with the FP64 form."""
+    kw = dict(Re=40, NN=49, xmax=2, ymax=1, cylinder_D_ratio=d_ratio, lattice_u=0.05, inflow_u=0.05,
+              bc_type="dirichlet_neumann", delta_type=delta, ibm_method="MDF", collision_model="TRT",
+              trt_magic_param=0.1875, mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+              marker_spacing_factor=1.0, max_steps=200, use_convergence=False, check_interval=50,
+              cylinder_center=center)
+    cfg = _cfg(kw)
+    r64, r32 = _pair(cfg)
+    assert r32["engine"].mdf_stats()["marker_space"] is marker_space
+    assert not r64["engine"].mdf_stats()["marker_space"]
+    _check_fields(cfg, r64, r32)
+    _check_forces(r64, r32)
