@@ -113,6 +113,45 @@ def apply_bc(bc_type, nx, ny, fstar, ro, U, inflow_u, dens, incompressible=False
         raise KeyError(bc_type)
 
 
+def tg_velocity(X, Y, t, u0, L, nu):
+    """Decaying Taylor-Green vortex — iblbm/diagnostics/core.py:216-241 (same expressions)."""
+    decay = np.exp(-2.0 * nu * (np.pi / L) ** 2 * t)
+    ux = -u0 * np.cos(np.pi * X / L) * np.sin(np.pi * Y / L) * decay
+    uy = u0 * np.sin(np.pi * X / L) * np.cos(np.pi * Y / L) * decay
+    return ux, uy
+
+
+def tg_params(cfg):
+    """Half-width and viscosity of the vortex (iblbm/boundary/tg_analytical.py:49-51)."""
+    L_lat = 0.5 * (cfg.NN - 1)
+    nu = cfg.lattice_u * (cfg.cylinder_D_ratio * (cfg.NN - 1)) / cfg.Re
+    return L_lat, nu
+
+
+def tg_face_velocities(cfg, nx, ny, t):
+    """The analytic velocities of iblbm/boundary/tg_analytical.py:53-163 at time t:
+    (left j=0..ny-1, right j=0..ny-1, bottom i=1..nx-2, top i=1..nx-2, corners),
+    each an (n, 2) array."""
+    L_lat, nu = tg_params(cfg)
+    X = np.arange(nx, dtype=float) - (nx - 1) / 2.0
+    Y = np.arange(ny, dtype=float) - (ny - 1) / 2.0
+    j = np.arange(ny)
+    i = np.arange(1, nx - 1)
+    out = []
+    for xs, ys in ((np.full_like(j, X[0], dtype=float), Y[j]), (np.full_like(j, X[nx - 1], dtype=float), Y[j]),
+                   (X[i], np.full_like(i, Y[0], dtype=float)), (X[i], np.full_like(i, Y[ny - 1], dtype=float)),
+                   (X[np.array([0, nx - 1, 0, nx - 1])], Y[np.array([0, 0, ny - 1, ny - 1])])):
+        ux, uy = tg_velocity(xs, ys, t, cfg.tg_u0, L_lat, nu)
+        out.append(np.ascontiguousarray(np.stack([ux, uy], axis=1)))
+    return out
+
+
+def apply_bc_tg(cfg, nx, ny, fstar, ro, U, t):
+    uL, uR, uB, uT, uC = tg_face_velocities(cfg, nx, ny, t)
+    lib().orc_bc_tg(ctypes.c_int(nx), ctypes.c_int(ny), _p(fstar), _p(ro), _p(U), _p(uL), _p(uR), _p(uB),
+                    _p(uT), _p(uC))
+
+
 def velocity_correction(U, fib, ro, dt, incompressible=False):
     lib().orc_velocity_correction(ctypes.c_int(U.shape[0]), _p(U), _p(fib), _p(ro),
                                   ctypes.c_double(dt), ctypes.c_int(int(incompressible)))
@@ -234,7 +273,13 @@ def init_state(cfg):
     lattice_r = (phy_char / Cx) / 2.0
     tau = 3.0 * (cfg.lattice_u * 2.0 * lattice_r / cfg.Re) + 0.5
     U = np.zeros((N, 2))
-    if cfg.motion_type not in ("oscillating", "sedimentation"):
+    if cfg.scenario_type == "taylor_green":
+        # iblbm/init.py:178-191: the vortex at t = 0 on centred lattice coordinates
+        L_lat, nu = tg_params(cfg)
+        XX, YY = np.meshgrid(np.arange(nx, dtype=float) - (nx - 1) / 2.0,
+                             np.arange(ny, dtype=float) - (ny - 1) / 2.0)
+        U[:, 0], U[:, 1] = tg_velocity(XX.ravel(), YY.ravel(), 0.0, cfg.tg_u0, L_lat, nu)
+    elif cfg.motion_type not in ("oscillating", "sedimentation"):
         U[:, 0] = cfg.inflow_u
     ro = np.ones(N)
     fe = feq(ro, U, cfg.incompressible_lbgk)
@@ -340,11 +385,16 @@ class OracleSim:
     def stream_boundary_macro(self):
         s, cfg = self.s, self.cfg
         s.fstar = stream(s.fstar, self.f, s.nx, s.ny)
-        apply_bc(cfg.bc_type, s.nx, s.ny, s.fstar, s.ro, s.U, s.in_u, s.dens, cfg.incompressible_lbgk)
+        if cfg.scenario_type == "taylor_green":  # iblbm/boundary/base.py:52-53
+            apply_bc_tg(cfg, s.nx, s.ny, s.fstar, s.ro, s.U, self.ttt * s.dt)
+        else:
+            apply_bc(cfg.bc_type, s.nx, s.ny, s.fstar, s.ro, s.U, s.in_u, s.dens, cfg.incompressible_lbgk)
         s.ro, s.U = macroscopic(s.fstar, cfg.incompressible_lbgk)
 
     def apply_ibm(self):
         s, cfg = self.s, self.cfg
+        if cfg.scenario_type == "taylor_green" and not cfg.tg_with_ibm:  # iblbm/ibm/dispatch.py:38-39
+            return
         if s.particles is not None:
             return self._apply_ibm_multi()
         if cfg.ibm_method == "DF":
@@ -436,6 +486,13 @@ class OracleSim:
     def step(self):
         """One iteration of iblbm/runtime/loop.py:63-138 (without the stop checks)."""
         s, cfg, ttt = self.s, self.cfg, self.ttt
+        if cfg.scenario_type == "taylor_green" and cfg.tg_with_ibm:
+            # iblbm/runtime/scenarios/taylor_green.py:21-31 (pre_step): analytic desired velocity
+            L_lat, nu = tg_params(cfg)
+            ux, uy = tg_velocity(s.Lx / s.dx - (s.nx - 1) / 2.0, s.Ly / s.dy - (s.ny - 1) / 2.0, ttt * s.dt,
+                                 cfg.tg_u0, L_lat, nu)
+            s.desired_velocity[:, 0] = ux
+            s.desired_velocity[:, 1] = uy
         if s.particles is not None and cfg.time_integrator != "euler_explicit":
             self._half_step()
         if not cfg.stream_first and not self.force_level:
@@ -461,8 +518,12 @@ class OracleSim:
                 self.history.append([(p.pos.copy(), p.vel.copy()) for p in s.particles])
                 self.Cd_history.append(0.0)
                 self.Cl_history.append(0.0)
+            elif cfg.scenario_type == "taylor_green" and not cfg.tg_with_ibm:
+                self.Cd_history.append(0.0)  # iblbm/runtime/scenarios/taylor_green.py:60-62
+                self.Cl_history.append(0.0)
             else:
-                Cd, Cl = self.cd_cl()
+                with np.errstate(divide="ignore", invalid="ignore"):  # no inflow: u_ref = 0
+                    Cd, Cl = self.cd_cl()
                 self.Cd_history.append(Cd)
                 self.Cl_history.append(Cl)
         self.ttt += 1

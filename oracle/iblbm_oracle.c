@@ -511,6 +511,54 @@ void orc_bc_velocity_inlet(int nx, int ny, double *fstar, double *ro, double *U,
     for (int c = 0; c < 2; ++c) feq_node(dens, UX(oc[c]), 0.0, 0, &FS(oc[c], 0));
 }
 
+/* iblbm/boundary/tg_analytical.py:26-170 — time-dependent Dirichlet on all four faces
+ * (Zou-He closures with the analytic velocity), then the four corners reset to
+ * feq(1, u).  The analytic velocities at this step come in per face: uL, uR over
+ * j = 0..ny-1 (the faces include the corners), uB, uT over i = 1..nx-2, uC for
+ * the corners (0,0), (nx-1,0), (0,ny-1), (nx-1,ny-1); each as (ux, uy) pairs. */
+void orc_bc_tg(int nx, int ny, double *fstar, double *ro, double *U, const double *uL, const double *uR,
+               const double *uB, const double *uT, const double *uC)
+{
+    for (int j = 0; j <= ny - 1; ++j) {
+        size_t n = (size_t)j * nx;
+        UX(n) = uL[2 * j]; UY(n) = uL[2 * j + 1];
+        ro[n] = (1.0 / (1.0 - UX(n))) * (FS(n, 0) + FS(n, 2) + FS(n, 4) + 2.0 * (FS(n, 3) + FS(n, 6) + FS(n, 7)));
+        FS(n, 1) = FS(n, 3) + (2.0 / 3.0) * ro[n] * UX(n);
+        FS(n, 5) = (FS(n, 7) - 0.5 * (FS(n, 2) - FS(n, 4)) + (1.0 / 6.0) * ro[n] * UX(n) + 0.5 * ro[n] * UY(n));
+        FS(n, 8) = (FS(n, 6) + 0.5 * (FS(n, 2) - FS(n, 4)) + (1.0 / 6.0) * ro[n] * UX(n) - 0.5 * ro[n] * UY(n));
+    }
+    for (int j = 0; j <= ny - 1; ++j) {
+        size_t n = (size_t)j * nx + nx - 1;
+        UX(n) = uR[2 * j]; UY(n) = uR[2 * j + 1];
+        ro[n] = (1.0 / (1.0 + UX(n))) * (FS(n, 0) + FS(n, 2) + FS(n, 4) + 2.0 * (FS(n, 1) + FS(n, 5) + FS(n, 8)));
+        FS(n, 3) = FS(n, 1) - (2.0 / 3.0) * ro[n] * UX(n);
+        FS(n, 7) = (FS(n, 5) + 0.5 * (FS(n, 2) - FS(n, 4)) - (1.0 / 6.0) * ro[n] * UX(n) - 0.5 * ro[n] * UY(n));
+        FS(n, 6) = (FS(n, 8) - 0.5 * (FS(n, 2) - FS(n, 4)) - (1.0 / 6.0) * ro[n] * UX(n) + 0.5 * ro[n] * UY(n));
+    }
+    for (int i = 1; i <= nx - 2; ++i) {
+        size_t n = (size_t)(ny - 1) * nx + i;
+        UX(n) = uT[2 * (i - 1)]; UY(n) = uT[2 * (i - 1) + 1];
+        ro[n] = (1.0 / (1.0 + UY(n))) * (FS(n, 0) + FS(n, 1) + FS(n, 3) + 2.0 * (FS(n, 2) + FS(n, 5) + FS(n, 6)));
+        FS(n, 4) = FS(n, 2) - (2.0 / 3.0) * ro[n] * UY(n);
+        FS(n, 7) = (FS(n, 5) + 0.5 * (FS(n, 1) - FS(n, 3)) - (1.0 / 6.0) * ro[n] * UY(n) - 0.5 * ro[n] * UX(n));
+        FS(n, 8) = (FS(n, 6) - 0.5 * (FS(n, 1) - FS(n, 3)) - (1.0 / 6.0) * ro[n] * UY(n) + 0.5 * ro[n] * UX(n));
+    }
+    for (int i = 1; i <= nx - 2; ++i) {
+        size_t n = (size_t)i;
+        UX(n) = uB[2 * (i - 1)]; UY(n) = uB[2 * (i - 1) + 1];
+        ro[n] = (1.0 / (1.0 - UY(n))) * (FS(n, 0) + FS(n, 1) + FS(n, 3) + 2.0 * (FS(n, 4) + FS(n, 7) + FS(n, 8)));
+        FS(n, 2) = FS(n, 4) + (2.0 / 3.0) * ro[n] * UY(n);
+        FS(n, 5) = (FS(n, 7) - 0.5 * (FS(n, 1) - FS(n, 3)) + (1.0 / 6.0) * ro[n] * UY(n) + 0.5 * ro[n] * UX(n));
+        FS(n, 6) = (FS(n, 8) + 0.5 * (FS(n, 1) - FS(n, 3)) + (1.0 / 6.0) * ro[n] * UY(n) - 0.5 * ro[n] * UX(n));
+    }
+    size_t corners[4] = {0, (size_t)nx - 1, (size_t)nx * (ny - 1), (size_t)nx * ny - 1};
+    for (int c = 0; c < 4; ++c) {
+        size_t n = corners[c];
+        ro[n] = 1.0; UX(n) = uC[2 * c]; UY(n) = uC[2 * c + 1];
+        feq_node(1.0, UX(n), UY(n), 0, &FS(n, 0));
+    }
+}
+
 /* bc_type ids: 0 dirichlet_neumann, 1 open_boundary, 2 settling_channel, 3 velocity_inlet */
 int orc_bc(int bc_type, int nx, int ny, double *fstar, double *ro, double *U, double inflow_u,
            double dens, int incomp)

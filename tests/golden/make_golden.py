@@ -96,6 +96,23 @@ RUN_CASES = {
                               bc_type="dirichlet_neumann", delta_type="hat", ibm_method="DFC",
                               collision_model="TRT", marker_spacing_factor=1.0, max_steps=200,
                               use_convergence=False, check_interval=50),
+    # Taylor-Green decaying vortex (scenario_type="taylor_green"): the analytic
+    # time-dependent closure on all four faces; pure lattice Boltzmann (no IBM step)
+    "tg_lbm_bgk": dict(Re=20, NN=41, xmax=1, ymax=1, cylinder_center=(0.5, 0.5), cylinder_D_ratio=0.25,
+                       lattice_u=0.05, inflow_u=0.0, scenario_type="taylor_green", tg_u0=0.05,
+                       tg_with_ibm=False, delta_type="hat", ibm_method="DF", collision_model="BGK",
+                       marker_spacing_factor=1.0, max_steps=300, use_convergence=False, check_interval=50),
+    "tg_lbm_cmmrt": dict(Re=20, NN=41, xmax=1, ymax=1, cylinder_center=(0.5, 0.5), cylinder_D_ratio=0.25,
+                         lattice_u=0.05, inflow_u=0.0, scenario_type="taylor_green", tg_u0=0.05,
+                         tg_with_ibm=False, delta_type="hat", ibm_method="MDF", collision_model="CM_MRT",
+                         marker_spacing_factor=1.0, max_steps=300, use_convergence=False, check_interval=50),
+    # ... and with the IBM step: markers driven to the analytic velocity every step
+    "tg_ibm_mdf_trt_p4": dict(Re=20, NN=41, xmax=1, ymax=1, cylinder_center=(0.5, 0.5), cylinder_D_ratio=0.25,
+                              lattice_u=0.05, inflow_u=0.0, scenario_type="taylor_green", tg_u0=0.05,
+                              tg_with_ibm=True, delta_type="peskin4pt", ibm_method="MDF",
+                              collision_model="TRT", trt_magic_param=0.1875, mdf_iterations=20,
+                              mdf_min_iterations=5, mdf_tolerance=1e-6, marker_spacing_factor=1.0,
+                              max_steps=300, use_convergence=False, check_interval=50),
     # incompressible LBGK branch (feq, macro, DF force law, velocity correction)
     "inc_df_bgk_hat": dict(Re=40, NN=81, xmax=2, ymax=1, cylinder_center=(0.5, 0.5),
                            cylinder_D_ratio=0.125, lattice_u=0.05, inflow_u=0.05,
