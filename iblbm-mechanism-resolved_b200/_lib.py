@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libiblbm_b200.so")
 
 COLL_IDS = {"BGK": 0, "TRT": 1, "CM_MRT": 2}
-BC_IDS = {"dirichlet_neumann": 0, "open_boundary": 1, "settling_channel": 2, "velocity_inlet": 3}
+BC_IDS = {"dirichlet_neumann": 0, "open_boundary": 1, "settling_channel": 2, "velocity_inlet": 3,
+          "tg_analytical": 4}
 IBM_IDS = {"NONE": 0, "DF": 1, "MDF": 2, "DFC": 3}
 DELTA_IDS = {"peskin4pt": 0, "hat": 1}
 DELTA_RADIUS = {"peskin4pt": 2, "hat": 1}
@@ -28,7 +29,8 @@ class Geom(ctypes.Structure):
 
 class Case(ctypes.Structure):
     _fields_ = [("collision", _i), ("bc", _i), ("incompressible", _i), ("tau", _d), ("dt", _d),
-                ("s_minus", _d), ("S", _d * 9), ("inflow_u", _d), ("dens", _d)]
+                ("s_minus", _d), ("S", _d * 9), ("inflow_u", _d), ("dens", _d), ("tg_face", _vp),
+                ("tg_decay", _vp)]
 
 
 class BandView(ctypes.Structure):
@@ -54,7 +56,8 @@ class IbmArgs(ctypes.Structure):
                 ("box_capacity", _i), ("band_fib", _vp), ("band_df", _vp), ("band_fib_part", _vp),
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
-                ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i)]
+                ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i),
+                ("dvel_scale", _vp)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee

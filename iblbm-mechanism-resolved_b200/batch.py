@@ -40,6 +40,8 @@ class Batch:
     def __init__(self, cfgs, device=None, tile="rows2"):
         if not cfgs:
             raise ValueError("empty batch")
+        if any(cfg.scenario_type == "taylor_green" for cfg in cfgs):
+            raise NotImplementedError("Taylor-Green cases (a per-step closure factor) are stepped one at a time")
         self.engines = [Engine(cfg, device, precision="f32") for cfg in cfgs]
         for e in self.engines:
             if e.st.particles is not None:

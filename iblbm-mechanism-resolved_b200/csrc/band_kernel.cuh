@@ -437,6 +437,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             y = a.Ly[l];
             vx = a.dvel[2 * l];
             vy = a.dvel[2 * l + 1];
+            if (a.dvel_scale) {  // the Taylor-Green markers' analytic decay
+                const double d = *a.dvel_scale;
+                vx = vx * d;
+                vy = vy * d;
+            }
         }
         sh.dvx[l] = (R)vx;
         sh.dvy[l] = (R)vy;
@@ -619,6 +624,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     case BC_DIRICHLET_NEUMANN: band_moments<SHIFTED, BC_DIRICHLET_NEUMANN>(a, g, bc, nb, sh, fs_keep); break;
     case BC_OPEN: band_moments<SHIFTED, BC_OPEN>(a, g, bc, nb, sh, fs_keep); break;
     case BC_SETTLING: band_moments<SHIFTED, BC_SETTLING>(a, g, bc, nb, sh, fs_keep); break;
+    case BC_TG: band_moments<SHIFTED, BC_TG>(a, g, bc, nb, sh, fs_keep); break;
     default: band_moments<SHIFTED, BC_VELOCITY_INLET>(a, g, bc, nb, sh, fs_keep); break;
     }
     __syncthreads();
@@ -1342,6 +1348,8 @@ static int check_ibm_args(const ARGS* a)
     if (!a->xt_table && (!a->Lx || !a->Ly || !a->dvel)) return IBLBM_E_ARG;
     if (a->xt_table && (!a->Lx_c || !a->Ly_c || !a->step_counter || a->xt_len < 1)) return IBLBM_E_ARG;
     if (!fields && (a->c.bc == BC_OPEN || a->c.bc == BC_VELOCITY_INLET) && !a->uring_prev) return IBLBM_E_ARG;
+    if (!fields && a->c.bc == BC_TG && (!a->c.tg_face || !a->c.tg_decay)) return IBLBM_E_ARG;
+    if (a->c.bc < BC_DIRICHLET_NEUMANN || a->c.bc > BC_TG) return IBLBM_E_ARG;
     if (a->band_capacity < 1 || a->band_capacity > MAX_BAND || a->g.nx < 4 || a->g.ny < 4)
         return IBLBM_E_ARG;
     if ((long long)a->lb_total * 32 >= (1LL << 31)) return IBLBM_E_ARG;

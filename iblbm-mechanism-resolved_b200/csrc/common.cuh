@@ -19,7 +19,7 @@ __host__ __device__ constexpr int opp_(int q) { return q == 0 ? 0 : (q <= 4 ? ((
 __host__ __device__ constexpr double w_(int q) { return q == 0 ? 4.0 / 9.0 : (q <= 4 ? 1.0 / 9.0 : 1.0 / 36.0); }
 
 enum Collision : int { COLL_BGK = 0, COLL_TRT = 1, COLL_CMMRT = 2 };
-enum Boundary : int { BC_DIRICHLET_NEUMANN = 0, BC_OPEN = 1, BC_SETTLING = 2, BC_VELOCITY_INLET = 3 };
+enum Boundary : int { BC_DIRICHLET_NEUMANN = 0, BC_OPEN = 1, BC_SETTLING = 2, BC_VELOCITY_INLET = 3, BC_TG = 4 };
 enum IbmMethod : int { IBM_NONE = 0, IBM_DF = 1, IBM_MDF = 2, IBM_DFC = 3 };
 
 // Lattice geometry in HBM: one structure-of-arrays plane per population q,
@@ -42,7 +42,21 @@ struct BcParams {
     int type;
     double inflow_u, dens;
     double feq_in[9];  // feq(dens, (inflow_u, 0)) for the Dirichlet faces
+    const double* tg_face;   // Taylor-Green: boundary-node velocities before decay
+    const double* tg_decay;  // Taylor-Green: decay factor of this step (device scalar)
 };
+
+// Slot of boundary node (i, j) in the Taylor-Green face table: left j, right j,
+// bottom i-1, top i-1, then the corners (0,0), (nx-1,0), (0,ny-1), (nx-1,ny-1).
+__host__ __device__ __forceinline__ int tg_slot(int nx, int ny, int i, int j)
+{
+    if ((i == 0 || i == nx - 1) && (j == 0 || j == ny - 1))
+        return 2 * ny + 2 * (nx - 2) + (i == 0 ? 0 : 1) + (j == 0 ? 0 : 2);
+    if (i == 0) return j;
+    if (i == nx - 1) return ny + j;
+    if (j == 0) return 2 * ny + (i - 1);
+    return 2 * ny + (nx - 2) + (i - 1);
+}
 
 // ---------------------------------------------------------------------------
 // Equilibrium — iblbm/lbm/equilibrium.py:27-43
@@ -286,6 +300,43 @@ __device__ __forceinline__ void bc_velocity_inlet(const double* __restrict__ ur,
     }
 }
 
+// iblbm/boundary/tg_analytical.py:26-170: the analytic velocity u imposed on all
+// four faces by Zou-He closures, the corners reset to feq(1, u); u is the node's
+// tabulated velocity times this step's decay factor (the reference's
+// ((-u0 cos) sin) * decay with the same rounding).
+__device__ __forceinline__ void bc_tg(const Geom& g, const BcParams& bc, int i, int j, double* f)
+{
+    const int nx = g.nx, ny = g.ny;
+    const int k = tg_slot(nx, ny, i, j);
+    const double d = *bc.tg_decay;
+    const double ux = bc.tg_face[2 * k] * d, uy = bc.tg_face[2 * k + 1] * d;
+    if ((i == 0 || i == nx - 1) && (j == 0 || j == ny - 1)) {
+        feq_all(1.0, ux, uy, false, f);
+        return;
+    }
+    if (i == 0) {
+        const double ro = (1.0 / (1.0 - ux)) * (f[0] + f[2] + f[4] + 2.0 * (f[3] + f[6] + f[7]));
+        f[1] = f[3] + (2.0 / 3.0) * ro * ux;
+        f[5] = (f[7] - 0.5 * (f[2] - f[4]) + (1.0 / 6.0) * ro * ux + 0.5 * ro * uy);
+        f[8] = (f[6] + 0.5 * (f[2] - f[4]) + (1.0 / 6.0) * ro * ux - 0.5 * ro * uy);
+    } else if (i == nx - 1) {
+        const double ro = (1.0 / (1.0 + ux)) * (f[0] + f[2] + f[4] + 2.0 * (f[1] + f[5] + f[8]));
+        f[3] = f[1] - (2.0 / 3.0) * ro * ux;
+        f[7] = (f[5] + 0.5 * (f[2] - f[4]) - (1.0 / 6.0) * ro * ux - 0.5 * ro * uy);
+        f[6] = (f[8] - 0.5 * (f[2] - f[4]) - (1.0 / 6.0) * ro * ux + 0.5 * ro * uy);
+    } else if (j == ny - 1) {
+        const double ro = (1.0 / (1.0 + uy)) * (f[0] + f[1] + f[3] + 2.0 * (f[2] + f[5] + f[6]));
+        f[4] = f[2] - (2.0 / 3.0) * ro * uy;
+        f[7] = (f[5] + 0.5 * (f[1] - f[3]) - (1.0 / 6.0) * ro * uy - 0.5 * ro * ux);
+        f[8] = (f[6] - 0.5 * (f[1] - f[3]) - (1.0 / 6.0) * ro * uy + 0.5 * ro * ux);
+    } else {  // j == 0
+        const double ro = (1.0 / (1.0 - uy)) * (f[0] + f[1] + f[3] + 2.0 * (f[4] + f[7] + f[8]));
+        f[2] = f[4] + (2.0 / 3.0) * ro * uy;
+        f[5] = (f[7] - 0.5 * (f[1] - f[3]) + (1.0 / 6.0) * ro * uy + 0.5 * ro * ux);
+        f[6] = (f[8] + 0.5 * (f[1] - f[3]) + (1.0 / 6.0) * ro * uy - 0.5 * ro * ux);
+    }
+}
+
 // Post-streaming, post-closure populations of node (i, j) — iblbm/runtime/step.py:49-60
 // (streaming_step then apply_boundary_step).
 template <int BC>
@@ -303,6 +354,7 @@ __device__ __forceinline__ void fstar_node(const double* __restrict__ fpost, con
     if (BC == BC_OPEN) bc_open(ur, g, bc, i, j, f);
     else if (BC == BC_SETTLING) bc_settling(g, bc, incomp, i, j, f);
     else if (BC == BC_VELOCITY_INLET) bc_velocity_inlet(ur, g, bc, i, j, f);
+    else if (BC == BC_TG) bc_tg(g, bc, i, j, f);
 }
 
 // ---------------------------------------------------------------------------

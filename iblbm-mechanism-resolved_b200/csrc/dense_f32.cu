@@ -148,6 +148,7 @@ static cudaError_t launch32_coll(const iblbm_dense32_args& a, const CollParams32
     case BC_OPEN: return launch32_bc<COLL, BC_OPEN>(a, cp, bc, s);
     case BC_SETTLING: return launch32_bc<COLL, BC_SETTLING>(a, cp, bc, s);
     case BC_VELOCITY_INLET: return launch32_bc<COLL, BC_VELOCITY_INLET>(a, cp, bc, s);
+    case BC_TG: return launch32_bc<COLL, BC_TG>(a, cp, bc, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -185,6 +186,7 @@ extern "C" int iblbm_dense_step_f32(const iblbm_dense32_args* a, void* stream)
     if (a->ibm != IBM_NONE && (!a->band.box || !a->band.map)) return IBLBM_E_ARG;
     if ((a->ibm == IBM_DF || a->ibm == IBM_MDF) && !a->band.fib) return IBLBM_E_ARG;
     if (a->ibm == IBM_DFC && !a->band.df) return IBLBM_E_ARG;
+    if (a->c.bc == BC_TG && (!a->c.tg_face || !a->c.tg_decay)) return IBLBM_E_ARG;
     if (a->skip_box && a->only_box) return IBLBM_E_ARG;
     if (a->tile < IBLBM_TILE_PIPE_4x2 || a->tile > IBLBM_TILE_ROWS4) return IBLBM_E_ARG;
     if ((reinterpret_cast<uintptr_t>(a->fpost_prev) & 15) || (reinterpret_cast<uintptr_t>(a->fpost_next) & 15) ||

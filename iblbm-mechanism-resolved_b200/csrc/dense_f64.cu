@@ -96,6 +96,7 @@ static cudaError_t launch_coll(const iblbm_dense_args& a, const CollParams& cp, 
     case BC_OPEN: return launch_bc<COLL, BC_OPEN>(a, cp, bc, s);
     case BC_SETTLING: return launch_bc<COLL, BC_SETTLING>(a, cp, bc, s);
     case BC_VELOCITY_INLET: return launch_bc<COLL, BC_VELOCITY_INLET>(a, cp, bc, s);
+    case BC_TG: return launch_bc<COLL, BC_TG>(a, cp, bc, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -113,6 +114,8 @@ void make_params(const iblbm_case& c, CollParams& cp, BcParams& bc)
     bc.type = c.bc;
     bc.inflow_u = c.inflow_u;
     bc.dens = c.dens;
+    bc.tg_face = c.tg_face;
+    bc.tg_decay = c.tg_decay;
     // feq(dens, (u_in, 0)) — equilibrium.py:39-42 with the same operation order
     const double u0 = c.inflow_u, u1 = 0.0, u2 = u0 * u0 + u1 * u1;
     for (int q = 0; q < 9; ++q) {
@@ -132,6 +135,7 @@ extern "C" int iblbm_dense_step_f64(const iblbm_dense_args* a, void* stream)
     if ((a->c.bc == BC_OPEN || a->c.bc == BC_VELOCITY_INLET) && (!a->uring_prev || !a->uring_next))
         return IBLBM_E_ARG;
     if (a->ibm != IBM_NONE && (!a->band.box || !a->band.map)) return IBLBM_E_ARG;
+    if (a->c.bc == BC_TG && (!a->c.tg_face || !a->c.tg_decay)) return IBLBM_E_ARG;
     if (a->skip_box && a->only_box) return IBLBM_E_ARG;
     if ((a->ibm == IBM_DF || a->ibm == IBM_MDF) && !a->band.fib) return IBLBM_E_ARG;
     if (a->ibm == IBM_DFC && !a->band.df) return IBLBM_E_ARG;

@@ -41,6 +41,9 @@ __device__ __forceinline__ void node_generic32(const iblbm_dense32_args& a, cons
     case BC_SETTLING:
         dense_node32<COLL, BC_SETTLING, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
         break;
+    case BC_TG:
+        dense_node32<COLL, BC_TG, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i, j);
+        break;
     default:
         dense_node32<COLL, BC_VELOCITY_INLET, INCOMP, IBM, false>(a.fpost_prev, a.uring_prev, g, cp, bc, bv, o, i,
                                                                    j);

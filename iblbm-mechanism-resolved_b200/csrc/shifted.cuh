@@ -24,6 +24,8 @@ namespace iblbm {
 struct BcParams32 {
     float inflow_u, dens;
     float geq_in[9];  // feq(dens, (inflow_u, 0)) - w, rounded from FP64
+    const double* tg_face;   // Taylor-Green: boundary-node velocities before decay (FP64)
+    const double* tg_decay;  // Taylor-Green: decay factor of this step (device scalar)
 };
 
 struct CollParams32 {
@@ -36,6 +38,8 @@ __host__ __device__ inline void make_bc(const iblbm_case& c, BcParams32& bc)
 {
     bc.inflow_u = (float)c.inflow_u;
     bc.dens = (float)c.dens;
+    bc.tg_face = c.tg_face;
+    bc.tg_decay = c.tg_decay;
     const double u0 = c.inflow_u, u2 = u0 * u0;
     for (int q = 0; q < 9; ++q) {
         const double eU = (double)ex_(q) * u0;
@@ -216,6 +220,42 @@ __device__ __forceinline__ void bc32_velocity_inlet(const float* __restrict__ ur
     f[6] = f[8] + 0.5f * (f[1] - f[3]) - 0.5f * ro * ux;
 }
 
+// Taylor-Green faces on g = f - w (iblbm/boundary/tg_analytical.py:26-170): the
+// weights of the known populations of a face sum to 1, so rho = (1 + G) / (1 -+ u)
+// with G their sum in g, and the unknowns keep the form of the closure on f.
+__device__ __forceinline__ void bc32_tg(const Geom& g, const BcParams32& bc, int i, int j, float* f)
+{
+    const int nx = g.nx, ny = g.ny;
+    const int k = tg_slot(nx, ny, i, j);
+    const double d = *bc.tg_decay;
+    const float ux = (float)(bc.tg_face[2 * k] * d), uy = (float)(bc.tg_face[2 * k + 1] * d);
+    if ((i == 0 || i == nx - 1) && (j == 0 || j == ny - 1)) {
+        geq_all(1.0f, ux, uy, false, f);
+        return;
+    }
+    if (i == 0) {
+        const float ro = (1.0f + (f[0] + f[2] + f[4] + 2.0f * (f[3] + f[6] + f[7]))) / (1.0f - ux);
+        f[1] = f[3] + (2.0f / 3.0f) * ro * ux;
+        f[5] = f[7] - 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+        f[8] = f[6] + 0.5f * (f[2] - f[4]) + (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+    } else if (i == nx - 1) {
+        const float ro = (1.0f + (f[0] + f[2] + f[4] + 2.0f * (f[1] + f[5] + f[8]))) / (1.0f + ux);
+        f[3] = f[1] - (2.0f / 3.0f) * ro * ux;
+        f[7] = f[5] + 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux - 0.5f * ro * uy;
+        f[6] = f[8] - 0.5f * (f[2] - f[4]) - (1.0f / 6.0f) * ro * ux + 0.5f * ro * uy;
+    } else if (j == ny - 1) {
+        const float ro = (1.0f + (f[0] + f[1] + f[3] + 2.0f * (f[2] + f[5] + f[6]))) / (1.0f + uy);
+        f[4] = f[2] - (2.0f / 3.0f) * ro * uy;
+        f[7] = f[5] + 0.5f * (f[1] - f[3]) - (1.0f / 6.0f) * ro * uy - 0.5f * ro * ux;
+        f[8] = f[6] - 0.5f * (f[1] - f[3]) - (1.0f / 6.0f) * ro * uy + 0.5f * ro * ux;
+    } else {
+        const float ro = (1.0f + (f[0] + f[1] + f[3] + 2.0f * (f[4] + f[7] + f[8]))) / (1.0f - uy);
+        f[2] = f[4] + (2.0f / 3.0f) * ro * uy;
+        f[5] = f[7] - 0.5f * (f[1] - f[3]) + (1.0f / 6.0f) * ro * uy + 0.5f * ro * ux;
+        f[6] = f[8] + 0.5f * (f[1] - f[3]) + (1.0f / 6.0f) * ro * uy - 0.5f * ro * ux;
+    }
+}
+
 template <int BC>
 __device__ __forceinline__ void gstar_node(const float* __restrict__ fp, const float* __restrict__ ur, const Geom& g,
                                            const BcParams32& bc, bool incomp, int i, int j, float* f)
@@ -230,6 +270,7 @@ __device__ __forceinline__ void gstar_node(const float* __restrict__ fp, const f
     if (BC == BC_OPEN) bc32_open(ur, g, bc, i, j, f);
     else if (BC == BC_SETTLING) bc32_settling(g, bc, incomp, i, j, f);
     else if (BC == BC_VELOCITY_INLET) bc32_velocity_inlet(ur, g, bc, i, j, f);
+    else if (BC == BC_TG) bc32_tg(g, bc, i, j, f);
 }
 
 // Pull offsets of an interior node relative to its own site: population q
@@ -267,6 +308,7 @@ __device__ __forceinline__ void closure_node(const float* __restrict__ fp, const
     if (BC == BC_DIRICHLET_NEUMANN) bc32_dirichlet_neumann(fp, g, bc, i, j, f);
     else if (BC == BC_OPEN) bc32_open(ur, g, bc, i, j, f);
     else if (BC == BC_SETTLING) bc32_settling(g, bc, incomp, i, j, f);
+    else if (BC == BC_TG) bc32_tg(g, bc, i, j, f);
     else bc32_velocity_inlet(ur, g, bc, i, j, f);
 }
 

@@ -77,10 +77,14 @@ def compute_slip_error(Eux, Euy, dx, dy, cx, cy, D, NN, delta_type, u_target_x=N
 def engine_slip(engine, u_ref=None):
     """Slip of the engine's last output velocity on its own markers (the
     simulation's ring, desired velocities as targets): mean, max and RMS over
-    U_ref (the inflow speed, or the oscillation speed scale)."""
+    U_ref (the inflow speed, the oscillation speed scale, or the Taylor-Green
+    vortex amplitude)."""
     st, cfg = engine.st, engine.cfg
     if u_ref is None:
-        u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
+        if cfg.scenario_type == "taylor_green":
+            u_ref = cfg.tg_u0  # no inflow: the vortex amplitude
+        else:
+            u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
     U = engine.U_out.double().reshape(st.ny, st.nx, 2)
     Lx = engine.d_Lx[: engine.Lb].cpu().numpy()
     Ly = engine.d_Ly[: engine.Lb].cpu().numpy()
@@ -92,6 +96,8 @@ def engine_slip(engine, u_ref=None):
         dv = np.stack([np.full(engine.Lb, xt), np.zeros(engine.Lb)], axis=1)
     else:
         dv = engine.d_dv[: 2 * engine.Lb].reshape(engine.Lb, 2).cpu().numpy()
+        if engine.tg:  # Taylor-Green markers: the analytic velocity of the last output step
+            dv = dv * float(engine.d_tg_table[engine.last_out_step].item())
     Lux, Luy = _interp_gpu(U[..., 0].cpu().numpy(), U[..., 1].cpu().numpy(), Lx, Ly, st.dx, st.dy, cfg.delta_type)
     mag = np.sqrt((Lux - dv[:, 0]) ** 2 + (Luy - dv[:, 1]) ** 2)
     return {"mean": float(np.mean(mag) / u_ref), "max": float(np.max(mag) / u_ref),

@@ -111,6 +111,20 @@ class Engine:
             c.S[q] = float(st.S_diag[q]) if st.S_diag is not None else 0.0
         c.inflow_u = st.in_u
         c.dens = st.dens
+        # Taylor-Green vortex: the analytic closure on all faces (iblbm/boundary/base.py:52-53)
+        # and no IBM step unless tg_with_ibm (iblbm/ibm/dispatch.py:38-39)
+        self.tg = cfg.scenario_type == "taylor_green"
+        self.no_ibm = self.tg and not cfg.tg_with_ibm
+        if self.tg:
+            from .physics import tg_face_table, tg_marker_base
+            c.bc = BC_IDS["tg_analytical"]
+            self.d_tg_face = torch.as_tensor(tg_face_table(cfg, nx, ny), device=dev)
+            self.d_tg_step = torch.ones(1, dtype=torch.int64, device=dev)
+            self.d_tg_cur = torch.ones(1, dtype=f64, device=dev)
+            self._tg_table(int(cfg.max_steps) + 2)
+            c.tg_face, c.tg_decay = ptr(self.d_tg_face), ptr(self.d_tg_cur)
+            if cfg.tg_with_ibm:
+                st.desired_velocity = tg_marker_base(cfg, np.asarray(st.Lx), np.asarray(st.Ly), st.dx, st.dy, nx, ny)
 
         # ---- initial populations: feq(1, U0), then the first collision ----------
         U0 = torch.as_tensor(initial_velocity(cfg, N), device=dev).contiguous()
@@ -199,7 +213,7 @@ class Engine:
         self.side = torch.cuda.Stream(self.dev, priority=-1)
         self.ev_bulk = torch.cuda.Event()
         self.ev_side = torch.cuda.Event()
-        self.overlap = True
+        self.overlap = not self.tg  # the per-step decay factor needs one stream
         self.rebuild_next = True
         self.last_out_step = 0
 
@@ -279,6 +293,19 @@ class Engine:
             rc = self.L.iblbm_collision_cm_mrt(ptr(fstar), ptr(U), ptr(fib), N, Sd, c.dt, ptr(out), s)
         check(rc, "initial collision")
 
+    def _tg_table(self, n):
+        """Decay factors of steps 0 .. n-1 on the device (host-computed with numpy,
+        as the reference computes them)."""
+        from .physics import tg_decay_table
+        self.d_tg_table = self.torch.as_tensor(tg_decay_table(self.cfg, n, self.st.dt), device=self.dev)
+        self.graphs = {}
+
+    def _tg_tick(self):
+        """This step's decay factor into the scalar the closures and the band
+        kernel read, then the step counter advances (graph-capturable)."""
+        self.torch.index_select(self.d_tg_table, 0, self.d_tg_step, out=self.d_tg_cur)
+        self.d_tg_step.add_(1)
+
     def _upload_markers(self):
         st = self.st
         if st.particles is not None:
@@ -302,6 +329,8 @@ class Engine:
         a.moff, a.Lx, a.Ly, a.dvel, a.larea = (ptr(x) for x in (self.d_moff, self.d_Lx, self.d_Ly, self.d_dv,
                                                                  self.d_larea))
         a.dx, a.dy = self.st.dx, self.st.dy
+        if self.tg and cfg.tg_with_ibm:
+            a.dvel_scale = ptr(self.d_tg_cur)
         if self.xt is not None:
             a.Lx_c, a.Ly_c, a.xt_table, a.step_counter = ptr(self.d_Lxc), ptr(self.d_Lyc), ptr(self.xt), ptr(
                 self.d_counter)
@@ -376,7 +405,7 @@ class Engine:
             a.tile = TILES[self.tile]
             a.status = ptr(self.d_pipe_status)
         a.g, a.c = self.geom, self.case
-        a.ibm = 0 if mode == "bulk" else IBM_IDS[self.method]
+        a.ibm = 0 if (mode == "bulk" or self.no_ibm) else IBM_IDS[self.method]
         a.fpost_prev, a.fpost_next = ptr(self.f[parity]), ptr(self.f[1 - parity])
         a.uring_prev, a.uring_next = ptr(self.uring[parity]), ptr(self.uring[1 - parity])
         a.band = BandView(ptr(self.d_box), ptr(self.d_map), ptr(self.d_fib), ptr(self.d_df))
@@ -414,10 +443,15 @@ class Engine:
         s = self.stream()
         if events:
             events[0].record()
+        if self.tg:
+            self._tg_tick()
         if self.dev_particles and not self.part_started:
             self._particles(s, 2)  # half step of the first timestep
             self.part_started = True
-        self._ibm(s, excl_check=False)
+        if self.no_ibm:
+            self.rebuild_next = False
+        else:
+            self._ibm(s, excl_check=False)
         if self.dev_particles:
             self._particles(s, 3)  # full step of this timestep, half step of the next
         if events:
@@ -502,6 +536,8 @@ class Engine:
         """Advance nsteps timesteps; the last one writes rho/U/f* when outputs_last."""
         if nsteps <= 0:
             return
+        if self.tg and self.ttt + nsteps >= self.d_tg_table.numel():
+            self._tg_table(2 * (self.ttt + nsteps) + 2)
         if self.st.particles is not None and not self.dev_particles:
             for k in range(nsteps):
                 self._sedimentation_step(outputs=outputs_last and k == nsteps - 1)
@@ -593,15 +629,19 @@ class Engine:
     def cd_cl(self):
         """Cd, Cl of the last output step — iblbm/diagnostics/core.py:53-113."""
         cfg, st = self.cfg, self.st
+        if self.no_ibm:
+            return 0.0, 0.0  # iblbm/runtime/scenarios/taylor_green.py:60-62
         u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
         ro_mean = float(self.ro_out.double().mean())
-        denom = ro_mean * u_ref ** 2 * st.lattice_r
+        denom = np.float64(ro_mean * u_ref ** 2 * st.lattice_r)
         if self.method == "DFC":
             force = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).sum(0).cpu().numpy()
-            return float(abs(force[0])) / denom, float(force[1]) / denom
-        nb = int(self.d_count.item())
-        sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).double().sum(0).cpu())
-        return abs(sx) / denom, sy / denom
+            sx, sy = float(force[0]), float(force[1])
+        else:
+            nb = int(self.d_count.item())
+            sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).double().sum(0).cpu())
+        with np.errstate(divide="ignore", invalid="ignore"):  # no inflow (Taylor-Green): numpy's inf / nan
+            return float(np.float64(abs(sx)) / denom), float(np.float64(sy) / denom)
 
     def mdf_stats(self):
         s = self.d_stats.cpu().numpy()
@@ -639,7 +679,7 @@ class Engine:
         st.fib = self.band_fib_dense().cpu().numpy()
         if self.method == "DFC":
             st.dfc_force_lagr = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).cpu().numpy()
-        if self.method == "MDF":
+        if self.method == "MDF" and not self.no_ibm:
             st.mdf_iter_stats = self.mdf_stats()
         return st
 

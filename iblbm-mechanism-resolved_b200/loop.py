@@ -139,7 +139,7 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
               "converged": converged, "final_step": ttt - 1, "termination_reason": termination}
     if sed:
         result["sedimentation_history"] = history
-    elif eng.last_out_step > 0:
+    elif eng.last_out_step > 0 and not eng.no_ibm:
         from .diagnostics import engine_slip
         result["slip"] = engine_slip(eng)  # marker slip of the last output step / U_ref
     result["engine"] = eng

@@ -114,3 +114,50 @@ def rigid_markers(Lx_c, Ly_c, cx0, cy0, pos, angle=0.0):
     rx = Lx_c - cx0
     ry = Ly_c - cy0
     return c * rx - s * ry + pos[0], s * rx + c * ry + pos[1]
+
+
+# ---- decaying Taylor-Green vortex (scenario_type="taylor_green") -------------------
+def tg_params(cfg):
+    """Half-width and viscosity of the vortex in lattice units
+    (iblbm/boundary/tg_analytical.py:49-51)."""
+    return 0.5 * (cfg.NN - 1), cfg.lattice_u * (cfg.cylinder_D_ratio * (cfg.NN - 1)) / cfg.Re
+
+
+def tg_base(X, Y, u0, L):
+    """The vortex without its decay factor: (-u0 cos(pi X/L)) sin(pi Y/L) and
+    (u0 sin(pi X/L)) cos(pi Y/L).  Times the decay factor this is
+    iblbm/diagnostics/core.py:216-241 with the same rounding (the reference
+    multiplies by the decay last)."""
+    ux = -u0 * np.cos(np.pi * X / L) * np.sin(np.pi * Y / L)
+    uy = u0 * np.sin(np.pi * X / L) * np.cos(np.pi * Y / L)
+    return ux, uy
+
+
+def tg_decay_table(cfg, n, dt):
+    """exp(-2 nu (pi/L)^2 t) at t = k dt, k = 0 .. n-1, each evaluated as the
+    reference evaluates it for one step (iblbm/diagnostics/core.py:238)."""
+    L, nu = tg_params(cfg)
+    return np.array([np.exp(-2.0 * nu * (np.pi / L) ** 2 * (k * dt)) for k in range(n)], dtype=np.float64)
+
+
+def tg_face_table(cfg, nx, ny):
+    """Velocities before decay of the boundary nodes, (ux, uy) pairs in the order
+    of iblbm/boundary/tg_analytical.py:53-163: left face j = 0..ny-1, right face
+    j = 0..ny-1, bottom i = 1..nx-2, top i = 1..nx-2, then the corners (0,0),
+    (nx-1,0), (0,ny-1), (nx-1,ny-1); coordinates centred on the lattice."""
+    L, _ = tg_params(cfg)
+    X = np.arange(nx, dtype=float) - (nx - 1) / 2.0
+    Y = np.arange(ny, dtype=float) - (ny - 1) / 2.0
+    j, i = np.arange(ny), np.arange(1, nx - 1)
+    faces = ((np.full_like(j, X[0], dtype=float), Y[j]), (np.full_like(j, X[nx - 1], dtype=float), Y[j]),
+             (X[i], np.full_like(i, Y[0], dtype=float)), (X[i], np.full_like(i, Y[ny - 1], dtype=float)),
+             (X[np.array([0, nx - 1, 0, nx - 1])], Y[np.array([0, 0, ny - 1, ny - 1])]))
+    out = [np.stack(tg_base(xs, ys, cfg.tg_u0, L), axis=1) for xs, ys in faces]
+    return np.ascontiguousarray(np.concatenate(out).reshape(-1))
+
+
+def tg_marker_base(cfg, Lx, Ly, dx, dy, nx, ny):
+    """Marker velocities before decay (iblbm/runtime/scenarios/taylor_green.py:21-31)."""
+    L, _ = tg_params(cfg)
+    ux, uy = tg_base(Lx / dx - (nx - 1) / 2.0, Ly / dy - (ny - 1) / 2.0, cfg.tg_u0, L)
+    return np.stack([ux, uy], axis=1)

@@ -86,8 +86,6 @@ def grid_shape(cfg):
 
 
 def initialize(cfg) -> HostState:
-    if cfg.scenario_type == "taylor_green":
-        raise NotImplementedError("the Taylor-Green scenario is not on the accelerated path")
     nx, ny, dx, dy = grid_shape(cfg)
     phy_char = cfg.phy_l * cfg.cylinder_D_ratio
     cell = (cfg.phy_l / (cfg.NN - 1)) / 1.0
@@ -136,8 +134,16 @@ def initialize(cfg) -> HostState:
 
 
 def initial_velocity(cfg, nodenums):
-    """U at t = 0 — iblbm/init.py:168-201: (inflow_u, 0) for fixed bodies, rest otherwise."""
+    """U at t = 0 — iblbm/init.py:168-201: the Taylor-Green vortex at t = 0 on
+    centred lattice coordinates, (inflow_u, 0) for fixed bodies, rest otherwise."""
     U = np.zeros((nodenums, 2))
-    if cfg.motion_type not in ("oscillating", "sedimentation"):
+    if cfg.scenario_type == "taylor_green":
+        from .physics import tg_base, tg_params
+        nx, ny, _, _ = grid_shape(cfg)
+        L, _ = tg_params(cfg)
+        XX, YY = np.meshgrid(np.arange(nx, dtype=float) - (nx - 1) / 2.0, np.arange(ny, dtype=float) - (ny - 1) / 2.0)
+        ux, uy = tg_base(XX.ravel(), YY.ravel(), cfg.tg_u0, L)
+        U[:, 0], U[:, 1] = ux * 1.0, uy * 1.0  # decay factor exp(-0.0) = 1 at t = 0
+    elif cfg.motion_type not in ("oscillating", "sedimentation"):
         U[:, 0] = cfg.inflow_u
     return U

@@ -36,6 +36,7 @@ extern "C" {
 #define IBLBM_BC_OPEN 1
 #define IBLBM_BC_SETTLING 2
 #define IBLBM_BC_VELOCITY_INLET 3
+#define IBLBM_BC_TG 4 /* Taylor-Green analytic faces (iblbm/boundary/tg_analytical.py) */
 /* immersed-boundary method ids (iblbm/ibm/strategies/*.py) */
 #define IBLBM_IBM_NONE 0
 #define IBLBM_IBM_DF 1
@@ -62,6 +63,14 @@ typedef struct {
     double s_minus;      /* TRT: 1/tau_minus */
     double S[9];         /* CM-MRT relaxation rates */
     double inflow_u, dens;
+    /* IBLBM_BC_TG only (else NULL): the analytic velocity of every boundary node
+     * without its decay factor, (ux, uy) pairs for the left face j = 0..ny-1, the
+     * right face j = 0..ny-1, the bottom face i = 1..nx-2, the top face
+     * i = 1..nx-2 and the corners (0,0), (nx-1,0), (0,ny-1), (nx-1,ny-1); and a
+     * device scalar holding the decay factor of the current step.  The closure
+     * imposes tg_face * (*tg_decay). */
+    const double *tg_face;
+    const double *tg_decay;
 } iblbm_case;
 
 /* Band: the lattice nodes under the marker stencils.  `box` holds x0, y0, w, h
@@ -158,6 +167,9 @@ typedef struct {
      * DFC reads the post-streaming populations field_fstar[9n + q].  NULL: off. */
     const double *field_ro, *field_ux, *field_uy, *field_fstar;
     int field_ustride;
+    /* NULL, or a device scalar scaling every desired velocity this step
+     * (dvel * (*dvel_scale); the Taylor-Green markers' analytic decay) */
+    const double *dvel_scale;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -231,7 +243,8 @@ int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
  * compressibility, band method, and all bulk/whole-lattice or all box passes)
  * in one launch; lattices may differ in size.  Bulk passes without a band
  * (ibm = IBLBM_IBM_NONE, no only_box) may mix kinds: each CTA then dispatches
- * on its case's collision, closure and compressibility.  Tile NODE, ROWS2 or ROWS4 (taken
+ * on its case's collision, closure and compressibility.  The Taylor-Green
+ * closure (IBLBM_BC_TG) is not batched.  Tile NODE, ROWS2 or ROWS4 (taken
  * from a[0]); no ro/U/fstar outputs.  Calls must not run concurrently on the
  * host (the parameter block is staged in one static buffer). */
 int iblbm_dense_step_f32_batch(const iblbm_dense32_args *a, int n, void *stream);
@@ -275,6 +288,7 @@ typedef struct {
     double *dstats;
     const float *field_ro, *field_ux, *field_uy, *field_fstar;
     int field_ustride;
+    const double *dvel_scale;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,

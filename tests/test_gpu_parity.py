@@ -145,6 +145,21 @@ def test_method_matrix(torch, collision, method, delta):
     _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
 
 
+def test_taylor_green_tracks_the_analytic_vortex(torch):
+    """The Taylor-Green run (no IBM step) stays within 2 % (L2) of the analytic
+    decaying vortex after 300 steps (the oracle's error on this lattice: 1.0 %)."""
+    from iblbm_b200 import run
+    from iblbm_b200.physics import tg_base, tg_params
+    cfg = _cfg(RUN_CASES["tg_lbm_bgk"])
+    s = run(cfg, verbose=False)["state"]
+    L, nu = tg_params(cfg)
+    XX, YY = np.meshgrid(np.arange(s.nx) - (s.nx - 1) / 2.0, np.arange(s.ny) - (s.ny - 1) / 2.0)
+    ux, uy = tg_base(XX.ravel(), YY.ravel(), cfg.tg_u0, L)
+    d = np.exp(-2.0 * nu * (np.pi / L) ** 2 * cfg.max_steps)
+    ana = np.stack([ux * d, uy * d], axis=1)
+    assert np.sqrt(np.sum((s.U - ana) ** 2)) / np.sqrt(np.sum(ana ** 2)) < 0.02
+
+
 def test_config1_full_geometry_1000_steps(torch):
     """Config 1 geometry (401 x 161, D = 20, DF + BGK + hat) for 1000 steps."""
     from iblbm_b200 import run
@@ -154,10 +169,12 @@ def test_config1_full_geometry_1000_steps(torch):
     _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
 
 
-def test_graph_and_eager_paths_agree(torch):
-    """Replaying captured CUDA graphs gives the same bits as eager launches."""
+@pytest.mark.parametrize("name", ["c2_mdf_trt_p4", "tg_ibm_mdf_trt_p4"])
+def test_graph_and_eager_paths_agree(torch, name):
+    """Replaying captured CUDA graphs gives the same bits as eager launches
+    (for Taylor-Green the graphs carry the per-step decay factor update)."""
     from iblbm_b200.engine import Engine
-    kw = dict(RUN_CASES["c2_mdf_trt_p4"], max_steps=60)
+    kw = dict(RUN_CASES[name], max_steps=60)
     e1, e2 = Engine(_cfg(kw)), Engine(_cfg(kw))
     e1.advance(60, outputs_last=True, use_graph=True)
     e2.advance(60, outputs_last=True, use_graph=False)
