@@ -138,16 +138,32 @@ class Clocks:
 
 
 def _dist():
+    """One process per GPU, launched by torchrun (RANK / LOCAL_RANK / WORLD_SIZE /
+    MASTER_* in the environment): NCCL on GPUs, gloo on a host without one.
+    Returns (torch.distributed or None, rank, world size, local rank)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws > 1:
         import datetime
+        import torch
         import torch.distributed as dist
         local = int(os.environ.get("LOCAL_RANK", "0"))
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        cuda = torch.cuda.is_available()
+        if cuda:
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if cuda else "gloo", timeout=datetime.timedelta(seconds=120))
         return dist, int(os.environ.get("RANK", "0")), ws, local
     return None, 0, 1, 0
+
+
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest of x over all ranks (every rank calls it at the same point);
+    x itself without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def cpu_baseline(seconds=20.0, threads=None):
@@ -258,11 +274,7 @@ def measure(eng, args, dist, ws):
     eng.parity ^= K & 1
     step_ms = [ev[k][0].elapsed_time(ev[k][3]) for k in range(K)]
     dense_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
-    tot_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(sum(step_ms), dist)
     dense_avg = sum(dense_ms) / K
     bpl = BYTES_PER_LU_F32 if eng.f32 else BYTES_PER_LU_F64
 
@@ -404,10 +416,7 @@ def measure_batch(b, K, W, dist, ws):
     b._bump(K)
     tot_ms = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(K))
     bulk_ms = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(K)) / K
-    if dist:
-        t = torch.tensor([tot_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms = float(t.item())
+    tot_ms = max_over_ranks(tot_ms, dist)
     box_nodes = sum(int(x[2]) * int(x[3]) for e in b.engines for x in [e.d_excl[b.parity].tolist()])
     achieved = BYTES_PER_LU_F32 * (b.N - box_nodes) / (bulk_ms / 1e3) / 1e9
     # steady state through one captured graph
