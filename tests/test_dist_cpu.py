@@ -7,7 +7,6 @@ import os
 import socket
 
 
-
 def _free_port():
     with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
         s.bind(("127.0.0.1", 0))
