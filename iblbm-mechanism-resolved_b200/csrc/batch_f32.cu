@@ -90,8 +90,13 @@ __device__ __forceinline__ void batch_rows(const BatchCase& c, int local)
     }
 }
 
+// Ten resident CTAs per SM (at most 51 registers a thread; 48 are used): more
+// loads in flight per SM than the 56-60 registers the kinds take unbounded.
+// Over the 72-case sweep the bulk passes took 0.757 ms per step this way
+// against 0.771-0.774 ms (the small spills it costs stay in L1); a bound of 12
+// CTAs (40 registers) spills more and lost the gain.
 template <int COLL, int BC, bool INCOMP, int IBM, int NR>
-__global__ void __launch_bounds__(128) dense32_batch_kernel(const __grid_constant__ BatchTable t)
+__global__ void __launch_bounds__(128, 10) dense32_batch_kernel(const __grid_constant__ BatchTable t)
 {
     const int ci = batch_case(t, blockIdx.x);
     batch_rows<COLL, BC, INCOMP, IBM, NR>(t.c[ci], blockIdx.x - t.off[ci]);
