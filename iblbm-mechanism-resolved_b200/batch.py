@@ -237,6 +237,42 @@ class Batch:
             self.graphs[key] = g
         return g
 
+    def step_io(self, host_in, host_out):
+        """One timestep with its host I/O, as a host program drives the batch:
+        every case's markers (the pooled marker_in layout) from pinned host
+        memory host_in, the step, and every case's per-marker forces (marker_out)
+        into pinned host memory host_out.  Replayed from one CUDA graph per parity
+        (copies included); returns when host_out holds this step's forces."""
+        torch = self.torch
+        if not self.started:
+            self.advance(1, outputs_last=False)
+        self.join()  # before a capture: events recorded inside one cannot be waited on outside
+        key = ("io", self.parity, host_in.data_ptr(), host_out.data_ptr())
+        g = self.graphs.get(key)
+        if g is None:
+            cap = torch.cuda.Stream(self.dev)
+            cap.wait_stream(torch.cuda.current_stream(self.dev))
+            cap.wait_stream(self.side)
+            g = torch.cuda.CUDAGraph()
+            p0 = self.parity
+            with torch.cuda.stream(cap):
+                with torch.cuda.graph(g, stream=cap):
+                    self.marker_in.copy_(host_in, non_blocking=True)
+                    self.ev_bulk.record(cap)  # the band kernels start after the copy lands
+                    self.ev_side.record(cap)
+                    self._step()
+                    self.join()
+                    host_out.copy_(self.marker_out, non_blocking=True)
+            torch.cuda.current_stream(self.dev).wait_stream(cap)
+            self.parity = p0
+            self.graphs[key] = g
+        g.replay()
+        self.parity ^= 1
+        self._bump(1)
+        self.fence()
+        torch.cuda.current_stream(self.dev).synchronize()
+        self._sync_engines()
+
     def advance(self, nsteps, outputs_last=True, use_graph=True):
         """Advance every case nsteps timesteps; with outputs_last the last step
         writes each case's rho / u / f* (read with its engine's cd_cl, read_state)."""

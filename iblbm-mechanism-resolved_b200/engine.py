@@ -532,6 +532,48 @@ class Engine:
             self.graphs[key] = g
         return g
 
+    def step_io(self, host_in, host_out):
+        """One timestep with its host I/O, as a host program drives a fixed body:
+        marker positions and desired velocities ([Lx, Ly, dvel], 4 Lb FP64
+        values) from pinned host memory host_in, the step, and the total force
+        on the band (2 FP64 values) into pinned host memory host_out.  Replayed
+        from one CUDA graph per parity (copies included); returns when host_out
+        holds this step's force."""
+        torch = self.torch
+        if self.moving or self.st.particles is not None:
+            raise NotImplementedError("step_io drives fixed bodies (moving markers come from the device)")
+        if self.rebuild_next:
+            self.advance(1, outputs_last=False)
+        main = torch.cuda.current_stream(self.dev)
+        self.join()  # before a capture: events recorded inside one cannot be waited on outside
+        key = ("io", self.parity, host_in.data_ptr(), host_out.data_ptr())
+        g = self.graphs.get(key)
+        if g is None:
+            Lb, nb = self.Lb, int(self.d_count.item())
+            cap = torch.cuda.Stream(self.dev)
+            cap.wait_stream(main)
+            cap.wait_stream(self.side)
+            g = torch.cuda.CUDAGraph()
+            p0 = self.parity
+            with torch.cuda.stream(cap):
+                with torch.cuda.graph(g, stream=cap):
+                    self.d_Lx.copy_(host_in[:Lb], non_blocking=True)
+                    self.d_Ly.copy_(host_in[Lb:2 * Lb], non_blocking=True)
+                    self.d_dv.copy_(host_in[2 * Lb:4 * Lb], non_blocking=True)
+                    self.ev_bulk.record(cap)  # the band kernel starts after the copies land
+                    self.ev_side.record(cap)
+                    self._launch(False)
+                    self.join()
+                    host_out.copy_(self.d_fib[: 2 * nb].view(nb, 2).double().sum(0), non_blocking=True)
+            main.wait_stream(cap)
+            self.parity = p0
+            self.graphs[key] = g
+        g.replay()
+        self.parity ^= 1
+        self.ttt += 1
+        self.fence()
+        main.synchronize()
+
     def advance(self, nsteps, outputs_last=True, use_graph=True):
         """Advance nsteps timesteps; the last one writes rho/U/f* when outputs_last."""
         if nsteps <= 0:

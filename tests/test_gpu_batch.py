@@ -61,3 +61,23 @@ def test_batch_matches_single_cases(torch, tile, merged):
             np.testing.assert_array_equal(getattr(sb, k), getattr(ss, k), err_msg=f"{cfg.ibm_method} {k}")
         np.testing.assert_array_equal(eb.fpost_aos(), es.fpost_aos())
         assert eb.cd_cl() == es.cd_cl()
+
+
+def test_step_io_matches_plain_steps(torch):
+    """A step driven with host I/O (markers in from pinned memory, forces out,
+    one graph per parity) computes the same bits as plain eager steps."""
+    from iblbm_b200.batch import Batch
+    cfgs = [_cfg(**kw) for kw in CASES]
+    a, b = Batch(cfgs), Batch(cfgs)
+    a.advance(5, outputs_last=False)
+    b.advance(5, outputs_last=False)
+    host_in = torch.empty(a.marker_in.numel(), dtype=torch.float64).pin_memory()
+    host_in.copy_(a.marker_in.cpu())
+    host_out = torch.empty(a.marker_out.numel(), dtype=torch.float64).pin_memory()
+    for _ in range(6):
+        a.step_io(host_in, host_out)
+    b.advance(6, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(host_out.numpy(), b.marker_out.cpu().numpy())
+    for ea, eb in zip(a.engines, b.engines):
+        np.testing.assert_array_equal(ea.fpost_aos(), eb.fpost_aos())

@@ -200,3 +200,27 @@ def test_overlapped_schedule_matches_serial(torch, name):
     for k in ("fstar", "U", "ro", "fib"):
         np.testing.assert_array_equal(getattr(s1, k), getattr(s2, k), err_msg=k)
     np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
+
+
+def test_step_io_matches_plain_steps(torch):
+    """A fixed-body step driven with host I/O (markers in from pinned memory,
+    the band force out, one graph per parity) gives the same bits as plain steps."""
+    from iblbm_b200.engine import Engine
+    kw = dict(RUN_CASES["c2_mdf_trt_p4"], max_steps=60)
+    e1, e2 = Engine(_cfg(kw)), Engine(_cfg(kw))
+    e1.advance(3, outputs_last=False)
+    e2.advance(3, outputs_last=False)
+    Lb = e1.Lb
+    host_in = torch.empty(4 * Lb, dtype=torch.float64).pin_memory()
+    host_in[:Lb] = torch.as_tensor(e1.st.Lx)
+    host_in[Lb:2 * Lb] = torch.as_tensor(e1.st.Ly)
+    host_in[2 * Lb:] = torch.as_tensor(e1.st.desired_velocity.reshape(-1))
+    host_out = torch.empty(2, dtype=torch.float64).pin_memory()
+    for _ in range(6):
+        e1.step_io(host_in, host_out)
+    e2.advance(6, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    nb = int(e2.d_count.item())
+    np.testing.assert_array_equal(host_out.numpy(), e2.d_fib[: 2 * nb].view(nb, 2).double().sum(0).cpu().numpy())
+    np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
+    assert e1.ttt == e2.ttt
