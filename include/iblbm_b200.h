@@ -191,6 +191,8 @@ int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args *a, void *stream);
 int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
 int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type);
+/* Shared memory of the band layout of one band step (lists, weights, band
+ * moments); the step itself adds what its options need and checks the total. */
 int iblbm_ibm_smem_bytes(int lb_total, int band_capacity, int delta_type);
 
 /* ---- FP32 shifted-population form ----------------------------------------
@@ -309,6 +311,8 @@ int iblbm_ibm_step_f32(const iblbm_ibm32_args *a, void *stream);
 int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args *host_args, const iblbm_ibm32_args *dev_args, int n,
                              void *stream);
 int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int delta_type);
+/* As iblbm_ibm_smem_bytes; a single body's MDF step adds the marker coupling
+ * matrix when it fits, and the learned warm start its buffers. */
 int iblbm_ibm32_smem_bytes(int lb_total, int band_capacity, int delta_type);
 
 /* ---- learned MDF warm start: the network's training and inference ---------
