@@ -13,7 +13,7 @@ run on the GPU in this library's own kernels (``iblbm_mlp_train_step``: fused
 forward, backward and Adam in one launch; ``iblbm_mlp_infer``).  With the warm
 start on, the band kernel spreads the predicted forces before the first
 iteration and then iterates as plain MDF does, to the same residual
-tolerance: plain MDF is both the fallback and the judge of the slip.
+tolerance: plain MDF is both the fallback and the arbiter of the slip.
 """
 from __future__ import annotations
 
