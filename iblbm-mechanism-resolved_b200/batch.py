@@ -237,41 +237,53 @@ class Batch:
             self.graphs[key] = g
         return g
 
-    def step_io(self, host_in, host_out):
+    def step_io(self, host_in, host_out, wait=True):
         """One timestep with its host I/O, as a host program drives the batch:
         every case's markers (the pooled marker_in layout) from pinned host
         memory host_in, the step, and every case's per-marker forces (marker_out)
-        into pinned host memory host_out.  Replayed from one CUDA graph per parity
-        (copies included); returns when host_out holds this step's forces."""
+        into pinned host memory host_out.  Replayed from one CUDA graph per
+        parity and buffer pair (copies included).  With wait, returns when
+        host_out holds this step's forces; otherwise returns at once with an
+        event that completes then, so a host program can run one step ahead
+        (alternating two buffer pairs, as step k+1's copy-in may run while the
+        host still reads step k's forces)."""
         torch = self.torch
         if not self.started:
             self.advance(1, outputs_last=False)
         self.join()  # before a capture: events recorded inside one cannot be waited on outside
+        main = torch.cuda.current_stream(self.dev)
         key = ("io", self.parity, host_in.data_ptr(), host_out.data_ptr())
         g = self.graphs.get(key)
         if g is None:
             cap = torch.cuda.Stream(self.dev)
-            cap.wait_stream(torch.cuda.current_stream(self.dev))
+            cap.wait_stream(main)
             cap.wait_stream(self.side)
             g = torch.cuda.CUDAGraph()
             p0 = self.parity
             with torch.cuda.stream(cap):
                 with torch.cuda.graph(g, stream=cap):
-                    self.marker_in.copy_(host_in, non_blocking=True)
-                    self.ev_bulk.record(cap)  # the band kernels start after the copy lands
-                    self.ev_side.record(cap)
+                    self.ev_bulk.record(cap)
+                    self.ev_side.record(cap)  # the bulk passes need no marker data: they start at once
+                    self.side.wait_event(self.ev_bulk)
+                    with torch.cuda.stream(self.side):  # markers in ahead of the band kernels (same stream)
+                        self.marker_in.copy_(host_in, non_blocking=True)
                     self._step()
                     self.join()
                     host_out.copy_(self.marker_out, non_blocking=True)
-            torch.cuda.current_stream(self.dev).wait_stream(cap)
+            main.wait_stream(cap)
             self.parity = p0
             self.graphs[key] = g
         g.replay()
         self.parity ^= 1
         self._bump(1)
         self.fence()
-        torch.cuda.current_stream(self.dev).synchronize()
         self._sync_engines()
+        if wait:
+            main.synchronize()
+            return None
+        done = torch.cuda.Event()
+        done.record(main)
+        return done
 
     def advance(self, nsteps, outputs_last=True, use_graph=True):
         """Advance every case nsteps timesteps; with outputs_last the last step

@@ -81,3 +81,14 @@ def test_step_io_matches_plain_steps(torch):
     np.testing.assert_array_equal(host_out.numpy(), b.marker_out.cpu().numpy())
     for ea, eb in zip(a.engines, b.engines):
         np.testing.assert_array_equal(ea.fpost_aos(), eb.fpost_aos())
+    # one step ahead with two alternating buffer pairs
+    ins = [host_in, torch.empty_like(host_in).pin_memory()]
+    ins[1].copy_(host_in)
+    outs = [host_out, torch.empty_like(host_out).pin_memory()]
+    evs = [a.step_io(ins[k % 2], outs[k % 2], wait=False) for k in range(5)]
+    evs[-1].synchronize()
+    b.advance(5, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(outs[0].numpy(), b.marker_out.cpu().numpy())  # the fifth step used outs[0]
+    for ea, eb in zip(a.engines, b.engines):
+        np.testing.assert_array_equal(ea.fpost_aos(), eb.fpost_aos())
