@@ -532,20 +532,21 @@ class Engine:
             self.graphs[key] = g
         return g
 
-    def step_io(self, host_in, host_out):
+    def step_io(self, host_in, host_out, wait=True):
         """One timestep with its host I/O, as a host program drives a fixed body:
         marker positions and desired velocities ([Lx, Ly, dvel], 4 Lb FP64
         values) from pinned host memory host_in, the step, and the total force
         on the band (2 FP64 values) into pinned host memory host_out.  Replayed
-        from one CUDA graph per parity (copies included); returns when host_out
-        holds this step's force."""
+        from one CUDA graph per parity and buffer pair (copies included).  With
+        wait, returns when host_out holds this step's force; otherwise returns
+        at once with an event that completes then (see Batch.step_io)."""
         torch = self.torch
         if self.moving or self.st.particles is not None:
             raise NotImplementedError("step_io drives fixed bodies (moving markers come from the device)")
         if self.rebuild_next:
             self.advance(1, outputs_last=False)
-        main = torch.cuda.current_stream(self.dev)
         self.join()  # before a capture: events recorded inside one cannot be waited on outside
+        main = torch.cuda.current_stream(self.dev)
         key = ("io", self.parity, host_in.data_ptr(), host_out.data_ptr())
         g = self.graphs.get(key)
         if g is None:
@@ -557,11 +558,15 @@ class Engine:
             p0 = self.parity
             with torch.cuda.stream(cap):
                 with torch.cuda.graph(g, stream=cap):
-                    self.d_Lx.copy_(host_in[:Lb], non_blocking=True)
-                    self.d_Ly.copy_(host_in[Lb:2 * Lb], non_blocking=True)
-                    self.d_dv.copy_(host_in[2 * Lb:4 * Lb], non_blocking=True)
-                    self.ev_bulk.record(cap)  # the band kernel starts after the copies land
-                    self.ev_side.record(cap)
+                    self.ev_bulk.record(cap)
+                    self.ev_side.record(cap)  # the bulk pass needs no marker data
+                    # markers in ahead of the band kernel, on the stream it runs on
+                    copy_stream = self.side if self.overlap else cap
+                    copy_stream.wait_event(self.ev_bulk)
+                    with torch.cuda.stream(copy_stream):
+                        self.d_Lx.copy_(host_in[:Lb], non_blocking=True)
+                        self.d_Ly.copy_(host_in[Lb:2 * Lb], non_blocking=True)
+                        self.d_dv.copy_(host_in[2 * Lb:4 * Lb], non_blocking=True)
                     self._launch(False)
                     self.join()
                     host_out.copy_(self.d_fib[: 2 * nb].view(nb, 2).double().sum(0), non_blocking=True)
@@ -572,7 +577,12 @@ class Engine:
         self.parity ^= 1
         self.ttt += 1
         self.fence()
-        main.synchronize()
+        if wait:
+            main.synchronize()
+            return None
+        done = torch.cuda.Event()
+        done.record(main)
+        return done
 
     def advance(self, nsteps, outputs_last=True, use_graph=True):
         """Advance nsteps timesteps; the last one writes rho/U/f* when outputs_last."""

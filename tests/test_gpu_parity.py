@@ -224,3 +224,13 @@ def test_step_io_matches_plain_steps(torch):
     np.testing.assert_array_equal(host_out.numpy(), e2.d_fib[: 2 * nb].view(nb, 2).double().sum(0).cpu().numpy())
     np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
     assert e1.ttt == e2.ttt
+    # one step ahead with two alternating buffer pairs
+    ins = [host_in, torch.empty_like(host_in).pin_memory()]
+    ins[1].copy_(host_in)
+    outs = [host_out, torch.empty_like(host_out).pin_memory()]
+    evs = [e1.step_io(ins[k % 2], outs[k % 2], wait=False) for k in range(5)]
+    evs[-1].synchronize()
+    e2.advance(5, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(outs[0].numpy(), e2.d_fib[: 2 * nb].view(nb, 2).double().sum(0).cpu().numpy())
+    np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
