@@ -556,10 +556,11 @@ def measure_learned(args, n_train=200, K=200):
 
 def sweep_cd_check(cfgs, batch, steps):
     """Cd/Cl of every batched case against the FP64 plain form of the same case
-    after the same number of steps (one case at a time)."""
+    after the same number of steps (one case at a time), and for DF / MDF cases
+    the interpolated marker velocities (so the marker slip) over U."""
     import torch
     from iblbm_b200.engine import Engine
-    worst_cd, worst_cl, rows = 0.0, 0.0, []
+    worst_cd, worst_cl, worst_u, rows = 0.0, 0.0, 0.0, []
     for cfg, eb in zip(cfgs, batch.engines):
         e = Engine(cfg, precision="f64")
         e.advance(steps, outputs_last=True)
@@ -569,10 +570,14 @@ def sweep_cd_check(cfgs, batch, steps):
         rc = abs(cd32 - cd64) / abs(cd64)
         rl = abs(cl32 - cl64) / abs(cd64)
         worst_cd, worst_cl = max(worst_cd, rc), max(worst_cl, rl)
+        if cfg.ibm_method in ("DF", "MDF"):
+            for k in ("d_Lux", "d_Luy"):
+                du = (getattr(eb, k)[: eb.Lb] - getattr(e, k)[: e.Lb]).abs().max().item()
+                worst_u = max(worst_u, du / cfg.inflow_u)
         rows.append((cfg.Re, cfg.ibm_method, cfg.delta_type, cfg.collision_model, cd64, rc))
         del e
     torch.cuda.empty_cache()
-    return worst_cd, worst_cl, rows
+    return worst_cd, worst_cl, worst_u, rows
 
 
 def run_b200(args):
@@ -591,9 +596,10 @@ def run_b200(args):
         cfgs = sweep_configs(max_steps=args.warmup + 4 * Kb + 16)
         batch = Batch(cfgs)
         bres = measure_batch(batch, Kb, args.warmup, dist, ws)
-        worst_cd, worst_cl, rows = sweep_cd_check(cfgs, batch, bres["steps_done"])
+        worst_cd, worst_cl, worst_u, rows = sweep_cd_check(cfgs, batch, bres["steps_done"])
         sweep = {"cases": len(cfgs), "lattice_nodes": batch.N, "max_cd_rel_err_vs_f64": worst_cd,
-                 "max_cl_err_vs_f64_rel_cd": worst_cl, "worst_case": max(rows, key=lambda r: r[5])[:4]}
+                 "max_cl_err_vs_f64_rel_cd": worst_cl, "max_marker_velocity_err_vs_f64_rel_u": worst_u,
+                 "worst_case": max(rows, key=lambda r: r[5])[:4]}
         del batch
     learned = measure_learned(args) if args.form == "chosen" else None
     if rank != 0:
