@@ -120,6 +120,7 @@ class Engine:
             c.bc = BC_IDS["tg_analytical"]
             self.d_tg_face = torch.as_tensor(tg_face_table(cfg, nx, ny), device=dev)
             self.d_tg_step = torch.ones(1, dtype=torch.int64, device=dev)
+            self.d_tg_idx = torch.ones(1, dtype=torch.int64, device=dev)
             self.d_tg_cur = torch.ones(1, dtype=f64, device=dev)
             self._tg_table(int(cfg.max_steps) + 2)
             c.tg_face, c.tg_decay = ptr(self.d_tg_face), ptr(self.d_tg_cur)
@@ -302,8 +303,12 @@ class Engine:
 
     def _tg_tick(self):
         """This step's decay factor into the scalar the closures and the band
-        kernel read, then the step counter advances (graph-capturable)."""
-        self.torch.index_select(self.d_tg_table, 0, self.d_tg_step, out=self.d_tg_cur)
+        kernel read, then the step counter advances (graph-capturable).  The host
+        keeps the table longer than the steps taken; the index is clamped to it on
+        the device all the same, so no step can read outside the table."""
+        torch = self.torch
+        torch.clamp(self.d_tg_step, max=self.d_tg_table.numel() - 1, out=self.d_tg_idx)
+        torch.index_select(self.d_tg_table, 0, self.d_tg_idx, out=self.d_tg_cur)
         self.d_tg_step.add_(1)
 
     def _upload_markers(self):
@@ -545,6 +550,8 @@ class Engine:
             raise NotImplementedError("step_io drives fixed bodies (moving markers come from the device)")
         if self.rebuild_next:
             self.advance(1, outputs_last=False)
+        if self.tg and self.ttt + 1 >= self.d_tg_table.numel():
+            self._tg_table(2 * (self.ttt + 1) + 2)  # drops the captured graphs
         self.join()  # before a capture: events recorded inside one cannot be waited on outside
         main = torch.cuda.current_stream(self.dev)
         key = ("io", self.parity, host_in.data_ptr(), host_out.data_ptr())

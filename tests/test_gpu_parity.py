@@ -234,3 +234,23 @@ def test_step_io_matches_plain_steps(torch):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(outs[0].numpy(), e2.d_fib[: 2 * nb].view(nb, 2).double().sum(0).cpu().numpy())
     np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
+
+
+def test_step_io_taylor_green(torch):
+    """Host-driven steps of a Taylor-Green case with markers (the decay factor's
+    per-step update inside the captured step) give the same bits as plain steps."""
+    from iblbm_b200.engine import Engine
+    kw = dict(RUN_CASES["tg_ibm_mdf_trt_p4"], max_steps=20)
+    e1, e2 = Engine(_cfg(kw)), Engine(_cfg(kw))
+    e1.advance(2, outputs_last=False)
+    e2.advance(2, outputs_last=False)
+    Lb = e1.Lb
+    host_in = torch.empty(4 * Lb, dtype=torch.float64).pin_memory()
+    host_in.copy_(torch.cat([e1.d_Lx[:Lb], e1.d_Ly[:Lb], e1.d_dv[:2 * Lb]]).cpu())
+    host_out = torch.empty(2, dtype=torch.float64).pin_memory()
+    for _ in range(24):  # past the decay table sized for max_steps: it grows
+        e1.step_io(host_in, host_out)
+    e2.advance(24, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
+    assert int(e1.d_tg_step.item()) == int(e2.d_tg_step.item()) == e1.ttt
