@@ -169,6 +169,16 @@ def test_config1_full_geometry_1000_steps(torch):
     _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
 
 
+def test_config1_full_geometry_10000_steps(torch):
+    """Config 1 (401 x 161, D = 20, DF + BGK + hat) for its full 10 000 steps:
+    every field bit for bit against the oracle, Cd/Cl to 1e-12."""
+    from iblbm_b200 import run
+    from oracle import harness as H
+    kw = dict(RUN_CASES["c1_df_bgk_hat"], max_steps=10000, check_interval=500)
+    cfg = _cfg(kw)
+    _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
+
+
 @pytest.mark.parametrize("name", ["c2_mdf_trt_p4", "tg_ibm_mdf_trt_p4"])
 def test_graph_and_eager_paths_agree(torch, name):
     """Replaying captured CUDA graphs gives the same bits as eager launches
