@@ -169,6 +169,22 @@ def test_config1_full_geometry_1000_steps(torch):
     _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
 
 
+@pytest.mark.parametrize("name", ["C2", "C3", "C5"])
+def test_benchmark_geometries_200_steps(torch, name):
+    """Configurations 2 (1601 x 641, MDF + Peskin-4, TRT), 3 (1281 x 1281,
+    oscillating DFC, open boundary) and 5 (321 x 1281, two settling discs,
+    coupled MDF, CM-MRT) at full size for 200 steps: every field bit for bit
+    against the oracle."""
+    from iblbm_b200 import run
+    from oracle import harness as H
+    from tests.golden.make_golden import INIT_CASES
+    kw = dict(INIT_CASES[name], max_steps=200, check_interval=50, use_convergence=False)
+    if name == "C2":
+        kw.update(mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6)
+    cfg = _cfg(kw)
+    _compare_runs(cfg, run(cfg, verbose=False), H.run(cfg))
+
+
 def test_config1_full_geometry_10000_steps(torch):
     """Config 1 (401 x 161, D = 20, DF + BGK + hat) for its full 10 000 steps:
     every field bit for bit against the oracle, Cd/Cl to 1e-12."""
