@@ -22,8 +22,6 @@ case's own engine.
 """
 from __future__ import annotations
 
-import ctypes
-
 from ._lib import IBM_IDS, TILES, Dense32Args, Ibm32Args, check
 from .engine import Engine
 
