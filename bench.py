@@ -55,11 +55,12 @@ BYTES_PER_LU_F64 = 144
 BYTES_PER_LU_F32 = 72
 # DRAM bytes per updated node measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum within the kernel window, caches flushed before the
-# launch): FP32 batched bulk pass on the Re 20/40 part of the sweep (23.77 MB
-# read + 0.05 MB written for 642 962 nodes), FP64 single-case bulk pass (73.81
-# MB read + 25.93 MB written for 1 023 949 nodes).  Most population writes stay
+# launch): FP32 batched bulk pass of one collision model on the Re 20/40 part of
+# the sweep (71.63 MB read + 28.31 MB written for the 1 930 092 nodes of its 12
+# lattices, exclusion boxes included), FP64 single-case bulk pass (73.81 MB read
+# + 25.93 MB written for 1 023 949 nodes).  Part of the population writes stays
 # in L2 until after the kernel, so the write share is a lower bound.
-TRAFFIC_PER_NODE_F32 = (23.77e6 + 0.05e6) / 642962
+TRAFFIC_PER_NODE_F32 = (71.63e6 + 28.31e6) / 1930092
 TRAFFIC_PER_NODE_F64 = (73.81e6 + 25.93e6) / 1023949
 METRIC = "MLUPS and HBM GB/s (1 B200), chosen vs plain form at Cd within 0.1% of FP64"
 
@@ -373,36 +374,37 @@ def sweep_configs(max_steps):
 
 
 def measure_batch(b, K, W, dist, ws):
-    """Time the batched sweep: per-kind tile tuning, K overlapped steps (every
+    """Time the batched sweep: per-group tile tuning, K overlapped steps (every
     step streams the whole sweep, ~4 GB, far above L2), graph-replayed steady
     state, and the host-buffer loop (all markers in, all marker forces out)."""
     import torch
     E = lambda: torch.cuda.Event(enable_timing=True)
     b.advance(max(W, 3), outputs_last=False)
     torch.cuda.synchronize()
-    # per-kind tile choice: the bulk pass is side-effect free when repeated without a parity flip
+    # tile choice per bulk group (cases of one collision, closure and compressibility):
+    # the bulk pass is side-effect free when repeated without a parity flip
     tiles = {}
     main = torch.cuda.current_stream()
-    for g in range(len(b.kinds)):
+    for g in range(len(b.bulk_groups)):
         best = None
         for tile in ("node", "rows2", "rows4"):
-            b.set_tile(g, tile)
-            b._dense(g, "bulk", main.cuda_stream)
+            b.set_bulk_tile(g, tile)
+            b._bulk(g, main.cuda_stream)
             ev = [(E(), E()) for _ in range(3)]
             for e0, e1 in ev:
                 e0.record()
-                b._dense(g, "bulk", main.cuda_stream)
+                b._bulk(g, main.cuda_stream)
                 e1.record()
             torch.cuda.synchronize()
             ms = min(e0.elapsed_time(e1) for e0, e1 in ev)
             if best is None or ms < best[1]:
                 best = (tile, ms)
-        b.set_tile(g, best[0])
+        b.set_bulk_tile(g, best[0])
         tiles[g] = best
-    # one bulk launch over every case against one launch per kind
-    per_kind_ms = sum(ms for _, ms in tiles.values())
+    # one bulk launch over every case against one launch per group
+    per_group_ms = sum(ms for _, ms in tiles.values())
     merged = {}
-    if b.C <= 72 and len(b.kinds) > 1:
+    if b.C <= 72 and len(b.bulk_groups) > 1:
         for tile in ("node", "rows2", "rows4"):
             b.set_tile_all(tile, merged=True)
             b._dense("all", "bulk", main.cuda_stream)
@@ -415,9 +417,9 @@ def measure_batch(b, K, W, dist, ws):
             merged[tile] = min(e0.elapsed_time(e1) for e0, e1 in ev)
         best_tile = min(merged, key=merged.get)
         # in the timed schedule the single launch also competes with the band and
-        # box kernels of the side stream, which slip in between per-kind launches:
+        # box kernels of the side stream, which slip in between per-group launches:
         # take it only on a clear win in isolation
-        b.set_tile_all(best_tile, merged=merged[best_tile] < 0.95 * per_kind_ms)
+        b.set_tile_all(best_tile, merged=merged[best_tile] < 0.95 * per_group_ms)
     b.fence()
     ev = [[E() for _ in range(4)] for _ in range(K)]
     if dist:
@@ -477,10 +479,11 @@ def measure_batch(b, K, W, dist, ws):
             "achieved": achieved, "box_nodes": box_nodes, "steady": steady,
             "e2e": b.N * Ke * ws / e2e_s / 1e6, "h2d": nin * 8, "d2h": host_out.numel() * 8,
             "clocks": clk.summary(), "wall_s_timed": t_wall, "status": b.status(),
-            "tiles": {str(g): {"tile": t, "bulk_ms": ms, "cases": len(b.kinds[g])} for g, (t, ms) in tiles.items()},
-            "bulk_one_launch_ms": merged, "bulk_per_kind_ms_sum": per_kind_ms, "bulk_merged": b.merged,
+            "tiles": {str(g): {"tile": t, "bulk_ms": ms, "cases": len(b.bulk_groups[g])}
+                      for g, (t, ms) in tiles.items()},
+            "bulk_one_launch_ms": merged, "bulk_per_group_ms_sum": per_group_ms, "bulk_merged": b.merged,
             "tile_merged": b.tile_all,
-            "launches_per_step": 1 + len(b.kinds) + (1 if b.merged else len(b.kinds)),
+            "launches_per_step": 1 + len(b.kinds) + (1 if b.merged else len(b.bulk_groups)),
             "steps_done": b.engines[0].ttt - 1}
 
 
@@ -638,13 +641,13 @@ def run_b200(args):
                        "parallelism": f"replicas x{ws}"},
             "steps_batch": max(20, args.steps),
             "schedule": "one batched band launch + box passes (side stream) concurrent with one bulk launch per "
-                        "kind of case; CUDA graph between outputs",
+                        "collision model (cases of every band method together); CUDA graph between outputs",
             "roofline": {"bound": "hbm", "achieved": bres["achieved"], "peak": peak, "unit": "GB/s",
                          "frac": bres["achieved"] / peak,
                          "traffic": TRAFFIC_PER_NODE_F32 * (sweep["lattice_nodes"] - bres["box_nodes"]),
                          "traffic_unit": "bytes per step (all bulk launches), scaled from an ncu capture of the "
                                          "36-case part of the sweep", "peak_kind": peak_kind,
-                         "kernel": "dense32_batch_kernel bulk passes of all kinds (fused pull-stream+BC+macro+"
+                         "kernel": "dense32_batch_kernel bulk passes of all groups (fused pull-stream+BC+macro+"
                                    "collide, FP32 shifted)", "bytes_per_lu": BYTES_PER_LU_F32,
                          "lattice_updates_per_step": bres and (sweep["lattice_nodes"] - bres["box_nodes"])},
             "e2e": {"value": bres["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": bres["h2d"],
@@ -655,7 +658,7 @@ def run_b200(args):
             "sweep": dict(sweep, steady_state_mlups_graph=bres["steady"], status_nonzero=[
                 k for k, st in enumerate(bres["status"]) if st], tiles=bres["tiles"],
                 bulk_ms_per_step=bres["bulk_ms"], bulk_one_launch_ms=bres["bulk_one_launch_ms"],
-                bulk_per_kind_ms_sum=bres["bulk_per_kind_ms_sum"], bulk_merged=bres["bulk_merged"],
+                bulk_per_group_ms_sum=bres["bulk_per_group_ms_sum"], bulk_merged=bres["bulk_merged"],
                 tile_merged=bres["tile_merged"])})
     else:
         line.update({"value": plain["value"], "ms_per_step": plain["ms_per_step"], "dtype": "f64",

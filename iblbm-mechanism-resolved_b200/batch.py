@@ -62,6 +62,16 @@ class Batch:
             for s in range(0, len(idx), MAX_KIND):
                 self.kinds.append(idx[s:s + MAX_KIND])
         self.tiles = [tile] * len(self.kinds)
+        # bulk passes run without the band (the box is left to the box passes),
+        # so cases that differ only in band method share one bulk launch
+        groups = {}
+        for key, idx in sorted(kinds.items()):
+            groups.setdefault(key[:3], []).extend(idx)
+        self.bulk_groups = []
+        for key, idx in sorted(groups.items()):
+            for s in range(0, len(idx), MAX_KIND):
+                self.bulk_groups.append(idx[s:s + MAX_KIND])
+        self.bulk_tiles = [tile] * len(self.bulk_groups)
         # bulk passes: one launch per kind, or one launch over every case
         # (CTAs dispatch on their case's kind) when `merged`
         self.merged = False
@@ -111,21 +121,30 @@ class Batch:
         self.markers_total = tot
 
     def _make_dense_arrays(self):
-        """Per kind and parity, the argument arrays of the whole-lattice, bulk
-        and box passes (tile of the kind set on every entry)."""
+        """Per kind and parity, the argument arrays of the whole-lattice and
+        box passes (tile of the kind set on every entry); per bulk group and
+        parity, those of the bulk passes."""
         self.dense = {}
         for g, idx in enumerate(self.kinds):
             for p in (0, 1):
-                for mode in ("full", "bulk", "box"):
+                for mode in ("full", "box"):
                     arr = (Dense32Args * len(idx))()
                     for n, k in enumerate(idx):
                         e = self.engines[k]
-                        src = {"full": e.dense_full, "bulk": e.dense_bulk, "box": e.dense_box}[mode][p][0]
+                        src = {"full": e.dense_full, "box": e.dense_box}[mode][p][0]
                         a = _copy(src)
                         a.tile = TILES[self.tiles[g]]
                         a.box_blocks = 8
                         arr[n] = a
                     self.dense[g, p, mode] = arr
+        for g, idx in enumerate(self.bulk_groups):
+            for p in (0, 1):
+                arr = (Dense32Args * len(idx))()
+                for n, k in enumerate(idx):
+                    a = _copy(self.engines[k].dense_bulk[p][0])
+                    a.tile = TILES[self.bulk_tiles[g]]
+                    arr[n] = a
+                self.dense["bulk", g, p] = arr
         if self.C <= MAX_KIND:
             order = [k for idx in self.kinds for k in idx]
             for p in (0, 1):
@@ -146,9 +165,19 @@ class Batch:
         self.graphs = {}
 
     def set_tile(self, kind, tile):
+        """Tile of the whole-lattice passes of one kind (the first step's)."""
         if tile not in ("node", "rows2", "rows4"):
             raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
         self.tiles[kind] = tile
+        self._make_dense_arrays()
+        self.graphs = {}
+
+    def set_bulk_tile(self, group, tile):
+        """Tile of the bulk launch of one group (cases of one collision,
+        closure and compressibility)."""
+        if tile not in ("node", "rows2", "rows4"):
+            raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
+        self.bulk_tiles[group] = tile
         self._make_dense_arrays()
         self.graphs = {}
 
@@ -160,6 +189,10 @@ class Batch:
 
     def _dense(self, g, mode, stream):
         arr = self.dense[g, self.parity, mode]
+        check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
+
+    def _bulk(self, g, stream):
+        arr = self.dense["bulk", g, self.parity]
         check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
 
     def _sync_engines(self):
@@ -182,7 +215,7 @@ class Batch:
 
     def _step(self, bulk_events=None):
         """Overlapped step: band kernels and box passes on the side stream,
-        bulk passes of every kind on the current stream (bulk_events: two
+        bulk passes of every group on the current stream (bulk_events: two
         events recorded around the bulk passes)."""
         torch = self.torch
         main = torch.cuda.current_stream(self.dev)
@@ -198,8 +231,8 @@ class Batch:
         if self.merged:
             self._dense("all", "bulk", main.cuda_stream)
         else:
-            for g in range(len(self.kinds)):
-                self._dense(g, "bulk", main.cuda_stream)
+            for g in range(len(self.bulk_groups)):
+                self._bulk(g, main.cuda_stream)
         if bulk_events:
             bulk_events[1].record(main)
         self.ev_bulk.record(main)
