@@ -152,33 +152,42 @@ struct Sm {
     double* wred;  // per-warp residual maxima (FP64 in both forms)
 };
 
+// The per-step-constant block (lists, stencil weights and origins) at sbase,
+// the rest at dbase, shifted down by `shift` bytes (the static block's size
+// when it lives elsewhere; every dynamic offset is at least that).
+template <typename R>
+__device__ inline Sm<R> carve2(char* sbase, char* dbase, const Layout& L, size_t shift)
+{
+    Sm<R> s;
+    s.sidx = reinterpret_cast<int*>(sbase + L.o_sidx);
+    s.ent = reinterpret_cast<int*>(sbase + L.o_ent);
+    s.cstart = reinterpret_cast<int*>(sbase + L.o_cstart);
+    s.nodes = reinterpret_cast<int*>(sbase + L.o_nodes);
+    s.part = reinterpret_cast<int*>(sbase + L.o_part);
+    s.wx = reinterpret_cast<R*>(sbase + L.o_wx);
+    s.wy = reinterpret_cast<R*>(sbase + L.o_wy);
+    s.entw = reinterpret_cast<R*>(sbase + L.o_entw);
+    s.ix0 = reinterpret_cast<int*>(sbase + L.o_ix0);
+    s.iy0 = reinterpret_cast<int*>(sbase + L.o_iy0);
+    s.dvx = reinterpret_cast<R*>(dbase + (L.o_dvx - shift));
+    s.dvy = reinterpret_cast<R*>(dbase + (L.o_dvy - shift));
+    s.R_ = reinterpret_cast<R*>(dbase + (L.o_R - shift));
+    s.Lux = reinterpret_cast<R*>(dbase + (L.o_Lux - shift));
+    s.Luy = reinterpret_cast<R*>(dbase + (L.o_Luy - shift));
+    s.Lfx = reinterpret_cast<R*>(dbase + (L.o_Lfx - shift));
+    s.Lfy = reinterpret_cast<R*>(dbase + (L.o_Lfy - shift));
+    s.bro = reinterpret_cast<R*>(dbase + (L.o_bro - shift));
+    s.bwx = reinterpret_cast<R*>(dbase + (L.o_bwx - shift));
+    s.bwy = reinterpret_cast<R*>(dbase + (L.o_bwy - shift));
+    s.wred = reinterpret_cast<double*>(dbase + (L.o_wred - shift));
+    s.ired = reinterpret_cast<int*>(dbase + (L.o_ired - shift));
+    return s;
+}
+
 template <typename R>
 __device__ inline Sm<R> carve(char* base, const Layout& L)
 {
-    Sm<R> s;
-    s.sidx = reinterpret_cast<int*>(base + L.o_sidx);
-    s.ent = reinterpret_cast<int*>(base + L.o_ent);
-    s.cstart = reinterpret_cast<int*>(base + L.o_cstart);
-    s.nodes = reinterpret_cast<int*>(base + L.o_nodes);
-    s.part = reinterpret_cast<int*>(base + L.o_part);
-    s.wx = reinterpret_cast<R*>(base + L.o_wx);
-    s.wy = reinterpret_cast<R*>(base + L.o_wy);
-    s.entw = reinterpret_cast<R*>(base + L.o_entw);
-    s.dvx = reinterpret_cast<R*>(base + L.o_dvx);
-    s.dvy = reinterpret_cast<R*>(base + L.o_dvy);
-    s.R_ = reinterpret_cast<R*>(base + L.o_R);
-    s.Lux = reinterpret_cast<R*>(base + L.o_Lux);
-    s.Luy = reinterpret_cast<R*>(base + L.o_Luy);
-    s.Lfx = reinterpret_cast<R*>(base + L.o_Lfx);
-    s.Lfy = reinterpret_cast<R*>(base + L.o_Lfy);
-    s.bro = reinterpret_cast<R*>(base + L.o_bro);
-    s.bwx = reinterpret_cast<R*>(base + L.o_bwx);
-    s.bwy = reinterpret_cast<R*>(base + L.o_bwy);
-    s.wred = reinterpret_cast<double*>(base + L.o_wred);
-    s.ix0 = reinterpret_cast<int*>(base + L.o_ix0);
-    s.iy0 = reinterpret_cast<int*>(base + L.o_iy0);
-    s.ired = reinterpret_cast<int*>(base + L.o_ired);
-    return s;
+    return carve2<R>(base, base, L, 0);
 }
 
 __device__ __forceinline__ double nanmax(double a, double b) { return (b > a || b != b) ? b : a; }
@@ -358,8 +367,11 @@ __device__ __forceinline__ void spread2(const Sm<R>& sh, const R* gx, const R* g
 template <bool SHIFTED>
 using BcOf = typename std::conditional<SHIFTED, BcParams32, BcParams>::type;
 
-// The band step of one case, run by one CTA of IBM_THREADS threads.
-template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED>
+// The band step of one case, run by one CTA of IBM_THREADS threads.  With GS
+// the per-step-constant block (contribution lists, stencil weights, origins)
+// stays in global memory (list_cache, L2-resident) instead of shared memory:
+// the form for bodies whose lists do not fit on chip.
+template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED, bool GS = false>
 __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>& bc)
 {
     constexpr int SW = Sten<A>::SW, S = Sten<A>::S;
@@ -368,7 +380,10 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     const int P = a.n_particles, Lb = a.lb_total, NB = a.band_capacity;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const Layout Lay = make_layout<R>(Lb, NB, S);
-    Sm<R> sh = carve<R>(smem_raw, Lay);
+    const size_t dyn_end = Lay.total - (GS ? Lay.static_bytes : 0);  // shared bytes of the layout
+    Sm<R> sh;
+    if constexpr (GS) sh = carve2<R>(reinterpret_cast<char*>(a.list_cache), smem_raw, Lay, Lay.static_bytes);
+    else sh = carve<R>(smem_raw, Lay);
     __shared__ int s_nb, s_status, s_box[4], s_step, s_cur;
     __shared__ __align__(8) uint64_t s_bar, s_wbar;
     const bool rebuild = a.rebuild || a.xt_table;
@@ -384,7 +399,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         if (tid == 0 && (a.mlp_mode & 2)) {
             mbar_init(&s_wbar);
             mbar_expect(&s_wbar, (uint32_t)(sizeof(float) * MLP_NP));
-            bulk_copy(smem_raw + Lay.total + mlp_act_bytes(Lb), a.mlp_params, (uint32_t)(sizeof(float) * MLP_NP),
+            bulk_copy(smem_raw + dyn_end + mlp_act_bytes(Lb), a.mlp_params, (uint32_t)(sizeof(float) * MLP_NP),
                       &s_wbar);
         }
     }
@@ -393,14 +408,16 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         s_step = a.step_counter ? *a.step_counter : 0;
         if (a.xt_table && (s_step < 0 || s_step >= a.xt_len)) s_status = ST_TABLE;
         if (!rebuild && s_status == ST_OK) {
-            // restore the per-step-constant block of a fixed body in one bulk copy
-            mbar_init(&s_bar);
-            const uint32_t bytes = (uint32_t)Lay.static_bytes;
-            mbar_expect(&s_bar, bytes);
-            const char* src = reinterpret_cast<const char*>(a.list_cache);
-            for (uint32_t off = 0; off < bytes; off += 65536u) {
-                const uint32_t chunk = min(65536u, bytes - off);
-                bulk_copy(smem_raw + off, src + off, chunk, &s_bar);
+            if constexpr (!GS) {
+                // restore the per-step-constant block of a fixed body in one bulk copy
+                mbar_init(&s_bar);
+                const uint32_t bytes = (uint32_t)Lay.static_bytes;
+                mbar_expect(&s_bar, bytes);
+                const char* src = reinterpret_cast<const char*>(a.list_cache);
+                for (uint32_t off = 0; off < bytes; off += 65536u) {
+                    const uint32_t chunk = min(65536u, bytes - off);
+                    bulk_copy(smem_raw + off, src + off, chunk, &s_bar);
+                }
             }
             s_nb = *a.band_count;
             s_box[0] = a.box[0];
@@ -574,7 +591,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             }
         }
         __syncthreads();
-        if (!a.xt_table) {
+        if (!GS && !a.xt_table) {
             // cache the per-step-constant block for the following steps
             const int4* s4 = reinterpret_cast<const int4*>(smem_raw);
             int4* d4 = reinterpret_cast<int4*>(a.list_cache);
@@ -584,7 +601,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         __syncthreads();
     } else {
         // wait for the bulk copy (bounded: a copy that does not land is reported)
-        bool done = false;
+        bool done = GS;
         for (long long it = 0; it < TMA_WAIT_LIMIT && !done; ++it) done = mbar_try_wait(&s_bar, 0);
         if (!done) {
             if (tid == 0) s_status = ST_COPY_TIMEOUT;
@@ -722,12 +739,12 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             mlp_rec = (mode & 1) != 0;
             const bool warm = (mode & 2) != 0;
             if (mode) {
-                float* mA = reinterpret_cast<float*>(smem_raw + Lay.total);
+                float* mA = reinterpret_cast<float*>(smem_raw + dyn_end);
                 float* mB = mA + MLP_CHUNK * MLP_LD;
                 float* mY = mB + MLP_CHUNK * MLP_LD;
                 float* mGx = mY + MLP_CHUNK * 2;
                 float* mGy = mGx + Lb;
-                const float* Pm = reinterpret_cast<const float*>(smem_raw + Lay.total + mlp_act_bytes(Lb));
+                const float* Pm = reinterpret_cast<const float*>(smem_raw + dyn_end + mlp_act_bytes(Lb));
                 bool use_net = false;
                 if (warm) {
                     // a copy that does not land leaves this step on plain MDF
@@ -847,7 +864,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             // loop's; that loop stays for coupled bodies, for marker sets that do
             // not fit, and wherever the overlaps do not account for every entry of
             // the node lists.
-            const size_t off = Lay.total + (a.mlp_mode ? mlp_smem_bytes(Lb) : 0);
+            const size_t off = dyn_end + (a.mlp_mode ? mlp_smem_bytes(Lb) : 0);
             if (ms_fits(off, Lb, S)) {
                 msA = reinterpret_cast<float*>(smem_raw + off);
                 float* msP = msA + (size_t)Lb * MS_W;  // W_lk vs(b_k) per stencil slot, while A is built
@@ -1258,10 +1275,10 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     }
 }
 
-template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED>
+template <class ARGS, typename R, bool SHIFTED, int A, int METHOD, bool COUPLED, bool GS>
 __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_step_kernel(const ARGS a, BcOf<SHIFTED> bc)
 {
-    ibm_step_body<ARGS, R, SHIFTED, A, METHOD, COUPLED>(a, bc);
+    ibm_step_body<ARGS, R, SHIFTED, A, METHOD, COUPLED, GS>(a, bc);
 }
 
 // Many independent cases in one launch: CTA b runs the band step of case b,
@@ -1310,10 +1327,11 @@ static cudaError_t launch_ibm(const ARGS& a, const BCP& bc, size_t smem, void* s
 
 // Dynamic shared memory of one band step.
 template <typename R, class ARGS>
-static size_t ibm_smem(const ARGS& a)
+static size_t ibm_smem(const ARGS& a, bool gs = false)
 {
     const int S = a.delta_type == 0 ? 25 : 9;
-    size_t t = make_layout<R>(a.lb_total, a.band_capacity, S).total;
+    const Layout L = make_layout<R>(a.lb_total, a.band_capacity, S);
+    size_t t = L.total - (gs ? L.static_bytes : 0);
     if (mlp_on(a)) t += mlp_smem_bytes(a.lb_total);
     if (ms_on(a) && ms_fits(t, a.lb_total, S)) t += ms_smem_bytes(a.lb_total, S);
     return t;
@@ -1329,9 +1347,18 @@ inline bool mlp_args_ok(const iblbm_ibm32_args& a)
     return a.mlp_uref > 0.0f;
 }
 
-// Argument checks shared by both forms; returns IBLBM_OK or an error code.
+// Whether a band step keeps its per-step-constant block in global memory: only
+// when the whole layout does not fit in shared memory.
 template <typename R, class ARGS>
-static int check_ibm_args(const ARGS* a)
+static bool ibm_global_static(const ARGS& a)
+{
+    return ibm_smem<R>(a) > (size_t)IBM_SMEM_LIMIT;
+}
+
+// Argument checks shared by both forms; returns IBLBM_OK or an error code.
+// allow_gs: the caller can launch the global-static form (single-case launches).
+template <typename R, class ARGS>
+static int check_ibm_args(const ARGS* a, bool allow_gs = false)
 {
     if (!a) return IBLBM_E_ARG;
     const bool fields = a->field_ro || a->field_fstar;
@@ -1354,7 +1381,9 @@ static int check_ibm_args(const ARGS* a)
         return IBLBM_E_ARG;
     if ((long long)a->lb_total * 32 >= (1LL << 31)) return IBLBM_E_ARG;
     if ((reinterpret_cast<uintptr_t>(a->list_cache) & 15) != 0) return IBLBM_E_ARG;  // bulk-copy source
-    if (ibm_smem<R>(*a) > (size_t)IBM_SMEM_LIMIT) return IBLBM_E_CAPACITY;
+    if (ibm_smem<R>(*a) > (size_t)IBM_SMEM_LIMIT &&
+        (!allow_gs || ibm_smem<R>(*a, true) > (size_t)IBM_SMEM_LIMIT))
+        return IBLBM_E_CAPACITY;
     if (!mlp_args_ok(*a)) return IBLBM_E_ARG;
     if (a->method == IBM_MDF && a->lb_total > IBM_THREADS) return IBLBM_E_CAPACITY;
     return IBLBM_OK;
@@ -1365,10 +1394,13 @@ template <class ARGS, typename R, bool SHIFTED>
 static int dispatch_ibm(const ARGS* a, const BcOf<SHIFTED>& bc, void* stream)
 {
     using BCP = BcOf<SHIFTED>;
-    const size_t smem = ibm_smem<R>(*a);
+    const bool gs = ibm_global_static<R>(*a);
+    const size_t smem = ibm_smem<R>(*a, gs);
     const bool coupled = a->method == IBM_MDF && a->mdf_coupled;
     cudaError_t e = cudaErrorInvalidValue;
-#define IBLBM_LAUNCH(AR, M, C) e = launch_ibm<ARGS, BCP, ibm_step_kernel<ARGS, R, SHIFTED, AR, M, C>>(*a, bc, smem, stream)
+#define IBLBM_LAUNCH(AR, M, C)                                                                              \
+    e = gs ? launch_ibm<ARGS, BCP, ibm_step_kernel<ARGS, R, SHIFTED, AR, M, C, true>>(*a, bc, smem, stream) \
+           : launch_ibm<ARGS, BCP, ibm_step_kernel<ARGS, R, SHIFTED, AR, M, C, false>>(*a, bc, smem, stream)
     if (a->delta_type == 0) {
         if (a->method == IBM_DF) IBLBM_LAUNCH(2, IBM_DF, false);
         else if (a->method == IBM_DFC) IBLBM_LAUNCH(2, IBM_DFC, false);

@@ -26,7 +26,7 @@ extern "C" int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int 
 
 extern "C" int iblbm_ibm_step_f32(const iblbm_ibm32_args* a, void* stream)
 {
-    const int chk = check_ibm_args<float>(a);
+    const int chk = check_ibm_args<float>(a, true);
     if (chk != IBLBM_OK) return chk;
     CollParams32 cp;
     BcParams32 bc;

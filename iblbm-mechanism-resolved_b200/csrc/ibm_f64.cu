@@ -38,7 +38,7 @@ extern "C" int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int de
 
 extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 {
-    const int chk = check_ibm_args<double>(a);
+    const int chk = check_ibm_args<double>(a, true);
     if (chk != IBLBM_OK) return chk;
     CollParams cp;
     BcParams bc;

@@ -7,7 +7,10 @@ series).  ``compute_slip_error`` restates iblbm/diagnostics/ibm_quality.py:
 132-188 (boundary slip of a velocity field on a diagnostic marker ring);
 its interpolation runs on the GPU through the band kernel (field-input mode),
 in the reference's summation order.  ``engine_slip`` evaluates the same on the
-engine's own markers and last output velocity.
+engine's own markers and last output velocity.  ``tg_analytical_velocity_field``
+and ``compute_l2_error`` restate iblbm/diagnostics/core.py:216-268 (the
+decaying Taylor-Green vortex and the relative L2 error against it), and
+``tg_l2_error`` applies them to a Taylor-Green run's final velocity.
 """
 from __future__ import annotations
 
@@ -102,3 +105,34 @@ def engine_slip(engine, u_ref=None):
     mag = np.sqrt((Lux - dv[:, 0]) ** 2 + (Luy - dv[:, 1]) ** 2)
     return {"mean": float(np.mean(mag) / u_ref), "max": float(np.max(mag) / u_ref),
             "rms": float(np.sqrt(np.mean(mag ** 2)) / u_ref)}
+
+
+def tg_analytical_velocity_field(X, Y, t, u0, L, nu):
+    """Velocity of the decaying vortex at centred coordinates (X, Y) and time t:
+    ux = -u0 cos(pi X/L) sin(pi Y/L) e^(-2 nu (pi/L)^2 t), uy = u0 sin(pi X/L)
+    cos(pi Y/L) e^(-2 nu (pi/L)^2 t), the decay factor multiplied last."""
+    decay = np.exp(-2.0 * nu * (np.pi / L) ** 2 * t)
+    ux = -u0 * np.cos(np.pi * X / L) * np.sin(np.pi * Y / L) * decay
+    uy = u0 * np.sin(np.pi * X / L) * np.cos(np.pi * Y / L) * decay
+    return ux, uy
+
+
+def compute_l2_error(U_num, U_ana):
+    """||U_num - U_ana||_2 / ||U_ana||_2 over all entries (inf when U_ana is 0)."""
+    diff = np.asarray(U_num) - np.asarray(U_ana)
+    den = np.sqrt(np.sum(np.asarray(U_ana) ** 2))
+    if den == 0.0:
+        return float("inf")
+    return float(np.sqrt(np.sum(diff ** 2)) / den)
+
+
+def tg_l2_error(U, cfg, nx, ny, step=None):
+    """Relative L2 error of a Taylor-Green run's velocity U (nx*ny x 2, row-major
+    in y) against the vortex at t = step (default cfg.max_steps), on the lattice
+    centred at ((nx-1)/2, (ny-1)/2) with half-width (NN-1)/2."""
+    from .physics import tg_params
+    L, nu = tg_params(cfg)
+    X, Y = np.meshgrid(np.arange(nx) - (nx - 1) / 2.0, np.arange(ny) - (ny - 1) / 2.0)
+    t = float(cfg.max_steps if step is None else step)
+    ux, uy = tg_analytical_velocity_field(X.ravel(), Y.ravel(), t, cfg.tg_u0, L, nu)
+    return compute_l2_error(U, np.stack([ux, uy], axis=1))

@@ -176,7 +176,12 @@ typedef struct {
  * ibm/strategies/df.py:27-49, the MDF loop of iblbm/ibm/mdf.py:61-229 (and the
  * coupled multi-particle loop of iblbm/ibm/multi_particle.py:62-316), and
  * compute_lambda_gpu + dfc_correction_gpu (gpu_kernels.py:1091-1223) called
- * from ibm/strategies/dfc.py:31-54. */
+ * from ibm/strategies/dfc.py:31-54.
+ * Sizes: the band layout (iblbm_ibm_smem_bytes) lives in shared memory while it
+ * fits (220 KB); beyond that the step keeps its contribution lists and stencil
+ * weights in list_cache (global memory, L2-resident) and only the per-step
+ * arrays on chip, so a single body of any marker count within the other limits
+ * runs (band_capacity <= 2048; an MDF body <= 512 markers). */
 int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
 /* Same band step for callers that cannot allocate device memory at call time
  * (a host framework that owns all device allocations, or a service that
@@ -303,11 +308,14 @@ typedef struct {
     float *mlp_features, *mlp_targets;
 } iblbm_ibm32_args;
 
+/* Sizes as iblbm_ibm_step_f64. */
 int iblbm_ibm_step_f32(const iblbm_ibm32_args *a, void *stream);
 /* Band steps of n independent cases in one launch (one CTA per case; stencil,
  * method and coupling may differ between cases).  host_args and dev_args hold
  * the same n argument blocks, on the host (checked here, sizes the shared
- * memory) and in device memory (read by the kernel). */
+ * memory) and in device memory (read by the kernel).  Every case's band layout
+ * must fit in shared memory (else IBLBM_E_CAPACITY): a larger body is stepped
+ * on its own. */
 int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args *host_args, const iblbm_ibm32_args *dev_args, int n,
                              void *stream);
 int iblbm_ibm32_list_cache_ints(int lb_total, int band_capacity, int delta_type);
