@@ -83,8 +83,11 @@ class Engine:
         if cfg.motion_type == "sedimentation":
             if st.particles is None:
                 raise NotImplementedError("single-particle sedimentation runtime is not on the accelerated path")
-            if cfg.settling_inertia_model == "full_volume" or cfg.enable_rotation:
-                raise NotImplementedError("full_volume inertia and particle rotation are not on the accelerated path")
+            if cfg.settling_inertia_model == "full_volume":
+                raise NotImplementedError("full_volume inertia is not on the accelerated path")
+            if cfg.enable_rotation and cfg.rotation_coupling not in ("indirect", "semi_implicit"):
+                raise NotImplementedError(f"rotation_coupling='{cfg.rotation_coupling}' (torque inside the MDF "
+                                          "loop) is not on the accelerated path; indirect and semi_implicit are")
             if cfg.time_integrator != "verlet":
                 raise NotImplementedError("only the Velocity-Verlet integrator is on the accelerated path")
             if cfg.ibm_method != "MDF":
@@ -209,6 +212,10 @@ class Engine:
         self.dev_particles = False
         if st.particles is not None:
             self.dev_particles = self.f32 if device_particles is None else bool(device_particles)
+            if cfg.enable_rotation:  # the torque and the angular Verlet step run on the host
+                if device_particles:
+                    raise NotImplementedError("rotating particles are stepped on the host")
+                self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
         self.side = torch.cuda.Stream(self.dev, priority=-1)
@@ -630,6 +637,7 @@ class Engine:
     # ---- multi-particle sedimentation (host Newton-Euler, as the reference) ----------
     def _sedimentation_step(self, outputs):
         cfg, st = self.cfg, self.st
+        rot = cfg.enable_rotation
         for p in st.particles:  # runtime/scenarios/sedimentation_multi.py:36-80
             F = p.force + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             vel_half = p.vel + 0.5 * st.dt * F / p.mass
@@ -637,10 +645,17 @@ class Engine:
             if hist is not None:
                 vel_half = vel_half + 0.5 * hist
             p.pos = p.pos + st.dt * vel_half * st.dx
-            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=0.0)
+            if rot:  # angular half kick, physics/rigid_body.py:65-74
+                p.omega_half = p.omega + 0.5 * st.dt * p.torque / p.I_particle
+                p.angle += st.dt * p.omega_half
+            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=p.angle if rot else 0.0)
             dv = np.empty((p.Lb, 2))
             dv[:, 0] = float(vel_half[0])
             dv[:, 1] = float(vel_half[1])
+            if rot and cfg.rotation_coupling == "semi_implicit" and p.omega != 0.0:
+                # U + omega x r with the last step's omega, physics/markers.py:41-60
+                dv[:, 0] += -p.omega * (p.Ly - float(p.pos[1])) / st.dx
+                dv[:, 1] += p.omega * (p.Lx - float(p.pos[0])) / st.dx
             p.desired_velocity = dv
             p.vel_half = vel_half
         self._upload_markers()
@@ -648,8 +663,11 @@ class Engine:
         self.ttt += 1
         if outputs:
             self.last_out_step = self.ttt - 1
-        forces = self.particle_forces()
-        for p, fp in zip(st.particles, forces):  # runtime/scenarios/sedimentation_multi.py:83-111
+        forces, torques = self.particle_forces(torques=rot)
+        for k, (p, fp) in enumerate(zip(st.particles, forces)):  # runtime/scenarios/sedimentation_multi.py:83-111
+            if rot:  # physics/rigid_body.py:77-82
+                p.omega = p.omega_half + 0.5 * st.dt * torques[k] / p.I_particle
+                p.torque = torques[k]
             p.fib_force = fp
             F = fp + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             vel_new = p.vel_half + 0.5 * st.dt * F / p.mass
@@ -662,19 +680,30 @@ class Engine:
             p.vel = vel_new
             p.force = fp
 
-    def particle_forces(self):
+    def particle_forces(self, torques=False):
         """-sum of each particle's spread force over the lattice, summed like the
-        reference (numpy over the dense N x 2 field: iblbm/ibm/multi_particle.py:233-241)."""
+        reference (numpy over the dense N x 2 field: iblbm/ibm/multi_particle.py:199-202);
+        with torques also T = -sum((i - cx) fy - (j - cy) fx) over the lattice, node
+        indices as floats and the particle centre in lattice units (:203-208).
+        Returns (forces, torques or None)."""
+        st = self.st
         nb = int(self.d_count.item())
         nodes = self.d_nodes[:nb].cpu().numpy()
         part = self.d_fib_part[: 2 * self.B * self.P].reshape(self.P, self.B, 2)[:, :nb].cpu().numpy()
         part = part.astype(np.float64)
-        out = []
+        out, tq = [], ([] if torques else None)
+        if torques:
+            II, JJ = np.meshgrid(np.arange(st.nx, dtype=float), np.arange(st.ny, dtype=float), indexing="xy")
         for p in range(self.P):
             dense = np.zeros((self.N, 2))
             dense[nodes] = part[p]
             out.append(np.array([-float(dense[:, 0].sum()), -float(dense[:, 1].sum())]))
-        return out
+            if torques:
+                pos = st.particles[p].pos
+                fx = np.ascontiguousarray(dense[:, 0]).reshape(st.ny, st.nx)
+                fy = np.ascontiguousarray(dense[:, 1]).reshape(st.ny, st.nx)
+                tq.append(-float(np.sum((II - float(pos[0]) / st.dx) * fy - (JJ - float(pos[1]) / st.dy) * fx)))
+        return out, tq
 
     # ---- read-back ----------------------------------------------------------------
     def band_fib_dense(self):

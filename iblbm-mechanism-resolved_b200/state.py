@@ -37,6 +37,11 @@ class Particle:
     cy_init: float
     fib_force: np.ndarray = field(default_factory=lambda: np.zeros(2))
     vel_half: np.ndarray = field(default_factory=lambda: np.zeros(2))
+    # rotation (enable_rotation): angular velocity, last torque, turned angle
+    omega: float = 0.0
+    torque: float = 0.0
+    angle: float = 0.0
+    omega_half: float = 0.0
 
 
 @dataclass

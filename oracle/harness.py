@@ -317,7 +317,7 @@ def init_state(cfg):
                     force=np.zeros(2), mass=mass, rho_ratio=rho_p, lattice_r=lattice_r, r_domain=r,
                     I_particle=0.5 * mass * lattice_r ** 2, Lx_c=plx.copy(), Ly_c=ply.copy(),
                     Lx=plx, Ly=ply, Lb=plb, Larea=pla, desired_velocity=np.zeros((plb, 2)),
-                    cx_init=pcx, cy_init=pcy))
+                    cx_init=pcx, cy_init=pcy, omega=0.0, torque=0.0, angle=0.0))
             s.particles = parts
     return s
 
@@ -437,11 +437,24 @@ class OracleSim:
         for p, particle in enumerate(s.particles):
             fp = fpart[p]
             particle._fib_force = np.array([-float(fp[:, 0].sum()), -float(fp[:, 1].sum())])
+            if cfg.enable_rotation:
+                # iblbm/ibm/multi_particle.py:203-208: T = -sum((i - cx) fy - (j - cy) fx)
+                # over the lattice, node indices as floats, centre in lattice units
+                II, JJ = np.meshgrid(np.arange(s.nx, dtype=float), np.arange(s.ny, dtype=float), indexing="xy")
+                cx_lat = float(particle.pos[0]) / s.dx
+                cy_lat = float(particle.pos[1]) / s.dy
+                fx = np.ascontiguousarray(fp[:, 0]).reshape(s.ny, s.nx)
+                fy = np.ascontiguousarray(fp[:, 1]).reshape(s.ny, s.nx)
+                particle._torque_new = -float(np.sum((II - cx_lat) * fy - (JJ - cy_lat) * fx))
         velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
 
-    # runtime/scenarios/sedimentation_multi.py:36-80 (Verlet half step, no rotation)
+    # runtime/scenarios/sedimentation_multi.py:36-80 (Verlet half step; with rotation
+    # the half kick of iblbm/physics/rigid_body.py:65-74, markers turned by the
+    # angle, and for semi-implicit coupling the desired velocity U + omega x r of
+    # iblbm/physics/markers.py:41-60 with the angular velocity of the last step)
     def _half_step(self):
         s, cfg = self.s, self.cfg
+        rot = cfg.enable_rotation
         for p in s.particles:
             F = p.force + _net_gravity(p.rho_ratio, p.lattice_r, s.gravity_lattice, cfg.gravity_direction)
             hist = _history_dv(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
@@ -449,10 +462,17 @@ class OracleSim:
             if hist is not None:
                 vel_half = vel_half + 0.5 * hist
             p.pos = p.pos + s.dt * vel_half * s.dx
-            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=0.0)
+            if rot:
+                omega_half = p.omega + 0.5 * s.dt * p.torque / p.I_particle
+                p.angle += s.dt * omega_half
+                p._omega_half = omega_half
+            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=p.angle if rot else 0.0)
             dv = np.empty((p.Lb, 2))
             dv[:, 0] = float(vel_half[0])
             dv[:, 1] = float(vel_half[1])
+            if rot and cfg.rotation_coupling == "semi_implicit" and p.omega != 0.0:
+                dv[:, 0] += -p.omega * (p.Ly - float(p.pos[1])) / s.dx
+                dv[:, 1] += p.omega * (p.Lx - float(p.pos[0])) / s.dx
             p.desired_velocity = dv
             p._vel_half = vel_half
 
@@ -468,6 +488,9 @@ class OracleSim:
                 vel_new = vel_new + 0.5 * hist
             if cfg.settling_inertia_model == "feng_b2":
                 vel_new = vel_new + (1.0 / p.rho_ratio) * (p.vel - p.vel_prev)
+            if cfg.enable_rotation:  # iblbm/physics/rigid_body.py:77-82
+                p.omega = p._omega_half + 0.5 * s.dt * p._torque_new / p.I_particle
+                p.torque = p._torque_new
             p.vel_prev = p.vel.copy()
             p.vel = vel_new
             p.force = p._fib_force

@@ -84,6 +84,31 @@ RUN_CASES = {
                                  mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
                                  marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
                                  check_interval=50),
+    # two settling discs that also rotate (torque from the spread force, Verlet on the
+    # angular velocity, markers turned by the angle); indirect and semi-implicit coupling
+    "c5r_sed2_mdf_rot_indirect": dict(Re=20, NN=81, xmax=1, ymax=4, cylinder_center=(0.5, 3.0),
+                                      cylinder_D_ratio=0.25, lattice_u=0.05, inflow_u=0.0,
+                                      bc_type="settling_channel", delta_type="peskin4pt",
+                                      ibm_method="MDF", collision_model="BGK",
+                                      motion_type="sedimentation", rho_ratio=3.0, gravity=2e-5,
+                                      particles_config=[{"center": (0.53, 3.4), "rho_ratio": 3.0},
+                                                        {"center": (0.48, 2.9), "rho_ratio": 3.0}],
+                                      settling_inertia_model="explicit_history", enable_rotation=True,
+                                      mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                                      marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
+                                      check_interval=50),
+    "c5r_sed2_mdf_rot_semi": dict(Re=20, NN=81, xmax=1, ymax=4, cylinder_center=(0.5, 3.0),
+                                  cylinder_D_ratio=0.25, lattice_u=0.05, inflow_u=0.0,
+                                  bc_type="settling_channel", delta_type="hat",
+                                  ibm_method="MDF", collision_model="TRT",
+                                  motion_type="sedimentation", rho_ratio=3.0, gravity=2e-5,
+                                  particles_config=[{"center": (0.47, 3.4), "rho_ratio": 3.0},
+                                                    {"center": (0.52, 2.9), "rho_ratio": 3.5}],
+                                  settling_inertia_model="feng_b2", enable_rotation=True,
+                                  rotation_coupling="semi_implicit",
+                                  mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                                  marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
+                                  check_interval=50),
     # default boundary family (velocity inlet / pressure outlet / no-slip walls), DF + P4
     "vin_df_bgk_p4": dict(Re=10, NN=81, xmax=2, ymax=1, cylinder_center=(0.5, 0.5),
                           cylinder_D_ratio=0.125, lattice_u=0.05, inflow_u=0.05,
@@ -290,6 +315,8 @@ def make_run(name, kw, out_dir):
     d["final_step"] = np.array([res["final_step"]])
     if st.particles:
         d["particles"] = np.array([[*p.pos, *p.vel, *p.force] for p in st.particles])
+        if cfg.enable_rotation:
+            d["rotation"] = np.array([[p.omega, p.angle, p.torque] for p in st.particles])
     if getattr(st, "_mdf_iter_stats", None):
         s = st._mdf_iter_stats
         d["mdf_stats"] = np.array([s["iter_count"], s["last_residual"]])

@@ -99,6 +99,8 @@ def _compare_runs(cfg, res, ref):
             np.testing.assert_array_equal(p.pos, q.pos)
             np.testing.assert_array_equal(p.vel, q.vel)
             np.testing.assert_array_equal(p.force, q.force)
+            if cfg.enable_rotation:
+                assert (p.omega, p.angle, p.torque) == (q.omega, q.angle, q.torque)
     if cfg.ibm_method == "DFC":
         np.testing.assert_allclose(s.dfc_force_lagr, r.dfc_force_lagr, rtol=1e-13, atol=1e-16)
 

@@ -133,6 +133,9 @@ def test_oracle_runs_match_reference(name):
     if "particles" in g:
         got = np.array([[*p.pos, *p.vel, *p.force] for p in s.particles])
         np.testing.assert_array_equal(got, g["particles"])
+    if "rotation" in g:
+        got = np.array([[p.omega, p.angle, p.torque] for p in s.particles])
+        np.testing.assert_array_equal(got, g["rotation"])
 
 
 def test_oracle_taylor_green_tracks_the_analytic_vortex():
