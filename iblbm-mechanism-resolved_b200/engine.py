@@ -85,9 +85,6 @@ class Engine:
                 raise NotImplementedError("single-particle sedimentation runtime is not on the accelerated path")
             if cfg.settling_inertia_model == "full_volume":
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
-            if cfg.enable_rotation and cfg.rotation_coupling not in ("indirect", "semi_implicit"):
-                raise NotImplementedError(f"rotation_coupling='{cfg.rotation_coupling}' (torque inside the MDF "
-                                          "loop) is not on the accelerated path; indirect and semi_implicit are")
             if cfg.time_integrator != "verlet":
                 raise NotImplementedError("only the Velocity-Verlet integrator is on the accelerated path")
             if cfg.ibm_method != "MDF":

@@ -109,6 +109,20 @@ RUN_CASES = {
                                   mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
                                   marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
                                   check_interval=50),
+    # the multi-particle runtime adds omega x r only for semi-implicit coupling, so
+    # iterative coupling steps like indirect there
+    "c5r_sed2_mdf_rot_iterative": dict(Re=20, NN=81, xmax=1, ymax=4, cylinder_center=(0.5, 3.0),
+                                       cylinder_D_ratio=0.25, lattice_u=0.05, inflow_u=0.0,
+                                       bc_type="settling_channel", delta_type="peskin4pt",
+                                       ibm_method="MDF", collision_model="CM_MRT",
+                                       motion_type="sedimentation", rho_ratio=3.0, gravity=2e-5,
+                                       particles_config=[{"center": (0.53, 3.4), "rho_ratio": 3.0},
+                                                         {"center": (0.48, 2.9), "rho_ratio": 3.0}],
+                                       settling_inertia_model="none", enable_rotation=True,
+                                       rotation_coupling="iterative",
+                                       mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                                       marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
+                                       check_interval=50),
     # default boundary family (velocity inlet / pressure outlet / no-slip walls), DF + P4
     "vin_df_bgk_p4": dict(Re=10, NN=81, xmax=2, ymax=1, cylinder_center=(0.5, 0.5),
                           cylinder_D_ratio=0.125, lattice_u=0.05, inflow_u=0.05,
