@@ -207,6 +207,7 @@ class Engine:
         # form; the FP64 form keeps the host step, whose force sums follow numpy's
         # pairwise order bit for bit)
         self.dev_particles = False
+        self._torque_ij = None
         if st.particles is not None:
             self.dev_particles = self.f32 if device_particles is None else bool(device_particles)
             if cfg.enable_rotation:  # the torque and the angular Verlet step run on the host
@@ -690,7 +691,10 @@ class Engine:
         part = part.astype(np.float64)
         out, tq = [], ([] if torques else None)
         if torques:
-            II, JJ = np.meshgrid(np.arange(st.nx, dtype=float), np.arange(st.ny, dtype=float), indexing="xy")
+            if self._torque_ij is None:  # node indices as floats, kept between steps
+                self._torque_ij = np.meshgrid(np.arange(st.nx, dtype=float), np.arange(st.ny, dtype=float),
+                                              indexing="xy")
+            II, JJ = self._torque_ij
         for p in range(self.P):
             dense = np.zeros((self.N, 2))
             dense[nodes] = part[p]
