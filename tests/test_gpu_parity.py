@@ -282,3 +282,24 @@ def test_step_io_taylor_green(torch):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(e1.fpost_aos(), e2.fpost_aos())
     assert int(e1.d_tg_step.item()) == int(e2.d_tg_step.item()) == e1.ttt
+
+
+@pytest.mark.parametrize("method,spacing", [("DF", 0.5), ("MDF", 0.65), ("DFC", 0.5)])
+def test_large_moving_body_keeps_lists_in_global_memory(torch, method, spacing):
+    """An oscillating cylinder of 100 nodes diameter with Peskin-4 markers every
+    0.5-0.65 dx (483-628 markers): its band layout exceeds the band kernel's
+    shared memory, so the step keeps its contribution lists in global memory
+    and rebuilds them there every step.  FP64, 20 steps, bit for bit against
+    the oracle."""
+    from iblbm_b200 import run
+    from iblbm_b200._lib import DELTA_IDS
+    from iblbm_b200.engine import Engine
+    from oracle import harness as H
+    cfg = _cfg(dict(Re=100, NN=401, xmax=1.5, ymax=1, cylinder_center=(0.75, 0.5), cylinder_D_ratio=0.25,
+                    lattice_u=0.05, inflow_u=0.0, bc_type="open_boundary", delta_type="peskin4pt",
+                    ibm_method=method, collision_model="TRT", motion_type="oscillating", KC=5.0,
+                    nx_formula="simple", mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                    marker_spacing_factor=spacing, max_steps=20, use_convergence=False, check_interval=10))
+    eng = Engine(cfg, precision="f64")
+    assert eng.L.iblbm_ibm_smem_bytes(eng.Lb, eng.B, DELTA_IDS[cfg.delta_type]) > 220 * 1024
+    _compare_runs(cfg, run(cfg, verbose=False, engine=eng), H.run(cfg))
