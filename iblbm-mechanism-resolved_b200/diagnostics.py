@@ -5,7 +5,8 @@ number from a Cl history: second half, detrended, peak of the rfft power
 spectrum without the DC term, with the reference's handling of rectified |Cl|
 series).  ``compute_slip_error`` restates iblbm/diagnostics/ibm_quality.py:
 132-188 (boundary slip of a velocity field on a diagnostic marker ring);
-its interpolation runs on the GPU through the band kernel (field-input mode),
+``compute_leakage_flux`` restates :189-251 (the normal flux through that ring);
+their interpolation runs on the GPU through the band kernel (field-input mode),
 in the reference's summation order.  ``engine_slip`` evaluates the same on the
 engine's own markers and last output velocity.  ``tg_analytical_velocity_field``
 and ``compute_l2_error`` restate iblbm/diagnostics/core.py:216-268 (the
@@ -75,6 +76,26 @@ def compute_slip_error(Eux, Euy, dx, dy, cx, cy, D, NN, delta_type, u_target_x=N
     mag = np.sqrt((Lux - tx) ** 2 + (Luy - ty) ** 2)
     return {"mean": float(np.mean(mag) / u_ref), "max": float(np.max(mag) / u_ref),
             "rms": float(np.sqrt(np.mean(mag ** 2)) / u_ref), "per_marker": mag / u_ref, "theta": theta}
+
+
+def compute_leakage_flux(Eux, Euy, dx, dy, cx, cy, D, NN, delta_type, u_target_x=None, u_target_y=None,
+                         u_ref=0.1):
+    """Flux through the body surface, the integral of (u(X_m) - u_target) . n ds
+    over the diagnostic ring (outward normal (cos t, sin t), ds = 2 pi r / N),
+    raw and over U_ref pi D, with the per-marker normal velocity over U_ref
+    (iblbm/diagnostics/ibm_quality.py:189-251).  Near zero when the boundary
+    holds.  The interpolation runs on the GPU as for compute_slip_error."""
+    Eux = np.asarray(Eux.cpu() if hasattr(Eux, "cpu") else Eux, dtype=np.float64)
+    Euy = np.asarray(Euy.cpu() if hasattr(Euy, "cpu") else Euy, dtype=np.float64)
+    r = D / 2.0
+    Lx, Ly, theta = diagnostic_markers(cx, cy, r, NN)
+    Lb = len(Lx)
+    Lux, Luy = _interp_gpu(Eux, Euy, Lx, Ly, dx, dy, delta_type)
+    tx = np.zeros(Lb) if u_target_x is None else u_target_x
+    ty = np.zeros(Lb) if u_target_y is None else u_target_y
+    un = (Lux - tx) * np.cos(theta) + (Luy - ty) * np.sin(theta)
+    raw = float(np.sum(un * (2.0 * np.pi * r / Lb)))
+    return {"total": raw / (u_ref * np.pi * D), "total_raw": raw, "per_marker": un / u_ref, "theta": theta}
 
 
 def engine_slip(engine, u_ref=None):

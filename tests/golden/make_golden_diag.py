@@ -1,7 +1,8 @@
 """Fixtures for the diagnostics (tests/test_diagnostics.py), made by running the
 reference's own functions: iblbm.diagnostics.compute_strouhal on seeded
 synthetic Cl series (signed, and rectified |Cl| on both sides of the aliasing
-threshold) and iblbm.diagnostics.compute_slip_error on a seeded velocity field.
+threshold), and iblbm.diagnostics.compute_slip_error and
+iblbm.diagnostics.ibm_quality.compute_leakage_flux on a seeded velocity field.
 
 Usage:  python tests/golden/make_golden_diag.py --reference /path/to/reference
 """
@@ -24,6 +25,7 @@ def main():
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/iblbm_numba_cache")
     sys.path.insert(0, args.reference)
     from iblbm.diagnostics import compute_slip_error, compute_strouhal
+    from iblbm.diagnostics.ibm_quality import compute_leakage_flux
     rng = np.random.default_rng(11)
     out = {}
     ci, D, u = 50, 20.0, 0.05
@@ -49,6 +51,9 @@ def main():
         out[f"slip_{delta}_mean"] = np.array([r["mean"]])
         out[f"slip_{delta}_max"] = np.array([r["max"]])
         out[f"slip_{delta}_per_marker"] = r["per_marker"]
+        q = compute_leakage_flux(Eux, Euy, dx, dy, 0.5, 0.5, 0.25, NN, delta, u_ref=0.05)
+        out[f"leak_{delta}_total"] = np.array([q["total"], q["total_raw"]])
+        out[f"leak_{delta}_per_marker"] = q["per_marker"]
     out["slip_Eux"], out["slip_Euy"] = Eux, Euy
     np.savez_compressed(os.path.join(HERE, "diag.npz"), **out)
     print("wrote", os.path.join(HERE, "diag.npz"))

@@ -42,6 +42,24 @@ def test_slip_error_matches_reference(diag, delta):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("delta", ["hat", "peskin4pt"])
+def test_leakage_flux_matches_reference(diag, delta):
+    """Normal flux through the diagnostic ring against the reference's
+    compute_leakage_flux on the same field: per-marker normal velocities to
+    1e-13 of the largest, the signed total (a sum with cancellation) to 1e-12."""
+    from iblbm_b200.diagnostics import compute_leakage_flux
+    NN = 81
+    dx = 1.0 / (NN - 1)
+    q = compute_leakage_flux(diag["slip_Eux"], diag["slip_Euy"], dx, dx, 0.5, 0.5, 0.25, NN, delta, u_ref=0.05)
+    want = diag[f"leak_{delta}_per_marker"]
+    scale = float(np.max(np.abs(want)))
+    np.testing.assert_allclose(q["per_marker"], want, rtol=0, atol=1e-13 * scale)
+    total, raw = diag[f"leak_{delta}_total"]
+    assert abs(q["total"] - total) <= 1e-12 * scale
+    assert abs(q["total_raw"] - raw) <= 1e-12 * scale * 0.05 * np.pi * 0.25
+
+
+@pytest.mark.gpu
 def test_run_reports_marker_slip():
     """run() adds the marker slip of the last output step (mean, max, RMS over
     U_ref), interpolated in the reference's order: equal to the oracle's
