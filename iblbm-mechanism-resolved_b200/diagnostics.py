@@ -11,7 +11,12 @@ in the reference's summation order.  ``engine_slip`` evaluates the same on the
 engine's own markers and last output velocity.  ``tg_analytical_velocity_field``
 and ``compute_l2_error`` restate iblbm/diagnostics/core.py:216-268 (the
 decaying Taylor-Green vortex and the relative L2 error against it), and
-``tg_l2_error`` applies them to a Taylor-Green run's final velocity.
+``tg_l2_error`` applies them to a Taylor-Green run's final velocity.  The
+post-processing statistics of the reference's histories and fields restate
+iblbm/diagnostics/core.py: ``tail_start_index`` / ``tail_values`` /
+``tail_mean`` / ``tail_peak_to_peak_amp`` (:31-51, the last 30 % of a
+series), ``check_convergence`` (:115-136), ``compute_recirculation_length``
+(:264-310) and ``compute_cl_amplitude`` (:312-333).
 """
 from __future__ import annotations
 
@@ -157,3 +162,64 @@ def tg_l2_error(U, cfg, nx, ny, step=None):
     t = float(cfg.max_steps if step is None else step)
     ux, uy = tg_analytical_velocity_field(X.ravel(), Y.ravel(), t, cfg.tg_u0, L, nu)
     return compute_l2_error(U, np.stack([ux, uy], axis=1))
+
+
+STEADY_TAIL_FRAC = 0.3
+
+
+def tail_start_index(length, frac=STEADY_TAIL_FRAC):
+    """First index of the tail: floor(length (1 - frac)), kept inside the series."""
+    if length <= 0:
+        raise ValueError("empty history array")
+    return min(max(int(length * (1.0 - frac)), 0), length - 1)
+
+
+def tail_values(values, frac=STEADY_TAIL_FRAC):
+    arr = np.asarray(values, dtype=np.float64)
+    if arr.size == 0:
+        raise ValueError("empty history array")
+    return arr[tail_start_index(arr.size, frac):]
+
+
+def tail_mean(values, frac=STEADY_TAIL_FRAC):
+    return float(np.mean(tail_values(values, frac)))
+
+
+def tail_peak_to_peak_amp(values, frac=STEADY_TAIL_FRAC):
+    """Half the peak-to-peak range of the tail."""
+    t = tail_values(values, frac)
+    return float((t.max() - t.min()) / 2.0)
+
+
+def check_convergence(Eux_new, Euy_new, Eux_old, Euy_old):
+    """sqrt(sum |u_new - u_old|^2 / sum |u_old|^2), 1.0 when the old field is zero."""
+    num = np.sum((Eux_new - Eux_old) ** 2 + (Euy_new - Euy_old) ** 2)
+    den = np.sum(Eux_old ** 2 + Euy_old ** 2)
+    return 1.0 if den == 0.0 else np.sqrt(num / den)
+
+
+def compute_recirculation_length(Eux, dx, dy, cx, cy, D):
+    """Length of the wake's reverse-flow region over D: along the centre row,
+    the first sign change of ux from negative to non-negative behind the body
+    (searched from one node past the rear), located by linear interpolation,
+    measured from the rear x = cx + D/2.  NaN when there is none."""
+    Eux = np.asarray(Eux)
+    nx = Eux.shape[1]
+    row = Eux[int(round(cy / dy)), :]
+    x_rear = cx + D / 2.0
+    for i in range(int(np.ceil(x_rear / dx)) + 1, nx - 1):
+        u0, u1 = row[i], row[i + 1]
+        if u0 < 0 and u1 >= 0:
+            x0, x1 = i * dx, (i + 1) * dx
+            return (x0 + (0.0 - u0) / (u1 - u0) * (x1 - x0) - x_rear) / D
+    return float("nan")
+
+
+def compute_cl_amplitude(Cl_history):
+    """Amplitude of the second half of a Cl series: its maximum for a rectified
+    |Cl| series (every value >= -1e-10), else half its peak-to-peak range."""
+    cl = np.asarray(Cl_history, dtype=float)
+    half = cl[len(cl) // 2:]
+    if np.all(cl >= -1e-10):
+        return float(np.max(half))
+    return float((np.max(half) - np.min(half)) / 2.0)

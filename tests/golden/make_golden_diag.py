@@ -26,6 +26,7 @@ def main():
     sys.path.insert(0, args.reference)
     from iblbm.diagnostics import compute_slip_error, compute_strouhal
     from iblbm.diagnostics.ibm_quality import compute_leakage_flux
+    from iblbm.diagnostics import core
     rng = np.random.default_rng(11)
     out = {}
     ci, D, u = 50, 20.0, 0.05
@@ -55,6 +56,21 @@ def main():
         out[f"leak_{delta}_total"] = np.array([q["total"], q["total_raw"]])
         out[f"leak_{delta}_per_marker"] = q["per_marker"]
     out["slip_Eux"], out["slip_Euy"] = Eux, Euy
+    # post-processing statistics on the same series and fields
+    for k in series:
+        cl = out[f"st_{k}_cl"]
+        out[f"tail_{k}"] = np.array([core.tail_start_index(len(cl)), core.tail_mean(cl),
+                                     core.tail_peak_to_peak_amp(cl), core.tail_mean(cl, 0.5),
+                                     core.compute_cl_amplitude(cl)])
+    Eold = 0.05 + 0.01 * rng.standard_normal((ny, nx))
+    out["conv_old"] = Eold
+    out["conv"] = np.array([core.check_convergence(Eux, Euy, Eold, Euy * 0.5)])
+    # a wake: reverse flow behind a body at (0.5, 0.5), D = 0.25, ending at x = 0.9
+    xs = np.arange(nx) * dx
+    wake = np.tile(np.where((xs > 0.62) & (xs < 0.9), -0.01 * np.sin(np.pi * (xs - 0.62) / 0.28), 0.02), (ny, 1))
+    out["recirc_field"] = wake
+    out["recirc"] = np.array([core.compute_recirculation_length(wake, dx, dy, 0.5, 0.5, 0.25),
+                              core.compute_recirculation_length(np.abs(wake), dx, dy, 0.5, 0.5, 0.25)])
     np.savez_compressed(os.path.join(HERE, "diag.npz"), **out)
     print("wrote", os.path.join(HERE, "diag.npz"))
 

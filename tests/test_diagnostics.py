@@ -79,3 +79,29 @@ def test_run_reports_marker_slip():
     assert res["slip"]["max"] == float(np.max(mag) / st.in_u)
     assert res["slip"]["mean"] == float(np.mean(mag) / st.in_u)
     assert res["slip"]["rms"] == float(np.sqrt(np.mean(mag ** 2)) / st.in_u)
+
+
+@pytest.mark.parametrize("kind", ["signed", "rect_low", "rect_high"])
+def test_tail_statistics_match_reference(diag, kind):
+    """Tail index, tail mean (30 % and 50 %), half peak-to-peak and Cl amplitude
+    of the reference's functions on the same series, bit for bit."""
+    from iblbm_b200 import diagnostics as D
+    cl = diag[f"st_{kind}_cl"]
+    got = [D.tail_start_index(len(cl)), D.tail_mean(cl), D.tail_peak_to_peak_amp(cl), D.tail_mean(cl, 0.5),
+           D.compute_cl_amplitude(cl)]
+    np.testing.assert_array_equal(np.array(got), diag[f"tail_{kind}"])
+    with pytest.raises(ValueError):
+        D.tail_values([])
+
+
+def test_convergence_and_recirculation_match_reference(diag):
+    from iblbm_b200 import diagnostics as D
+    NN = 81
+    dx = 1.0 / (NN - 1)
+    Eux, Euy = diag["slip_Eux"], diag["slip_Euy"]
+    assert D.check_convergence(Eux, Euy, diag["conv_old"], Euy * 0.5) == diag["conv"][0]
+    assert D.check_convergence(Eux, Euy, 0 * Eux, 0 * Euy) == 1.0
+    w = diag["recirc_field"]
+    got = [D.compute_recirculation_length(w, dx, dx, 0.5, 0.5, 0.25),
+           D.compute_recirculation_length(np.abs(w), dx, dx, 0.5, 0.5, 0.25)]
+    np.testing.assert_array_equal(np.array(got), diag["recirc"])
