@@ -85,8 +85,11 @@ class Engine:
                 raise NotImplementedError("single-particle sedimentation runtime is not on the accelerated path")
             if cfg.settling_inertia_model == "full_volume":
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
-            if cfg.time_integrator != "verlet":
-                raise NotImplementedError("only the Velocity-Verlet integrator is on the accelerated path")
+            if cfg.time_integrator not in ("verlet", "euler_explicit"):
+                raise NotImplementedError(f"time_integrator='{cfg.time_integrator}' (verlet, euler_explicit)")
+            if cfg.time_integrator == "euler_explicit" and cfg.enable_rotation:
+                raise NotImplementedError("explicit Euler with rotation (internal angular momentum of the fluid "
+                                          "inside each disc) is not on the accelerated path")
             if cfg.ibm_method != "MDF":
                 raise NotImplementedError("multi-particle sedimentation is accelerated for MDF")
         if cfg.stream_first:
@@ -210,9 +213,10 @@ class Engine:
         self._torque_ij = None
         if st.particles is not None:
             self.dev_particles = self.f32 if device_particles is None else bool(device_particles)
-            if cfg.enable_rotation:  # the torque and the angular Verlet step run on the host
+            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit":
+                # the torque, the angular Verlet step and the explicit Euler step run on the host
                 if device_particles:
-                    raise NotImplementedError("rotating particles are stepped on the host")
+                    raise NotImplementedError("rotating particles and explicit Euler steps run on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -634,6 +638,8 @@ class Engine:
 
     # ---- multi-particle sedimentation (host Newton-Euler, as the reference) ----------
     def _sedimentation_step(self, outputs):
+        if self.cfg.time_integrator == "euler_explicit":
+            return self._sedimentation_step_euler(outputs)
         cfg, st = self.cfg, self.st
         rot = cfg.enable_rotation
         for p in st.particles:  # runtime/scenarios/sedimentation_multi.py:36-80
@@ -677,6 +683,43 @@ class Engine:
             p.vel_prev = p.vel.copy()
             p.vel = vel_new
             p.force = fp
+
+    def _sedimentation_step_euler(self, outputs):
+        """Explicit Euler (runtime/scenarios/sedimentation_multi.py:126-190, no
+        rotation): the IB step with the markers and desired velocity the last
+        step left, then velocity and position from this step's force
+        (physics/inertia/{none,explicit_history}.py euler_explicit,
+        physics/rigid_body.py:84-98, feng_b2 post-correction), then the next
+        step's markers and desired velocity."""
+        cfg, st = self.cfg, self.st
+        self._upload_markers()
+        self._launch(outputs)
+        self.ttt += 1
+        if outputs:
+            self.last_out_step = self.ttt - 1
+        forces, _ = self.particle_forces()
+        for p, fp in zip(st.particles, forces):
+            p.fib_force = fp
+            F = fp + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
+            vel_new = p.vel + st.dt * F / p.mass
+            hist = history_increment(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            if hist is not None:
+                vel_new = vel_new + hist
+            if cfg.sedimentation_euler_update_scheme == "trapezoidal":
+                pos_new = p.pos + 0.5 * st.dt * (p.vel + vel_new) * st.dx
+            else:
+                pos_new = p.pos + st.dt * vel_new * st.dx
+            if cfg.settling_inertia_model == "feng_b2":
+                vel_new = vel_new + (1.0 / p.rho_ratio) * (p.vel - p.vel_prev)
+            p.vel_prev = p.vel.copy()
+            p.vel = vel_new
+            p.pos = pos_new
+            p.force = fp
+            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=0.0)
+            dv = np.empty((p.Lb, 2))
+            dv[:, 0] = float(vel_new[0])
+            dv[:, 1] = float(vel_new[1])
+            p.desired_velocity = dv
 
     def particle_forces(self, torques=False):
         """-sum of each particle's spread force over the lattice, summed like the

@@ -495,6 +495,34 @@ class OracleSim:
             p.vel = vel_new
             p.force = p._fib_force
 
+    # runtime/scenarios/sedimentation_multi.py:126-190 without rotation: explicit Euler
+    # after the IB step (iblbm/physics/inertia/{none,explicit_history}.py euler_explicit,
+    # iblbm/physics/rigid_body.py:84-98 position update, feng_b2 post-correction), then
+    # the markers and desired velocity of the next step
+    def _euler_step(self):
+        s, cfg = self.s, self.cfg
+        for p in s.particles:
+            F = p._fib_force + _net_gravity(p.rho_ratio, p.lattice_r, s.gravity_lattice, cfg.gravity_direction)
+            vel_new = p.vel + s.dt * F / p.mass
+            hist = _history_dv(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
+            if hist is not None:
+                vel_new = vel_new + hist
+            if cfg.sedimentation_euler_update_scheme == "trapezoidal":
+                pos_new = p.pos + 0.5 * s.dt * (p.vel + vel_new) * s.dx
+            else:
+                pos_new = p.pos + s.dt * vel_new * s.dx
+            if cfg.settling_inertia_model == "feng_b2":
+                vel_new = vel_new + (1.0 / p.rho_ratio) * (p.vel - p.vel_prev)
+            p.vel_prev = p.vel.copy()
+            p.vel = vel_new
+            p.pos = pos_new
+            p.force = p._fib_force
+            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=0.0)
+            dv = np.empty((p.Lb, 2))
+            dv[:, 0] = float(vel_new[0])
+            dv[:, 1] = float(vel_new[1])
+            p.desired_velocity = dv
+
     def cd_cl(self):
         """iblbm/diagnostics/core.py:53-113 via the strategies' compute_cd_cl."""
         s, cfg = self.s, self.cfg
@@ -523,7 +551,10 @@ class OracleSim:
         self.stream_boundary_macro()
         self.apply_ibm()
         if s.particles is not None:
-            self._full_step()
+            if cfg.time_integrator == "euler_explicit":
+                self._euler_step()
+            else:
+                self._full_step()
         s.feq = feq(s.ro, s.U, cfg.incompressible_lbgk)
         if cfg.stream_first or self.force_level:
             self.f = self.collide()

@@ -203,6 +203,17 @@ def test_f32_rotating_sedimentation(torch, name):
         assert abs(p.omega - q.omega) <= 1e-3 * abs(q.omega)
 
 
+@pytest.mark.parametrize("name", ["c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap"])
+def test_f32_euler_sedimentation(torch, name):
+    """Explicit Euler integration of two settling discs: the FP32 form's
+    positions within 1e-4 lattice units of the FP64 form's."""
+    cfg = _cfg(RUN_CASES[name])
+    r64, r32 = _pair(cfg)
+    for p, q in zip(r32["state"].particles, r64["state"].particles):
+        dxl = (np.asarray(p.pos) - np.asarray(q.pos)) / r64["state"].dx
+        assert np.max(np.abs(dxl)) <= 1e-4
+
+
 def test_f32_config1_geometry_long(torch):
     """Config-1 geometry (401 x 161, D = 20, DF + BGK + hat) for 3000 steps:
     Cd/Cl of the FP32 form within 0.1 % of the FP64 form throughout."""
