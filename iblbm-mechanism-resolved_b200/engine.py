@@ -87,9 +87,6 @@ class Engine:
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
             if cfg.time_integrator not in ("verlet", "euler_explicit"):
                 raise NotImplementedError(f"time_integrator='{cfg.time_integrator}' (verlet, euler_explicit)")
-            if cfg.time_integrator == "euler_explicit" and cfg.enable_rotation:
-                raise NotImplementedError("explicit Euler with rotation (internal angular momentum of the fluid "
-                                          "inside each disc) is not on the accelerated path")
             if cfg.ibm_method != "MDF":
                 raise NotImplementedError("multi-particle sedimentation is accelerated for MDF")
         if cfg.stream_first:
@@ -684,21 +681,52 @@ class Engine:
             p.vel = vel_new
             p.force = fp
 
+    def _l_int_z(self, p):
+        """Angular momentum of the fluid inside particle p's disc from this step's
+        velocity and density (diagnostics/internal_flow.py:220-262): the box of
+        the disc copied to the host, summed like the reference."""
+        st = self.st
+        ci, cj, r_lat = float(p.pos[0]) / st.dx, float(p.pos[1]) / st.dx, p.r_domain / st.dx
+        ii, jj, rr = int(round(ci)), int(round(cj)), int(r_lat) + 2
+        i0, i1 = max(0, ii - rr), min(st.nx, ii + rr + 1)
+        j0, j1 = max(0, jj - rr), min(st.ny, jj + rr + 1)
+        U = self.U_out.reshape(st.ny, st.nx, 2)[j0:j1, i0:i1].double().cpu().numpy()
+        ro = self.ro_out.reshape(st.ny, st.nx)[j0:j1, i0:i1].double().cpu().numpy()
+        RX, RY = np.meshgrid(np.arange(i0, i1, dtype=float) - ci, np.arange(j0, j1, dtype=float) - cj)
+        m = RX ** 2 + RY ** 2 <= r_lat ** 2
+        sux, suy = np.ascontiguousarray(U[..., 0]), np.ascontiguousarray(U[..., 1])
+        return float(np.sum(RX[m] * ro[m] * suy[m] - RY[m] * ro[m] * sux[m]))
+
     def _sedimentation_step_euler(self, outputs):
-        """Explicit Euler (runtime/scenarios/sedimentation_multi.py:126-190, no
-        rotation): the IB step with the markers and desired velocity the last
-        step left, then velocity and position from this step's force
-        (physics/inertia/{none,explicit_history}.py euler_explicit,
-        physics/rigid_body.py:84-98, feng_b2 post-correction), then the next
-        step's markers and desired velocity."""
+        """Explicit Euler (runtime/scenarios/sedimentation_multi.py:126-190): the
+        IB step with the markers and desired velocity the last step left, then
+        velocity and position from this step's force (physics/inertia/
+        {none,explicit_history}.py euler_explicit, physics/rigid_body.py:84-98,
+        feng_b2 post-correction); with rotation the angular step of
+        rigid_body.py:101-121, whose angular momentum change of the fluid inside
+        each disc needs this step's velocity and density (every step writes
+        them); then the next step's markers and desired velocity."""
         cfg, st = self.cfg, self.st
+        rot = cfg.enable_rotation
+        outputs = outputs or rot
         self._upload_markers()
         self._launch(outputs)
         self.ttt += 1
         if outputs:
             self.last_out_step = self.ttt - 1
-        forces, _ = self.particle_forces()
-        for p, fp in zip(st.particles, forces):
+        forces, torques = self.particle_forces(torques=rot)
+        for k, (p, fp) in enumerate(zip(st.particles, forces)):
+            if rot:
+                l_now = self._l_int_z(p)
+                dl = l_now - p.l_int_prev
+                p.l_int_prev = l_now
+                omega_new = p.omega + (dl + st.dt * torques[k]) / p.I_particle
+                if cfg.sedimentation_euler_update_scheme == "trapezoidal":
+                    p.angle += 0.5 * st.dt * (p.omega + omega_new)
+                else:
+                    p.angle += st.dt * omega_new
+                p.torque = torques[k]
+                p.omega = omega_new
             p.fib_force = fp
             F = fp + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             vel_new = p.vel + st.dt * F / p.mass
@@ -715,10 +743,13 @@ class Engine:
             p.vel = vel_new
             p.pos = pos_new
             p.force = fp
-            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=0.0)
+            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=p.angle if rot else 0.0)
             dv = np.empty((p.Lb, 2))
             dv[:, 0] = float(vel_new[0])
             dv[:, 1] = float(vel_new[1])
+            if rot and p.omega != 0.0:  # U + omega x r, physics/markers.py:41-60
+                dv[:, 0] += -p.omega * (p.Ly - float(pos_new[1])) / st.dx
+                dv[:, 1] += p.omega * (p.Lx - float(pos_new[0])) / st.dx
             p.desired_velocity = dv
 
     def particle_forces(self, torques=False):

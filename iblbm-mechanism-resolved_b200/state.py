@@ -42,6 +42,7 @@ class Particle:
     torque: float = 0.0
     angle: float = 0.0
     omega_half: float = 0.0
+    l_int_prev: float = 0.0  # fluid angular momentum inside the disc at the last Euler step
 
 
 @dataclass

@@ -317,7 +317,7 @@ def init_state(cfg):
                     force=np.zeros(2), mass=mass, rho_ratio=rho_p, lattice_r=lattice_r, r_domain=r,
                     I_particle=0.5 * mass * lattice_r ** 2, Lx_c=plx.copy(), Ly_c=ply.copy(),
                     Lx=plx, Ly=ply, Lb=plb, Larea=pla, desired_velocity=np.zeros((plb, 2)),
-                    cx_init=pcx, cy_init=pcy, omega=0.0, torque=0.0, angle=0.0))
+                    cx_init=pcx, cy_init=pcy, omega=0.0, torque=0.0, angle=0.0, l_int_prev=0.0))
             s.particles = parts
     return s
 
@@ -335,6 +335,20 @@ def _history_dv(model, vel, vel_prev, mass, r_lat):
     if model == "explicit_history":
         return (np.pi * r_lat ** 2 / mass) * (vel - vel_prev)
     return None
+
+
+def _l_int_z(U, ro, nx, ny, dx, cx, cy, r_domain):
+    """Angular momentum of the fluid inside a disc, sum of rx ro uy - ry ro ux over
+    the nodes within r of the centre, lattice units — iblbm/diagnostics/internal_flow.py:220-262."""
+    Eux, Euy, ro2 = U[:, 0].reshape(ny, nx), U[:, 1].reshape(ny, nx), ro.reshape(ny, nx)
+    ci, cj, r_lat = cx / dx, cy / dx, r_domain / dx
+    ii, jj, rr = int(round(ci)), int(round(cj)), int(r_lat) + 2
+    i0, i1 = max(0, ii - rr), min(nx, ii + rr + 1)
+    j0, j1 = max(0, jj - rr), min(ny, jj + rr + 1)
+    RX, RY = np.meshgrid(np.arange(i0, i1, dtype=float) - ci, np.arange(j0, j1, dtype=float) - cj)
+    m = RX ** 2 + RY ** 2 <= r_lat ** 2
+    sro, sux, suy = ro2[j0:j1, i0:i1], Eux[j0:j1, i0:i1], Euy[j0:j1, i0:i1]
+    return float(np.sum(RX[m] * sro[m] * suy[m] - RY[m] * sro[m] * sux[m]))
 
 
 def _update_markers(Lx_c, Ly_c, cx0, cy0, pos, angle=0.0):
@@ -495,13 +509,27 @@ class OracleSim:
             p.vel = vel_new
             p.force = p._fib_force
 
-    # runtime/scenarios/sedimentation_multi.py:126-190 without rotation: explicit Euler
-    # after the IB step (iblbm/physics/inertia/{none,explicit_history}.py euler_explicit,
-    # iblbm/physics/rigid_body.py:84-98 position update, feng_b2 post-correction), then
-    # the markers and desired velocity of the next step
+    # runtime/scenarios/sedimentation_multi.py:126-190: explicit Euler after the IB step
+    # (iblbm/physics/inertia/{none,explicit_history}.py euler_explicit,
+    # iblbm/physics/rigid_body.py:84-98 position update, feng_b2 post-correction); with
+    # rotation the angular step of rigid_body.py:101-121 with the change of the fluid's
+    # angular momentum inside the disc (diagnostics/internal_flow.py:220-262); then the
+    # markers and desired velocity (U + omega x r) of the next step
     def _euler_step(self):
         s, cfg = self.s, self.cfg
+        rot = cfg.enable_rotation
         for p in s.particles:
+            if rot:
+                l_now = _l_int_z(s.U, s.ro, s.nx, s.ny, s.dx, float(p.pos[0]), float(p.pos[1]), p.r_domain)
+                dl = l_now - p.l_int_prev
+                p.l_int_prev = l_now
+                omega_new = p.omega + (dl + s.dt * p._torque_new) / p.I_particle
+                if cfg.sedimentation_euler_update_scheme == "trapezoidal":
+                    p.angle += 0.5 * s.dt * (p.omega + omega_new)
+                else:
+                    p.angle += s.dt * omega_new
+                p.torque = p._torque_new
+                p.omega = omega_new
             F = p._fib_force + _net_gravity(p.rho_ratio, p.lattice_r, s.gravity_lattice, cfg.gravity_direction)
             vel_new = p.vel + s.dt * F / p.mass
             hist = _history_dv(cfg.settling_inertia_model, p.vel, p.vel_prev, p.mass, p.lattice_r)
@@ -517,10 +545,13 @@ class OracleSim:
             p.vel = vel_new
             p.pos = pos_new
             p.force = p._fib_force
-            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=0.0)
+            p.Lx, p.Ly = _update_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=p.angle if rot else 0.0)
             dv = np.empty((p.Lb, 2))
             dv[:, 0] = float(vel_new[0])
             dv[:, 1] = float(vel_new[1])
+            if rot and p.omega != 0.0:
+                dv[:, 0] += -p.omega * (p.Ly - float(pos_new[1])) / s.dx
+                dv[:, 1] += p.omega * (p.Lx - float(pos_new[0])) / s.dx
             p.desired_velocity = dv
 
     def cd_cl(self):

@@ -148,6 +148,18 @@ RUN_CASES = {
                                          mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
                                          marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
                                          check_interval=50),
+    "c5e_sed2_mdf_euler_rot": dict(Re=20, NN=81, xmax=1, ymax=4, cylinder_center=(0.5, 3.0),
+                                   cylinder_D_ratio=0.125, lattice_u=0.05, inflow_u=0.0,
+                                   bc_type="settling_channel", delta_type="hat",
+                                   ibm_method="MDF", collision_model="CM_MRT",
+                                   motion_type="sedimentation", rho_ratio=3.0, gravity=2e-5,
+                                   particles_config=[{"center": (0.5, 3.4375), "rho_ratio": 3.0},
+                                                     {"center": (0.50625, 3.1875), "rho_ratio": 3.0}],
+                                   settling_inertia_model="none", time_integrator="euler_explicit",
+                                   enable_rotation=True,
+                                   mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6,
+                                   marker_spacing_factor=1.0, max_steps=300, use_convergence=False,
+                                   check_interval=50),
     # default boundary family (velocity inlet / pressure outlet / no-slip walls), DF + P4
     "vin_df_bgk_p4": dict(Re=10, NN=81, xmax=2, ymax=1, cylinder_center=(0.5, 0.5),
                           cylinder_D_ratio=0.125, lattice_u=0.05, inflow_u=0.05,
