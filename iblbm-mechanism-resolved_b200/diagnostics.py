@@ -16,7 +16,11 @@ post-processing statistics of the reference's histories and fields restate
 iblbm/diagnostics/core.py: ``tail_start_index`` / ``tail_values`` /
 ``tail_mean`` / ``tail_peak_to_peak_amp`` (:31-51, the last 30 % of a
 series), ``check_convergence`` (:115-136), ``compute_recirculation_length``
-(:264-310) and ``compute_cl_amplitude`` (:312-333).
+(:264-310) and ``compute_cl_amplitude`` (:312-333).  The flow inside a body
+restates iblbm/diagnostics/internal_flow.py: ``compute_inside_residual``
+(:32-85), ``compute_internal_momentum`` (:87-119),
+``compute_internal_angular_momentum`` (:121-154) and ``compute_l_int_z``
+(:220-262).
 """
 from __future__ import annotations
 
@@ -223,3 +227,56 @@ def compute_cl_amplitude(Cl_history):
     if np.all(cl >= -1e-10):
         return float(np.max(half))
     return float((np.max(half) - np.min(half)) / 2.0)
+
+
+def _node_grid(shape, dx, dy):
+    ny, nx = shape
+    return np.meshgrid(np.arange(nx) * dx, np.arange(ny) * dy)
+
+
+def compute_inside_residual(Eux, Euy, dx, dy, cx, cy, D, kappa=2.0, u_ref=0.1):
+    """Speed of the flow left inside a body, over the nodes deeper than kappa dx
+    below its surface: mean, max, count, and mean / max over u_ref (zeros when
+    no node is that deep)."""
+    XX, YY = _node_grid(Eux.shape, dx, dy)
+    inside = np.sqrt((XX - cx) ** 2 + (YY - cy) ** 2) - D / 2.0 < -kappa * dx
+    n = int(np.sum(inside))
+    if n == 0:
+        return {"mean": 0.0, "max": 0.0, "n_points": 0, "mean_normalized": 0.0, "max_normalized": 0.0}
+    speed = np.sqrt(Eux[inside] ** 2 + Euy[inside] ** 2)
+    return {"mean": float(np.mean(speed)), "max": float(np.max(speed)), "n_points": n,
+            "mean_normalized": float(np.mean(speed) / u_ref), "max_normalized": float(np.max(speed) / u_ref)}
+
+
+def compute_internal_momentum(Eux, Euy, ro, dx, dy, cx, cy, r):
+    """Momentum of the fluid inside a disc of radius r: sum of ro u over the
+    nodes within r, times the cell area."""
+    XX, YY = _node_grid(Eux.shape, dx, dy)
+    m = (XX - cx) ** 2 + (YY - cy) ** 2 <= r ** 2
+    dA = dx * dy
+    return float(np.sum(ro[m] * Eux[m]) * dA), float(np.sum(ro[m] * Euy[m]) * dA)
+
+
+def compute_internal_angular_momentum(Eux, Euy, ro, dx, dy, cx, cy, r):
+    """Angular momentum of the fluid inside a disc about its centre:
+    sum of rx ro uy - ry ro ux over the nodes within r, times the cell area."""
+    XX, YY = _node_grid(Eux.shape, dx, dy)
+    m = (XX - cx) ** 2 + (YY - cy) ** 2 <= r ** 2
+    rx, ry = XX[m] - cx, YY[m] - cy
+    return float(np.sum((rx * ro[m] * Euy[m] - ry * ro[m] * Eux[m])) * (dx * dy))
+
+
+def compute_l_int_z(U, ro, nx, ny, dx, cx, cy, r_domain):
+    """The same angular momentum in lattice units, from (N, 2) / (N,) arrays,
+    summed over the box of the disc only."""
+    U, ro = np.asarray(U), np.asarray(ro)
+    ci, cj, r_lat = cx / dx, cy / dx, r_domain / dx
+    ii, jj, rr = int(round(ci)), int(round(cj)), int(r_lat) + 2
+    i0, i1 = max(0, ii - rr), min(nx, ii + rr + 1)
+    j0, j1 = max(0, jj - rr), min(ny, jj + rr + 1)
+    RX, RY = np.meshgrid(np.arange(i0, i1, dtype=float) - ci, np.arange(j0, j1, dtype=float) - cj)
+    m = RX ** 2 + RY ** 2 <= r_lat ** 2
+    sro = ro.reshape(ny, nx)[j0:j1, i0:i1]
+    sux = U[:, 0].reshape(ny, nx)[j0:j1, i0:i1]
+    suy = U[:, 1].reshape(ny, nx)[j0:j1, i0:i1]
+    return float(np.sum(RX[m] * sro[m] * suy[m] - RY[m] * sro[m] * sux[m]))

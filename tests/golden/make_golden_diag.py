@@ -2,7 +2,9 @@
 reference's own functions: iblbm.diagnostics.compute_strouhal on seeded
 synthetic Cl series (signed, and rectified |Cl| on both sides of the aliasing
 threshold), and iblbm.diagnostics.compute_slip_error and
-iblbm.diagnostics.ibm_quality.compute_leakage_flux on a seeded velocity field.
+iblbm.diagnostics.ibm_quality.compute_leakage_flux on a seeded velocity field,
+with the reference's post-processing statistics and internal-flow sums on the
+same series and fields.
 
 Usage:  python tests/golden/make_golden_diag.py --reference /path/to/reference
 """
@@ -27,6 +29,7 @@ def main():
     from iblbm.diagnostics import compute_slip_error, compute_strouhal
     from iblbm.diagnostics.ibm_quality import compute_leakage_flux
     from iblbm.diagnostics import core
+    from iblbm.diagnostics import internal_flow as inf
     rng = np.random.default_rng(11)
     out = {}
     ci, D, u = 50, 20.0, 0.05
@@ -69,6 +72,18 @@ def main():
     xs = np.arange(nx) * dx
     wake = np.tile(np.where((xs > 0.62) & (xs < 0.9), -0.01 * np.sin(np.pi * (xs - 0.62) / 0.28), 0.02), (ny, 1))
     out["recirc_field"] = wake
+    # flow inside a disc at (0.5, 0.5), D = 0.25, on the seeded field
+    ro = 1.0 + 0.01 * rng.standard_normal((ny, nx))
+    out["inside_ro"] = ro
+    res = inf.compute_inside_residual(Eux, Euy, dx, dy, 0.5, 0.5, 0.25, kappa=2.0, u_ref=0.05)
+    out["inside_residual"] = np.array([res["mean"], res["max"], res["n_points"], res["mean_normalized"],
+                                       res["max_normalized"]])
+    out["internal_momentum"] = np.array(inf.compute_internal_momentum(Eux, Euy, ro, dx, dy, 0.5, 0.5, 0.125))
+    out["internal_angular_momentum"] = np.array([inf.compute_internal_angular_momentum(Eux, Euy, ro, dx, dy,
+                                                                                        0.5, 0.5, 0.125)])
+    U = np.stack([Eux.ravel(), Euy.ravel()], axis=1)
+    out["l_int_z"] = np.array([inf.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.5, 0.5, 0.125),
+                               inf.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.02, 0.97, 0.125)])
     out["recirc"] = np.array([core.compute_recirculation_length(wake, dx, dy, 0.5, 0.5, 0.25),
                               core.compute_recirculation_length(np.abs(wake), dx, dy, 0.5, 0.5, 0.25)])
     np.savez_compressed(os.path.join(HERE, "diag.npz"), **out)

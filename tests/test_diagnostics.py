@@ -105,3 +105,26 @@ def test_convergence_and_recirculation_match_reference(diag):
     got = [D.compute_recirculation_length(w, dx, dx, 0.5, 0.5, 0.25),
            D.compute_recirculation_length(np.abs(w), dx, dx, 0.5, 0.5, 0.25)]
     np.testing.assert_array_equal(np.array(got), diag["recirc"])
+
+
+def test_internal_flow_matches_reference(diag):
+    """Residual flow inside the body, and the momentum and angular momentum of
+    the fluid inside a disc (two forms, one clipped at the lattice corner),
+    against the reference's functions on the same fields, bit for bit."""
+    from iblbm_b200 import diagnostics as D
+    NN = 81
+    dx = 1.0 / (NN - 1)
+    Eux, Euy, ro = diag["slip_Eux"], diag["slip_Euy"], diag["inside_ro"]
+    r = D.compute_inside_residual(Eux, Euy, dx, dx, 0.5, 0.5, 0.25, kappa=2.0, u_ref=0.05)
+    got = [r["mean"], r["max"], r["n_points"], r["mean_normalized"], r["max_normalized"]]
+    np.testing.assert_array_equal(np.array(got), diag["inside_residual"])
+    assert D.compute_inside_residual(Eux, Euy, dx, dx, 0.5, 0.5, 0.01)["n_points"] == 0
+    np.testing.assert_array_equal(np.array(D.compute_internal_momentum(Eux, Euy, ro, dx, dx, 0.5, 0.5, 0.125)),
+                                  diag["internal_momentum"])
+    assert D.compute_internal_angular_momentum(Eux, Euy, ro, dx, dx, 0.5, 0.5, 0.125) == \
+        diag["internal_angular_momentum"][0]
+    ny, nx = Eux.shape
+    U = np.stack([Eux.ravel(), Euy.ravel()], axis=1)
+    got = [D.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.5, 0.5, 0.125),
+           D.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.02, 0.97, 0.125)]
+    np.testing.assert_array_equal(np.array(got), diag["l_int_z"])
