@@ -20,7 +20,9 @@ series), ``check_convergence`` (:115-136), ``compute_recirculation_length``
 restates iblbm/diagnostics/internal_flow.py: ``compute_inside_residual``
 (:32-85), ``compute_internal_momentum`` (:87-119),
 ``compute_internal_angular_momentum`` (:121-154) and ``compute_l_int_z``
-(:220-262).
+(:220-262).  ``compute_stress_tensor`` and ``integrate_surface_force`` restate
+iblbm/diagnostics/surface.py:30-163 (force on a cylinder from the stress of
+the non-equilibrium populations).
 """
 from __future__ import annotations
 
@@ -280,3 +282,49 @@ def compute_l_int_z(U, ro, nx, ny, dx, cx, cy, r_domain):
     sux = U[:, 0].reshape(ny, nx)[j0:j1, i0:i1]
     suy = U[:, 1].reshape(ny, nx)[j0:j1, i0:i1]
     return float(np.sum(RX[m] * sro[m] * suy[m] - RY[m] * sro[m] * sux[m]))
+
+
+# D2Q9 velocities in the reference's order (rest, E, N, W, S, NE, NW, SW, SE)
+D2Q9_E = np.array([[0, 0], [1, 0], [0, 1], [-1, 0], [0, -1], [1, 1], [-1, 1], [-1, -1], [1, -1]], dtype=np.float64)
+
+
+def compute_stress_tensor(fstar, feq, ro, tau, lattice, ny, nx):
+    """Cauchy stress (ny, nx, 2, 2) of a D2Q9 state: -(1 - 1/(2 tau)) sum_i
+    (f*_i - feq_i) e_ia e_ib, minus rho / 3 on the diagonal.  lattice: an object
+    with the velocities as .e (9 x 2), or None for D2Q9."""
+    e = D2Q9_E if lattice is None else np.asarray(lattice.e)
+    f_neq = fstar - feq
+    visc = -(1.0 - 1.0 / (2.0 * tau))
+    out = np.zeros((ny, nx, 2, 2))
+    for a in range(2):
+        for b in range(2):
+            out[:, :, a, b] = visc * np.sum(f_neq * (e[:, a] * e[:, b])[None, :], axis=1).reshape(ny, nx)
+    ro2 = ro.reshape(ny, nx)
+    out[:, :, 0, 0] -= (1.0 / 3.0) * ro2
+    out[:, :, 1, 1] -= (1.0 / 3.0) * ro2
+    return out
+
+
+def integrate_surface_force(stress, cx, cy, r, dx, dy, nx, ny, n_points=360):
+    """Force on a cylinder: the traction sigma . n, bilinearly interpolated at
+    n_points equally spaced points of the circle (cell of each point clamped
+    inside the lattice), times the arc length in lattice units, summed point
+    by point in order."""
+    th = np.linspace(0, 2 * np.pi, n_points, endpoint=False)
+    ds = (r / dx) * (2.0 * np.pi / n_points)
+    xi = (cx + r * np.cos(th)) / dx
+    yi = (cy + r * np.sin(th)) / dy
+    i0 = np.clip(np.floor(xi).astype(int), 0, nx - 2)
+    j0 = np.clip(np.floor(yi).astype(int), 0, ny - 2)
+    fx, fy = xi - i0, yi - j0
+    w00, w10, w01, w11 = (1 - fx) * (1 - fy), fx * (1 - fy), (1 - fx) * fy, fx * fy
+    n = (np.cos(th), np.sin(th))
+    F = np.zeros(2)
+    for a in range(2):
+        t = 0.0
+        for b in range(2):
+            s_ab = (w00 * stress[j0, i0, a, b] + w10 * stress[j0, i0 + 1, a, b]
+                    + w01 * stress[j0 + 1, i0, a, b] + w11 * stress[j0 + 1, i0 + 1, a, b])
+            t = t + s_ab * n[b]
+        F[a] = np.cumsum(np.concatenate([[0.0], t * ds]))[-1]
+    return F

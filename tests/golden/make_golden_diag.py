@@ -11,6 +11,7 @@ Usage:  python tests/golden/make_golden_diag.py --reference /path/to/reference
 from __future__ import annotations
 
 import argparse
+import hashlib
 import os
 import sys
 
@@ -30,6 +31,8 @@ def main():
     from iblbm.diagnostics.ibm_quality import compute_leakage_flux
     from iblbm.diagnostics import core
     from iblbm.diagnostics import internal_flow as inf
+    from iblbm.diagnostics import surface
+    from iblbm.lbm import make_d2q9
     rng = np.random.default_rng(11)
     out = {}
     ci, D, u = 50, 20.0, 0.05
@@ -81,6 +84,17 @@ def main():
     out["internal_momentum"] = np.array(inf.compute_internal_momentum(Eux, Euy, ro, dx, dy, 0.5, 0.5, 0.125))
     out["internal_angular_momentum"] = np.array([inf.compute_internal_angular_momentum(Eux, Euy, ro, dx, dy,
                                                                                         0.5, 0.5, 0.125)])
+    # stress of a seeded D2Q9 state and the force it puts on a cylinder (the circle
+    # near the lattice edge exercises the clamped cells)
+    # (populations from their own seed, 12, so the test makes them again instead of loading them)
+    rng12 = np.random.default_rng(12)
+    fst = (1.0 / 9.0) + 0.01 * rng12.standard_normal((nx * ny, 9))
+    feq_s = (1.0 / 9.0) + 0.01 * rng12.standard_normal((nx * ny, 9))
+    sig = surface.compute_stress_tensor(fst, feq_s, ro.ravel(), 0.8, make_d2q9(), ny, nx)
+    out["stress_sha"] = np.frombuffer(hashlib.sha256(np.ascontiguousarray(sig).tobytes()).digest(), dtype=np.uint8)
+    out["stress_sample"] = sig.reshape(-1, 4)[::97]
+    out["surface_force"] = np.stack([surface.integrate_surface_force(sig, 0.5, 0.5, 0.125, dx, dy, nx, ny),
+                                     surface.integrate_surface_force(sig, 0.05, 0.5, 0.125, dx, dy, nx, ny, 100)])
     U = np.stack([Eux.ravel(), Euy.ravel()], axis=1)
     out["l_int_z"] = np.array([inf.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.5, 0.5, 0.125),
                                inf.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.02, 0.97, 0.125)])

@@ -128,3 +128,24 @@ def test_internal_flow_matches_reference(diag):
     got = [D.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.5, 0.5, 0.125),
            D.compute_l_int_z(U, ro.ravel(), nx, ny, dx, 0.02, 0.97, 0.125)]
     np.testing.assert_array_equal(np.array(got), diag["l_int_z"])
+
+
+def test_surface_stress_force_matches_reference(diag):
+    """Stress of a seeded D2Q9 state and the force it puts on a cylinder (one
+    circle inside the lattice, one clamped at its edge), against the reference's
+    surface functions, bit for bit."""
+    import hashlib
+    from iblbm_b200 import diagnostics as D
+    NN = 81
+    dx = 1.0 / (NN - 1)
+    ro = diag["inside_ro"]
+    ny, nx = ro.shape
+    rng = np.random.default_rng(12)
+    fst = (1.0 / 9.0) + 0.01 * rng.standard_normal((nx * ny, 9))
+    feq = (1.0 / 9.0) + 0.01 * rng.standard_normal((nx * ny, 9))
+    sig = D.compute_stress_tensor(fst, feq, ro.ravel(), 0.8, None, ny, nx)
+    np.testing.assert_array_equal(sig.reshape(-1, 4)[::97], diag["stress_sample"])
+    assert hashlib.sha256(np.ascontiguousarray(sig).tobytes()).digest() == bytes(diag["stress_sha"])
+    got = np.stack([D.integrate_surface_force(sig, 0.5, 0.5, 0.125, dx, dx, nx, ny),
+                    D.integrate_surface_force(sig, 0.05, 0.5, 0.125, dx, dx, nx, ny, 100)])
+    np.testing.assert_array_equal(got, diag["surface_force"])
