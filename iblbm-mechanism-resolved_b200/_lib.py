@@ -57,7 +57,7 @@ class IbmArgs(ctypes.Structure):
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
                 ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i),
-                ("dvel_scale", _vp)]
+                ("dvel_scale", _vp), ("dfc_rho_f", _d)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee

@@ -1209,10 +1209,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 sh.bwx[b] = wt;  // W_total
             }
             __syncthreads();
+            const R rho_f = a.dfc_rho_f > 0.0 ? (R)a.dfc_rho_f : (R)1;
             for (int l = tid; l < Lb; l += IBM_THREADS) {
                 R ws, dummy;
                 interp2<A>(sh, sh.bwx, sh.bwx, l, ws, dummy);
-                a.lambda[l] = (R)1 / ((R)2 * (R)1 * La * ws);
+                a.lambda[l] = (R)1 / ((R)2 * rho_f * La * ws);
             }
             __syncthreads();
             if (tid == 0 && a.dfc_cache_lambda && a.lambda_valid) *a.lambda_valid = 1;

@@ -219,7 +219,9 @@ extern "C" int iblbm_dense_step_f32_batch(const iblbm_dense32_args* a, int n, vo
     else if (a0.tile == IBLBM_TILE_ROWS2) nr = 2;
     else if (a0.tile == IBLBM_TILE_ROWS4) nr = 4;
     else return IBLBM_E_ARG;
-    static BatchTable t;  // host staging of the parameter block (calls are serialised by the caller)
+    // the parameter block is built on this call's stack and copied into the
+    // launch, so concurrent calls from several host threads do not interfere
+    BatchTable t;
     t.n = n;
     t.off[0] = 0;
     bool mixed = false;

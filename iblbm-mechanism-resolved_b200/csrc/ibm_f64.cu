@@ -3,6 +3,8 @@
 // The kernel itself is band_kernel.cuh instantiated with R = double; this unit
 // is compiled without multiply-add contraction, so every sum runs in the
 // reference's order and results are bit-identical to the reference CPU path.
+#include <atomic>
+#include <mutex>
 #include "band_kernel.cuh"
 
 namespace iblbm {
@@ -66,7 +68,10 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 // the GPU race on it: issue them on one stream, or order them.  The first call
 // on each device looks up the array's device address (cudaGetSymbolAddress) with
 // that device current; make that first call before any stream capture.  The
-// caller still passes every input, output and persistent band array.
+// address is kept per device ordinal for the life of the process, which
+// assumes the device's primary context does too: after cudaDeviceReset, make
+// no further call into this entry point on that device.  The caller still
+// passes every input, output and persistent band array.
 // ---------------------------------------------------------------------------
 namespace iblbm {
 constexpr int NOALLOC_MAX_BAND = MAX_BAND;  // the band kernel's own limit (2048)
@@ -74,8 +79,31 @@ constexpr int NOALLOC_MAX_MARKERS = 1024;
 constexpr int NOALLOC_MAX_DEVICES = 64;
 static __device__ __align__(256) double g_noalloc_scratch[9 * NOALLOC_MAX_BAND + 9 * NOALLOC_MAX_MARKERS];
 static __device__ __align__(256) int g_noalloc_iscratch[NOALLOC_MAX_BAND];
-static void* g_noalloc_scratch_ptr[NOALLOC_MAX_DEVICES];
-static void* g_noalloc_iscratch_ptr[NOALLOC_MAX_DEVICES];
+// Device addresses of the two arrays, resolved once per device.  A thread that
+// finds no entry resolves both under the lock and publishes the pair with one
+// release store, so a reader that sees the pair sees both addresses.
+struct NoallocPtrs {
+    double* scratch;
+    int* iscratch;
+};
+static NoallocPtrs g_noalloc_store[NOALLOC_MAX_DEVICES];
+static std::atomic<const NoallocPtrs*> g_noalloc_ptrs[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_lock;
+
+static const NoallocPtrs* noalloc_ptrs(int dev)
+{
+    const NoallocPtrs* p = g_noalloc_ptrs[dev].load(std::memory_order_acquire);
+    if (p) return p;
+    std::lock_guard<std::mutex> hold(g_noalloc_lock);
+    p = g_noalloc_ptrs[dev].load(std::memory_order_relaxed);
+    if (p) return p;
+    void *s = nullptr, *q = nullptr;
+    if (cudaGetSymbolAddress(&s, g_noalloc_scratch) != cudaSuccess) return nullptr;
+    if (cudaGetSymbolAddress(&q, g_noalloc_iscratch) != cudaSuccess) return nullptr;
+    g_noalloc_store[dev] = NoallocPtrs{static_cast<double*>(s), static_cast<int*>(q)};
+    g_noalloc_ptrs[dev].store(&g_noalloc_store[dev], std::memory_order_release);
+    return &g_noalloc_store[dev];
+}
 }  // namespace iblbm
 
 extern "C" int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args* a, void* stream)
@@ -85,15 +113,10 @@ extern "C" int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args* a, void* stream)
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return IBLBM_E_LAUNCH;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return IBLBM_E_ARG;
-    if (!g_noalloc_scratch_ptr[dev]) {
-        void *p = nullptr, *q = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return IBLBM_E_LAUNCH;
-        if (cudaGetSymbolAddress(&q, g_noalloc_iscratch) != cudaSuccess) return IBLBM_E_LAUNCH;
-        g_noalloc_iscratch_ptr[dev] = q;
-        g_noalloc_scratch_ptr[dev] = p;
-    }
+    const NoallocPtrs* p = noalloc_ptrs(dev);
+    if (!p) return IBLBM_E_LAUNCH;
     iblbm_ibm_args b = *a;
-    b.scratch = static_cast<double*>(g_noalloc_scratch_ptr[dev]);
-    b.iscratch = static_cast<int*>(g_noalloc_iscratch_ptr[dev]);
+    b.scratch = p->scratch;
+    b.iscratch = p->iscratch;
     return iblbm_ibm_step_f64(&b, stream);
 }

@@ -103,7 +103,7 @@ _DELTA_STENCIL_A = {"peskin4pt": 2, "hat": 1}
 
 
 def _band_call(method, Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_type, incompressible,
-               ro=None, ux=None, uy=None, ustride=1, fstar=None, lambda_k=None):
+               ro=None, ux=None, uy=None, ustride=1, fstar=None, lambda_k=None, rho_f=1.0):
     """One band-kernel launch on caller-given fields (iblbm_ibm_step_f64 with
     field_*): returns the band's node list and outputs."""
     import numpy as np
@@ -141,6 +141,7 @@ def _band_call(method, Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_typ
     a.moff, a.Lx, a.Ly, a.dvel, a.larea = (ptr(x) for x in (keep["moff"], Lx, Ly, dv, keep["larea"]))
     a.dx, a.dy = float(dx), float(dy)
     a.lambda_, a.lambda_valid = ptr(keep["lam"]), ptr(keep["valid"])
+    a.dfc_rho_f = float(rho_f)
     if lambda_k is not None:
         keep["valid"].fill_(1)
         a.dfc_cache_lambda = 1
@@ -195,13 +196,15 @@ def ibm_direct_forcing_fields_gpu(Lx, Ly, desired_vel, Eux, Euy, Ro, dx, dy, dt,
 
 def compute_lambda_gpu(Lx, Ly, rho_f, Larea, dx, dy, ny, nx, delta_type):
     """DFC lambda(k) = 1 / (2 rho_f ds W_sum(k)) — replaces gpu_kernels.py:1091-1141
-    (<- ibm/dfc.py:126-186).  Bit-identical to the reference for rho_f = 1 (the
-    solver's value); other rho_f divide the rho_f = 1 result."""
+    (<- ibm/dfc.py:126-186), bit-identical to the reference for every fluid
+    density rho_f > 0 (the band kernel evaluates ((2 rho_f) ds) W_sum as the
+    reference does).  rho_f <= 0 has no physical meaning and raises ValueError."""
+    if not float(rho_f) > 0.0:
+        raise ValueError(f"rho_f={rho_f!r}: the fluid density must be positive")
     torch = _t()
     fz = torch.zeros(ny * nx * 9, dtype=torch.float64, device=_dev(Lx, "Lx").device)
-    k = _band_call("DFC", Lx, Ly, None, dx, dy, 1.0, Larea, ny, nx, delta_type, False, fstar=fz)
-    lam = k["lam"][: Lx.numel()].clone()
-    return lam if float(rho_f) == 1.0 else lam / float(rho_f)
+    k = _band_call("DFC", Lx, Ly, None, dx, dy, 1.0, Larea, ny, nx, delta_type, False, fstar=fz, rho_f=rho_f)
+    return k["lam"][: Lx.numel()].clone()
 
 
 def dfc_correction_gpu(Lx, Ly, desired_vel, fstar, lambda_k, dx, dy, Larea, ny, nx, delta_type, lattice=None):

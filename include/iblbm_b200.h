@@ -170,6 +170,9 @@ typedef struct {
     /* NULL, or a device scalar scaling every desired velocity this step
      * (dvel * (*dvel_scale); the Taylor-Green markers' analytic decay) */
     const double *dvel_scale;
+    /* DFC: fluid density rho_f of lambda(k) = 1 / (2 rho_f ds W_sum(k))
+     * (iblbm/ibm/dfc.py:126-186); 0 means 1.0, the solver's value */
+    double dfc_rho_f;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -191,7 +194,9 @@ int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
  * Limits: band_capacity <= 2048, lb_total <= 1024, else IBLBM_E_CAPACITY.
  * Calls share that array, so calls that overlap on the GPU race; the first
  * call on a device resolves the array's address and should precede any stream
- * capture.  Allocates nothing. */
+ * capture.  The address is kept for the life of the process (it assumes the
+ * device's primary context lives as long: no call after cudaDeviceReset).
+ * Allocates nothing. */
 int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args *a, void *stream);
 int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
 int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
@@ -252,8 +257,8 @@ int iblbm_dense_step_f32(const iblbm_dense32_args *a, void *stream);
  * (ibm = IBLBM_IBM_NONE, no only_box) may mix kinds: each CTA then dispatches
  * on its case's collision, closure and compressibility.  The Taylor-Green
  * closure (IBLBM_BC_TG) is not batched.  Tile NODE, ROWS2 or ROWS4 (taken
- * from a[0]); no ro/U/fstar outputs.  Calls must not run concurrently on the
- * host (the parameter block is staged in one static buffer). */
+ * from a[0]); no ro/U/fstar outputs.  Host threads may call it concurrently
+ * (the parameter block is built per call). */
 int iblbm_dense_step_f32_batch(const iblbm_dense32_args *a, int n, void *stream);
 /* f (FP64 AoS, the reference's f[N, 9]) -> g = f - w (FP32 SoA), and back. */
 int iblbm_to_shifted_f32(const double *aos, iblbm_geom g, float *soa, void *stream);
@@ -296,6 +301,7 @@ typedef struct {
     const float *field_ro, *field_ux, *field_uy, *field_fstar;
     int field_ustride;
     const double *dvel_scale;
+    double dfc_rho_f;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,

@@ -6,8 +6,10 @@ checkout given by ``--reference`` and run on small inputs.  The fixtures pin the
 CPU oracle in ``oracle/`` (tests/test_oracle_golden.py) and, through it, the CUDA
 product path.
 
-Two kinds of fixture are written:
+Three kinds of fixture are written:
 
+* ``lambda_rho.npz`` — the reference's DFC lambda(k) for fluid densities 1.3
+  and 0.7 on the marker inputs of units.npz;
 * ``units.npz``   — seeded random inputs and the reference's outputs for every
   kernel on the hot path (feq, macroscopic, BGK/TRT/CM-MRT collision, streaming,
   the four boundary closures, velocity correction, DF, MDF, DFC lambda and
@@ -351,6 +353,19 @@ def make_units(out):
     np.savez_compressed(out, **d)
 
 
+def make_lambda_rho(units_path, out):
+    """lambda(k) of the reference's compute_lambda for fluid densities other
+    than 1, on the marker inputs stored in units.npz."""
+    from iblbm.ibm.dfc import compute_lambda
+    u = np.load(units_path)
+    nx, ny, dx, La = int(u["i_nx"][0]), int(u["i_ny"][0]), float(u["i_dx"][0]), float(u["i_Larea"][0])
+    d = {}
+    for dt_name in ("hat", "peskin4pt"):
+        for rho_f in (1.3, 0.7):
+            d[f"lam_{dt_name}_{rho_f}"] = compute_lambda(u["i_Lx"], u["i_Ly"], rho_f, La, dx, dx, ny, nx, dt_name)
+    np.savez_compressed(out, **d)
+
+
 def make_run(name, kw, out_dir):
     from iblbm import SimConfig, run
     cfg = SimConfig(**kw)
@@ -379,13 +394,18 @@ def make_run(name, kw, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("IBLBM_REFERENCE"),
+                    required="IBLBM_REFERENCE" not in os.environ,
+                    help="reference checkout (or set IBLBM_REFERENCE)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     _import_reference(args.reference)
     if args.only in (None, "units"):
         make_units(os.path.join(HERE, "units.npz"))
         print("units.npz written")
+    if args.only in (None, "units", "lambda_rho"):
+        make_lambda_rho(os.path.join(HERE, "units.npz"), os.path.join(HERE, "lambda_rho.npz"))
+        print("lambda_rho.npz written")
     for name, kw in RUN_CASES.items():
         if args.only not in (None, name):
             continue

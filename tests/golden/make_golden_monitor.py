@@ -66,7 +66,9 @@ def sequence(kind):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", required=True)
+    ap.add_argument("--reference", default=os.environ.get("IBLBM_REFERENCE"),
+                    required="IBLBM_REFERENCE" not in os.environ,
+                    help="reference checkout (or set IBLBM_REFERENCE)")
     args = ap.parse_args()
     os.environ["IBLBM_GPU"] = "0"
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/iblbm_numba_cache")

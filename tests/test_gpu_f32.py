@@ -203,15 +203,22 @@ def test_f32_rotating_sedimentation(torch, name):
         assert abs(p.omega - q.omega) <= 1e-3 * abs(q.omega)
 
 
-@pytest.mark.parametrize("name", ["c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap"])
+@pytest.mark.parametrize("name", ["c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap",
+                                  "c5e_sed2_mdf_euler_rot"])
 def test_f32_euler_sedimentation(torch, name):
     """Explicit Euler integration of two settling discs: the FP32 form's
-    positions within 1e-4 lattice units of the FP64 form's."""
+    positions within 1e-4 lattice units of the FP64 form's; with rotation (the
+    fluid's angular momentum inside each disc read from the FP32 fields) its
+    angles and angular velocities within 1e-3 of their FP64 magnitudes."""
     cfg = _cfg(RUN_CASES[name])
     r64, r32 = _pair(cfg)
     for p, q in zip(r32["state"].particles, r64["state"].particles):
         dxl = (np.asarray(p.pos) - np.asarray(q.pos)) / r64["state"].dx
         assert np.max(np.abs(dxl)) <= 1e-4
+        if cfg.enable_rotation:
+            print(f"{name}: angle {p.angle:.6e} / {q.angle:.6e}, omega {p.omega:.6e} / {q.omega:.6e}")
+            assert abs(p.angle - q.angle) <= 1e-3 * abs(q.angle)
+            assert abs(p.omega - q.omega) <= 1e-3 * abs(q.omega)
 
 
 def test_f32_config1_geometry_long(torch):

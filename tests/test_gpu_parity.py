@@ -72,6 +72,10 @@ def test_reference_shaped_ibm_wrappers(torch, units, delta):
     np.testing.assert_array_equal(Efx.cpu().numpy().ravel(), u[f"df_{delta}_0_fib"][:, 0])
     lam = gk.compute_lambda_gpu(Lx, Ly, 1.0, La, dx, dx, ny, nx, delta)
     np.testing.assert_array_equal(lam.cpu().numpy(), u[f"lam_{delta}"])
+    lr = np.load(os.path.join(GOLD, "lambda_rho.npz"))
+    for rho_f in (1.3, 0.7):  # lambda(k) = 1 / (2 rho_f ds W_sum), the reference's own outputs
+        lam_r = gk.compute_lambda_gpu(Lx, Ly, rho_f, La, dx, dx, ny, nx, delta)
+        np.testing.assert_array_equal(lam_r.cpu().numpy(), lr[f"lam_{delta}_{rho_f}"])
     fstar = d(u[f"dfc_{delta}_fstar"])
     corr, force = gk.dfc_correction_gpu(Lx, Ly, dv, fstar, lam, dx, dx, La, ny, nx, delta)
     np.testing.assert_array_equal((fstar + corr).cpu().numpy(), u[f"dfc_{delta}_fc"])

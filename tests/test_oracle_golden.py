@@ -87,6 +87,10 @@ def test_ibm_kernels(units, delta):
     assert st["iter_count"] == int(ref[0]) and st["last_residual"] == ref[1]
     lam = H.dfc_lambda(Lx, Ly, La, dx, dx, ny, nx, delta)
     np.testing.assert_array_equal(lam, u[f"lam_{delta}"])
+    lr = np.load(os.path.join(GOLD, "lambda_rho.npz"))
+    for rho_f in (1.3, 0.7):
+        np.testing.assert_array_equal(H.dfc_lambda(Lx, Ly, La, dx, dx, ny, nx, delta, rho_f=rho_f),
+                                      lr[f"lam_{delta}_{rho_f}"])
     fc, force = H.dfc_correction(Lx, Ly, dv, u[f"dfc_{delta}_fstar"], lam, dx, dx, La, ny, nx, delta)
     np.testing.assert_array_equal(fc, u[f"dfc_{delta}_fc"])
     np.testing.assert_allclose(force, u[f"dfc_{delta}_force"], rtol=1e-14, atol=1e-18)
