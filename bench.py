@@ -3,49 +3,59 @@
 
 Two forms of the hot path are timed on one GPU:
 
-plain   the FP64 form (the reference's arithmetic, bit for bit) on the
-        reference's single-case benchmark: fixed cylinder at Re = 100 on a
-        1601 x 641 D2Q9 lattice, D = 40, 126 Lagrangian markers, inflow
-        u = 0.04, TRT (magic Lambda = 3/16), multi-direct forcing with the
-        Peskin 4-point kernel (5 to 20 iterations until the slip residual
-        < 1e-6), Dirichlet/Neumann channel.  One step = the band kernel (all MDF
-        iterations) and the fused collide-stream pass; L2 flushed between steps.
+plain   the FP64 form (the reference's arithmetic, bit for bit).
 chosen  the FP32 shifted-population form (FP64 force sums and MDF residual
-        norm) run batched: the 72-case sweep Re {20, 40, 100, 200} x
-        {DF, MDF, DFC} x {hat, Peskin-4} x {BGK, TRT, CM-MRT} of fixed cylinders
-        on 401x161 to 1921x961 lattices, all cases stepped together (one
-        batched band launch, one collide-stream launch per kind of case).  The
-        same workload as the plain form is also timed in the FP32 form, one
-        case alone (chosen_single_case).
+        norm) run batched.
+
+Workloads:
+
+sweep   the 72-case sweep Re {20, 40, 100, 200} x {DF, MDF, DFC} x {hat,
+        Peskin-4} x {BGK, TRT, CM-MRT} of fixed cylinders on 401x161 to
+        1921x961 lattices, all cases stepped together (one batched band
+        launch, box passes, one collide-stream launch per collision model).
+        Timed in both forms: `value` is the chosen form, `plain_sweep` the
+        FP64 form on the same workload (the reference arm's workload), so the
+        GPU/CPU ratio exists at equal precision.  `sweep` compares the two
+        forms' Cd / Cl tail statistics after the configuration's 50 000 steps.
+C2      the reference's single-case benchmark: fixed cylinder at Re = 100 on a
+        1601 x 641 lattice, D = 40, 126 markers, TRT (Lambda = 3/16), MDF with
+        Peskin-4 (5 to 20 iterations to a 1e-6 slip residual); `plain` (FP64)
+        and `chosen_single_case` (FP32), L2 evicted between steps.
+C3      oscillating cylinder, Re 100, KC 5, 1281 x 1281, DFC + Peskin-4, BGK,
+        open boundary (`config3`, both forms).
+C5      two settling discs, 321 x 1281, coupled MDF + Peskin-4, CM-MRT,
+        Velocity-Verlet (`config5`, both forms).
 
 Reported (one JSON line on rank 0):
-  value       aggregate MLUPS of the chosen form (device time, CUDA events);
-              plain.mlups is the plain form's.
+  value       aggregate MLUPS of the chosen form on the sweep (device time,
+              CUDA events, at least one second of timed steps); `windows` has
+              the median and spread of 20-step windows.
   e2e         the same through the public API with host buffers: every step
               uploads all cases' markers from pinned host memory and reads all
-              marker forces back.
+              marker forces back (at least one second).
   roofline    the collide-stream launches of a step against the measured HBM
               copy bandwidth: 72 algorithmic bytes per lattice update in FP32
               (9 populations read + 9 written), 144 in FP64.
-  sweep       Cd/Cl of every batched case against the FP64 plain form of the
-              same case after the same steps (target: within 0.1 %).
   cpu_baseline  the CPU oracle (a C + OpenMP restatement of the reference's
-              CPU path) on a bounded sample of the single-case workload.
+              CPU path) on a bounded sample of the sweep, in a fresh process.
 
-Inputs are deterministic initial states (no dataset).  --form plain times the
-plain form alone.  --impl reference times the CPU restatement of the
-reference's own path (the reference is a Python package whose CPU path cannot
-travel to the GPU box).  Multi-GPU: cases do not shard; N ranks run N
-independent replicas (weak scaling), timed as the max over ranks.
+Inputs are deterministic initial states (no dataset).  --impl reference times
+the CPU restatement of the reference's own path (the reference is a Python
+package whose CPU path cannot travel to the GPU box).  Multi-GPU: the sweep's
+cases are partitioned over the ranks by estimated cost (no collective on the
+data path; results gathered on the host), so total work is fixed (strong
+scaling); the single-case workloads run as replicas.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
+import statistics
 import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -63,6 +73,9 @@ BYTES_PER_LU_F32 = 72
 TRAFFIC_PER_NODE_F32 = (71.63e6 + 28.31e6) / 1930092
 TRAFFIC_PER_NODE_F64 = (73.81e6 + 25.93e6) / 1023949
 METRIC = "MLUPS and HBM GB/s (1 B200), chosen vs plain form at Cd within 0.1% of FP64"
+MIN_TIMED_S = 1.0     # every headline number rests on at least this much device time
+CPU_PER_CASE = 4      # timed oracle steps per sweep case (both arms)
+SWEEP_STEPS = 50_000  # configuration 4: steps per case
 
 
 def workload_config(collision="TRT", max_steps=1_000_000):
@@ -71,6 +84,32 @@ def workload_config(collision="TRT", max_steps=1_000_000):
                      lattice_u=0.04, inflow_u=0.04, bc_type="dirichlet_neumann", delta_type="peskin4pt",
                      ibm_method="MDF", collision_model=collision, trt_magic_param=0.1875, mdf_iterations=20,
                      mdf_min_iterations=5, mdf_tolerance=1e-6, marker_spacing_factor=1.0, max_steps=max_steps,
+                     use_convergence=False, check_interval=100)
+
+
+def config3(max_steps=100_000, method="DFC"):
+    """Oscillating cylinder, Re 100, KC 5: D = 40 on 1281 x 1281, x_c = -A sin(2 pi t / T),
+    T = KC D / U = 10 000 steps, DFC + Peskin-4, BGK, open boundary (scenarios/oscillating.py:12-44)."""
+    from iblbm_b200 import SimConfig
+    return SimConfig(Re=100, NN=1281, xmax=1, ymax=1, cylinder_center=(0.5, 0.5), cylinder_D_ratio=0.03125,
+                     lattice_u=0.02, inflow_u=0.0, bc_type="open_boundary", delta_type="peskin4pt",
+                     ibm_method=method, collision_model="BGK", motion_type="oscillating", KC=5.0,
+                     nx_formula="simple", marker_spacing_factor=1.0, mdf_iterations=20, mdf_min_iterations=5,
+                     mdf_tolerance=1e-6, max_steps=max_steps, use_convergence=False, check_interval=100)
+
+
+def config5(max_steps=300_000, rho_ratio=1.5):
+    """Two settling discs (drafting, kissing, tumbling): D = 40 in a 321 x 1281 walled channel,
+    centres (160, 1100) and (162, 1020) lattice units, coupled MDF + Peskin-4, CM-MRT,
+    Velocity-Verlet (runtime/scenarios/sedimentation_multi.py:199-323)."""
+    from iblbm_b200 import SimConfig
+    return SimConfig(Re=20, NN=321, xmax=1, ymax=4, cylinder_center=(0.5, 3.4375), cylinder_D_ratio=0.125,
+                     lattice_u=0.05, inflow_u=0.0, bc_type="settling_channel", delta_type="peskin4pt",
+                     ibm_method="MDF", collision_model="CM_MRT", motion_type="sedimentation",
+                     rho_ratio=rho_ratio, gravity=1e-5,
+                     particles_config=[{"center": (0.5, 1100 / 320), "rho_ratio": rho_ratio},
+                                       {"center": (0.5 + 2 / 320, 1020 / 320), "rho_ratio": rho_ratio}],
+                     settling_inertia_model="explicit_history", marker_spacing_factor=1.0, max_steps=max_steps,
                      use_convergence=False, check_interval=100)
 
 
@@ -91,51 +130,72 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled during a timed region: a thread
+    runs one read-only nvidia-smi query every 200 ms (each query's output is
+    complete when it exits, so no sample is lost to buffering) for this
+    process's GPU, selected by UUID."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
-        self.index = index
-        self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
+        self.sel = str(index)
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(index).uuid)
+            if u:
+                self.sel = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
+        self.rows, self.err = [], None
+        self._stop = threading.Event()
+        self._t = None
+
+    def _query(self):
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", self.sel, f"--query-gpu={self.Q}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=10)
+        except Exception as exc:  # no nvidia-smi on this host
+            self.err = type(exc).__name__
+            return
+        for line in out.stdout.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+        if out.returncode != 0 and not self.rows:
+            self.err = (out.stderr.strip() or f"rc {out.returncode}")[:120]
+
+    def _run(self):
+        while not self._stop.is_set():
+            self._query()
+            if self.err and not self.rows:
+                return
+            self._stop.wait(0.2)
 
     def __enter__(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
-                                      stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
         return self
 
     def __exit__(self, *exc):
-        if self.p is not None:
-            self.p.terminate()
-            try:
-                self.p.wait(timeout=5)
-            except Exception:
-                self.p.kill()
+        self._stop.set()
+        if self._t is not None:
+            self._t.join(timeout=15)
 
     def summary(self):
-        self.fh.flush()
-        rows = []
-        with open(self.fh.name) as fh:
-            for line in fh:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.fh.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        import statistics
-        mhz = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(mhz) if mhz else None,
-                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": reasons, "samples": len(rows)}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "error": self.err}
+        mhz = [v for v in (num(r[0]) for r in self.rows) if v is not None]
+        reasons = sorted({n for r in self.rows for n, v in zip(self.NAMES, r[3:7]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": num(self.rows[0][1]),
+                "power_w_max": max((num(r[2]) or 0.0) for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows), "gpu": self.sel}
 
 
 def _dist():
@@ -151,7 +211,7 @@ def _dist():
         cuda = torch.cuda.is_available()
         if cuda:
             torch.cuda.set_device(local)
-        dist.init_process_group("nccl" if cuda else "gloo", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl" if cuda else "gloo", timeout=datetime.timedelta(seconds=300))
         return dist, int(os.environ.get("RANK", "0")), ws, local
     return None, 0, 1, 0
 
@@ -167,6 +227,7 @@ def max_over_ranks(x, dist, device="cuda"):
     return float(t.item())
 
 
+# ---- CPU baseline -------------------------------------------------------------------
 def oracle_sweep_sample(per_case, threads=None):
     """The CPU oracle on the sweep: every case in turn (one in memory at a time),
     one warm-up step and `per_case` timed steps each, so the mix of lattices and
@@ -190,35 +251,26 @@ def oracle_sweep_sample(per_case, threads=None):
                                           f"warm-up step each ({dt:.1f} s timed)"}
 
 
-def cpu_baseline(seconds=20.0, threads=None):
-    """Time the CPU oracle on a bounded sample of the workload (whole timesteps)."""
-    threads = threads or os.cpu_count()
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    from oracle import harness as H
-    sim = H.OracleSim(workload_config())
-    sim.step()  # warm-up (first touch, library load)
-    n, t0 = 0, time.perf_counter()
-    while True:
-        sim.step()
-        n += 1
-        dt = time.perf_counter() - t0
-        if dt > seconds or n >= 400:
-            break
-    N = sim.s.nx * sim.s.ny
-    return {"value": N * n / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": f"{n} timesteps of the workload after 1 warm-up step ({dt:.1f} s)"}
+def cpu_baseline_subprocess(per_case=CPU_PER_CASE):
+    """oracle_sweep_sample in a fresh interpreter (no CUDA context, no torch
+    thread pool beside the oracle's OpenMP threads), as the reference arm runs."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--cpu-sample", str(per_case)],
+                         capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(f"CPU baseline failed: {out.stderr[-400:]}")
+    return json.loads(out.stdout.strip().splitlines()[-1])
 
 
 def run_reference(args):
     dist, rank, ws, _ = _dist()
     if rank != 0:
         return
-    per_case = max(1, min(args.steps, 2))
-    base = oracle_sweep_sample(per_case)
+    base = oracle_sweep_sample(CPU_PER_CASE)
     v, dt, threads, cfgs = base["value"], base["timed_s"], base["cores"], base["cases"]
-    line = {"metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": per_case,
-            "warmup": 1, "ms_per_step": dt / per_case * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic initial state)",
+    line = {"metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus, "steps": CPU_PER_CASE,
+            "warmup": 1, "ms_per_step": dt / CPU_PER_CASE * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (deterministic initial state)",
             "config": {"workload": SWEEP_WORKLOAD, "cases": cfgs, "form": "reference CPU path (C + OpenMP "
                        "restatement of the reference's numba/numpy path), FP64"}, "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "port", "sample": base["sample"]},
@@ -226,6 +278,7 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# ---- single case ---------------------------------------------------------------------
 def _flushed_steps_graph(eng, K, flush, sink):
     """K overlapped steps of one engine, each followed by a 256 MB read that evicts
     the populations from L2, captured as one CUDA graph so that the host's launch
@@ -254,13 +307,35 @@ def _flushed_steps_graph(eng, K, flush, sink):
     return g, ev
 
 
+def _timed_flushed(eng, K, flush, sink, clk=None):
+    """Per-step times (ms) of at least K overlapped steps and at least
+    MIN_TIMED_S of device time: a flushed graph of up to 100 steps replayed as
+    often as needed.  Returns (step_ms list, bulk_ms list, wall seconds)."""
+    import torch
+    Kg = min(max(K, 1), 100)
+    graph, ev = _flushed_steps_graph(eng, Kg, flush, sink)
+    graph.replay()  # first replay uploads the graph
+    eng.parity ^= Kg & 1
+    eng.ttt += Kg
+    torch.cuda.synchronize()
+    step_ms, dense_ms = [], []
+    t_wall = time.perf_counter()
+    while len(step_ms) < K or sum(step_ms) < MIN_TIMED_S * 1e3:
+        graph.replay()
+        eng.parity ^= Kg & 1
+        eng.ttt += Kg
+        torch.cuda.synchronize()
+        step_ms += [ev[k][0].elapsed_time(ev[k][3]) for k in range(Kg)]
+        dense_ms += [ev[k][1].elapsed_time(ev[k][2]) for k in range(Kg)]
+    return step_ms, dense_ms, time.perf_counter() - t_wall
+
+
 def measure(eng, args, dist, ws):
-    """Time one engine on the workload: per-step (L2 flushed) overlapped steps,
-    the band kernel alone, graph-replayed steady state and the host-buffer e2e
-    loop.  Returns a dict of the numbers (all ranks)."""
+    """Time one fixed-body engine: per-step (L2 flushed) overlapped steps, the
+    band kernel alone, graph-replayed steady state and the host-buffer e2e loop.
+    Returns a dict of the numbers (all ranks)."""
     import torch
     N = eng.N
-    # warm-up: graph chunks and eager steps; tile choice of the FP32 pass
     eng.advance(max(args.warmup, 3), outputs_last=True)
     torch.cuda.synchronize()
     from iblbm_b200.autotune import tune_dense
@@ -269,22 +344,14 @@ def measure(eng, args, dist, ws):
     torch.cuda.synchronize()
     flush = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     sink = torch.zeros((), dtype=torch.float32, device="cuda")
-    K = args.steps
     E = lambda: torch.cuda.Event(enable_timing=True)
     excl = eng.d_excl[eng.parity].tolist()
     box_nodes = excl[2] * excl[3]
-    graph, ev = _flushed_steps_graph(eng, K, flush, sink)
     if dist:
         dist.barrier()
-    torch.cuda.synchronize()
     with Clocks(torch.cuda.current_device()) as clk:
-        t_wall = time.perf_counter()
-        graph.replay()
-        torch.cuda.synchronize()
-        t_wall = time.perf_counter() - t_wall
-    eng.parity ^= K & 1
-    step_ms = [ev[k][0].elapsed_time(ev[k][3]) for k in range(K)]
-    dense_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
+        step_ms, dense_ms, t_wall = _timed_flushed(eng, args.steps, flush, sink)
+    K = len(step_ms)
     tot_ms = max_over_ranks(sum(step_ms), dist)
     dense_avg = sum(dense_ms) / K
     bpl = BYTES_PER_LU_F32 if eng.f32 else BYTES_PER_LU_F64
@@ -294,29 +361,28 @@ def measure(eng, args, dist, ws):
     for k in range(8):
         eng._step_serial(False, events=sev[k])
         eng.fence()
+    eng.ttt += 8
     torch.cuda.synchronize()
     ibm_ms = sum(sev[k][0].elapsed_time(sev[k][1]) for k in range(8)) / 8
     full_ms = sum(sev[k][1].elapsed_time(sev[k][2]) for k in range(8)) / 8
 
     # steady state: CUDA-graph replay, no flush (L2-warm; reported, not the headline)
-    torch.cuda.synchronize()
     e0, e1 = E(), E()
-    eng.advance(K, outputs_last=False)  # capture
+    eng.advance(200, outputs_last=False)  # capture
     torch.cuda.synchronize()
     e0.record()
-    eng.advance(K, outputs_last=False)
+    eng.advance(200, outputs_last=False)
     e1.record()
     torch.cuda.synchronize()
-    steady = N * K / (e0.elapsed_time(e1) / 1e3) / 1e6
+    steady = N * 200 / (e0.elapsed_time(e1) / 1e3) / 1e6
 
-    # end to end through the engine with host buffers
+    # end to end through the engine with host buffers, at least MIN_TIMED_S
     Lb = eng.Lb
     host_in = torch.empty(4 * Lb, dtype=torch.float64).pin_memory()
     host_in[:Lb] = torch.as_tensor(eng.st.Lx)
     host_in[Lb:2 * Lb] = torch.as_tensor(eng.st.Ly)
     host_in[2 * Lb:] = torch.as_tensor(eng.st.desired_velocity.reshape(-1))
     host_out = torch.empty(2, dtype=torch.float64).pin_memory()
-    Ke = max(10, K // 2)
     # a host program one step ahead, two pinned buffer pairs alternating (as for the batch)
     ins = [host_in, torch.empty_like(host_in).pin_memory()]
     ins[1].copy_(host_in)
@@ -324,6 +390,7 @@ def measure(eng, args, dist, ws):
     for k in range(2):  # capture the two (parity, buffer) graphs
         eng.step_io(ins[k], outs[k])
     torch.cuda.synchronize()
+    Ke = max(10, int(math.ceil(MIN_TIMED_S * 1e3 / (sum(step_ms) / K))))
     t0 = time.perf_counter()
     prev = None
     for k in range(Ke):
@@ -333,26 +400,26 @@ def measure(eng, args, dist, ws):
         prev = ev
     prev.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)  # the slowest rank
-    # one output step so both forms can be compared at the same step
     eng.advance(1, outputs_last=True)
     torch.cuda.synchronize()
     cd, cl = eng.cd_cl()
-    return {"value": N * K * ws / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "dense_ms": dense_avg,
+    return {"value": N * K * ws / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "steps": K, "dense_ms": dense_avg,
             "box_nodes": box_nodes, "bytes_per_lu": bpl,
             "achieved": bpl * (N - box_nodes) / (dense_avg / 1e3) / 1e9, "band_ms": ibm_ms, "full_ms": full_ms,
-            "steady": steady, "e2e": N * Ke * ws / e2e_s / 1e6, "e2e_h2d": 4 * Lb * 8, "e2e_d2h": 16,
-            "clocks": clk.summary(), "wall_s_timed": t_wall, "status": eng.status(), "mdf": eng.mdf_stats(),
-            "cd": cd, "cl": cl, "steps_done": eng.ttt - 1,
+            "steady": steady, "e2e": N * Ke * ws / e2e_s / 1e6, "e2e_steps": Ke, "e2e_s": e2e_s,
+            "e2e_h2d": 4 * Lb * 8, "e2e_d2h": 16, "clocks": clk.summary(), "wall_s_timed": t_wall,
+            "status": eng.status(), "mdf": eng.mdf_stats(), "cd": cd, "cl": cl, "steps_done": eng.ttt - 1,
             "tile": tile, "tile_ms": tile_ms}
 
 
-# Batched sweep: fixed cylinders, Re x band method x delta kernel x collision
-# model on uneven lattices (Re -> NN, xmax, D/(NN-1), inflow u).
+# ---- the sweep -------------------------------------------------------------------------
+# Fixed cylinders, Re x band method x delta kernel x collision model on uneven
+# lattices (Re -> NN, xmax, D/(NN-1), inflow u).
 SWEEP_SIZES = {20: (161, 2.5, 0.125, 0.05), 40: (321, 2.5, 0.1, 0.05), 100: (641, 2.5, 0.0625, 0.04),
                200: (961, 2.0, 0.05, 0.04)}
 
 
-SWEEP_WORKLOAD = ("chosen form: batched sweep of 72 fixed-cylinder cases, Re {20,40,100,200} x {DF,MDF,DFC} x "
+SWEEP_WORKLOAD = ("batched sweep of 72 fixed-cylinder cases, Re {20,40,100,200} x {DF,MDF,DFC} x "
                   "{hat,P4} x {BGK,TRT,CM-MRT} on 401x161 (D=20), 801x321 (D=32), 1601x641 (D=40), 1921x961 "
                   "(D=48) lattices")
 
@@ -373,18 +440,14 @@ def sweep_configs(max_steps):
     return out
 
 
-def measure_batch(b, K, W, dist, ws):
-    """Time the batched sweep: per-group tile tuning, K overlapped steps (every
-    step streams the whole sweep, ~4 GB, far above L2), graph-replayed steady
-    state, and the host-buffer loop (all markers in, all marker forces out)."""
+def _tune_batch(b):
+    """Tile of each bulk group of an FP32 batch (the bulk pass is side-effect
+    free when repeated without a parity flip), and whether one merged bulk
+    launch over every case beats the per-group launches."""
     import torch
     E = lambda: torch.cuda.Event(enable_timing=True)
-    b.advance(max(W, 3), outputs_last=False)
-    torch.cuda.synchronize()
-    # tile choice per bulk group (cases of one collision, closure and compressibility):
-    # the bulk pass is side-effect free when repeated without a parity flip
-    tiles = {}
     main = torch.cuda.current_stream()
+    tiles = {}
     for g in range(len(b.bulk_groups)):
         best = None
         for tile in ("node", "rows2", "rows4"):
@@ -401,7 +464,6 @@ def measure_batch(b, K, W, dist, ws):
                 best = (tile, ms)
         b.set_bulk_tile(g, best[0])
         tiles[g] = best
-    # one bulk launch over every case against one launch per group
     per_group_ms = sum(ms for _, ms in tiles.values())
     merged = {}
     if b.C <= 72 and len(b.bulk_groups) > 1:
@@ -417,10 +479,36 @@ def measure_batch(b, K, W, dist, ws):
             merged[tile] = min(e0.elapsed_time(e1) for e0, e1 in ev)
         best_tile = min(merged, key=merged.get)
         # in the timed schedule the single launch also competes with the band and
-        # box kernels of the side stream, which slip in between per-group launches:
-        # take it only on a clear win in isolation
+        # box kernels of the side stream: take it only on a clear win in isolation
         b.set_tile_all(best_tile, merged=merged[best_tile] < 0.95 * per_group_ms)
     b.fence()
+    return tiles, merged, per_group_ms
+
+
+def measure_batch(b, K, W, dist, n_total):
+    """Time a batch: at least K overlapped steps and MIN_TIMED_S of device time
+    (every step streams the whole sweep, several GB, far above L2, so no flush),
+    per-step events around the bulk passes, graph-replayed steady state, and
+    the host-buffer loop (all markers in, all marker forces out) for at least
+    MIN_TIMED_S.  `n_total`: lattice nodes per step over all ranks."""
+    import torch
+    E = lambda: torch.cuda.Event(enable_timing=True)
+    b.advance(max(W, 3), outputs_last=False)
+    torch.cuda.synchronize()
+    tiles, merged, per_group_ms = _tune_batch(b) if b.f32 else ({}, {}, None)
+    main = torch.cuda.current_stream()
+    # a probe of 10 steps sizes the timed region
+    b._step()
+    b.join()
+    e0, e1 = E(), E()
+    e0.record(main)
+    for _ in range(10):
+        b._step()
+    b.join()
+    e1.record(main)
+    torch.cuda.synchronize()
+    b._bump(11)
+    K = max(K, int(math.ceil(MIN_TIMED_S * 1e3 / (e0.elapsed_time(e1) / 10))))
     ev = [[E() for _ in range(4)] for _ in range(K)]
     if dist:
         dist.barrier()
@@ -435,26 +523,28 @@ def measure_batch(b, K, W, dist, ws):
         torch.cuda.synchronize()
         t_wall = time.perf_counter() - t_wall
     b._bump(K)
-    tot_ms = sum(ev[k][0].elapsed_time(ev[k][3]) for k in range(K))
+    step_ms = [ev[k][0].elapsed_time(ev[k][3]) for k in range(K)]
     bulk_ms = sum(ev[k][1].elapsed_time(ev[k][2]) for k in range(K)) / K
-    tot_ms = max_over_ranks(tot_ms, dist)
+    tot_ms = max_over_ranks(sum(step_ms), dist)
+    win = [sum(step_ms[s:s + 20]) for s in range(0, K - 19, 20)]
+    win_mlups = sorted(b.N * 20 / (w / 1e3) / 1e6 for w in win)
     box_nodes = sum(int(x[2]) * int(x[3]) for e in b.engines for x in [e.d_excl[b.parity].tolist()])
-    achieved = BYTES_PER_LU_F32 * (b.N - box_nodes) / (bulk_ms / 1e3) / 1e9
-    # steady state through one captured graph
-    e0, e1 = E(), E()
-    b.advance(K, outputs_last=False)
+    bpl = BYTES_PER_LU_F32 if b.f32 else BYTES_PER_LU_F64
+    achieved = bpl * (b.N - box_nodes) / (bulk_ms / 1e3) / 1e9
+    # steady state through one captured graph of 200 steps
+    b.advance(200, outputs_last=False)
     torch.cuda.synchronize()
     e0.record()
-    b.advance(K, outputs_last=False)
+    b.advance(200, outputs_last=False)
     e1.record()
     torch.cuda.synchronize()
-    steady = b.N * K / (e0.elapsed_time(e1) / 1e3) / 1e6
+    steady = b.N * 200 / (e0.elapsed_time(e1) / 1e3) / 1e6
     # host buffers: every step uploads all cases' markers and reads all marker forces back
     nin = b.marker_in.numel()
     host_in = torch.empty(nin, dtype=torch.float64).pin_memory()
     host_in.copy_(b.marker_in.cpu())
     host_out = torch.empty(b.marker_out.numel(), dtype=torch.float64).pin_memory()
-    Ke = max(10, K // 2)
+    Ke = max(10, int(math.ceil(MIN_TIMED_S * 1e3 / (sum(step_ms) / K))))
     # a host program one step ahead: step k runs while the host reads step k-1's
     # forces; two pinned buffer pairs alternate (each step still copies all its
     # markers in and all its forces out)
@@ -464,29 +554,182 @@ def measure_batch(b, K, W, dist, ws):
     for k in range(2):  # capture the two (parity, buffer) graphs
         b.step_io(ins[k], outs[k])
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     prev = None
     for k in range(Ke):
-        ev = b.step_io(ins[k % 2], outs[k % 2], wait=False)
+        evk = b.step_io(ins[k % 2], outs[k % 2], wait=False)
         if prev is not None:
             prev.synchronize()  # the previous step's forces are in outs[(k - 1) % 2]
-        prev = ev
+        prev = evk
     prev.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist)  # the slowest rank
     b.advance(1, outputs_last=True)
     torch.cuda.synchronize()
-    return {"value": b.N * K * ws / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "bulk_ms": bulk_ms,
-            "achieved": achieved, "box_nodes": box_nodes, "steady": steady,
-            "e2e": b.N * Ke * ws / e2e_s / 1e6, "h2d": nin * 8, "d2h": host_out.numel() * 8,
-            "clocks": clk.summary(), "wall_s_timed": t_wall, "status": b.status(),
+    return {"value": n_total * K / (tot_ms / 1e3) / 1e6, "ms_per_step": tot_ms / K, "steps": K, "bulk_ms": bulk_ms,
+            "achieved": achieved, "box_nodes": box_nodes, "steady": steady, "bytes_per_lu": bpl,
+            "windows": {"size_steps": 20, "count": len(win_mlups), "median_mlups": statistics.median(win_mlups),
+                        "min_mlups": win_mlups[0], "max_mlups": win_mlups[-1]},
+            "e2e": n_total * Ke / e2e_s / 1e6, "e2e_steps": Ke, "e2e_s": e2e_s, "h2d": nin * 8,
+            "d2h": host_out.numel() * 8, "clocks": clk.summary(), "wall_s_timed": t_wall, "status": b.status(),
             "tiles": {str(g): {"tile": t, "bulk_ms": ms, "cases": len(b.bulk_groups[g])}
                       for g, (t, ms) in tiles.items()},
             "bulk_one_launch_ms": merged, "bulk_per_group_ms_sum": per_group_ms, "bulk_merged": b.merged,
-            "tile_merged": b.tile_all,
             "launches_per_step": 1 + len(b.kinds) + (1 if b.merged else len(b.bulk_groups)),
             "steps_done": b.engines[0].ttt - 1}
 
 
+def sweep_accuracy(b32, b64, steps, every=500, tail=0.2):
+    """Both forms of every case of the batch advanced to `steps` (the
+    configuration's step count), Cd / Cl sampled every `every` steps; per case
+    the FP32 form's error against the FP64 form (oracle-exact) in the tail
+    statistics over the last `tail` of the run (mean Cd, mean Cl, Cl standard
+    deviation, largest pointwise Cd difference), at the last step, and for DF /
+    MDF the interpolated marker velocities (so the slip) at the last step.
+    Returns {local case index: dict}."""
+    import torch
+    import numpy as np
+    done = [b.engines[0].ttt - 1 for b in (b32, b64)]
+    first = (max(done) // every + 1) * every
+    targets = list(range(first, steps + 1, every))
+    if not targets or targets[-1] != steps:
+        targets.append(steps)
+    hist = {"f32": [[] for _ in b32.engines], "f64": [[] for _ in b64.engines]}
+    for t in targets:
+        for name, b in (("f32", b32), ("f64", b64)):
+            b.advance(t - (b.engines[0].ttt - 1), outputs_last=True)
+            torch.cuda.synchronize()
+            for k, e in enumerate(b.engines):
+                hist[name][k].append((t,) + e.cd_cl())
+    out = {}
+    t_tail = steps - tail * steps
+    for k, (e32, e64) in enumerate(zip(b32.engines, b64.engines)):
+        h32, h64 = np.array(hist["f32"][k]), np.array(hist["f64"][k])
+        m = h64[:, 0] >= t_tail
+        cd32, cd64, cl32, cl64 = h32[m, 1], h64[m, 1], h32[m, 2], h64[m, 2]
+        ref = abs(float(np.mean(cd64)))
+        r = {"cd_tail_mean_f64": float(np.mean(cd64)), "cl_tail_std_f64": float(np.std(cl64)),
+             "cd_tail_mean_rel_err": abs(float(np.mean(cd32) - np.mean(cd64))) / ref,
+             "cl_tail_mean_err_rel_cd": abs(float(np.mean(cl32) - np.mean(cl64))) / ref,
+             "cl_tail_std_err_rel_cd": abs(float(np.std(cl32) - np.std(cl64))) / ref,
+             "cd_tail_max_pointwise_rel_err": float(np.max(np.abs(cd32 - cd64))) / ref,
+             "cd_last_rel_err": abs(float(h32[-1, 1] - h64[-1, 1])) / abs(float(h64[-1, 1])),
+             "finite": bool(np.all(np.isfinite(h32[:, 1:])) and np.all(np.isfinite(h64[:, 1:]))),
+             "samples_tail": int(m.sum()), "case": [e64.cfg.Re, e64.cfg.ibm_method, e64.cfg.delta_type,
+                                                    e64.cfg.collision_model]}
+        if e64.method in ("DF", "MDF"):
+            u = float(e64.cfg.inflow_u)
+            du = max((getattr(e32, a)[: e32.Lb] - getattr(e64, a)[: e64.Lb]).abs().max().item()
+                     for a in ("d_Lux", "d_Luy"))
+            r["marker_velocity_err_rel_u"] = du / u
+        out[k] = r
+    return out
+
+
+def _accuracy_summary(acc):
+    keys = ["cd_tail_mean_rel_err", "cl_tail_mean_err_rel_cd", "cl_tail_std_err_rel_cd",
+            "cd_tail_max_pointwise_rel_err", "cd_last_rel_err", "marker_velocity_err_rel_u"]
+    s = {}
+    for key in keys:
+        vals = [(r[key], k) for k, r in acc.items() if key in r]
+        if vals:
+            v, k = max(vals)
+            s["max_" + key] = v
+            s["worst_case_" + key] = acc[k]["case"]
+    s["cases_not_finite"] = [acc[k]["case"] for k, r in acc.items() if not r["finite"]]
+    s["cases_within_0p1pct_tail_cd"] = sum(r["cd_tail_mean_rel_err"] <= 1e-3 for r in acc.values())
+    s["cases"] = len(acc)
+    return s
+
+
+# ---- configurations 3 and 5 ----------------------------------------------------------
+def measure_case(cfg_fn, precision, K, W, flush, sink, e2e_steps):
+    """One moving-body case in one form: device MLUPS over at least MIN_TIMED_S
+    (L2 evicted between steps when the step can be graph-captured, i.e. the
+    markers move on the device; otherwise eager steps, each with the host
+    Newton-Euler update, wall-clock), the bulk pass's HBM rate, and e2e through
+    the public run() with its per-check host outputs."""
+    import torch
+    from iblbm_b200 import run
+    from iblbm_b200.autotune import tune_dense
+    from iblbm_b200.engine import Engine
+    E = lambda: torch.cuda.Event(enable_timing=True)
+    eng = Engine(cfg_fn(max_steps=1_000_000), precision=precision)
+    N = eng.N
+    host_step = eng.st.particles is not None and not eng.dev_particles
+    eng.advance(max(W, 3), outputs_last=True)
+    torch.cuda.synchronize()
+    tile_ms, tile = tune_dense(eng)
+    eng.advance(2, outputs_last=False)
+    torch.cuda.synchronize()
+    bpl = BYTES_PER_LU_F32 if eng.f32 else BYTES_PER_LU_F64
+    out = {"form": "FP32 shifted" if eng.f32 else "FP64 plain", "lattice_nodes": N, "bytes_per_lu": bpl,
+           "tile": tile}
+    if not host_step:
+        step_ms, dense_ms, _ = _timed_flushed(eng, K, flush, sink)
+        n = len(step_ms)
+        excl = eng.d_excl[eng.parity].tolist()
+        dense = sum(dense_ms) / n
+        out.update({"mlups": N * n / (sum(step_ms) / 1e3) / 1e6, "ms_per_step": sum(step_ms) / n, "steps": n,
+                    "bulk_kernel_ms": dense, "hbm_gbs_bulk": bpl * (N - excl[2] * excl[3]) / (dense / 1e3) / 1e9,
+                    "timing": "device, one CUDA graph of overlapped steps, L2 evicted between steps"})
+    else:
+        ev = [(E(), E()) for _ in range(50)]
+        for e0, e1 in ev:  # probe
+            e0.record()
+            eng._sedimentation_step(False)
+            e1.record()
+        torch.cuda.synchronize()
+        per = sum(a.elapsed_time(b) for a, b in ev) / len(ev)
+        n = max(K, int(math.ceil(MIN_TIMED_S * 1e3 / per)))
+        t0 = time.perf_counter()
+        for _ in range(n):
+            eng._sedimentation_step(False)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out.update({"mlups": N * n / wall / 1e6, "ms_per_step": wall / n * 1e3, "steps": n,
+                    "timing": "wall clock of eager steps: every step waits for the band kernel's particle "
+                              "forces on the host (host Newton-Euler, the FP64 form's default)"})
+    # serial step breakdown: band kernel, then the whole lattice
+    sev = [[E() for _ in range(3)] for _ in range(8)]
+    if not host_step:
+        for k in range(8):
+            eng._step_serial(False, events=sev[k])
+            eng.fence()
+        eng.ttt += 8
+        torch.cuda.synchronize()
+        out["band_kernel_ms"] = sum(sev[k][0].elapsed_time(sev[k][1]) for k in range(8)) / 8
+        out["whole_lattice_kernel_ms_serial"] = sum(sev[k][1].elapsed_time(sev[k][2]) for k in range(8)) / 8
+    out["status"] = eng.status()
+    del eng
+    # end to end: the public run() on a fresh engine (its first run captures the graphs, the second is timed)
+    cfg = cfg_fn(max_steps=e2e_steps)
+    eng = Engine(cfg_fn(max_steps=2 * e2e_steps + 16), precision=precision)
+    run(cfg, verbose=False, engine=eng)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = run(cfg, verbose=False, engine=eng)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    nb = int(eng.d_count.item())
+    ci = int(cfg.check_interval)
+    if eng.st.particles is not None:
+        h2d = 0 if eng.dev_particles else eng.Lb * 4 * 8  # markers + desired velocities of every step
+        d2h = (96 * eng.P / ci) if eng.dev_particles else (nb * 4 + eng.P * nb * 2 * (4 if eng.f32 else 8))
+    else:
+        h2d, d2h = 0, 24 / ci  # the markers move on the device; Cd / Cl read at every check
+    out["e2e"] = {"value": N * e2e_steps / wall / 1e6, "unit": "MLUPS", "steps": e2e_steps, "seconds": wall,
+                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                  "how": "iblbm_b200.run(cfg) (the public API) with its per-check host outputs, graphs captured by "
+                         "a first run on the same engine"}
+    out["final_step"] = res["final_step"]
+    del eng
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---- learned warm start -------------------------------------------------------------------
 def measure_learned(args, n_train=200, K=200):
     """The learned MDF warm start on the single-case workload (FP32 form).
 
@@ -497,7 +740,6 @@ def measure_learned(args, n_train=200, K=200):
     below the level plain MDF reached in 20 iterations (median over the last
     50 training steps).  Reports both forms' step rate, mean iterations and
     residual, and Cd against the FP64 form at the same step."""
-    import statistics
     import torch
     from iblbm_b200.autotune import tune_dense
     from iblbm_b200.engine import Engine
@@ -557,129 +799,126 @@ def measure_learned(args, n_train=200, K=200):
     return out
 
 
-def sweep_cd_check(cfgs, batch, steps):
-    """Cd/Cl of every batched case against the FP64 plain form of the same case
-    after the same number of steps (one case at a time), and for DF / MDF cases
-    the interpolated marker velocities (so the marker slip) over U."""
-    import torch
-    from iblbm_b200.engine import Engine
-    worst_cd, worst_cl, worst_u, rows = 0.0, 0.0, 0.0, []
-    for cfg, eb in zip(cfgs, batch.engines):
-        e = Engine(cfg, precision="f64")
-        e.advance(steps, outputs_last=True)
-        torch.cuda.synchronize()
-        cd64, cl64 = e.cd_cl()
-        cd32, cl32 = eb.cd_cl()
-        rc = abs(cd32 - cd64) / abs(cd64)
-        rl = abs(cl32 - cl64) / abs(cd64)
-        worst_cd, worst_cl = max(worst_cd, rc), max(worst_cl, rl)
-        if cfg.ibm_method in ("DF", "MDF"):
-            for k in ("d_Lux", "d_Luy"):
-                du = (getattr(eb, k)[: eb.Lb] - getattr(e, k)[: e.Lb]).abs().max().item()
-                worst_u = max(worst_u, du / cfg.inflow_u)
-        rows.append((cfg.Re, cfg.ibm_method, cfg.delta_type, cfg.collision_model, cd64, rc))
-        del e
-    torch.cuda.empty_cache()
-    return worst_cd, worst_cl, worst_u, rows
-
-
+# ---- the run ---------------------------------------------------------------------------------
 def run_b200(args):
     import torch
     dist, rank, ws, local = _dist()
     torch.cuda.set_device(local)
-    from iblbm_b200.batch import Batch
+    from iblbm_b200.batch import Batch, gather_case_results, partition_cases
     from iblbm_b200.engine import Engine
-    cfg = workload_config(max_steps=args.warmup + 4 * args.steps + 16)
+    from iblbm_b200.state import grid_shape
     peak, peak_kind = _peaks()
+    flush = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    sink = torch.zeros((), dtype=torch.float32, device="cuda")
+
+    # single case, configuration 2 (replicas)
+    cfg = workload_config(max_steps=10_000_000)
     plain = measure(Engine(cfg, precision="f64"), args, dist, ws)
     single = measure(Engine(cfg, precision="f32"), args, dist, ws)
-    bres, sweep = None, None
-    if args.form == "chosen":
-        Kb = max(20, args.steps)
-        cfgs = sweep_configs(max_steps=args.warmup + 4 * Kb + 16)
-        batch = Batch(cfgs)
-        bres = measure_batch(batch, Kb, args.warmup, dist, ws)
-        worst_cd, worst_cl, worst_u, rows = sweep_cd_check(cfgs, batch, bres["steps_done"])
-        sweep = {"cases": len(cfgs), "lattice_nodes": batch.N, "max_cd_rel_err_vs_f64": worst_cd,
-                 "max_cl_err_vs_f64_rel_cd": worst_cl, "max_marker_velocity_err_vs_f64_rel_u": worst_u,
-                 "worst_case": max(rows, key=lambda r: r[5])[:4]}
-        del batch
-    learned = measure_learned(args) if args.form == "chosen" else None
+    torch.cuda.empty_cache()
+
+    # the sweep, this rank's share of its cases
+    acc_steps = args.accuracy_steps
+    cfgs_all = sweep_configs(max_steps=max(acc_steps, 1) + 400_000)
+    mine = partition_cases(cfgs_all, ws)[rank]
+    n_total = sum(grid_shape(c)[0] * grid_shape(c)[1] for c in cfgs_all)
+    cfgs = [cfgs_all[k] for k in mine]
+    b32 = Batch(cfgs, precision="f32")
+    bres = measure_batch(b32, args.steps, args.warmup, dist, n_total)
+    b64 = Batch(cfgs, precision="f64")
+    pres = measure_batch(b64, args.steps, args.warmup, dist, n_total)
+    acc = {}
+    if acc_steps > 0:
+        acc_local = sweep_accuracy(b32, b64, acc_steps)
+        acc = gather_case_results({mine[k]: v for k, v in acc_local.items()}, dist)
+    nodes_local = b32.N
+    del b32, b64
+    torch.cuda.empty_cache()
+
+    # configurations 3 and 5, both forms (replicas)
+    c35 = {}
+    if not args.skip_c35:
+        for name, fn in (("config3", config3), ("config5", config5)):
+            c35[name] = {p: measure_case(fn, p, args.steps, args.warmup, flush, sink, args.e2e_case_steps)
+                         for p in ("f64", "f32")}
+            f64, f32 = c35[name]["f64"], c35[name]["f32"]
+            c35[name]["chosen_vs_plain"] = f32["mlups"] / f64["mlups"]
+            for f in (f64, f32):
+                if "hbm_gbs_bulk" in f:
+                    f["roofline_frac_bulk"] = f["hbm_gbs_bulk"] / peak
+    learned = measure_learned(args) if args.form == "chosen" and not args.skip_learned else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
-    N = 1601 * 641
-    cpu = None
-    if ws == 1:  # the oracle on a bounded sample of the line's own workload
-        if bres:
-            cpu = {k: v for k, v in oracle_sweep_sample(2).items() if k not in ("timed_s", "cases")}
-        else:
-            cpu = cpu_baseline(seconds=float(os.environ.get("IBLBM_CPU_SECONDS", "20")))
+    cpu = cpu_baseline_subprocess() if ws == 1 else None
 
     def summary(m):
-        return {"mlups": m["value"], "ms_per_step": m["ms_per_step"], "bulk_kernel_ms": m["dense_ms"],
-                "hbm_gbs_bulk": m["achieved"], "bytes_per_lu": m["bytes_per_lu"], "band_kernel_ms": m["band_ms"],
-                "whole_lattice_kernel_ms_serial": m["full_ms"], "steady_state_mlups_graph_l2_warm": m["steady"],
-                "e2e_mlups": m["e2e"], "mdf_last_iterations": m["mdf"]["iter_count"], "status": m["status"],
-                "Cd": m["cd"], "Cl": m["cl"], "step": m["steps_done"], "tile": m["tile"],
-                "tile_ms_whole_lattice": m["tile_ms"]}
+        return {"mlups": m["value"], "ms_per_step": m["ms_per_step"], "steps_timed": m["steps"],
+                "bulk_kernel_ms": m["dense_ms"], "hbm_gbs_bulk": m["achieved"], "bytes_per_lu": m["bytes_per_lu"],
+                "band_kernel_ms": m["band_ms"], "whole_lattice_kernel_ms_serial": m["full_ms"],
+                "steady_state_mlups_graph_l2_warm": m["steady"], "e2e_mlups": m["e2e"], "e2e_steps": m["e2e_steps"],
+                "mdf_last_iterations": m["mdf"]["iter_count"], "status": m["status"], "Cd": m["cd"], "Cl": m["cl"],
+                "step": m["steps_done"], "tile": m["tile"], "tile_ms_whole_lattice": m["tile_ms"],
+                "roofline_frac_bulk": m["achieved"] / peak, "clocks": m["clocks"]}
 
-    line = {"metric": METRIC, "unit": "MLUPS", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    line = {"metric": METRIC, "unit": "MLUPS", "n_gpus": ws, "steps": bres["steps"], "steps_requested": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "data": "synthetic (deterministic initial states of the workloads)"}
     single_s = summary(single)
     single_s["cd_rel_err_vs_f64"] = abs(single["cd"] - plain["cd"]) / abs(plain["cd"])
     single_s["cl_err_vs_f64_rel_cd"] = abs(single["cl"] - plain["cl"]) / abs(plain["cd"])
-    if bres:
-        line.update({
-            "value": bres["value"], "ms_per_step": bres["ms_per_step"], "dtype": "f32",
-            "config": {"workload": SWEEP_WORKLOAD + ", FP32 shifted populations with FP64 force sums; plain form: "
-                                   + WORKLOAD["workload"] + ", FP64",
-                       "cases": sweep["cases"], "lattice_nodes_per_step": bres and sweep["lattice_nodes"],
-                       "l2": "per-step traffic ~4 GB (inputs far larger than L2), no flush",
-                       "parallelism": f"replicas x{ws}"},
-            "steps_batch": max(20, args.steps),
-            "schedule": "one batched band launch + box passes (side stream) concurrent with one bulk launch per "
-                        "collision model (cases of every band method together); CUDA graph between outputs",
-            "roofline": {"bound": "hbm", "achieved": bres["achieved"], "peak": peak, "unit": "GB/s",
-                         "frac": bres["achieved"] / peak,
-                         "traffic": TRAFFIC_PER_NODE_F32 * (sweep["lattice_nodes"] - bres["box_nodes"]),
-                         "traffic_unit": "bytes per step (all bulk launches), scaled from an ncu capture of the "
-                                         "36-case part of the sweep", "peak_kind": peak_kind,
-                         "kernel": "dense32_batch_kernel bulk passes of all groups (fused pull-stream+BC+macro+"
-                                   "collide, FP32 shifted)", "bytes_per_lu": BYTES_PER_LU_F32,
-                         "lattice_updates_per_step": bres and (sweep["lattice_nodes"] - bres["box_nodes"])},
-            "e2e": {"value": bres["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": bres["h2d"],
-                    "d2h_bytes_per_step": bres["d2h"]},
-            "gpu_launches": bres["launches_per_step"] * max(20, args.steps),
-            "clocks": bres["clocks"], "wall_s_timed": bres["wall_s_timed"],
-            "chosen_vs_plain": bres["value"] / plain["value"],
-            "sweep": dict(sweep, steady_state_mlups_graph=bres["steady"], status_nonzero=[
-                k for k, st in enumerate(bres["status"]) if st], tiles=bres["tiles"],
-                bulk_ms_per_step=bres["bulk_ms"], bulk_one_launch_ms=bres["bulk_one_launch_ms"],
-                bulk_per_group_ms_sum=bres["bulk_per_group_ms_sum"], bulk_merged=bres["bulk_merged"],
-                tile_merged=bres["tile_merged"])})
-    else:
-        line.update({"value": plain["value"], "ms_per_step": plain["ms_per_step"], "dtype": "f64",
-                     "config": dict(WORKLOAD, form="FP64 plain", parallelism=f"replicas x{ws}"),
-                     "roofline": {"bound": "hbm", "achieved": plain["achieved"], "peak": peak, "unit": "GB/s",
-                                  "frac": plain["achieved"] / peak,
-                                  "traffic": TRAFFIC_PER_NODE_F64 * (N - plain["box_nodes"]),
-                                  "peak_kind": peak_kind,
-                                  "kernel": "dense_step_kernel bulk pass (FP64)", "bytes_per_lu": BYTES_PER_LU_F64,
-                                  "lattice_updates_per_launch": N - plain["box_nodes"]},
-                     "e2e": {"value": plain["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": plain["e2e_h2d"],
-                             "d2h_bytes_per_step": plain["e2e_d2h"]},
-                     "gpu_launches": 3 * args.steps, "clocks": plain["clocks"],
-                     "wall_s_timed": plain["wall_s_timed"]})
+    line.update({
+        "value": bres["value"], "ms_per_step": bres["ms_per_step"], "dtype": "f32",
+        "config": {"workload": "chosen form: " + SWEEP_WORKLOAD + ", FP32 shifted populations with FP64 force sums",
+                   "cases": len(cfgs_all), "lattice_nodes_per_step": n_total,
+                   "l2": "per-step traffic ~4 GB (inputs far larger than L2), no flush",
+                   "parallelism": f"cases partitioned over {ws} rank(s) by bytes x steps"},
+        "windows": bres["windows"],
+        "schedule": "one batched band launch + box passes (side stream) concurrent with one bulk launch per "
+                    "collision model (cases of every band method together); eager launches in the timed region, "
+                    "CUDA graphs between outputs otherwise",
+        "roofline": {"bound": "hbm", "achieved": bres["achieved"], "peak": peak, "unit": "GB/s",
+                     "frac": bres["achieved"] / peak,
+                     "traffic": TRAFFIC_PER_NODE_F32 * (nodes_local - bres["box_nodes"]),
+                     "traffic_unit": "bytes per step (all bulk launches), scaled from an ncu capture of the "
+                                     "36-case part of the sweep; writes leaving L2 after a launch are not counted",
+                     "peak_kind": peak_kind,
+                     "kernel": "dense32_batch_kernel bulk passes of all groups (fused pull-stream+BC+macro+"
+                               "collide, FP32 shifted)", "bytes_per_lu": BYTES_PER_LU_F32,
+                     "lattice_updates_per_step": nodes_local - bres["box_nodes"]},
+        "e2e": {"value": bres["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": bres["h2d"],
+                "d2h_bytes_per_step": bres["d2h"], "steps": bres["e2e_steps"], "seconds": bres["e2e_s"]},
+        "gpu_launches": bres["launches_per_step"] * bres["steps"],
+        "clocks": bres["clocks"], "wall_s_timed": bres["wall_s_timed"],
+        "chosen_vs_plain": bres["value"] / plain["value"],
+        "chosen_vs_plain_sweep": bres["value"] / pres["value"],
+        "plain_sweep": {"mlups": pres["value"], "ms_per_step": pres["ms_per_step"], "steps_timed": pres["steps"],
+                        "windows": pres["windows"], "bulk_ms_per_step": pres["bulk_ms"],
+                        "hbm_gbs_bulk": pres["achieved"], "roofline_frac_bulk": pres["achieved"] / peak,
+                        "bytes_per_lu": BYTES_PER_LU_F64, "steady_state_mlups_graph": pres["steady"],
+                        "e2e": {"value": pres["e2e"], "unit": "MLUPS", "h2d_bytes_per_step": pres["h2d"],
+                                "d2h_bytes_per_step": pres["d2h"], "steps": pres["e2e_steps"],
+                                "seconds": pres["e2e_s"]},
+                        "status_nonzero": [k for k, st in enumerate(pres["status"]) if st],
+                        "launches_per_step": pres["launches_per_step"], "clocks": pres["clocks"],
+                        "form": "FP64 plain (the reference's arithmetic, bit for bit per case), batched"},
+        "sweep": {"steady_state_mlups_graph": bres["steady"],
+                  "status_nonzero": [k for k, st in enumerate(bres["status"]) if st], "tiles": bres["tiles"],
+                  "bulk_ms_per_step": bres["bulk_ms"], "bulk_one_launch_ms": bres["bulk_one_launch_ms"],
+                  "bulk_per_group_ms_sum": bres["bulk_per_group_ms_sum"], "bulk_merged": bres["bulk_merged"],
+                  "accuracy_vs_f64": dict(_accuracy_summary(acc), steps=acc_steps, sample_every=500,
+                                          tail="last 20 % of the run") if acc else None}})
     line["cpu_baseline"] = cpu
     line["plain"] = summary(plain)
-    line["plain"]["roofline_frac_bulk"] = plain["achieved"] / peak
     line["chosen_single_case"] = single_s
+    line.update(c35)
     if learned:
         line["learned_mdf_single_case"] = learned
     print(json.dumps(line))
+    if args.accuracy_out and acc:
+        with open(args.accuracy_out, "w") as fh:
+            json.dump({str(k): v for k, v in acc.items()}, fh, indent=1)
     if dist:
         dist.destroy_process_group()
 
@@ -700,11 +939,12 @@ def run_profile(args):
 
 def run_profile_batch(args):
     """A short eager batched run for ncu captures: the Re 20 and 40 part of the
-    sweep (36 cases, ~1.5 GB on the device), warm-up steps then args.steps."""
+    sweep (36 cases, ~1.5 GB on the device in FP32), warm-up steps then
+    args.steps."""
     import torch
     from iblbm_b200.batch import Batch
     cfgs = [c for c in sweep_configs(max_steps=args.warmup + args.steps + 8) if c.Re in (20, 40)]
-    b = Batch(cfgs)
+    b = Batch(cfgs, precision=args.precision if args.precision_set else "f32")
     b.advance(1, outputs_last=False)
     for _ in range(args.warmup + args.steps):
         b._step()
@@ -723,13 +963,25 @@ def main():
     ap.add_argument("--profile", action="store_true", help="short eager run for ncu captures")
     ap.add_argument("--profile-batch", action="store_true", help="short eager batched run for ncu captures")
     ap.add_argument("--collision", default="TRT", choices=["BGK", "TRT", "CM_MRT"])
-    ap.add_argument("--form", default="chosen", choices=["chosen", "plain"],
-                    help="chosen: time the FP32 shifted form and the FP64 plain form; plain: FP64 only")
-    ap.add_argument("--precision", default="f64", choices=["f64", "f32"], help="form used by --profile")
+    ap.add_argument("--form", default="chosen", choices=["chosen", "plain"])
+    ap.add_argument("--precision", default=None, choices=["f64", "f32"], help="form used by the profile runs")
+    ap.add_argument("--accuracy-steps", type=int, default=SWEEP_STEPS,
+                    help="steps of the sweep's FP32-vs-FP64 accuracy run (0: skip)")
+    ap.add_argument("--accuracy-out", default=None, help="write the per-case accuracy table here (JSON)")
+    ap.add_argument("--e2e-case-steps", type=int, default=10000, help="steps of the run() e2e of configs 3 and 5")
+    ap.add_argument("--skip-c35", action="store_true")
+    ap.add_argument("--skip-learned", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    args.precision_set = args.precision is not None
+    if args.precision is None:
+        args.precision = "f64"
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile_batch:
+    if args.cpu_sample is not None:
+        base = oracle_sweep_sample(args.cpu_sample)
+        print(json.dumps({k: v for k, v in base.items() if k not in ("timed_s", "cases")}))
+    elif args.profile_batch:
         run_profile_batch(args)
     elif args.profile:
         run_profile(args)

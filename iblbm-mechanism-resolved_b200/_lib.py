@@ -106,6 +106,8 @@ _SIGS = {
     "iblbm_mlp_infer": [_vp, _vp, _i, _vp, _vp],
     "iblbm_mlp_train_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_float, _i, _vp, _i, _vp],
     "iblbm_dense_step_f32_batch": [ctypes.POINTER(Dense32Args), _i, _vp],
+    "iblbm_dense_step_f64_batch": [ctypes.POINTER(DenseArgs), _i, _vp],
+    "iblbm_ibm_step_f64_batch": [ctypes.POINTER(IbmArgs), _vp, _i, _vp],
     "iblbm_ibm32_list_cache_ints": [_i, _i, _i],
     "iblbm_ibm32_smem_bytes": [_i, _i, _i],
     "iblbm_to_shifted_f32": [_vp, Geom, _vp, _vp],

@@ -1,4 +1,5 @@
-"""Many independent cases advancing together on one GPU (shifted FP32 form).
+"""Many independent cases advancing together on one GPU (shifted FP32 form,
+or the FP64 plain form with ``precision="f64"``).
 
 A parameter sweep (Reynolds number x band method x delta kernel x collision
 model, lattices of uneven size) is a set of independent cases.  Run one at a
@@ -19,13 +20,71 @@ captured once into a CUDA graph and replayed.  Each case keeps its own
 ``Engine`` (device buffers, host-side state, diagnostics); the batch only
 drives their kernels together.  Output steps (rho, u, Cd, Cl) run through each
 case's own engine.
+
+The FP64 batch (``iblbm_ibm_step_f64_batch`` / ``iblbm_dense_step_f64_batch``)
+runs the single-case FP64 device functions per case, so each case's results
+are bit for bit those of its own engine; it has one tile shape (one node per
+thread) and no merged bulk launch.
 """
 from __future__ import annotations
 
-from ._lib import IBM_IDS, TILES, Dense32Args, Ibm32Args, check
+from ._lib import IBM_IDS, TILES, Dense32Args, DenseArgs, Ibm32Args, IbmArgs, check
 from .engine import Engine
+from .state import grid_shape
 
 MAX_KIND = 72  # cases per batched collide-stream launch (iblbm_dense_step_f32_batch)
+BYTES_PER_LU = {"f32": 72, "f64": 144}  # populations read + written per lattice update
+
+
+def case_cost(cfg, precision="f32", steps=None):
+    """Estimated cost of a case: the population bytes its lattice streams per
+    step (the bound of a batched step) times its steps (cfg.max_steps unless
+    given)."""
+    nx, ny, _, _ = grid_shape(cfg)
+    return nx * ny * BYTES_PER_LU[precision] * int(cfg.max_steps if steps is None else steps)
+
+
+def partition_cases(cfgs, world, precision="f32", steps=None):
+    """Case indices of each of `world` ranks for a sweep of independent cases
+    sharded over GPUs.  The cases, largest estimated cost first (ties by
+    index), each go to the rank with the least cost so far (ties to the lower
+    rank): the longest-processing-time rule, whose largest load exceeds the
+    smallest by at most one case's cost.  Every rank computes the same
+    partition from the same list, so no communication is needed; the cases
+    exchange nothing, so the data path has no collective.  (The reference
+    packs its sweep's cases onto GPUs by memory, scripts/experiments/
+    _runner_common.py:83-152; here they are balanced by the bytes each step
+    streams, which bounds a batched step's time.)  Returns a list of `world`
+    sorted index lists."""
+    if world < 1:
+        raise ValueError(f"world={world}")
+    cost = [case_cost(c, precision, steps) for c in cfgs]
+    order = sorted(range(len(cfgs)), key=lambda k: (-cost[k], k))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += cost[k]
+    return [sorted(p) for p in parts]
+
+
+def gather_case_results(local, dist=None):
+    """Per-case results of all ranks on every rank: `local` maps this rank's
+    case indices to its results (any picklable value); returns the union as
+    one dict ordered by case index.  Host-side, after the run (one object
+    all-gather; the identity without a process group)."""
+    if not dist:
+        return dict(sorted(local.items()))
+    got = [None] * dist.get_world_size()
+    dist.all_gather_object(got, dict(local))
+    out = {}
+    for part in got:
+        for k, v in part.items():
+            if k in out:
+                raise RuntimeError(f"case {k} reported by two ranks")
+            out[k] = v
+    return dict(sorted(out.items()))
 
 
 def _copy(struct):
@@ -33,14 +92,20 @@ def _copy(struct):
 
 
 class Batch:
-    """Independent cases on one GPU, stepped together (FP32 shifted form)."""
+    """Independent cases on one GPU, stepped together (FP32 shifted form, or
+    the FP64 plain form)."""
 
-    def __init__(self, cfgs, device=None, tile="rows2"):
+    def __init__(self, cfgs, device=None, tile="rows2", precision="f32"):
         if not cfgs:
             raise ValueError("empty batch")
+        if precision not in ("f32", "f64"):
+            raise ValueError(f"precision='{precision}' (f32 or f64)")
         if any(cfg.scenario_type == "taylor_green" for cfg in cfgs):
             raise NotImplementedError("Taylor-Green cases (a per-step closure factor) are stepped one at a time")
-        self.engines = [Engine(cfg, device, precision="f32") for cfg in cfgs]
+        self.precision = precision
+        self.f32 = precision == "f32"
+        self._IA, self._DA = (Ibm32Args, Dense32Args) if self.f32 else (IbmArgs, DenseArgs)
+        self.engines = [Engine(cfg, device, precision=precision) for cfg in cfgs]
         for e in self.engines:
             if e.st.particles is not None:
                 raise NotImplementedError("free particles (host Newton-Euler) are stepped one case at a time")
@@ -81,7 +146,7 @@ class Batch:
         self.ibm_dev = {}
         for first in (True, False):
             for p in (0, 1):
-                arr = (Ibm32Args * self.C)()
+                arr = (self._IA * self.C)()
                 for k, e in enumerate(self.engines):
                     a = _copy(e.ibm_args[p])
                     a.rebuild = 1 if (first or e.moving) else 0
@@ -125,27 +190,30 @@ class Batch:
         box passes (tile of the kind set on every entry); per bulk group and
         parity, those of the bulk passes."""
         self.dense = {}
+        DA = self._DA
         for g, idx in enumerate(self.kinds):
             for p in (0, 1):
                 for mode in ("full", "box"):
-                    arr = (Dense32Args * len(idx))()
+                    arr = (DA * len(idx))()
                     for n, k in enumerate(idx):
                         e = self.engines[k]
                         src = {"full": e.dense_full, "box": e.dense_box}[mode][p][0]
                         a = _copy(src)
-                        a.tile = TILES[self.tiles[g]]
+                        if self.f32:
+                            a.tile = TILES[self.tiles[g]]
                         a.box_blocks = 8
                         arr[n] = a
                     self.dense[g, p, mode] = arr
         for g, idx in enumerate(self.bulk_groups):
             for p in (0, 1):
-                arr = (Dense32Args * len(idx))()
+                arr = (DA * len(idx))()
                 for n, k in enumerate(idx):
                     a = _copy(self.engines[k].dense_bulk[p][0])
-                    a.tile = TILES[self.bulk_tiles[g]]
+                    if self.f32:
+                        a.tile = TILES[self.bulk_tiles[g]]
                     arr[n] = a
                 self.dense["bulk", g, p] = arr
-        if self.C <= MAX_KIND:
+        if self.f32 and self.C <= MAX_KIND:
             order = [k for idx in self.kinds for k in idx]
             for p in (0, 1):
                 arr = (Dense32Args * len(order))()
@@ -155,8 +223,13 @@ class Batch:
                     arr[n] = a
                 self.dense["all", p, "bulk"] = arr
 
+    def _need_f32(self, what):
+        if not self.f32:
+            raise NotImplementedError(f"{what}: the FP64 batch has one tile shape and no merged launch")
+
     def set_tile_all(self, tile, merged=True):
         """Tile of the single bulk launch over all cases (and whether to use it)."""
+        self._need_f32("set_tile_all")
         if tile not in ("node", "rows2", "rows4"):
             raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
         self.tile_all = tile
@@ -166,6 +239,7 @@ class Batch:
 
     def set_tile(self, kind, tile):
         """Tile of the whole-lattice passes of one kind (the first step's)."""
+        self._need_f32("set_tile")
         if tile not in ("node", "rows2", "rows4"):
             raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
         self.tiles[kind] = tile
@@ -175,6 +249,7 @@ class Batch:
     def set_bulk_tile(self, group, tile):
         """Tile of the bulk launch of one group (cases of one collision,
         closure and compressibility)."""
+        self._need_f32("set_bulk_tile")
         if tile not in ("node", "rows2", "rows4"):
             raise ValueError(f"batched tile {tile!r} (node, rows2, rows4)")
         self.bulk_tiles[group] = tile
@@ -184,16 +259,25 @@ class Batch:
     # ---------------------------------------------------------------------------------
     def _band(self, first, stream):
         p = self.parity
-        check(self.L.iblbm_ibm_step_f32_batch(self.ibm_host[first, p], self.ibm_dev[first, p].data_ptr(), self.C,
-                                              stream), "iblbm_ibm_step_f32_batch")
+        if self.f32:
+            rc = self.L.iblbm_ibm_step_f32_batch(self.ibm_host[first, p], self.ibm_dev[first, p].data_ptr(), self.C,
+                                                 stream)
+        else:
+            rc = self.L.iblbm_ibm_step_f64_batch(self.ibm_host[first, p], self.ibm_dev[first, p].data_ptr(), self.C,
+                                                 stream)
+        check(rc, "batched band step")
+
+    def _dense_call(self, arr, stream):
+        if self.f32:
+            check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
+        else:
+            check(self.L.iblbm_dense_step_f64_batch(arr, len(arr), stream), "iblbm_dense_step_f64_batch")
 
     def _dense(self, g, mode, stream):
-        arr = self.dense[g, self.parity, mode]
-        check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
+        self._dense_call(self.dense[g, self.parity, mode], stream)
 
     def _bulk(self, g, stream):
-        arr = self.dense["bulk", g, self.parity]
-        check(self.L.iblbm_dense_step_f32_batch(arr, len(arr), stream), "iblbm_dense_step_f32_batch")
+        self._dense_call(self.dense["bulk", g, self.parity], stream)
 
     def _sync_engines(self):
         for e in self.engines:

@@ -27,6 +27,7 @@ UNITS = {
     "ibm_f64.cu": ["-fmad=false"],
     "ops_f64.cu": ["-fmad=false"],
     "particles_f64.cu": ["-fmad=false"],
+    "batch_f64.cu": ["-fmad=false"],
     "dense_f32.cu": [],
     "pipe_f32.cu": [],
     "batch_f32.cu": [],

@@ -9,6 +9,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "../../include/iblbm_b200.h"
 
 namespace iblbm {
 
@@ -45,6 +46,24 @@ struct BcParams {
     const double* tg_face;   // Taylor-Green: boundary-node velocities before decay
     const double* tg_decay;  // Taylor-Green: decay factor of this step (device scalar)
 };
+
+// Closure constants of a case; feq(dens, (u_in, 0)) in the operation order of
+// iblbm/lbm/equilibrium.py:39-42.  Host and device evaluate the same IEEE
+// expression (no contraction: x86-64 host code has no FMA, device units are
+// compiled with -fmad=false), so both give the same bits.
+__host__ __device__ inline void make_bc(const iblbm_case& c, BcParams& bc)
+{
+    bc.type = c.bc;
+    bc.inflow_u = c.inflow_u;
+    bc.dens = c.dens;
+    bc.tg_face = c.tg_face;
+    bc.tg_decay = c.tg_decay;
+    const double u0 = c.inflow_u, u1 = 0.0, u2 = u0 * u0 + u1 * u1;
+    for (int q = 0; q < 9; ++q) {
+        const double a0 = (double)ex_(q) * u0, a1 = (double)ey_(q) * u1, eU = a0 + a1;
+        bc.feq_in[q] = c.dens * w_(q) * (1.0 + 3.0 * eU + 4.5 * eU * eU - 1.5 * u2);
+    }
+}
 
 // Slot of boundary node (i, j) in the Taylor-Green face table: left j, right j,
 // bottom i-1, top i-1, then the corners (0,0), (nx-1,0), (0,ny-1), (nx-1,ny-1).

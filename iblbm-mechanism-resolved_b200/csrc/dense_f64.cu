@@ -111,17 +111,7 @@ void make_params(const iblbm_case& c, CollParams& cp, BcParams& bc)
     cp.s_minus = c.s_minus;
     for (int q = 0; q < 9; ++q) cp.S[q] = c.S[q];
     cp.dt = c.dt;
-    bc.type = c.bc;
-    bc.inflow_u = c.inflow_u;
-    bc.dens = c.dens;
-    bc.tg_face = c.tg_face;
-    bc.tg_decay = c.tg_decay;
-    // feq(dens, (u_in, 0)) — equilibrium.py:39-42 with the same operation order
-    const double u0 = c.inflow_u, u1 = 0.0, u2 = u0 * u0 + u1 * u1;
-    for (int q = 0; q < 9; ++q) {
-        const double a0 = (double)ex_(q) * u0, a1 = (double)ey_(q) * u1, eU = a0 + a1;
-        bc.feq_in[q] = c.dens * w_(q) * (1.0 + 3.0 * eU + 4.5 * eU * eU - 1.5 * u2);
-    }
+    make_bc(c, bc);
 }
 
 }  // namespace iblbm

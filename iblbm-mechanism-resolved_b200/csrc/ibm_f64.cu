@@ -3,6 +3,7 @@
 // The kernel itself is band_kernel.cuh instantiated with R = double; this unit
 // is compiled without multiply-add contraction, so every sum runs in the
 // reference's order and results are bit-identical to the reference CPU path.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include "band_kernel.cuh"
@@ -46,6 +47,31 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
     BcParams bc;
     make_params(a->c, cp, bc);
     return dispatch_ibm<iblbm_ibm_args, double, false>(a, bc, stream);
+}
+
+// Band steps of n independent cases in one launch (one CTA per case), the
+// FP64 counterpart of iblbm_ibm_step_f32_batch: each CTA runs the same band
+// step body as the single-case kernel, so every case's results are bit for bit
+// those of its own step.
+extern "C" int iblbm_ibm_step_f64_batch(const iblbm_ibm_args* host_args, const iblbm_ibm_args* dev_args, int n,
+                                        void* stream)
+{
+    if (!host_args || !dev_args || n < 1 || n > 65535) return IBLBM_E_ARG;
+    size_t smem = 0;
+    for (int b = 0; b < n; ++b) {
+        const int chk = check_ibm_args<double>(&host_args[b]);
+        if (chk != IBLBM_OK) return chk;
+        smem = std::max(smem, ibm_smem<double>(host_args[b]));
+    }
+    auto K = ibm_batch_kernel<iblbm_ibm_args, double, false>;
+    static std::once_flag configured;
+    cudaError_t attr = cudaSuccess;
+    std::call_once(configured, [&] {
+        attr = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT);
+    });
+    if (attr != cudaSuccess) return IBLBM_E_LAUNCH;
+    K<<<n, IBM_THREADS, smem, (cudaStream_t)stream>>>(dev_args);
+    return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
 
 // ---------------------------------------------------------------------------

@@ -198,6 +198,18 @@ int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
  * device's primary context lives as long: no call after cudaDeviceReset).
  * Allocates nothing. */
 int iblbm_ibm_step_f64_noalloc(const iblbm_ibm_args *a, void *stream);
+/* The plain form of the batched sweep: band steps of n independent cases in
+ * one launch (one CTA per case), as iblbm_ibm_step_f32_batch on the FP64
+ * lattice; each case's results are bit for bit those of iblbm_ibm_step_f64.
+ * No reference counterpart (the reference steps one case at a time). */
+int iblbm_ibm_step_f64_batch(const iblbm_ibm_args *host_args, const iblbm_ibm_args *dev_args, int n,
+                             void *stream);
+/* The FP64 collide-stream pass of n <= 72 cases of one kind (collision,
+ * closure, compressibility, band method; all bulk/whole-lattice or all box
+ * passes) in one launch, lattices of any size; no ro/U/fstar outputs, no
+ * Taylor-Green closure.  Same per-node arithmetic as iblbm_dense_step_f64, so
+ * bit-identical per case.  No reference counterpart. */
+int iblbm_dense_step_f64_batch(const iblbm_dense_args *a, int n, void *stream);
 int iblbm_ibm_scratch_doubles(int lb_total, int band_capacity, int n_particles);
 int iblbm_ibm_scratch_ints(int lb_total, int band_capacity, int delta_type);
 int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int delta_type);

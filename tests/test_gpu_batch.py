@@ -92,3 +92,26 @@ def test_step_io_matches_plain_steps(torch):
     np.testing.assert_array_equal(outs[0].numpy(), b.marker_out.cpu().numpy())  # the fifth step used outs[0]
     for ea, eb in zip(a.engines, b.engines):
         np.testing.assert_array_equal(ea.fpost_aos(), eb.fpost_aos())
+
+
+def test_fp64_batch_matches_single_cases(torch):
+    """The FP64 batch (plain form): every case bit for bit equal to its own
+    FP64 engine, whose arithmetic is the reference's (moving and fixed bodies,
+    every band method and collision model of CASES)."""
+    from iblbm_b200.batch import Batch
+    from iblbm_b200.engine import Engine
+    cfgs = [_cfg(**kw) for kw in CASES]
+    b = Batch(cfgs, precision="f64")
+    b.advance(61, outputs_last=True)
+    torch.cuda.synchronize()
+    assert b.status() == [0] * len(cfgs)
+    for cfg, eb in zip(cfgs, b.engines):
+        es = Engine(cfg, precision="f64")
+        es.advance(61, outputs_last=True)
+        torch.cuda.synchronize()
+        assert es.status() == 0
+        sb, ss = eb.read_state(), es.read_state()
+        for k in ("ro", "U", "fstar", "fib", "feq"):
+            np.testing.assert_array_equal(getattr(sb, k), getattr(ss, k), err_msg=f"{cfg.ibm_method} {k}")
+        np.testing.assert_array_equal(eb.fpost_aos(), es.fpost_aos())
+        assert eb.cd_cl() == es.cd_cl()
