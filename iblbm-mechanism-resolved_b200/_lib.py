@@ -57,7 +57,7 @@ class IbmArgs(ctypes.Structure):
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
                 ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i),
-                ("dvel_scale", _vp), ("dfc_rho_f", _d)]
+                ("dvel_scale", _vp), ("dfc_rho_f", _d), ("wait_limit", ctypes.c_longlong), ("test_skip_copy", _i)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee
@@ -69,7 +69,8 @@ class Ibm32Args(ctypes.Structure):
 
 
 class Dense32Args(ctypes.Structure):
-    _fields_ = DenseArgs._fields_ + [("tile", _i), ("status", _vp)]
+    _fields_ = DenseArgs._fields_ + [("tile", _i), ("status", _vp), ("wait_limit", ctypes.c_longlong),
+                                     ("test_skip_copy", _i)]
 
 
 TILES = {"pipe4x2": 0, "node": 1, "pipe8x2": 2, "rows2": 3, "rows4": 4}
@@ -78,10 +79,22 @@ class ParticlesArgs(ctypes.Structure):
     _fields_ = [("n_particles", _i), ("phase", _i), ("model", _i), ("fib_f32", _i), ("moff", _vp), ("Lx_c", _vp),
                 ("Ly_c", _vp), ("Lx", _vp), ("Ly", _vp), ("dvel", _vp), ("state", _vp), ("consts", _vp),
                 ("dt", _d), ("dx", _d), ("band_fib_part", _vp), ("band_count", _vp), ("band_capacity", _i),
-                ("forces_out", _vp)]
+                ("forces_out", _vp), ("n_nodes", _i), ("band_nodes", _vp), ("pw_leaves", _i), ("pw_internal", _i),
+                ("pw_levels", _i), ("pw_leaf", _vp), ("pw_node", _vp), ("pw_level", _vp), ("pw_scratch", _vp)]
 
 
 INERTIA_IDS = {"none": 0, "explicit_history": 1, "feng_b2": 2}
+
+
+class ForceCoeffArgs(ctypes.Structure):
+    _fields_ = [("ro", _vp), ("n_nodes", _i), ("f32", _i), ("method", _i), ("band_fib", _vp), ("band_count", _vp),
+                ("dfc_force", _vp), ("lb_total", _i), ("u_ref", _d), ("lattice_r", _d), ("partials", _vp),
+                ("ticket", _vp), ("ring", _vp), ("ring_len", _i), ("ring_pos", _vp)]
+
+
+class VelocityChangeArgs(ctypes.Structure):
+    _fields_ = [("U", _vp), ("U_prev", _vp), ("n_nodes", _i), ("f32", _i), ("partials", _vp), ("ticket", _vp),
+                ("out", _vp)]
 
 # entry point -> argtypes (all return int status)
 _SIGS = {
@@ -113,6 +126,9 @@ _SIGS = {
     "iblbm_to_shifted_f32": [_vp, Geom, _vp, _vp],
     "iblbm_from_shifted_f32": [_vp, Geom, _vp, _vp],
     "iblbm_particles_step_f64": [ctypes.POINTER(ParticlesArgs), _vp],
+    "iblbm_force_coeffs": [ctypes.POINTER(ForceCoeffArgs), _vp],
+    "iblbm_velocity_change": [ctypes.POINTER(VelocityChangeArgs), _vp],
+    "iblbm_diag_partials": [_i],
     "iblbm_aos_to_soa": [_vp, Geom, _vp, _vp],
     "iblbm_soa_to_aos": [_vp, Geom, _vp, _vp],
 }

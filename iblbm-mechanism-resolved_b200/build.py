@@ -28,6 +28,7 @@ UNITS = {
     "ops_f64.cu": ["-fmad=false"],
     "particles_f64.cu": ["-fmad=false"],
     "batch_f64.cu": ["-fmad=false"],
+    "diag.cu": ["-fmad=false"],
     "dense_f32.cu": [],
     "pipe_f32.cu": [],
     "batch_f32.cu": [],

@@ -387,10 +387,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     __shared__ int s_nb, s_status, s_box[4], s_step, s_cur;
     __shared__ __align__(8) uint64_t s_bar, s_wbar;
     const bool rebuild = a.rebuild || a.xt_table;
+    const long long wait_limit = a.wait_limit > 0 ? a.wait_limit : TMA_WAIT_LIMIT;
     // an early return first waits (bounded) for the network copy in flight
     auto drain_weights = [&]() {
         if constexpr (SHIFTED && METHOD == IBM_MDF && !COUPLED) {
-            if (a.mlp_mode & 2) mbar_wait_bounded(&s_wbar, 0, TMA_WAIT_LIMIT);
+            if (a.mlp_mode & 2) mbar_wait_bounded(&s_wbar, 0, wait_limit);
         }
     };
     if constexpr (SHIFTED && METHOD == IBM_MDF && !COUPLED) {
@@ -414,7 +415,8 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 const uint32_t bytes = (uint32_t)Lay.static_bytes;
                 mbar_expect(&s_bar, bytes);
                 const char* src = reinterpret_cast<const char*>(a.list_cache);
-                for (uint32_t off = 0; off < bytes; off += 65536u) {
+                // (test_skip_copy: the wait below runs out with nothing in flight)
+                for (uint32_t off = 0; off < (a.test_skip_copy ? 0u : bytes); off += 65536u) {
                     const uint32_t chunk = min(65536u, bytes - off);
                     bulk_copy(smem_raw + off, src + off, chunk, &s_bar);
                 }
@@ -602,10 +604,10 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     } else {
         // wait for the bulk copy (bounded: a copy that does not land is reported)
         bool done = GS;
-        for (long long it = 0; it < TMA_WAIT_LIMIT && !done; ++it) done = mbar_try_wait(&s_bar, 0);
+        for (long long it = 0; it < wait_limit && !done; ++it) done = mbar_try_wait(&s_bar, 0);
         if (!done) {
             if (tid == 0) s_status = ST_COPY_TIMEOUT;
-            for (long long it = 0; it < TMA_WAIT_LIMIT && !done; ++it) done = mbar_try_wait(&s_bar, 0);
+            for (long long it = 0; it < wait_limit && !done; ++it) done = mbar_try_wait(&s_bar, 0);
         }
         __syncthreads();
         if (s_status != ST_OK) {
@@ -748,7 +750,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 bool use_net = false;
                 if (warm) {
                     // a copy that does not land leaves this step on plain MDF
-                    const bool ok = mbar_wait_bounded(&s_wbar, 0, TMA_WAIT_LIMIT);
+                    const bool ok = mbar_wait_bounded(&s_wbar, 0, wait_limit);
                     use_net = __syncthreads_and(ok) != 0;
                 }
                 const float inv_u = 1.0f / a.mlp_uref;

@@ -13,9 +13,19 @@
 // explicit_history.py:53-66; the rho-ratio term for feng_b2, feng_b2.py:33-48).
 // One launch after the band kernel does the full step of this timestep and the
 // half step of the next, so the whole step stays on the device and can be
-// captured in a CUDA graph.  The force sum runs in a fixed order (per-thread
-// strided partial sums, then a fixed tree), so it is deterministic but not in
-// numpy's pairwise order: trajectories agree with the host step to round-off.
+// captured in a CUDA graph.
+//
+// The force is -sum of the particle's spread force over the lattice.  The
+// reference sums its dense n_nodes x 2 field with numpy (np.sum: pairwise
+// summation, iblbm/ibm/multi_particle.py:199-202); given that summation tree
+// (pw_* fields, built on the host from n_nodes) the kernel evaluates it over
+// the band's nonzero entries: every block of the tree sums its entries in
+// numpy's order (8 strided accumulators, their fixed combination, the tail),
+// a block without band entries sums to +0.0, and the inner nodes add their
+// children level by level.  Adding the zeros numpy adds would change no
+// partial sum, so the force equals numpy's bit for bit and the trajectories
+// equal the host step's.  Without a tree the sum runs in another fixed order
+// (deterministic, round-off apart from numpy's).
 #include <cstdint>
 #include "common.cuh"
 #include "../../include/iblbm_b200.h"
@@ -55,6 +65,59 @@ __device__ void particle_forces(const iblbm_particles_args& a, const F* fib, dou
     }
 }
 
+// numpy's pairwise sum of the dense field, over the band entries only (see the
+// file comment).  val(p, c, b): component c of particle p's force at band entry b.
+template <typename F>
+__device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fib, double* s_force)
+{
+    const int nb = *a.band_count;
+    const int P = a.n_particles, PC = 2 * P;
+    const int L = a.pw_leaves;
+    const size_t pstride = 2 * (size_t)a.band_capacity;
+    double* v = a.pw_scratch;  // node id x PC
+    for (int li = threadIdx.x; li < L; li += PART_THREADS) {
+        const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
+        // first band entry at or after off (band nodes ascend)
+        int lo = 0, hi = nb;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (a.band_nodes[mid] < off) lo = mid + 1;
+            else hi = mid;
+        }
+        const int cut = m - m % 8;
+        for (int pc = 0; pc < PC; ++pc) {
+            const F* src = fib + (pc >> 1) * pstride + (pc & 1);
+            double res;
+            if (m < 8) {
+                res = 0.0;
+                for (int b = lo; b < nb && a.band_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+            } else {
+                double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                int b = lo;
+                for (; b < nb && a.band_nodes[b] < off + cut; ++b) {
+                    const int k = a.band_nodes[b] - off;
+                    r[k & 7] += (double)src[2 * (size_t)b];
+                }
+                res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+                for (; b < nb && a.band_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+            }
+            v[(size_t)li * PC + pc] = res;
+        }
+    }
+    __syncthreads();
+    for (int d = 0; d < a.pw_levels; ++d) {
+        for (int k = a.pw_level[d] + threadIdx.x; k < a.pw_level[d + 1]; k += PART_THREADS) {
+            const int c0 = a.pw_node[2 * k], c1 = a.pw_node[2 * k + 1];
+            for (int pc = 0; pc < PC; ++pc)
+                v[(size_t)(L + k) * PC + pc] = v[(size_t)c0 * PC + pc] + v[(size_t)c1 * PC + pc];
+        }
+        __syncthreads();
+    }
+    const int root = a.pw_internal > 0 ? L + a.pw_internal - 1 : 0;
+    if (threadIdx.x < PC) s_force[threadIdx.x] = -(0.0 + v[(size_t)root * PC + threadIdx.x]);
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_particles_args a)
 {
     __shared__ double s_force[2 * PART_MAXP];
@@ -62,8 +125,14 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
     const int P = a.n_particles;
     const double dt = a.dt, dx = a.dx;
     if (a.phase & IBLBM_PARTICLES_FULL) {
-        if (a.fib_f32) particle_forces(a, static_cast<const float*>(a.band_fib_part), s_force);
-        else particle_forces(a, static_cast<const double*>(a.band_fib_part), s_force);
+        if (a.pw_leaf) {
+            if (a.fib_f32) particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_force);
+            else particle_forces_exact(a, static_cast<const double*>(a.band_fib_part), s_force);
+        } else if (a.fib_f32) {
+            particle_forces(a, static_cast<const float*>(a.band_fib_part), s_force);
+        } else {
+            particle_forces(a, static_cast<const double*>(a.band_fib_part), s_force);
+        }
         if (threadIdx.x < P) {
             const int p = threadIdx.x;
             double* s = a.state + IBLBM_PARTICLE_STATE * p;
@@ -130,6 +199,10 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
     if ((a->phase & IBLBM_PARTICLES_HALF) && (!a->Lx_c || !a->Ly_c || !a->Lx || !a->Ly || !a->dvel))
         return IBLBM_E_ARG;
     if (a->model < IBLBM_INERTIA_NONE || a->model > IBLBM_INERTIA_FENG_B2) return IBLBM_E_ARG;
+    if (a->pw_leaf && (!a->pw_node && a->pw_internal > 0)) return IBLBM_E_ARG;
+    if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || a->pw_leaves < 1 || a->pw_internal < 0 ||
+                       a->pw_levels < 0 || a->n_nodes < 1))
+        return IBLBM_E_ARG;
     particles_kernel<<<1, PART_THREADS, 0, (cudaStream_t)stream>>>(*a);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

@@ -76,12 +76,14 @@ __global__ void __launch_bounds__(32 * (ROWS + 1), MINB) dense32_pipe_kernel(con
         sy1 = sy0 + __ldg(a.skip_box + 3) - 1;
     }
     constexpr int STAGE_F = 9 * ROWS * PIPE_SW;
+    const long long wait_limit = a.wait_limit > 0 ? a.wait_limit : PIPE_WAIT_LIMIT;
     if (warp == ROWS) {
-        // producer
+        // producer (test_skip_copy: issues nothing, so every consumer wait runs out)
+        if (a.test_skip_copy) return;
         int k = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
             const int s = k % STAGES;
-            if (k >= STAGES && !mbar_wait_bounded(&empty[s], ((k / STAGES) & 1) ^ 1, PIPE_WAIT_LIMIT)) {
+            if (k >= STAGES && !mbar_wait_bounded(&empty[s], ((k / STAGES) & 1) ^ 1, wait_limit)) {
                 if (lane == 0 && a.status) atomicExch(a.status, PIPE_TIMEOUT);
                 break;
             }
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(32 * (ROWS + 1), MINB) dense32_pipe_kernel(con
     int k = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
         const int s = k % STAGES;
-        if (!mbar_wait_bounded(&full[s], (k / STAGES) & 1, PIPE_WAIT_LIMIT)) {
+        if (!mbar_wait_bounded(&full[s], (k / STAGES) & 1, wait_limit)) {
             if (lane == 0 && a.status) atomicExch(a.status, PIPE_TIMEOUT);
             break;
         }

@@ -31,6 +31,7 @@ from .physics import (history_increment, mdf_relaxation_factor, net_gravity, osc
 from .state import initial_velocity, initialize
 
 MDF_COUPLED_OMEGA_MAX = 0.8  # iblbm/ibm/multi_particle.py:33
+OUT_MOMENTS = 2  # output flag of a step that writes rho and U but not f*
 MOVING_ROTATION_OMEGA_MAX = 1.0  # iblbm/ibm/strategies/mdf.py:23
 
 
@@ -185,6 +186,15 @@ class Engine:
         self.d_stats, self.d_dstats = t(5, i32), t(2)
         self.d_lambda, self.d_lambda_valid = t(self.Lb), t(1, i32)
         self.d_counter = t(1, i32)
+        # diagnostics reduced on the device: force coefficients ring, convergence error
+        self.ring_len = 4096
+        self.d_ring = torch.zeros(self.ring_len, 5, dtype=f64, device=dev)
+        self.d_ring_pos = t(1, i32)
+        self.ring_read = 0  # entries queued so far (the host's copy of the device counter)
+        self.d_diag_part = t(self.L.iblbm_diag_partials(N))
+        self.d_diag_ticket = t(1, i32)
+        self.d_uprev = None
+        self.d_vchange = t(3)
         self.xt = None
         if cfg.motion_type == "oscillating":
             table = oscillation_table(cfg.max_steps + 2, cfg.lattice_u, cfg.KC, st.r, st.lattice_r)
@@ -203,13 +213,13 @@ class Engine:
         self.d_pipe_status = torch.zeros(1, dtype=i32, device=dev)
         self.graphs = {}
         self._make_dense_variants()
-        # free particles: their Verlet step on the device (default in the FP32
-        # form; the FP64 form keeps the host step, whose force sums follow numpy's
-        # pairwise order bit for bit)
+        # free particles: their Verlet step on the device by default (its force
+        # sums follow numpy's pairwise order, so it equals the host step bit for
+        # bit); device_particles=False keeps the host step
         self.dev_particles = False
         self._torque_ij = None
         if st.particles is not None:
-            self.dev_particles = self.f32 if device_particles is None else bool(device_particles)
+            self.dev_particles = True if device_particles is None else bool(device_particles)
             if cfg.enable_rotation or cfg.time_integrator == "euler_explicit":
                 # the torque, the angular Verlet step and the explicit Euler step run on the host
                 if device_particles:
@@ -255,6 +265,18 @@ class Engine:
         a.dt, a.dx = float(st.dt), float(st.dx)
         a.band_fib_part, a.band_count, a.band_capacity = ptr(self.d_fib_part), ptr(self.d_count), self.B
         a.forces_out = ptr(self.d_pforces)
+        # the force sums in numpy's pairwise order over the dense lattice field
+        from .physics import pairwise_tree
+        leaves, inner, levels = pairwise_tree(self.N)
+        self.d_pw_leaf = torch.as_tensor(leaves.reshape(-1), device=self.dev)
+        self.d_pw_node = torch.as_tensor(inner.reshape(-1) if inner.size else np.zeros(2, np.int32), device=self.dev)
+        self.d_pw_level = torch.as_tensor(levels, device=self.dev)
+        self.d_pw_scratch = torch.zeros((len(leaves) + len(inner)) * 2 * len(ps), dtype=torch.float64,
+                                        device=self.dev)
+        a.n_nodes, a.band_nodes = self.N, ptr(self.d_nodes)
+        a.pw_leaves, a.pw_internal, a.pw_levels = len(leaves), len(inner), len(levels) - 1
+        a.pw_leaf, a.pw_node, a.pw_level = ptr(self.d_pw_leaf), ptr(self.d_pw_node), ptr(self.d_pw_level)
+        a.pw_scratch = ptr(self.d_pw_scratch)
         self.part_args = a
         self.part_started = False
 
@@ -368,11 +390,13 @@ class Engine:
         return a
 
     def _make_dense_variants(self):
-        """Dense pass variants per parity and output flag: whole lattice, bulk
-        (skips the exclusion box), box (only the exclusion box)."""
-        self.dense_full = [[self._make_dense_args(p, out, "full") for out in (False, True)] for p in (0, 1)]
-        self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in (False, True)] for p in (0, 1)]
-        self.dense_box = [[self._make_dense_args(p, out, "box") for out in (False, True)] for p in (0, 1)]
+        """Dense pass variants per parity and output flag (0: none, 1: rho, U and
+        f*, 2: rho and U only): whole lattice, bulk (skips the exclusion box), box
+        (only the exclusion box)."""
+        outs = (False, True, OUT_MOMENTS)
+        self.dense_full = [[self._make_dense_args(p, out, "full") for out in outs] for p in (0, 1)]
+        self.dense_bulk = [[self._make_dense_args(p, out, "bulk") for out in outs] for p in (0, 1)]
+        self.dense_box = [[self._make_dense_args(p, out, "box") for out in outs] for p in (0, 1)]
 
     def set_mlp(self, mode, net=None):
         """Learned MDF warm start of the FP32 form (single-body MDF): mode bit 1
@@ -421,7 +445,8 @@ class Engine:
         a.uring_prev, a.uring_next = ptr(self.uring[parity]), ptr(self.uring[1 - parity])
         a.band = BandView(ptr(self.d_box), ptr(self.d_map), ptr(self.d_fib), ptr(self.d_df))
         if outputs:
-            a.ro_out, a.U_out, a.fstar_out = ptr(self.ro_out), ptr(self.U_out), ptr(self.fstar_out)
+            a.ro_out, a.U_out = ptr(self.ro_out), ptr(self.U_out)
+            a.fstar_out = 0 if outputs == OUT_MOMENTS else ptr(self.fstar_out)
         if mode == "bulk":
             a.skip_box = ptr(self.d_excl[parity])
         elif mode == "box":
@@ -441,7 +466,7 @@ class Engine:
         self.rebuild_next = False
 
     def _dense(self, variant, outputs, stream):
-        da = variant[self.parity][1 if outputs else 0]
+        da = variant[self.parity][2 if outputs == OUT_MOMENTS else (1 if outputs else 0)]
         if self.f32:
             check(self.L.iblbm_dense_step_f32(ctypes.byref(da), stream), "iblbm_dense_step_f32")
         else:
@@ -708,9 +733,10 @@ class Engine:
         them); then the next step's markers and desired velocity."""
         cfg, st = self.cfg, self.st
         rot = cfg.enable_rotation
-        outputs = outputs or rot
         self._upload_markers()
-        self._launch(outputs)
+        # with rotation every step writes rho and U (not f*) for the angular
+        # momentum of the fluid inside each disc
+        self._launch(outputs or (OUT_MOMENTS if rot else False))
         self.ttt += 1
         if outputs:
             self.last_out_step = self.ttt - 1
@@ -789,22 +815,67 @@ class Engine:
             fib[self.d_nodes[:nb].long()] = self.d_fib[: 2 * nb].reshape(nb, 2).double()
         return fib
 
-    def cd_cl(self):
-        """Cd, Cl of the last output step — iblbm/diagnostics/core.py:53-113."""
+    def queue_force_coeffs(self):
+        """Queue, on the current stream, the reduction of the last output step's
+        Cd / Cl (iblbm/diagnostics/core.py:53-113) into the device ring buffer;
+        no host synchronisation.  Returns the entry's sequence number (read it
+        with read_force_coeffs)."""
+        from ._lib import ForceCoeffArgs
         cfg, st = self.cfg, self.st
+        a = ForceCoeffArgs()
+        a.ro, a.n_nodes, a.f32 = ptr(self.ro_out), self.N, int(self.f32)
+        a.method = 0 if self.no_ibm else IBM_IDS[self.method]
+        a.band_fib, a.band_count = ptr(self.d_fib), ptr(self.d_count)
+        a.dfc_force, a.lb_total = ptr(self.d_dfc_force), self.Lb
+        a.u_ref = float(cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u)
+        a.lattice_r = float(st.lattice_r)
+        a.partials, a.ticket = ptr(self.d_diag_part), ptr(self.d_diag_ticket)
+        a.ring, a.ring_len, a.ring_pos = ptr(self.d_ring), self.ring_len, ptr(self.d_ring_pos)
+        check(self.L.iblbm_force_coeffs(ctypes.byref(a), self.stream()), "iblbm_force_coeffs")
+        self.ring_read += 1
+        return self.ring_read - 1
+
+    def read_force_coeffs(self, first, count):
+        """Entries first .. first + count - 1 of the ring (at most ring_len
+        back) as a (count, 5) host array: Cd, Cl, mean rho, sum Fx, sum Fy.
+        Waits for the work queued on the current stream."""
+        if count <= 0:
+            return np.zeros((0, 5))
+        if count > self.ring_len or self.ring_read - first > self.ring_len:
+            raise ValueError("ring entries overwritten: read the ring at least every ring_len checks")
+        s0 = first % self.ring_len
+        n0 = min(count, self.ring_len - s0)
+        rows = self.d_ring[s0:s0 + n0].cpu().numpy()
+        if n0 < count:  # wrapped past the end of the ring
+            rows = np.concatenate([rows, self.d_ring[: count - n0].cpu().numpy()])
+        return rows
+
+    def cd_cl(self):
+        """Cd, Cl of the last output step — iblbm/diagnostics/core.py:53-113,
+        reduced on the device (iblbm_force_coeffs); 0, 0 without an immersed
+        body (iblbm/runtime/scenarios/taylor_green.py:60-62)."""
         if self.no_ibm:
-            return 0.0, 0.0  # iblbm/runtime/scenarios/taylor_green.py:60-62
-        u_ref = cfg.lattice_u if cfg.motion_type == "oscillating" else st.in_u
-        ro_mean = float(self.ro_out.double().mean())
-        denom = np.float64(ro_mean * u_ref ** 2 * st.lattice_r)
-        if self.method == "DFC":
-            force = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).sum(0).cpu().numpy()
-            sx, sy = float(force[0]), float(force[1])
-        else:
-            nb = int(self.d_count.item())
-            sx, sy = (float(v) for v in self.d_fib[: 2 * nb].reshape(nb, 2).double().sum(0).cpu())
-        with np.errstate(divide="ignore", invalid="ignore"):  # no inflow (Taylor-Green): numpy's inf / nan
-            return float(np.float64(abs(sx)) / denom), float(np.float64(sy) / denom)
+            return 0.0, 0.0
+        k = self.queue_force_coeffs()
+        r = self.read_force_coeffs(k, 1)[0]
+        return float(r[0]), float(r[1])
+
+    def velocity_change(self):
+        """Queue the velocity-convergence error of the last output step against
+        the previous check's field (iblbm/diagnostics/core.py:116-135) and make
+        this step's field the next reference; returns the device array
+        [sum (U - U_prev)^2, sum U_prev^2, error].  The first call compares
+        against zeros (error 1.0), as the reference's first check only stores
+        the field."""
+        from ._lib import VelocityChangeArgs
+        torch = self.torch
+        if self.d_uprev is None:
+            self.d_uprev = torch.zeros(2 * self.N, dtype=torch.float64, device=self.dev)
+        a = VelocityChangeArgs()
+        a.U, a.U_prev, a.n_nodes, a.f32 = ptr(self.U_out), ptr(self.d_uprev), self.N, int(self.f32)
+        a.partials, a.ticket, a.out = ptr(self.d_diag_part), ptr(self.d_diag_ticket), ptr(self.d_vchange)
+        check(self.L.iblbm_velocity_change(ctypes.byref(a), self.stream()), "iblbm_velocity_change")
+        return self.d_vchange
 
     def mdf_stats(self):
         s = self.d_stats.cpu().numpy()

@@ -5,7 +5,11 @@ state, converged, final_step, termination_reason, and sedimentation_history
 for sedimentation runs).  Between diagnostics the engine replays CUDA graphs of
 whole timesteps; at every ``check_interval`` step the moments are written out
 and Cd/Cl, the velocity-convergence error and the stop rules are evaluated as
-in the reference.
+in the reference.  Cd / Cl and the convergence error are reduced on the
+device (``iblbm_force_coeffs``, ``iblbm_velocity_change``); when no stop rule,
+callback or particle record needs them at each check, the coefficients of up
+to SPAN_CHECKS checks collect in the engine's device ring and reach the host
+in one copy, so the host never waits on the GPU between those checks.
 """
 from __future__ import annotations
 
@@ -66,17 +70,44 @@ def _near_wall(p, cfg, dx, safety=2.0):
             or x + r > cfg.xmax - margin)
 
 
+SPAN_CHECKS = 256  # checks queued on the device between host reads when no stop rule needs them
+
+
 def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine | None = None) -> dict:
     eng = engine if engine is not None else Engine(cfg)
     torch = eng.torch
     Cd_history, Cl_history, history = [], [], []
     converged, error, termination = False, 1.0, "max_steps"
-    pre_U = None
+    have_prev = False
     t0 = time.time()
     ttt = 1
     ci = int(cfg.check_interval)
     sed = eng.st.particles is not None
     d_lattice = 2.0 * eng.st.lattice_r
+    # Without a stop rule, a callback or particle records nothing at a check
+    # needs its values on the host before the run goes on: the Cd / Cl of many
+    # checks are reduced into the engine's device ring and read in one copy.
+    span = not sed and callback is None and not cfg.use_convergence and cfg.cd_convergence_tol is None
+    pending = []  # (step, ring entry or None for no immersed body)
+
+    def flush():
+        if not pending:
+            return
+        idx = [k for _, k in pending if k is not None]
+        rows = eng.read_force_coeffs(idx[0], len(idx)) if idx else None
+        r = 0
+        for step, k in pending:
+            if k is None:
+                Cd, Cl = 0.0, 0.0
+            else:
+                Cd, Cl = float(rows[r, 0]), float(rows[r, 1])
+                r += 1
+            Cd_history.append(Cd)
+            Cl_history.append(Cl)
+            if verbose:
+                print(f"step {step:>7d} | Cd={Cd:.6f} Cl={Cl:.6f} | err={error:.2e} | {time.time() - t0:.1f}s")
+        pending.clear()
+
     while True:
         if converged and (cfg.use_convergence or cfg.cd_convergence_tol is not None):
             if termination == "max_steps":
@@ -87,6 +118,13 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
         target = min(((ttt - 1) // ci + 1) * ci, cfg.max_steps)
         eng.advance(target - ttt + 1, outputs_last=True)
         ttt = target
+        if span:
+            if ttt % ci == 0:
+                pending.append((ttt, None if eng.no_ibm else eng.queue_force_coeffs()))
+            if len(pending) >= SPAN_CHECKS or ttt >= cfg.max_steps:
+                flush()
+            ttt += 1
+            continue
         if ttt % ci == 0:
             if sed:
                 rec = {"step": ttt, "particles": [
@@ -116,14 +154,12 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
                     with open(save_dir + "/sedimentation_history.json", "w") as fh:
                         json.dump(history, fh)
             if cfg.use_convergence:
-                U_now = eng.U_out.reshape(-1, 2).clone()
+                # iblbm/diagnostics/core.py:116-135, reduced on the device
                 if ttt == cfg.convergence_start:
-                    pre_U = U_now
-                elif ttt > cfg.convergence_start and pre_U is not None:
-                    # iblbm/diagnostics/core.py:116-135
-                    den = float((pre_U * pre_U).sum())
-                    error = 1.0 if den == 0.0 else math.sqrt(float(((U_now - pre_U) ** 2).sum()) / den)
-                    pre_U = U_now
+                    eng.velocity_change()  # stores this step's field as the reference
+                    have_prev = True
+                elif ttt > cfg.convergence_start and have_prev:
+                    error = float(eng.velocity_change()[2].item())
                     if error < cfg.convergence_threshold:
                         converged = True
             if (cfg.cd_convergence_tol is not None and ttt > cfg.cd_convergence_start_step
@@ -133,6 +169,7 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
                     converged = True
                     termination = "cd_converged"
         ttt += 1
+    flush()
     torch.cuda.synchronize(eng.dev)
     state = eng.read_state() if eng.last_out_step > 0 else eng.st
     result = {"Cd_history": np.array(Cd_history), "Cl_history": np.array(Cl_history), "state": state,

@@ -108,6 +108,73 @@ def history_increment(model, vel, vel_prev, mass, r_lattice):
     return None
 
 
+def pairwise_tree(n):
+    """The summation tree numpy's np.sum applies to n float64 values (its
+    pairwise summation: blocks of at most 128 values, each summed in 8 strided
+    accumulators combined as ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)) and then its
+    tail; a longer range splits at half its length rounded down to a multiple
+    of 8 and adds the two halves' sums).  Returns (leaves, inner, levels):
+    leaves an (L, 2) int32 array of (offset, length) left to right; inner an
+    (I, 2) int32 array of child ids (ids below L are leaves, inner node k has
+    id L + k) ordered by depth from the deepest, so children come before
+    parents; levels the I + 1 boundaries of the equal-depth groups.  The root
+    is the last inner node (or leaf 0 when n <= 128)."""
+    leaves, inner = [], []
+
+    def rec(off, m, depth):
+        if m <= 128:
+            leaves.append((off, m))
+            return ("L", len(leaves) - 1)
+        m2 = m // 2
+        m2 -= m2 % 8
+        a = rec(off, m2, depth + 1)
+        b = rec(off + m2, m - m2, depth + 1)
+        inner.append((a, b, depth))
+        return ("I", len(inner) - 1)
+
+    rec(0, int(n), 0)
+    L = len(leaves)
+    order = sorted(range(len(inner)), key=lambda k: -inner[k][2])  # stable: deepest first
+    pos = {k: i for i, k in enumerate(order)}
+    ids = lambda c: c[1] if c[0] == "L" else L + pos[c[1]]
+    nodes = np.array([[ids(inner[k][0]), ids(inner[k][1])] for k in order], dtype=np.int32).reshape(-1, 2)
+    depths = [inner[k][2] for k in order]
+    levels = [0] + [i for i in range(1, len(depths)) if depths[i] != depths[i - 1]] + [len(depths)]
+    return np.array(leaves, dtype=np.int32).reshape(-1, 2), nodes, np.array(levels, dtype=np.int32)
+
+
+def pairwise_sum_sparse(n, idx, val):
+    """np.sum of a length-n float64 array that is zero except val at the
+    sorted indices idx, evaluated over the pairwise_tree without the zeros
+    (a zero term leaves every partial sum unchanged): the host model of the
+    device's force sums."""
+    leaves, nodes, _ = pairwise_tree(n)
+    idx = np.asarray(idx)
+    vals = np.zeros(len(leaves) + len(nodes))
+    for li, (off, m) in enumerate(leaves):
+        lo, hi = np.searchsorted(idx, off), np.searchsorted(idx, off + m)
+        if m < 8:
+            res = 0.0
+            for b in range(lo, hi):
+                res += float(val[b])
+        else:
+            r, res, cut = [0.0] * 8, None, m - m % 8
+            tail = []
+            for b in range(lo, hi):
+                k = int(idx[b]) - off
+                if k < cut:
+                    r[k % 8] += float(val[b])
+                else:
+                    tail.append(float(val[b]))
+            res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]))
+            for v in tail:
+                res += v
+        vals[li] = res
+    for k, (a, b) in enumerate(nodes):
+        vals[len(leaves) + k] = vals[a] + vals[b]
+    return 0.0 + float(vals[-1] if len(nodes) else vals[0])
+
+
 def rigid_markers(Lx_c, Ly_c, cx0, cy0, pos, angle=0.0):
     """X = R(angle) (X_c - X_0) + x_p — iblbm/physics/markers.py:23-38."""
     c, s = np.cos(angle), np.sin(angle)

@@ -173,6 +173,13 @@ typedef struct {
     /* DFC: fluid density rho_f of lambda(k) = 1 / (2 rho_f ds W_sum(k))
      * (iblbm/ibm/dfc.py:126-186); 0 means 1.0, the solver's value */
     double dfc_rho_f;
+    /* polls of each bounded wait on a bulk copy before the step gives up with
+     * status 6 (0: the default, 2^22) */
+    long long wait_limit;
+    /* failure-path testing only (0 in normal use): 1 skips issuing a fixed
+     * body's restore copy while its wait still expects it, so the wait runs
+     * out and the step reports status 6 with no copy in flight */
+    int test_skip_copy;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -247,6 +254,11 @@ typedef struct {
     int box_blocks;
     int tile;      /* IBLBM_TILE_*: shape of the whole-lattice / bulk pass */
     int *status;   /* optional device int: set to 1 if a pipeline wait ran out */
+    /* PIPE tiles: polls of each bounded pipeline wait (0: the default, 2^24);
+     * test_skip_copy = 1 (failure-path testing only) makes the producer issue
+     * no copy, so the consumers' waits run out (status 1, nothing in flight) */
+    long long wait_limit;
+    int test_skip_copy;
 } iblbm_dense32_args;
 
 /* Tile shapes of the FP32 pass.  PIPE_RxS: persistent CTAs of R consumer warps
@@ -314,6 +326,8 @@ typedef struct {
     int field_ustride;
     const double *dvel_scale;
     double dfc_rho_f;
+    long long wait_limit;
+    int test_skip_copy;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,
@@ -387,9 +401,68 @@ typedef struct {
     const int *band_count;
     int band_capacity;
     double *forces_out;   /* optional: particles x 2, the forces of the full step */
+    /* Optional (pw_leaf NULL: a fixed tree order instead): each force as numpy
+     * sums the reference's dense n_nodes x 2 force field (np.sum, pairwise
+     * summation), bit for bit.  The summation tree depends only on n_nodes and
+     * comes from the host (iblbm_b200.physics.pairwise_tree): pw_leaf holds the
+     * (offset, length) of its pw_leaves leaf blocks left to right, pw_node the
+     * two child ids of each of its pw_internal inner nodes (ids below
+     * pw_leaves are leaves, inner node k has id pw_leaves + k), ordered by
+     * depth from the deepest, pw_level[d] .. pw_level[d + 1] the nodes of the
+     * d-th group.  band_nodes: the band's lattice indices, ascending.
+     * pw_scratch: (pw_leaves + pw_internal) x 2 x n_particles doubles. */
+    int n_nodes;
+    const int *band_nodes;
+    int pw_leaves, pw_internal, pw_levels;
+    const int *pw_leaf;
+    const int *pw_node;
+    const int *pw_level;
+    double *pw_scratch;
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);
+
+/* ---- diagnostics reduced on the device -----------------------------------
+ * Replaces the host reductions of iblbm/runtime/loop.py:97-126: Cd / Cl
+ * (iblbm/diagnostics/core.py:53-113, compute_drag_lift_coefficient) and the
+ * velocity-convergence error (core.py:116-135).  Deterministic FP64 sums in a
+ * fixed order (equal to numpy's pairwise sums up to rounding); each call is
+ * one launch that reads the output step's fields in place and leaves its
+ * result in device memory, so calls can be queued (and graph-captured)
+ * without a host synchronisation.  `partials` holds iblbm_diag_partials(n)
+ * doubles and `ticket` one unsigned zero before the first call (each call
+ * leaves it zero); calls sharing them must be ordered (one stream). */
+typedef struct {
+    const void *ro;          /* n_nodes densities of the output step (FP32 when f32, else FP64) */
+    int n_nodes;
+    int f32;
+    int method;              /* IBLBM_IBM_*: DF/MDF sum band_fib, DFC sums dfc_force, NONE no force */
+    const void *band_fib;    /* band x 2 (FP32 when f32) */
+    const int *band_count;   /* device: band nodes */
+    const double *dfc_force; /* lb_total x 2 */
+    int lb_total;
+    double u_ref, lattice_r; /* Cd = |sum Fx| / (mean(rho) u_ref^2 R), Cl = sum Fy / (...) */
+    double *partials;
+    unsigned *ticket;
+    double *ring;            /* ring_len x 5: Cd, Cl, mean rho, sum Fx, sum Fy */
+    int ring_len;
+    int *ring_pos;           /* device counter: the call writes entry (*ring_pos % ring_len), then increments */
+} iblbm_force_coeff_args;
+
+int iblbm_force_coeffs(const iblbm_force_coeff_args *a, void *stream);
+
+typedef struct {
+    const void *U;           /* n_nodes x 2 velocities of the output step (FP32 when f32) */
+    double *U_prev;          /* n_nodes x 2 FP64: the last check's field; replaced by U */
+    int n_nodes;
+    int f32;
+    double *partials;
+    unsigned *ticket;
+    double *out;             /* 3 doubles: sum (U - U_prev)^2, sum U_prev^2, the error sqrt(ratio) (1 if 0) */
+} iblbm_velocity_change_args;
+
+int iblbm_velocity_change(const iblbm_velocity_change_args *a, void *stream);
+int iblbm_diag_partials(int n_nodes);
 
 /* ---- reference-shaped kernels (AoS, one op per call, FP64) ------------- */
 /* Replaces feq_gpu (iblbm/gpu_kernels.py:906-927) <- lbm/equilibrium.py:45-50 */

@@ -32,7 +32,10 @@ def test_struct_layout_matches_c(tmp_path):
               "iblbm_dense_args": [f for f, _ in _lib.DenseArgs._fields_],
               "iblbm_ibm32_args": [f for f, _ in _lib.Ibm32Args._fields_],
               "iblbm_dense32_args": [f for f, _ in _lib.Dense32Args._fields_],
-              "iblbm_case": [f for f, _ in _lib.Case._fields_]}
+              "iblbm_case": [f for f, _ in _lib.Case._fields_],
+              "iblbm_force_coeff_args": [f for f, _ in _lib.ForceCoeffArgs._fields_],
+              "iblbm_velocity_change_args": [f for f, _ in _lib.VelocityChangeArgs._fields_],
+              "iblbm_particles_args": [f for f, _ in _lib.ParticlesArgs._fields_]}
     lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){"]
     for st, fl in fields.items():
         lines.append(f'printf("{st} %zu\\n", sizeof({st}));')
@@ -46,7 +49,9 @@ def test_struct_layout_matches_c(tmp_path):
     out = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().split("\n") if l)
     for st, cls in (("iblbm_ibm_args", _lib.IbmArgs), ("iblbm_dense_args", _lib.DenseArgs),
                     ("iblbm_ibm32_args", _lib.Ibm32Args), ("iblbm_dense32_args", _lib.Dense32Args),
-                    ("iblbm_case", _lib.Case)):
+                    ("iblbm_case", _lib.Case), ("iblbm_force_coeff_args", _lib.ForceCoeffArgs),
+                    ("iblbm_velocity_change_args", _lib.VelocityChangeArgs),
+                    ("iblbm_particles_args", _lib.ParticlesArgs)):
         assert int(out[st]) == ctypes.sizeof(cls), st
         for f, _ in cls._fields_:
             assert int(out[f"{st}.{f}"]) == getattr(cls, f).offset, (st, f)
