@@ -34,6 +34,7 @@ namespace iblbm {
 
 constexpr int PART_THREADS = 256;
 constexpr int PART_MAXP = 8;
+constexpr int PART_MAXB = 2048;  // band capacity limit of the band kernel
 
 template <typename F>
 __device__ void particle_forces(const iblbm_particles_args& a, const F* fib, double* s_force)
@@ -66,22 +67,40 @@ __device__ void particle_forces(const iblbm_particles_args& a, const F* fib, dou
 }
 
 // numpy's pairwise sum of the dense field, over the band entries only (see the
-// file comment).  val(p, c, b): component c of particle p's force at band entry b.
+// file comment).  The band's lattice indices go to shared memory; only the
+// leaves between the band's first and last index (the window, found through
+// pw_lut) are summed, and an inner node outside the window is +0.0, which its
+// parent adds like numpy adds the sum of a block of zeros.
+__device__ __forceinline__ int pw_leaf_of(const iblbm_particles_args& a, int e)
+{
+    int l = a.pw_lut[e >> 6];
+    if (l + 1 < a.pw_leaves && a.pw_leaf[2 * (l + 1)] <= e) ++l;
+    return l;
+}
+
 template <typename F>
 __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fib, double* s_force)
 {
-    const int nb = *a.band_count;
+    __shared__ int s_nodes[PART_MAXB];
+    const int nb = min(*a.band_count, PART_MAXB);
     const int P = a.n_particles, PC = 2 * P;
     const int L = a.pw_leaves;
     const size_t pstride = 2 * (size_t)a.band_capacity;
     double* v = a.pw_scratch;  // node id x PC
-    for (int li = threadIdx.x; li < L; li += PART_THREADS) {
+    for (int b = threadIdx.x; b < nb; b += PART_THREADS) s_nodes[b] = a.band_nodes[b];
+    __syncthreads();
+    if (nb == 0) {
+        if (threadIdx.x < PC) s_force[threadIdx.x] = -(0.0 + 0.0);
+        __syncthreads();
+        return;
+    }
+    const int l0 = pw_leaf_of(a, s_nodes[0]), l1 = pw_leaf_of(a, s_nodes[nb - 1]);
+    for (int li = l0 + (int)threadIdx.x; li <= l1; li += PART_THREADS) {
         const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
-        // first band entry at or after off (band nodes ascend)
-        int lo = 0, hi = nb;
+        int lo = 0, hi = nb;  // first band entry at or after off
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if (a.band_nodes[mid] < off) lo = mid + 1;
+            if (s_nodes[mid] < off) lo = mid + 1;
             else hi = mid;
         }
         const int cut = m - m % 8;
@@ -90,26 +109,34 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
             double res;
             if (m < 8) {
                 res = 0.0;
-                for (int b = lo; b < nb && a.band_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+                for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
             } else {
                 double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                 int b = lo;
-                for (; b < nb && a.band_nodes[b] < off + cut; ++b) {
-                    const int k = a.band_nodes[b] - off;
-                    r[k & 7] += (double)src[2 * (size_t)b];
-                }
+                for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += (double)src[2 * (size_t)b];
                 res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-                for (; b < nb && a.band_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+                for (; b < nb && s_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
             }
             v[(size_t)li * PC + pc] = res;
         }
     }
     __syncthreads();
+    // a child is in the window when its leaves meet [l0, l1]; outside it sums to +0.0
+    auto in_window = [&](int id) {
+        if (id < L) return id >= l0 && id <= l1;
+        const int k = id - L;
+        return a.pw_span[2 * k + 1] >= l0 && a.pw_span[2 * k] <= l1;
+    };
     for (int d = 0; d < a.pw_levels; ++d) {
         for (int k = a.pw_level[d] + threadIdx.x; k < a.pw_level[d + 1]; k += PART_THREADS) {
+            if (a.pw_span[2 * k + 1] < l0 || a.pw_span[2 * k] > l1) continue;
             const int c0 = a.pw_node[2 * k], c1 = a.pw_node[2 * k + 1];
-            for (int pc = 0; pc < PC; ++pc)
-                v[(size_t)(L + k) * PC + pc] = v[(size_t)c0 * PC + pc] + v[(size_t)c1 * PC + pc];
+            const bool w0 = in_window(c0), w1 = in_window(c1);
+            for (int pc = 0; pc < PC; ++pc) {
+                const double x0 = w0 ? v[(size_t)c0 * PC + pc] : 0.0;
+                const double x1 = w1 ? v[(size_t)c1 * PC + pc] : 0.0;
+                v[(size_t)(L + k) * PC + pc] = x0 + x1;
+            }
         }
         __syncthreads();
     }
@@ -200,9 +227,10 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
         return IBLBM_E_ARG;
     if (a->model < IBLBM_INERTIA_NONE || a->model > IBLBM_INERTIA_FENG_B2) return IBLBM_E_ARG;
     if (a->pw_leaf && (!a->pw_node && a->pw_internal > 0)) return IBLBM_E_ARG;
-    if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || a->pw_leaves < 1 || a->pw_internal < 0 ||
-                       a->pw_levels < 0 || a->n_nodes < 1))
+    if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || !a->pw_lut || !a->pw_span ||
+                       a->pw_leaves < 1 || a->pw_internal < 0 || a->pw_levels < 0 || a->n_nodes < 1))
         return IBLBM_E_ARG;
+    if (a->pw_leaf && a->band_capacity > PART_MAXB) return IBLBM_E_CAPACITY;
     particles_kernel<<<1, PART_THREADS, 0, (cudaStream_t)stream>>>(*a);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

@@ -213,9 +213,9 @@ class Engine:
         self.d_pipe_status = torch.zeros(1, dtype=i32, device=dev)
         self.graphs = {}
         self._make_dense_variants()
-        # free particles: their Verlet step on the device by default (its force
-        # sums follow numpy's pairwise order, so it equals the host step bit for
-        # bit); device_particles=False keeps the host step
+        # free particles: their Verlet step on the device by default (in the FP64
+        # form its force sums follow numpy's pairwise order, so it equals the
+        # host step bit for bit); device_particles=False keeps the host step
         self.dev_particles = False
         self._torque_ij = None
         if st.particles is not None:
@@ -265,18 +265,25 @@ class Engine:
         a.dt, a.dx = float(st.dt), float(st.dx)
         a.band_fib_part, a.band_count, a.band_capacity = ptr(self.d_fib_part), ptr(self.d_count), self.B
         a.forces_out = ptr(self.d_pforces)
-        # the force sums in numpy's pairwise order over the dense lattice field
-        from .physics import pairwise_tree
-        leaves, inner, levels = pairwise_tree(self.N)
-        self.d_pw_leaf = torch.as_tensor(leaves.reshape(-1), device=self.dev)
-        self.d_pw_node = torch.as_tensor(inner.reshape(-1) if inner.size else np.zeros(2, np.int32), device=self.dev)
-        self.d_pw_level = torch.as_tensor(levels, device=self.dev)
-        self.d_pw_scratch = torch.zeros((len(leaves) + len(inner)) * 2 * len(ps), dtype=torch.float64,
-                                        device=self.dev)
-        a.n_nodes, a.band_nodes = self.N, ptr(self.d_nodes)
-        a.pw_leaves, a.pw_internal, a.pw_levels = len(leaves), len(inner), len(levels) - 1
-        a.pw_leaf, a.pw_node, a.pw_level = ptr(self.d_pw_leaf), ptr(self.d_pw_node), ptr(self.d_pw_level)
-        a.pw_scratch = ptr(self.d_pw_scratch)
+        if not self.f32:
+            # the FP64 form sums the forces in numpy's pairwise order over the
+            # dense lattice field, so the device step equals the host step bit
+            # for bit; the FP32 form keeps the cheaper fixed-order sum
+            from .physics import pairwise_tree, pairwise_tree_index
+            leaves, inner, levels = pairwise_tree(self.N)
+            lut, span = pairwise_tree_index(self.N, leaves, inner)
+            z2 = np.zeros(2, np.int32)
+            self.d_pw_leaf = torch.as_tensor(leaves.reshape(-1), device=self.dev)
+            self.d_pw_node = torch.as_tensor(inner.reshape(-1) if inner.size else z2, device=self.dev)
+            self.d_pw_level = torch.as_tensor(levels, device=self.dev)
+            self.d_pw_lut = torch.as_tensor(lut, device=self.dev)
+            self.d_pw_span = torch.as_tensor(span.reshape(-1) if span.size else z2, device=self.dev)
+            self.d_pw_scratch = torch.zeros((len(leaves) + len(inner)) * 2 * len(ps), dtype=torch.float64,
+                                            device=self.dev)
+            a.n_nodes, a.band_nodes = self.N, ptr(self.d_nodes)
+            a.pw_leaves, a.pw_internal, a.pw_levels = len(leaves), len(inner), len(levels) - 1
+            a.pw_leaf, a.pw_node, a.pw_level = ptr(self.d_pw_leaf), ptr(self.d_pw_node), ptr(self.d_pw_level)
+            a.pw_lut, a.pw_span, a.pw_scratch = ptr(self.d_pw_lut), ptr(self.d_pw_span), ptr(self.d_pw_scratch)
         self.part_args = a
         self.part_started = False
 

@@ -143,6 +143,21 @@ def pairwise_tree(n):
     return np.array(leaves, dtype=np.int32).reshape(-1, 2), nodes, np.array(levels, dtype=np.int32)
 
 
+def pairwise_tree_index(n, leaves, nodes):
+    """Look-up tables for evaluating pairwise_tree(n) on the device: lut[i] is
+    the leaf holding element 64 i (every leaf but one holds at least 64
+    elements, so the leaf of element e is lut[e // 64] or the next one), and
+    span[k] the first and last leaf under inner node k."""
+    starts = leaves[:, 0]
+    lut = (np.searchsorted(starts, np.arange(0, int(n), 64), side="right") - 1).astype(np.int32)
+    L = len(leaves)
+    span = np.zeros((len(nodes), 2), dtype=np.int32)
+    for k, (a, b) in enumerate(nodes):  # children come before parents
+        span[k, 0] = a if a < L else span[a - L, 0]
+        span[k, 1] = b if b < L else span[b - L, 1]
+    return lut, span
+
+
 def pairwise_sum_sparse(n, idx, val):
     """np.sum of a length-n float64 array that is zero except val at the
     sorted indices idx, evaluated over the pairwise_tree without the zeros

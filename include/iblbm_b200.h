@@ -409,14 +409,18 @@ typedef struct {
      * two child ids of each of its pw_internal inner nodes (ids below
      * pw_leaves are leaves, inner node k has id pw_leaves + k), ordered by
      * depth from the deepest, pw_level[d] .. pw_level[d + 1] the nodes of the
-     * d-th group.  band_nodes: the band's lattice indices, ascending.
-     * pw_scratch: (pw_leaves + pw_internal) x 2 x n_particles doubles. */
+     * d-th group; pw_lut[i] the leaf holding element 64 i and pw_span the
+     * first and last leaf under each inner node (pairwise_tree_index).
+     * band_nodes: the band's lattice indices, ascending.  pw_scratch:
+     * (pw_leaves + pw_internal) x 2 x n_particles doubles. */
     int n_nodes;
     const int *band_nodes;
     int pw_leaves, pw_internal, pw_levels;
     const int *pw_leaf;
     const int *pw_node;
     const int *pw_level;
+    const int *pw_lut;
+    const int *pw_span;
     double *pw_scratch;
 } iblbm_particles_args;
 

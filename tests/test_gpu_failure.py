@@ -111,14 +111,16 @@ def test_fixed_body_moved_past_the_exclusion_box_reports(torch):
 
 
 def test_oscillation_table_exhausted_reports(torch):
-    """An oscillating body whose motion table holds max_steps + 2 entries:
-    stepping past it reports status 4 (the kernel reads no entry beyond)."""
+    """An oscillating body whose motion table covers its configured run
+    (entry t is the displacement of step t): stepping past the table reports
+    status 4 (the kernel reads no entry beyond it)."""
     from iblbm_b200.engine import Engine
     kw = dict(NN=97, xmax=1, ymax=1, cylinder_center=(0.5, 0.5), cylinder_D_ratio=0.125, lattice_u=0.02,
               inflow_u=0.0, bc_type="open_boundary", ibm_method="DFC", motion_type="oscillating", KC=5.0,
               nx_formula="simple", Re=20, collision_model="BGK", max_steps=10)
     e = Engine(_cfg(**kw), precision="f64")
-    e.advance(11, outputs_last=False)
+    n = int(e.xt.numel())  # steps 1 .. n - 1 have an entry
+    e.advance(n - 1, outputs_last=False)
     torch.cuda.synchronize()
     assert e.status() == 0
     e.advance(1, outputs_last=False)

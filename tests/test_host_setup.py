@@ -57,3 +57,29 @@ def test_oscillation_table_matches_reference_motion():
     assert tab[1] == 0.0
     for t in (1, 7, 50):
         assert tab[t + 1] == A * np.sin(f0 * 2.0 * np.pi * t)
+
+
+def test_pairwise_tree_reproduces_numpy_sum():
+    """The summation tree the device uses for the particle forces: evaluated
+    over only the nonzero entries of a sparse field, it equals np.sum of the
+    dense field bit for bit (lattice sizes of the sedimentation runs and random
+    ones; band-shaped and scattered nonzeros)."""
+    import numpy as np
+    from iblbm_b200.physics import pairwise_sum_sparse, pairwise_tree, pairwise_tree_index
+    rng = np.random.default_rng(7)
+    for n in (3, 64, 128, 129, 1000, 4097, 321 * 1281, 161 * 161):
+        for _ in range(3):
+            nb = int(rng.integers(1, min(n, 1500) + 1))
+            idx = np.sort(rng.choice(n, nb, replace=False))
+            val = rng.normal(size=nb) * 10.0 ** rng.integers(-6, 2)
+            dense = np.zeros((n, 2))
+            dense[idx, 0] = val
+            assert pairwise_sum_sparse(n, idx, val) == dense[:, 0].sum()
+        leaves, nodes, levels = pairwise_tree(n)
+        lut, span = pairwise_tree_index(n, leaves, nodes)
+        e = np.arange(n)
+        leaf = np.searchsorted(leaves[:, 0], e, side="right") - 1
+        assert np.all((leaf == lut[e // 64]) | (leaf == lut[e // 64] + 1))
+        if len(nodes):
+            assert tuple(span[-1]) == (0, len(leaves) - 1)
+            assert levels[0] == 0 and levels[-1] == len(nodes)
