@@ -95,11 +95,40 @@ __host__ __device__ inline bool ms_fits(size_t base, int Lb, int S)
     return Lb >= MS_W && base + ms_smem_bytes(Lb, S) <= (size_t)IBM_SMEM_LIMIT;
 }
 __device__ __forceinline__ int ms_ring(int m, int Lb) { return m + (m < 0 ? Lb : 0) - (m >= Lb ? Lb : 0); }
+
+// Node-space MDF of one body in the FP64 form, restructured for the shared
+// memory of one CTA (same operations in the same order as the plain loop, so
+// the same bits).  An iteration is bound by shared-memory traffic: gathers of
+// the band velocities and of the marker forces, FP64 words with bank
+// conflicts.  Each band node therefore walks its contribution list in
+// jagged-diagonal order (list position j of the nodes ranked by list length
+// lies contiguously), so a warp's list loads are consecutive words, and the
+// residual is one maximum over squared slips.  Shared memory after the band
+// layout: staging of the reordered lists, and per rank the node and its list
+// length, the jagged-diagonal offsets and a histogram of list lengths.
+constexpr int NSF_MAX_MARKERS = IBM_THREADS;  // one thread per marker
+__host__ __device__ inline size_t nsf_stage_bytes(int Lb, int S)
+{
+    return up16(sizeof(int) * (size_t)Lb * S) + up16(sizeof(double) * (size_t)Lb * S);
+}
+__host__ __device__ inline size_t nsf_smem_bytes(int Lb, int NB, int S)
+{
+    return nsf_stage_bytes(Lb, S) + up16(sizeof(int) * (2 * (size_t)NB + 3 * ((size_t)S + 2)));
+}
+// Whether the restructured loop runs: a body of at most NSF_MAX_MARKERS
+// markers whose extra room fits beside the band layout (`base` bytes).  Host
+// sizing and kernel use the same test.
+__host__ __device__ inline bool nsf_fits(size_t base, int Lb, int NB, int S)
+{
+    return Lb <= NSF_MAX_MARKERS && base + nsf_smem_bytes(Lb, NB, S) <= (size_t)IBM_SMEM_LIMIT;
+}
 // Barrier `id` over the first n threads of the block (n a multiple of 32).
 __device__ __forceinline__ void bar_sync_n(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 inline bool mlp_on(const iblbm_ibm_args&) { return false; }
 inline bool ms_on(const iblbm_ibm_args&) { return false; }
 inline bool ms_on(const iblbm_ibm32_args& a) { return a.method == IBM_MDF && !a.mdf_coupled; }
+inline bool nsf_on(const iblbm_ibm_args& a) { return a.method == IBM_MDF && !a.mdf_coupled; }
+inline bool nsf_on(const iblbm_ibm32_args&) { return false; }
 inline bool mlp_on(const iblbm_ibm32_args& a)
 {
     return a.mlp_mode != 0 && a.method == IBM_MDF && !a.mdf_coupled;
@@ -701,9 +730,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         // most one marker (its slot -> band map and separable weights in registers).
         const bool incomp = COUPLED && a.c.incompressible != 0;  // mdf.py always uses the compressible law
         R vs[NPT], ftx[NPT], fty[NPT];
+        int slot_node[NPT];  // the band node of each accumulator slot (-1: none)
 #pragma unroll
         for (int jn = 0; jn < NPT; ++jn) {
             const int b = tid + jn * IBM_THREADS;
+            slot_node[jn] = b < nb ? b : -1;
             vs[jn] = b < nb ? dt / ((R)2 * sh.bro[b]) : (R)0;
             ftx[jn] = 0;
             fty[jn] = 0;
@@ -939,6 +970,17 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 marker_space = !__syncthreads_or(over);
             }
         }
+        // the restructured node-space loop (FP64, one body): when its room fits
+        // and no node's list is longer than the stencil (lists of clamped edge
+        // nodes can be; they take the plain loop)
+        bool nsf = false;
+        if constexpr (!SHIFTED && !COUPLED && !GS) {
+            if (nsf_fits(Lay.total, Lb, NB, S)) {
+                int mx = 0;
+                for (int b = tid; b < nb; b += IBM_THREADS) mx = max(mx, sh.cstart[b + 1] - sh.cstart[b]);
+                nsf = !__syncthreads_or(mx > S);
+            }
+        }
         if (marker_space) {
             if constexpr (SHIFTED && !COUPLED) {
                 // MDF iterations on the markers: u_l = u0_l + sum_j A_l,j G_(l+j-MS_D)
@@ -1032,6 +1074,147 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                         spread2(sh, Gx, Gy, sh.cstart[b], sh.cstart[b + 1], tx, ty);
                         ftx[jn] += tx;
                         fty[jn] += ty;
+                    }
+                }
+            }
+        } else if (nsf) {
+            if constexpr (!SHIFTED && !COUPLED && !GS) {
+                char* xs = smem_raw + dyn_end;
+                int* rk_node = reinterpret_cast<int*>(xs + nsf_stage_bytes(Lb, S));
+                int* rk_len = rk_node + NB;
+                int* jd_off = rk_len + NB;     // S + 2: list position j starts at jd_off[j]
+                int* hist = jd_off + (S + 2);  // S + 2: nodes per list length
+                int* cur = hist + (S + 2);     // S + 2: rank cursors per list length
+                // ---- lists in jagged-diagonal order ---------------------------------
+                if (tid < S + 2) hist[tid] = 0;
+                __syncthreads();
+                for (int b = tid; b < nb; b += IBM_THREADS) atomicAdd(&hist[sh.cstart[b + 1] - sh.cstart[b]], 1);
+                __syncthreads();
+                if (tid == 0) {
+                    // ranks by decreasing length: nodes of length n start after every longer one
+                    int acc = 0;
+                    for (int n = S; n >= 0; --n) { cur[n] = acc; acc += hist[n]; }
+                    // position j holds the nodes longer than j: ranks 0 .. cur[j] - 1
+                    int off = 0;
+                    for (int j = 0; j <= S; ++j) { jd_off[j] = off; off += cur[j]; }
+                    jd_off[S + 1] = off;
+                }
+                __syncthreads();
+                for (int b = tid; b < nb; b += IBM_THREADS) {
+                    const int n = sh.cstart[b + 1] - sh.cstart[b];
+                    const int r = atomicAdd(&cur[n], 1);  // any order within a length class
+                    rk_node[r] = b;
+                    rk_len[r] = n;
+                }
+                __syncthreads();
+                int* jl = reinterpret_cast<int*>(xs);                                    // staging: marker of entry
+                R* jw = reinterpret_cast<R*>(xs + up16(sizeof(int) * (size_t)Lb * S));  // staging: its weight
+                for (int r = tid; r < nb; r += IBM_THREADS) {
+                    const int b = rk_node[r], u0 = sh.cstart[b];
+                    for (int j = 0; j < rk_len[r]; ++j) {
+                        jl[jd_off[j] + r] = sh.ent[u0 + j] >> 5;
+                        jw[jd_off[j] + r] = sh.entw[u0 + j];
+                    }
+                }
+                __syncthreads();
+                for (int u = tid; u < Lb * S; u += IBM_THREADS) {  // the plain lists are not read again this step
+                    sh.ent[u] = jl[u];
+                    sh.entw[u] = jw[u];
+                }
+                // ---- per thread: its accumulator slots (ranks) and its marker slots ----
+#pragma unroll
+                for (int jn = 0; jn < NPT; ++jn) {
+                    const int r = tid + jn * IBM_THREADS;
+                    slot_node[jn] = r < nb ? rk_node[r] : -1;
+                    vs[jn] = r < nb ? dt / ((R)2 * sh.bro[rk_node[r]]) : (R)0;
+                }
+                __syncthreads();
+                for (int it = 0; it < a.mdf_iterations; ++it) {
+                    unsigned long long* wk = reinterpret_cast<unsigned long long*>(sh.wred) + (it & 1) * NWARP;
+                    const R omega = (R)omega_d;
+                    // phase A: interpolate the working velocity (one thread per marker, slots in
+                    // order), squared slip, force
+                    unsigned long long key = 0;  // squared slip as its bit pattern
+                    if (own) {
+                        R ux = 0, uy = 0;
+#pragma unroll
+                        for (int gi = 0; gi < SW; ++gi) {
+                            R vx[SW], vy[SW];
+#pragma unroll
+                            for (int gj = 0; gj < SW; ++gj) {
+                                const int bk = sh.sidx[lo * S + gi * SW + gj];
+                                vx[gj] = sh.bwx[bk];
+                                vy[gj] = sh.bwy[bk];
+                            }
+#pragma unroll
+                            for (int gj = 0; gj < SW; ++gj) {
+                                const R w = sh.wx[lo * 5 + gi] * sh.wy[lo * 5 + gj];
+                                ux += vx[gj] * w;
+                                uy += vy[gj] * w;
+                            }
+                        }
+                        sh.Lux[lo] = ux;
+                        sh.Luy[lo] = uy;
+                        const double ex = (double)dvx - (double)ux, ey = (double)dvy - (double)uy;
+                        key = (unsigned long long)__double_as_longlong(ex * ex + ey * ey);
+                        const R fx = (R)2 * Rl * (dvx - ux), fy = (R)2 * Rl * (dvy - uy);
+                        sh.Lfx[lo] = unit_dt ? fx : fx / dt;
+                        sh.Lfy[lo] = unit_dt ? fy : fy / dt;
+                    }
+                    // residual = max_l sqrt(slip^2) = sqrt(max_l slip^2): sqrt is monotone and
+                    // correctly rounded; the max runs on the bit patterns (NaN above all numbers)
+                    const unsigned long long wmax = warp_max_bits(key);
+                    if (lane == 0) wk[wid] = wmax;
+                    __syncthreads();  // (a)
+                    const double residual =
+                        sqrt(__longlong_as_double((long long)warp_max_bits(lane < NWARP ? wk[lane] : 0ull)));
+                    last = residual;
+                    if (it > 0 && residual > prev * 1.5) {
+                        diverged = 1;
+                        iter_count = it + 1;
+                        break;
+                    }
+                    // phase B: spread, relax, update the working velocity of the owned nodes
+#pragma unroll
+                    for (int jn = 0; jn < NPT; ++jn) {
+                        const int r = tid + jn * IBM_THREADS;
+                        if (r < nb) {
+                            const int n = rk_len[r];
+                            R ax = 0, ay = 0;
+                            int j = 0;
+                            for (; j + 4 <= n; j += 4) {
+                                const int u0 = jd_off[j] + r, u1 = jd_off[j + 1] + r;
+                                const int u2 = jd_off[j + 2] + r, u3 = jd_off[j + 3] + r;
+                                const int l0 = sh.ent[u0], l1 = sh.ent[u1], l2 = sh.ent[u2], l3 = sh.ent[u3];
+                                const R w0 = sh.entw[u0], w1 = sh.entw[u1], w2 = sh.entw[u2], w3 = sh.entw[u3];
+                                const R p0 = sh.Lfx[l0] * w0, p1 = sh.Lfx[l1] * w1, p2 = sh.Lfx[l2] * w2,
+                                        p3 = sh.Lfx[l3] * w3;
+                                const R q0 = sh.Lfy[l0] * w0, q1 = sh.Lfy[l1] * w1, q2 = sh.Lfy[l2] * w2,
+                                        q3 = sh.Lfy[l3] * w3;
+                                ax += p0; ax += p1; ax += p2; ax += p3;
+                                ay += q0; ay += q1; ay += q2; ay += q3;
+                            }
+                            for (; j < n; ++j) {
+                                const int u = jd_off[j] + r;
+                                const int l = sh.ent[u];
+                                const R w = sh.entw[u];
+                                ax += sh.Lfx[l] * w;
+                                ay += sh.Lfy[l] * w;
+                            }
+                            const R tx = ax * omega, ty = ay * omega;
+                            ftx[jn] += tx;
+                            fty[jn] += ty;
+                            const int b = slot_node[jn];
+                            sh.bwx[b] += tx * vs[jn];
+                            sh.bwy[b] += ty * vs[jn];
+                        }
+                    }
+                    __syncthreads();  // (b)
+                    prev = residual;
+                    iter_count = it + 1;
+                    if ((it + 1) >= min_iter && residual < a.mdf_tol) {
+                        converged = 1;
+                        break;
                     }
                 }
             }
@@ -1171,8 +1354,8 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         }
 #pragma unroll
         for (int jn = 0; jn < NPT; ++jn) {
-            const int b = tid + jn * IBM_THREADS;
-            if (b < nb) {
+            const int b = slot_node[jn];
+            if (b >= 0) {
                 a.band_fib[2 * b] = ftx[jn];
                 a.band_fib[2 * b + 1] = fty[jn];
                 if (!COUPLED && a.band_fib_part) {
@@ -1185,7 +1368,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
             a.stats[0] = iter_count;
             a.stats[1] = diverged;
             a.stats[2] = converged;
-            a.stats[3] = guard;
+            a.stats[3] = nsf ? -2 : guard;
             a.dstats[0] = last;
             a.dstats[1] = omega_d;
         }
@@ -1337,6 +1520,8 @@ static size_t ibm_smem(const ARGS& a, bool gs = false)
     size_t t = L.total - (gs ? L.static_bytes : 0);
     if (mlp_on(a)) t += mlp_smem_bytes(a.lb_total);
     if (ms_on(a) && ms_fits(t, a.lb_total, S)) t += ms_smem_bytes(a.lb_total, S);
+    if (!gs && nsf_on(a) && nsf_fits(t, a.lb_total, a.band_capacity, S))
+        t += nsf_smem_bytes(a.lb_total, a.band_capacity, S);
     return t;
 }
 

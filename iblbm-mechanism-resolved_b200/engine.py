@@ -889,6 +889,7 @@ class Engine:
         d = self.d_dstats.cpu().numpy()
         return {"iter_count": int(s[0]), "diverged": bool(s[1]), "converged": bool(s[2]),
                 "guard_trips": max(int(s[3]), 0), "marker_space": int(s[3]) == -1,
+                "restructured_node_space": int(s[3]) == -2,
                 "last_residual": float(d[0]), "omega_used": float(d[1])}
 
     def status(self):

@@ -157,7 +157,8 @@ typedef struct {
     double *Lux, *Luy, *Lfx, *Lfy, *dfc_force;
     /* stats: [iter_count, diverged, converged, guard_trips, status]
      * (guard_trips: coupled MDF; -1 when the FP32 band step ran a single
-     * body's MDF iterations in marker space), dstats: [last_residual, omega_used] */
+     * body's MDF iterations in marker space, -2 when the FP64 step ran them in
+     * the restructured node-space loop), dstats: [last_residual, omega_used] */
     int *stats;
     double *dstats;
     /* reference-shaped calls (iblbm/gpu_kernels.py:956-1223): the band takes
