@@ -748,73 +748,83 @@ def measure_case(cfg_fn, precision, K, W, flush, sink, e2e_steps):
 
 
 # ---- learned warm start -------------------------------------------------------------------
-def measure_learned(args, n_train=200, K=200):
-    """The learned MDF warm start on the single-case workload (FP32 form).
+def measure_learned(cfg, n_train, K):
+    """The learned MDF warm start (FP32 form) against plain MDF at the same
+    residual, step by step.
 
-    Plain MDF (the workload's 20 iterations per step) records n_train steps of
-    (features, accumulated force) pairs and its final slip residual; the
-    network is trained on them (GPU kernels); then two copies of that state
-    continue K steps, warm-started and plain, both iterating until the slip residual is
-    below the level plain MDF reached in 20 iterations (median over the last
-    50 training steps).  Reports both forms' step rate, mean iterations and
-    residual, and Cd against the FP64 form at the same step."""
+    Plain MDF at 20 iterations per step records n_train steps of (features,
+    accumulated force) pairs; the network is trained on them (GPU kernels).
+    A second engine, in the same state, then steps alongside the warm-started
+    one for K steps: at each step the warm-started loop iterates until its slip
+    residual is down to what plain MDF reached in its 20 iterations at that
+    step (20 at most).  Reports both step times (CUDA events around each
+    engine's whole step), the mean iterations and the steps that reached the
+    residual."""
     import torch
     from iblbm_b200.autotune import tune_dense
     from iblbm_b200.engine import Engine
     from iblbm_b200.learned import MdfNet, collect
-    total = n_train + K + 8
-    cfg = workload_config(max_steps=total + 8)
-    cfg.mdf_min_iterations = 20
-    engs = {}
-    for name in ("warm", "plain"):
-        e = Engine(cfg, precision="f32")
+    cfg.mdf_iterations, cfg.mdf_min_iterations, cfg.mdf_tolerance = 20, 20, 1e-12
+    cfg.max_steps = n_train + K + 16
+    plain, warm = Engine(cfg, precision="f32"), Engine(cfg, precision="f32")
+    for e in (plain, warm):
         tune_dense(e)
-        engs[name] = e
-    X, T, _ = collect(engs["warm"], n_train)
-    res = []
+    X, T, _ = collect(warm, n_train)
     for _ in range(n_train):
-        engs["plain"].advance(1, outputs_last=False, use_graph=False)
-        res.append(float(engs["plain"].d_dstats[0].item()))
-    tol = statistics.median(res[-50:])
+        plain.advance(1, outputs_last=False, use_graph=False)
+    torch.cuda.synchronize()
     net = MdfNet(seed=0)
-    hist = net.fit(X, T, epochs=80, batch=512, lr=2e-3)
-    engs["warm"].set_mlp(mode=2, net=net)
-    out = {"train_pairs": int(X.shape[0]), "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
-           "tolerance": tol}
+    t0 = time.perf_counter()
+    hist = net.fit(X, T, epochs=40, batch=512, lr=2e-3)
+    train_s = time.perf_counter() - t0
     E = lambda: torch.cuda.Event(enable_timing=True)
-    for name, e in engs.items():
-        for a in e.ibm_args:
-            a.mdf_min_iterations = 1
-            a.mdf_tol = tol
-        e.graphs = {}
-        its, resid = [], []
-        ev = [(E(), E()) for _ in range(K)]
-        for k in range(K):
-            ev[k][0].record()
+    # the network alone (iblbm_mlp_infer, tensor-core layers) on one body's markers
+    xb = X[: warm.Lb].contiguous()
+    for _ in range(10):
+        net.predict(xb)
+    i0, i1 = E(), E()
+    i0.record()
+    for _ in range(100):
+        net.predict(xb)
+    i1.record()
+    torch.cuda.synchronize()
+    infer_us = i0.elapsed_time(i1) / 100 * 1e3
+    warm.set_mlp(mode=2, net=net)
+    for a in warm.ibm_args:
+        a.mdf_min_iterations = 1
+    ms = {"plain": [], "warm": []}
+    its, conv = [], []
+    for k in range(K):
+        for name, e in (("plain", plain), ("warm", warm)):
+            if name == "warm":
+                r = float(plain.d_dstats[0].item())
+                for a in e.ibm_args:
+                    a.mdf_tol = r * (1.0 + 1e-6)
+            e0, e1 = E(), E()
+            e0.record()
             e._launch(False)
             e.join()
-            ev[k][1].record()
-            its.append(e.d_stats[0].clone())
-            resid.append(e.d_dstats[0].clone())
-        torch.cuda.synchronize()
-        e.ttt += K
-        ms = sum(a.elapsed_time(b) for a, b in ev) / K
+            e1.record()
+            e.ttt += 1
+            torch.cuda.synchronize()
+            ms[name].append(e0.elapsed_time(e1))
+        its.append(int(warm.d_stats[0].item()))
+        conv.append(int(warm.d_stats[2].item()))
+    for e in (plain, warm):
         e.advance(1, outputs_last=True, use_graph=False)
-        torch.cuda.synchronize()
-        its = [int(x.item()) for x in its]
-        resid = [float(x.item()) for x in resid]
-        out[name] = {"mlups": e.N / (ms / 1e3) / 1e6, "ms_per_step": ms, "mean_iterations": statistics.mean(its),
-                     "max_residual": max(resid), "steps_at_tolerance": sum(r < tol for r in resid),
-                     "Cd": e.cd_cl()[0], "step": e.ttt - 1}
-    ref = Engine(cfg, precision="f64")
-    ref.advance(engs["warm"].ttt - 1, outputs_last=True)
     torch.cuda.synchronize()
-    cd64 = ref.cd_cl()[0]
-    for name in ("warm", "plain"):
-        out[name]["cd_rel_err_vs_f64"] = abs(out[name]["Cd"] - cd64) / abs(cd64)
-    out["iterations_saved"] = out["plain"]["mean_iterations"] - out["warm"]["mean_iterations"]
-    out["speedup_vs_plain_fp32"] = out["warm"]["mlups"] / out["plain"]["mlups"]
-    return out
+    cdp, cdw = plain.cd_cl()[0], warm.cd_cl()[0]
+    mp, mw = statistics.median(ms["plain"]), statistics.median(ms["warm"])
+    return {"train_pairs": int(X.shape[0]), "train_epochs": 40, "train_s": train_s,
+            "infer_us_per_body": infer_us, "markers": warm.Lb, "loss_first_epoch": hist[0],
+            "loss_last_epoch": hist[-1], "steps_train": n_train, "steps_eval": K,
+            "plain": {"iterations": 20, "ms_per_step_median": mp, "mlups": plain.N / (mp / 1e3) / 1e6},
+            "warm": {"mean_iterations": statistics.mean(its), "ms_per_step_median": mw,
+                     "mlups": warm.N / (mw / 1e3) / 1e6, "steps_at_plain_residual": sum(conv)},
+            "iterations_saved": 20 - statistics.mean(its), "speedup_vs_plain_fp32": mp / mw,
+            "cd_rel_diff_warm_vs_plain": abs(cdw - cdp) / abs(cdp),
+            "how": "per-step residual matching: the warm-started loop iterates to the residual plain MDF reached "
+                   "in 20 iterations at the same step"}
 
 
 # ---- the run ---------------------------------------------------------------------------------
@@ -872,7 +882,12 @@ def run_b200(args):
             for f in (f64, f32):
                 if "hbm_gbs_bulk" in f:
                     f["roofline_frac_bulk"] = f["hbm_gbs_bulk"] / peak
-    learned = measure_learned(args) if args.form == "chosen" and not args.skip_learned else None
+    learned = None
+    if args.form == "chosen" and not args.skip_learned:
+        # config 3's motion sets the markers' desired velocity to their displacement (up to 32
+        # lattice units per step), so its flow stays meaningful only for its first ~100 steps
+        learned = {"config3_mdf": measure_learned(config3(method="MDF"), 60, 40),
+                   "config2": measure_learned(workload_config(), 200, 200)}
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -940,7 +955,7 @@ def run_b200(args):
     line["chosen_single_case"] = single_s
     line.update(c35)
     if learned:
-        line["learned_mdf_single_case"] = learned
+        line["learned_mdf"] = learned
     print(json.dumps(line))
     if args.accuracy_out and acc:
         with open(args.accuracy_out, "w") as fh:

@@ -118,7 +118,8 @@ _SIGS = {
     "iblbm_ibm_step_f32_batch": [ctypes.POINTER(Ibm32Args), _vp, _i, _vp],
     "iblbm_mlp_param_count": [],
     "iblbm_mlp_infer": [_vp, _vp, _i, _vp, _vp],
-    "iblbm_mlp_train_step": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_float, _i, _vp, _i, _vp],
+    "iblbm_mlp_grad_floats": [_i],
+    "iblbm_mlp_train_step": [_vp, _vp, _vp, _vp, _vp, _vp, _i, ctypes.c_float, _i, _vp, _i, _vp],
     "iblbm_dense_step_f32_batch": [ctypes.POINTER(Dense32Args), _i, _vp],
     "iblbm_dense_step_f64_batch": [ctypes.POINTER(DenseArgs), _i, _vp],
     "iblbm_ibm_step_f64_batch": [ctypes.POINTER(IbmArgs), _vp, _i, _vp],

@@ -69,12 +69,16 @@ constexpr int MLP_CHUNK = IBM_THREADS / 4;  // markers per network tile (128)
 
 // Shared memory of the learned warm start, placed after the band layout: two
 // activation tiles, the outputs of a tile, the predicted force per marker, and
-// the network's parameter block (restored by one bulk copy at kernel start).
+// the header of the network's parameter block (restored by one bulk copy at
+// kernel start).
 __host__ __device__ inline size_t mlp_act_bytes(int Lb)
 {
-    return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * MLP_LD + 2 * MLP_CHUNK + 4 * (size_t)Lb));
+    return up16(sizeof(float) * ((size_t)2 * MLP_CHUNK * MLP_LD + 2 * MLP_CHUNK + 4 * (size_t)Lb + MLP_WBUF));
 }
-__host__ __device__ inline size_t mlp_smem_bytes(int Lb) { return mlp_act_bytes(Lb) + sizeof(float) * MLP_NP; }
+// (only the parameter block's header, the feature normalisation and target
+// scales, is copied; the layers read their weights from global memory, where
+// the 57 KB block stays in L1 / L2)
+__host__ __device__ inline size_t mlp_smem_bytes(int Lb) { return mlp_act_bytes(Lb) + sizeof(float) * MLP_HDR; }
 
 // Marker-space MDF of the FP32 form: row l of the marker coupling matrix keeps
 // the markers l - MS_D .. l + MS_D (neighbours along the body).
@@ -424,12 +428,12 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
         }
     };
     if constexpr (SHIFTED && METHOD == IBM_MDF && !COUPLED) {
-        // the warm start's network: one bulk copy into shared memory, waited for
+        // the warm start's normalisation header: one bulk copy into shared memory, waited for
         // just before its first use
         if (tid == 0 && (a.mlp_mode & 2)) {
             mbar_init(&s_wbar);
-            mbar_expect(&s_wbar, (uint32_t)(sizeof(float) * MLP_NP));
-            bulk_copy(smem_raw + dyn_end + mlp_act_bytes(Lb), a.mlp_params, (uint32_t)(sizeof(float) * MLP_NP),
+            mbar_expect(&s_wbar, (uint32_t)(sizeof(float) * MLP_HDR));
+            bulk_copy(smem_raw + dyn_end + mlp_act_bytes(Lb), a.mlp_params, (uint32_t)(sizeof(float) * MLP_HDR),
                       &s_wbar);
         }
     }
@@ -777,6 +781,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                 float* mY = mB + MLP_CHUNK * MLP_LD;
                 float* mGx = mY + MLP_CHUNK * 2;
                 float* mGy = mGx + Lb;
+                float* mWb = mGy + 3 * Lb;  // one hidden layer's weights (after the slips mSx, mSy)
                 const float* Pm = reinterpret_cast<const float*>(smem_raw + dyn_end + mlp_act_bytes(Lb));
                 bool use_net = false;
                 if (warm) {
@@ -809,10 +814,11 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                             if (grow) grow[i] = v;
                             if (use_net) row[i] = (v - Pm[i]) * Pm[64 + i];
                         };
-#pragma unroll
+#pragma unroll 1
                         for (int k = 0; k < S; ++k) {
-                            put(2 + 2 * k, sh.bwx[hb[k]] * inv_u);
-                            put(3 + 2 * k, sh.bwy[hb[k]] * inv_u);
+                            const int bk = sh.sidx[lo * S + k];
+                            put(2 + 2 * k, sh.bwx[bk] * inv_u);
+                            put(3 + 2 * k, sh.bwy[bk] * inv_u);
                         }
                         for (int k = S; k < 25; ++k) { put(2 + 2 * k, 0.0f); put(3 + 2 * k, 0.0f); }
                         put(0, mSx[lo]);
@@ -841,7 +847,7 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
                     }
                     __syncthreads();
                     if (use_net) {
-                        mlp_forward_tile<IBM_THREADS>(Pm, mA, mB, mY, rows);
+                        mlp_forward_tile<IBM_THREADS>(a.mlp_params, mA, mB, mY, rows, mWb);
                         if (own && lo >= c0 && lo < c0 + rows) {
                             mGx[lo] = mY[(lo - c0) * 2] / Pm[128];
                             mGy[lo] = mY[(lo - c0) * 2 + 1] / Pm[129];

@@ -1,11 +1,15 @@
 // mlp_f32.cu — fused training and inference kernels of the learned MDF warm start.
 //
-// Training step (one launch): every CTA takes 64 samples, runs the forward pass
-// keeping all activations in shared memory, back-propagates the mean squared
-// error, and adds its weight and bias gradients into one global gradient
-// buffer; the last CTA to finish (counted with an atomic ticket after a memory
-// fence, no waiting) applies the Adam update to every parameter and clears the
-// buffer for the next step.  Inference: 128 samples per CTA.
+// Training step (two launches, no atomics, the same bits on every run): every
+// CTA of the first kernel takes 64 samples, runs the forward pass keeping all
+// activations in shared memory, back-propagates the mean squared error and
+// writes its own weight and bias gradients (and its share of the loss) to its
+// slot of the gradient buffer; the second kernel sums the CTAs' slots in CTA
+// order for every parameter and applies the Adam update (or leaves the summed
+// gradient).  The three 64 x 64 layers' forward products, their weight
+// gradients (A^T D) and the back-propagated deltas (D W^T) all run on the
+// tensor cores (mlp.cuh tc_gemm64); the 64 -> 2 output layer stays on CUDA
+// cores.  Inference: 128 samples per CTA.
 #include <cstdint>
 #include "mlp.cuh"
 #include "../../include/iblbm_b200.h"
@@ -13,16 +17,16 @@
 namespace iblbm {
 
 constexpr int TRAIN_ROWS = 64;
-constexpr int TRAIN_THREADS = 256;
+constexpr int TRAIN_THREADS = 256;  // 8 warps: the 64 x 64 products in 16 x 32 blocks
 constexpr int INFER_THREADS = 512;
 constexpr int INFER_ROWS = INFER_THREADS / 4;  // 128
+constexpr int REDUCE_THREADS = 256;
+constexpr int GRAD_SLOT = MLP_NP + 4;  // one CTA's gradient, then its loss, padded to 16 bytes
 constexpr float ADAM_B1 = 0.9f, ADAM_B2 = 0.999f, ADAM_EPS = 1e-8f;
 
-// Smem layout of the training kernel (floats): A0..A3 activations, two delta
-// buffers, the staged weight matrix (row stride 65), outputs and output deltas.
 static_assert(TRAIN_ROWS == TRAIN_THREADS / 4, "one layer tile per CTA");
 constexpr int TR_A = TRAIN_ROWS * MLP_LD;
-constexpr size_t TRAIN_SMEM = sizeof(float) * (size_t)(4 * TR_A + 2 * TR_A + 64 * 65 + 2 * TRAIN_ROWS * 2);
+constexpr size_t TRAIN_SMEM = sizeof(float) * (size_t)(4 * TR_A + 2 * TR_A + 2 * TRAIN_ROWS * 2 + 32);
 
 // Normalised input tile: rows beyond n are zero.
 __device__ __forceinline__ void load_inputs(const float* __restrict__ P, const float* __restrict__ X, int r0, int rows,
@@ -34,57 +38,57 @@ __device__ __forceinline__ void load_inputs(const float* __restrict__ P, const f
     }
 }
 
-// gW[i][o] += sum_m A[m][i] D[m][o], gb[o] += sum_m D[m][o]  (64 x 64, TRAIN_ROWS rows)
-__device__ __forceinline__ void grad_w64(const float* A, const float* D, float* gW, float* gb)
+// g[W + i * MLP_WLD + o] = sum_m A[m][i] D[m][o] (tensor cores), g[b + o] =
+// sum_m D[m][o], and the 8 unused floats of every weight row are zero.
+__device__ __forceinline__ void grad_layer(const float* A, const float* D, float* g, int W, int b)
 {
-    const int o = threadIdx.x & 63, g = threadIdx.x >> 6, G = blockDim.x >> 6;
-    float acc[16];
+    float acc[4][4];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) acc[k] = 0.0f;
-    for (int m = 0; m < TRAIN_ROWS; ++m) {
-        const float d = D[m * MLP_LD + o];
+    for (int t = 0; t < 4; ++t)
 #pragma unroll
-        for (int k = 0; k < 16; ++k) acc[k] += A[m * MLP_LD + g + k * G] * d;
-    }
+        for (int e = 0; e < 4; ++e) acc[t][e] = 0.0f;
+    // C(i, o) = sum_m A(i, m) B(m, o) with A(i, m) = A[m][i], B(m, o) = D[m][o]
+    tc_gemm64<64>(A, 1, MLP_LD, D, MLP_LD, 1, acc);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) atomicAdd(gW + (g + k * G) * 64 + o, acc[k]);
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int i, o;
+            tc_coords<64>(t, e, i, o);
+            g[W + i * MLP_WLD + o] = acc[t][e];
+        }
+    for (int e = threadIdx.x; e < 64 * (MLP_WLD - 64); e += blockDim.x)
+        g[W + (e >> 3) * MLP_WLD + 64 + (e & 7)] = 0.0f;
     if (threadIdx.x < 64) {
         float s = 0.0f;
         for (int m = 0; m < TRAIN_ROWS; ++m) s += D[m * MLP_LD + threadIdx.x];
-        atomicAdd(gb + threadIdx.x, s);
+        g[b + threadIdx.x] = s;
     }
 }
 
-// Din[m][i] = (A[m][i] > 0) * sum_o W[i][o] Dout[m][o] with W staged in sW (stride 65)
-__device__ __forceinline__ void backprop64(const float* __restrict__ W, float* sW, const float* Dout, const float* A,
-                                           float* Din)
+// Din[m][i] = (A[m][i] > 0) * sum_o Dout[m][o] W[i][o] (tensor cores)
+__device__ __forceinline__ void backprop_layer(const float* __restrict__ W, const float* Dout, const float* A, float* Din)
 {
-    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) sW[(e >> 6) * 65 + (e & 63)] = __ldg(W + e);
-    __syncthreads();
-    const int i = threadIdx.x & 63, g = threadIdx.x >> 6, G = blockDim.x >> 6;
-    float acc[16];
+    float acc[4][4];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) acc[k] = 0.0f;
-    for (int o = 0; o < 64; ++o) {
-        const float w = sW[i * 65 + o];
+    for (int t = 0; t < 4; ++t)
 #pragma unroll
-        for (int k = 0; k < 16; ++k) acc[k] += Dout[(g + k * G) * MLP_LD + o] * w;
-    }
+        for (int e = 0; e < 4; ++e) acc[t][e] = 0.0f;
+    // C(m, i) = sum_o A(m, o) B(o, i) with A(m, o) = Dout[m][o], B(o, i) = W[i][o]
+    tc_gemm64<64>(Dout, MLP_LD, 1, W, 1, MLP_WLD, acc);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const int m = g + k * G;
-        Din[m * MLP_LD + i] = A[m * MLP_LD + i] > 0.0f ? acc[k] : 0.0f;
-    }
-    __syncthreads();
+    for (int t = 0; t < 4; ++t)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            int m, i;
+            tc_coords<64>(t, e, m, i);
+            Din[m * MLP_LD + i] = A[m * MLP_LD + i] > 0.0f ? acc[t][e] : 0.0f;
+        }
 }
 
-__global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restrict__ P, float* __restrict__ am,
-                                                                  float* __restrict__ av, float* __restrict__ grad,
-                                                                  unsigned* __restrict__ ticket,
-                                                                  const float* __restrict__ X,
-                                                                  const float* __restrict__ T, int n, float lr,
-                                                                  float c1, float c2, float* __restrict__ loss,
-                                                                  int apply)
+__global__ void __launch_bounds__(TRAIN_THREADS) mlp_grad_kernel(const float* __restrict__ P, float* __restrict__ grad,
+                                                                 const float* __restrict__ X,
+                                                                 const float* __restrict__ T, int n)
 {
     extern __shared__ __align__(16) float sm[];
     float* A0 = sm;
@@ -93,18 +97,18 @@ __global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restr
     float* A3 = A2 + TR_A;
     float* Da = A3 + TR_A;
     float* Db = Da + TR_A;
-    float* sW = Db + TR_A;
-    float* Y = sW + 64 * 65;
+    float* Y = Db + TR_A;
     float* D4 = Y + TRAIN_ROWS * 2;
-    __shared__ int s_last;
+    float* red = D4 + TRAIN_ROWS * 2;  // 8 warp partial losses
+    float* g = grad + (size_t)GRAD_SLOT * (1 + blockIdx.x);
     const int r0 = blockIdx.x * TRAIN_ROWS, rows = min(TRAIN_ROWS, n - r0);
     load_inputs(P, X, r0, rows, TRAIN_ROWS, A0);
     __syncthreads();
-    mlp_layer64<TRAIN_THREADS>(P + MLP_W1, P + MLP_B1, A0, A1, true);
+    mlp_layer64_tc<TRAIN_ROWS>(P + MLP_W1, P + MLP_B1, A0, A1, true);
     __syncthreads();
-    mlp_layer64<TRAIN_THREADS>(P + MLP_W2, P + MLP_B2, A1, A2, true);
+    mlp_layer64_tc<TRAIN_ROWS>(P + MLP_W2, P + MLP_B2, A1, A2, true);
     __syncthreads();
-    mlp_layer64<TRAIN_THREADS>(P + MLP_W3, P + MLP_B3, A2, A3, true);
+    mlp_layer64_tc<TRAIN_ROWS>(P + MLP_W3, P + MLP_B3, A2, A3, true);
     __syncthreads();
     mlp_layer_out(P, A3, Y, TRAIN_ROWS);
     __syncthreads();
@@ -120,55 +124,72 @@ __global__ void __launch_bounds__(TRAIN_THREADS) mlp_train_kernel(float* __restr
         }
         D4[e] = d;
     }
-    if (loss) {
 #pragma unroll
-        for (int s = 16; s > 0; s >>= 1) part += __shfl_xor_sync(0xffffffffu, part, s);
-        if ((threadIdx.x & 31) == 0 && part != 0.0f) atomicAdd(loss, part / (float)n);
-    }
+    for (int s = 16; s > 0; s >>= 1) part += __shfl_xor_sync(0xffffffffu, part, s);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
+    if (threadIdx.x == 0) {
+        float L = 0.0f;
+        for (int w = 0; w < TRAIN_THREADS / 32; ++w) L += red[w];  // warps in order
+        g[MLP_NP] = L / (float)n;
+    }
     // output layer: gW4[i][o] = sum_m A3[m][i] D4[m][o], gb4; D3 = (D4 W4^T) * (A3 > 0)
     for (int e = threadIdx.x; e < 64 * 2; e += blockDim.x) {
         const int i = e >> 1, o = e & 1;
         float s = 0.0f;
         for (int m = 0; m < TRAIN_ROWS; ++m) s += A3[m * MLP_LD + i] * D4[m * 2 + o];
-        atomicAdd(grad + MLP_W4 + e, s);
+        g[MLP_W4 + e] = s;
     }
     if (threadIdx.x < 2) {
         float s = 0.0f;
         for (int m = 0; m < TRAIN_ROWS; ++m) s += D4[m * 2 + threadIdx.x];
-        atomicAdd(grad + MLP_B4 + threadIdx.x, s);
+        g[MLP_B4 + threadIdx.x] = s;
     }
+    for (int p = MLP_B4 + 2 + threadIdx.x; p < MLP_NP; p += blockDim.x) g[p] = 0.0f;
     for (int e = threadIdx.x; e < TRAIN_ROWS * 64; e += blockDim.x) {
         const int m = e >> 6, i = e & 63;
         const float s = __ldg(P + MLP_W4 + i * 2) * D4[m * 2] + __ldg(P + MLP_W4 + i * 2 + 1) * D4[m * 2 + 1];
         Da[m * MLP_LD + i] = A3[m * MLP_LD + i] > 0.0f ? s : 0.0f;
     }
     __syncthreads();
-    grad_w64(A2, Da, grad + MLP_W3, grad + MLP_B3);
-    backprop64(P + MLP_W3, sW, Da, A2, Db);
-    grad_w64(A1, Db, grad + MLP_W2, grad + MLP_B2);
-    backprop64(P + MLP_W2, sW, Db, A1, Da);
-    grad_w64(A0, Da, grad + MLP_W1, grad + MLP_B1);
-    if (!apply) return;
-    // the last CTA applies Adam to the summed gradients and clears them
+    grad_layer(A2, Da, g, MLP_W3, MLP_B3);
+    backprop_layer(P + MLP_W3, Da, A2, Db);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    }
+    grad_layer(A1, Db, g, MLP_W2, MLP_B2);
+    backprop_layer(P + MLP_W2, Db, A1, Da);
     __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    for (int p = MLP_HDR + threadIdx.x; p < MLP_NP; p += blockDim.x) {
-        const float gp = __ldcg(grad + p);
-        const float m = ADAM_B1 * am[p] + (1.0f - ADAM_B1) * gp;
-        const float v = ADAM_B2 * av[p] + (1.0f - ADAM_B2) * gp * gp;
-        am[p] = m;
-        av[p] = v;
-        P[p] -= lr * (m * c1) / (sqrtf(v * c2) + ADAM_EPS);
-        grad[p] = 0.0f;
+    grad_layer(A0, Da, g, MLP_W1, MLP_B1);
+}
+
+// Sum of the CTAs' gradient slots in CTA order; then Adam (apply) or the sum
+// into grad[0 .. MLP_NP) (header entries zero).  Block 0 adds the loss.
+__global__ void __launch_bounds__(REDUCE_THREADS) mlp_reduce_kernel(float* __restrict__ P, float* __restrict__ am,
+                                                                    float* __restrict__ av, float* __restrict__ grad,
+                                                                    int nslots, float lr, float c1, float c2,
+                                                                    float* __restrict__ loss, int apply)
+{
+    const int p = blockIdx.x * REDUCE_THREADS + threadIdx.x;
+    if (p < MLP_NP) {
+        float gp = 0.0f;
+        if (p >= MLP_HDR)
+            for (int c = 0; c < nslots; ++c) gp += grad[(size_t)GRAD_SLOT * (1 + c) + p];
+        if (apply) {
+            if (p >= MLP_HDR) {
+                const float m = ADAM_B1 * am[p] + (1.0f - ADAM_B1) * gp;
+                const float v = ADAM_B2 * av[p] + (1.0f - ADAM_B2) * gp * gp;
+                am[p] = m;
+                av[p] = v;
+                P[p] -= lr * (m * c1) / (sqrtf(v * c2) + ADAM_EPS);
+            }
+        } else {
+            grad[p] = gp;
+        }
     }
-    if (threadIdx.x == 0) *ticket = 0u;
+    if (loss && blockIdx.x == 0 && threadIdx.x == 0) {
+        float L = 0.0f;
+        for (int c = 0; c < nslots; ++c) L += grad[(size_t)GRAD_SLOT * (1 + c) + MLP_NP];
+        *loss += L;
+    }
 }
 
 __global__ void __launch_bounds__(INFER_THREADS) mlp_infer_kernel(const float* __restrict__ P,
@@ -192,6 +213,12 @@ using namespace iblbm;
 
 extern "C" int iblbm_mlp_param_count(void) { return MLP_NP; }
 
+extern "C" int iblbm_mlp_grad_floats(int n)
+{
+    if (n < 1) return GRAD_SLOT;
+    return GRAD_SLOT * (1 + (n + TRAIN_ROWS - 1) / TRAIN_ROWS);
+}
+
 extern "C" int iblbm_mlp_infer(const float* params, const float* x, int n, float* y, void* stream)
 {
     if (!params || !x || !y || n < 0) return IBLBM_E_ARG;
@@ -209,15 +236,14 @@ extern "C" int iblbm_mlp_infer(const float* params, const float* x, int n, float
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
 
-extern "C" int iblbm_mlp_train_step(float* params, float* adam_m, float* adam_v, float* grad, unsigned* ticket,
-                                    const float* x, const float* t, int n, float lr, int step, float* loss,
-                                    int apply, void* stream)
+extern "C" int iblbm_mlp_train_step(float* params, float* adam_m, float* adam_v, float* grad, const float* x,
+                                    const float* t, int n, float lr, int step, float* loss, int apply, void* stream)
 {
-    if (!params || !grad || !ticket || !x || !t || n < 1 || step < 1) return IBLBM_E_ARG;
+    if (!params || !grad || !x || !t || n < 1 || step < 1) return IBLBM_E_ARG;
     if (apply && (!adam_m || !adam_v)) return IBLBM_E_ARG;
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) !=
+        if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) !=
             cudaSuccess)
             return IBLBM_E_LAUNCH;
         configured = true;
@@ -225,7 +251,10 @@ extern "C" int iblbm_mlp_train_step(float* params, float* adam_m, float* adam_v,
     // Adam bias corrections 1 / (1 - beta^step)
     const float c1 = (float)(1.0 / (1.0 - pow((double)ADAM_B1, step)));
     const float c2 = (float)(1.0 / (1.0 - pow((double)ADAM_B2, step)));
-    mlp_train_kernel<<<(n + TRAIN_ROWS - 1) / TRAIN_ROWS, TRAIN_THREADS, TRAIN_SMEM, (cudaStream_t)stream>>>(
-        params, adam_m, adam_v, grad, ticket, x, t, n, lr, c1, c2, loss, apply);
+    const int nslots = (n + TRAIN_ROWS - 1) / TRAIN_ROWS;
+    cudaStream_t s = (cudaStream_t)stream;
+    mlp_grad_kernel<<<nslots, TRAIN_THREADS, TRAIN_SMEM, s>>>(params, grad, x, t, n);
+    mlp_reduce_kernel<<<(MLP_NP + REDUCE_THREADS - 1) / REDUCE_THREADS, REDUCE_THREADS, 0, s>>>(
+        params, adam_m, adam_v, grad, nslots, lr, c1, c2, loss, apply);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

@@ -10,7 +10,10 @@ it in total, sum over iterations of omega * Lf (``collect`` can run the loop
 past its usual limit to record forces closer to convergence).
 Training pairs come from plain MDF runs (``collect``); training and inference
 run on the GPU in this library's own kernels (``iblbm_mlp_train_step``: fused
-forward, backward and Adam in one launch; ``iblbm_mlp_infer``).  With the warm
+forward and backward per block of 64 samples, then an ordered sum of the
+blocks' gradients and Adam, so training is deterministic;
+``iblbm_mlp_infer``), the hidden layers on the tensor cores (TF32 operands,
+FP32 accumulation).  With the warm
 start on, the band kernel spreads the predicted forces before the first
 iteration and then iterates as plain MDF does, to the same residual
 tolerance: plain MDF is both the fallback and the arbiter of the slip.
@@ -24,6 +27,19 @@ from ._lib import check, lib, ptr
 N_FEATURES = 64
 N_OUT = 2
 HIDDEN = 64
+HDR = 132   # header of the parameter block (normalisation and target scales)
+WLD = 72    # row stride of the hidden layers' weight matrices (csrc/mlp.cuh)
+
+
+def layer_offsets():
+    """(weight offset, row stride, bias offset, fan_in, fan_out) of the four
+    layers in the parameter block."""
+    out, off = [], HDR
+    for fan_in, fan_out in ((N_FEATURES, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, N_OUT)):
+        ld = WLD if fan_out == HIDDEN else fan_out
+        out.append((off, ld, off + fan_in * ld, fan_in, fan_out))
+        off += fan_in * ld + fan_out
+    return out
 
 
 class MdfNet:
@@ -39,17 +55,15 @@ class MdfNet:
         p = np.zeros(self.NP, dtype=np.float32)
         p[64:128] = 1.0
         p[128:130] = 1.0
-        off = 132
-        for fan_in, fan_out in ((N_FEATURES, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, HIDDEN), (HIDDEN, N_OUT)):
-            n = fan_in * fan_out
-            p[off:off + n] = rng.standard_normal(n).astype(np.float32) * np.float32(np.sqrt(2.0 / fan_in))
-            off += n + fan_out  # biases start at zero
-        assert off <= self.NP  # the block is padded to a multiple of 4 floats
+        for w0, ld, b0, fan_in, fan_out in layer_offsets():
+            W = rng.standard_normal((fan_in, fan_out)).astype(np.float32) * np.float32(np.sqrt(2.0 / fan_in))
+            for i in range(fan_in):  # row i of W, then the row's unused floats; biases start at zero
+                p[w0 + i * ld:w0 + i * ld + fan_out] = W[i]
+        assert b0 + fan_out <= self.NP  # the block is padded to a multiple of 4 floats
         self.params = torch.as_tensor(p, device=self.dev)
         self.m = torch.zeros(self.NP, dtype=torch.float32, device=self.dev)
         self.v = torch.zeros_like(self.m)
-        self.grad = torch.zeros_like(self.m)
-        self.ticket = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.grad = torch.zeros(int(self.L.iblbm_mlp_grad_floats(512)), dtype=torch.float32, device=self.dev)
         self.loss = torch.zeros(1, dtype=torch.float32, device=self.dev)
         self.step = 0
 
@@ -70,10 +84,18 @@ class MdfNet:
         """One optimiser step on the rows of X (n x 64) and T (n x 2); returns
         nothing (the loss accumulates in self.loss)."""
         s = self.torch.cuda.current_stream(self.dev).cuda_stream
+        n = int(X.shape[0])
+        need = int(self.L.iblbm_mlp_grad_floats(n))
+        if self.grad.numel() < need:
+            self.grad = self.torch.zeros(need, dtype=self.torch.float32, device=self.dev)
         self.step += 1 if apply else 0
-        check(self.L.iblbm_mlp_train_step(ptr(self.params), ptr(self.m), ptr(self.v), ptr(self.grad),
-                                          ptr(self.ticket), ptr(X), ptr(T), int(X.shape[0]), float(lr),
-                                          max(self.step, 1), ptr(self.loss), int(apply), s), "iblbm_mlp_train_step")
+        check(self.L.iblbm_mlp_train_step(ptr(self.params), ptr(self.m), ptr(self.v), ptr(self.grad), ptr(X),
+                                          ptr(T), n, float(lr), max(self.step, 1), ptr(self.loss), int(apply), s),
+              "iblbm_mlp_train_step")
+
+    def summed_gradient(self):
+        """The gradient a train_step(..., apply=False) left (param_count floats)."""
+        return self.grad[: self.NP]
 
     def fit(self, X, T, epochs=30, batch=512, lr=1e-3, seed=0):
         """Minibatch Adam over shuffled data; returns the mean loss of each epoch."""

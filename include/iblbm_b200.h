@@ -359,19 +359,25 @@ int iblbm_ibm32_smem_bytes(int lb_total, int band_capacity, int delta_type);
 /* ---- learned MDF warm start: the network's training and inference ---------
  * A 64 -> 64 -> 64 -> 64 -> 2 ReLU MLP in FP32 whose parameter block holds the
  * feature normalisation (mean, inverse scale), the target scales and the
- * weights (layout in csrc/mlp.cuh).  No reference counterpart: the reference
- * has no learned component. */
+ * weights (layout in csrc/mlp.cuh: hidden weight rows padded to 72 floats).
+ * The hidden layers run on the tensor cores (TF32 operands, FP32
+ * accumulation).  No reference counterpart: the reference has no learned
+ * component. */
 int iblbm_mlp_param_count(void);
+/* Floats of the gradient buffer of a training step on n samples: the summed
+ * gradient (param_count floats, padded), then one slot per 64 samples. */
+int iblbm_mlp_grad_floats(int n);
 /* y[n x 2] = network(x[n x 64]) in the targets' units. */
 int iblbm_mlp_infer(const float *params, const float *x, int n, float *y, void *stream);
 /* One training step on n samples (x[n x 64], t[n x 2]), mean squared error on
- * the scaled targets.  grad (param_count floats) and *ticket must be zero on
- * entry.  apply = 1: the last CTA applies Adam (step >= 1, learning rate lr;
- * adam_m / adam_v: param_count floats each) and re-zeroes grad and ticket;
- * apply = 0: the summed gradient is left in grad.  loss (optional, zeroed by
- * the caller) receives the batch loss. */
-int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *grad, unsigned *ticket, const float *x,
-                         const float *t, int n, float lr, int step, float *loss, int apply, void *stream);
+ * the scaled targets; deterministic (every block of 64 samples writes its own
+ * gradient slot, a second launch sums the slots in order).  grad holds
+ * iblbm_mlp_grad_floats(n) floats (no initial contents needed).  apply = 1:
+ * Adam (step >= 1, learning rate lr; adam_m / adam_v: param_count floats
+ * each); apply = 0: the summed gradient is left in grad[0 .. param_count).
+ * loss (optional) has the batch loss added to it. */
+int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *grad, const float *x, const float *t,
+                         int n, float lr, int step, float *loss, int apply, void *stream);
 
 /* ---- rigid particles of sedimentation runs on the device -------------------
  * Replaces the host Velocity-Verlet step of runtime/scenarios/

@@ -39,3 +39,21 @@ def test_adam_first_step_is_a_sign_step():
     P1, m, v = M.adam_step(P, g, np.zeros(npar), np.zeros(npar), 1, 1e-3)
     np.testing.assert_allclose(P1[M.HDR:] - P[M.HDR:], -1e-3 * np.sign(g[M.HDR:]), rtol=1e-6, atol=1e-9)
     np.testing.assert_array_equal(P1[:M.HDR], P[:M.HDR])
+
+
+def test_tf32_rounding():
+    """The oracle's TF32 rounding (cvt.rna.tf32.f32: 10 explicit mantissa bits,
+    to nearest, ties away from zero) and the tensor-core mode's closeness to the
+    exact one."""
+    one = np.float32(1.0)
+    ulp = np.float32(2.0 ** -10)
+    assert M.tf32(one + ulp / 2) == one + ulp  # a tie rounds away from zero
+    assert M.tf32(-(one + ulp / 2)) == -(one + ulp)
+    assert M.tf32(one + ulp / 2 - np.float32(2.0 ** -20)) == one
+    assert M.tf32(np.float32(3.0)) == 3.0
+    rng = np.random.default_rng(3)
+    npar = M.unpack(np.zeros(20000))[4]
+    P = _params(rng, npar)
+    X = rng.standard_normal((50, 64))
+    ye, yt = M.predict(P, X), M.predict(P, X, tc=True)
+    assert 0 < np.abs(ye - yt).max() <= 1e-2 * np.abs(ye).max()
