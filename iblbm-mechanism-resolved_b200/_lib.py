@@ -57,7 +57,8 @@ class IbmArgs(ctypes.Structure):
                 ("scratch", _vp), ("iscratch", _vp), ("Lux", _vp), ("Luy", _vp), ("Lfx", _vp),
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
                 ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i),
-                ("dvel_scale", _vp), ("dfc_rho_f", _d), ("wait_limit", ctypes.c_longlong), ("test_skip_copy", _i)]
+                ("dvel_scale", _vp), ("dfc_rho_f", _d), ("wait_limit", ctypes.c_longlong), ("test_skip_copy", _i),
+                ("cluster_plan", _vp), ("cluster_size", _i)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee
@@ -105,6 +106,7 @@ _SIGS = {
     "iblbm_ibm_scratch_doubles": [_i, _i, _i],
     "iblbm_ibm_scratch_ints": [_i, _i, _i],
     "iblbm_ibm_list_cache_ints": [_i, _i, _i],
+    "iblbm_ibm_cluster_plan_ints": [_i, _i, _i],
     "iblbm_ibm_smem_bytes": [_i, _i, _i],
     "iblbm_feq": [_vp, _vp, _i, _i, _vp, _vp],
     "iblbm_macroscopic": [_vp, _i, _i, _vp, _vp, _vp],

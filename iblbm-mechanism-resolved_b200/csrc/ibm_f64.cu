@@ -6,7 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <mutex>
-#include "band_kernel.cuh"
+#include "band_cluster.cuh"
 
 namespace iblbm {
 void make_params(const iblbm_case& c, CollParams& cp, BcParams& bc);
@@ -39,6 +39,16 @@ extern "C" int iblbm_ibm_list_cache_ints(int lb_total, int band_capacity, int de
     return (int)(make_layout<double>(lb_total, band_capacity, S).static_bytes / sizeof(int));
 }
 
+extern "C" int iblbm_ibm_cluster_plan_ints(int lb_total, int delta_type, int cluster_size)
+{
+    if (lb_total < 1 || (delta_type != 0 && delta_type != 1)) return 0;
+    if (cluster_size != 2 && cluster_size != 4 && cluster_size != 8) return 0;
+    const int S = delta_type == 0 ? 25 : 9;
+    const ClusterDims d = cluster_dims(lb_total, S, cluster_size);
+    if (lb_total < cluster_size || d.MW * 32 + d.nm * S > IBM_THREADS || d.MW * cluster_size > 32) return 0;
+    return (int)cluster_plan_ints(lb_total, S, cluster_size);
+}
+
 extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
 {
     const int chk = check_ibm_args<double>(a, true);
@@ -46,6 +56,15 @@ extern "C" int iblbm_ibm_step_f64(const iblbm_ibm_args* a, void* stream)
     CollParams cp;
     BcParams bc;
     make_params(a->c, cp, bc);
+    if (cluster_eligible(*a)) {
+        if (a->rebuild) {
+            // the single-CTA step builds the band and caches its lists; the plan follows from them
+            const int rc = dispatch_ibm<iblbm_ibm_args, double, false>(a, bc, stream);
+            if (rc != IBLBM_OK) return rc;
+            return a->delta_type == 0 ? launch_cluster_plan<2>(*a, stream) : launch_cluster_plan<1>(*a, stream);
+        }
+        return a->delta_type == 0 ? launch_cluster_step<2>(*a, bc, stream) : launch_cluster_step<1>(*a, bc, stream);
+    }
     return dispatch_ibm<iblbm_ibm_args, double, false>(a, bc, stream);
 }
 

@@ -62,7 +62,10 @@ class Engine:
     """One lattice case on one GPU: FP64 form (the reference's arithmetic) or
     the shifted FP32 form (``precision="f32"``)."""
 
-    def __init__(self, cfg, device=None, precision="f64", device_particles=None):
+    def __init__(self, cfg, device=None, precision="f64", device_particles=None, cluster=None):
+        """cluster: CTAs of the thread-block cluster that runs the MDF band step
+        of one fixed body in the FP64 form (2, 4 or 8; None: 8 where the body
+        fits, 0: the single-CTA step)."""
         torch = _torch()
         if precision not in ("f64", "f32"):
             raise ValueError(f"precision='{precision}' (f64 or f32)")
@@ -180,6 +183,15 @@ class Engine:
         self.d_iscr = t(self.L.iblbm_ibm_scratch_ints(self.Lb, B, delta_id), i32)
         cache_ints = self.L.iblbm_ibm32_list_cache_ints if self.f32 else self.L.iblbm_ibm_list_cache_ints
         self.d_lists = t(cache_ints(self.Lb, B, delta_id), i32)
+        # the cluster plan of a fixed body's FP64 MDF step (built at each band rebuild)
+        self.cluster, self.d_plan = 0, None
+        if not self.f32 and cfg.ibm_method == "MDF" and self.P == 1 and not self.moving and cluster != 0:
+            size = 8 if cluster is None else int(cluster)
+            n = self.L.iblbm_ibm_cluster_plan_ints(self.Lb, delta_id, size)
+            if n > 0:
+                self.cluster, self.d_plan = size, t(n, i32)
+            elif cluster is not None:
+                raise ValueError(f"cluster={cluster}: a body of {self.Lb} markers does not fit")
         self.d_excl = torch.zeros(2, 4, dtype=i32, device=dev)
         self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy = (t(self.Lb) for _ in range(4))
         self.d_dfc_force = t(2 * self.Lb)
@@ -394,6 +406,8 @@ class Engine:
         a.Lux, a.Luy, a.Lfx, a.Lfy = (ptr(x) for x in (self.d_Lux, self.d_Luy, self.d_Lfx, self.d_Lfy))
         a.dfc_force = ptr(self.d_dfc_force)
         a.stats, a.dstats = ptr(self.d_stats), ptr(self.d_dstats)
+        if self.d_plan is not None:
+            a.cluster_plan, a.cluster_size = ptr(self.d_plan), self.cluster
         return a
 
     def _make_dense_variants(self):
@@ -889,7 +903,7 @@ class Engine:
         d = self.d_dstats.cpu().numpy()
         return {"iter_count": int(s[0]), "diverged": bool(s[1]), "converged": bool(s[2]),
                 "guard_trips": max(int(s[3]), 0), "marker_space": int(s[3]) == -1,
-                "restructured_node_space": int(s[3]) == -2,
+                "restructured_node_space": int(s[3]) == -2, "cluster": int(s[3]) == -3,
                 "last_residual": float(d[0]), "omega_used": float(d[1])}
 
     def status(self):

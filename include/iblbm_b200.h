@@ -181,6 +181,15 @@ typedef struct {
      * body's restore copy while its wait still expects it, so the wait runs
      * out and the step reports status 6 with no copy in flight */
     int test_skip_copy;
+    /* MDF of one fixed body on a thread-block cluster of cluster_size CTAs
+     * (2, 4 or 8) instead of one CTA: NULL / 0 keep the single-CTA step.  The
+     * plan (iblbm_ibm_cluster_plan_ints(lb_total, delta_type, cluster_size)
+     * ints, 8-byte aligned) is built by every rebuild step and read by the
+     * steps after it, so pass the same buffer on every step of the body.
+     * Results are bit for bit those of the single-CTA step; stats[3] is -3
+     * when the cluster ran the iterations. */
+    int *cluster_plan;
+    int cluster_size;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -194,6 +203,11 @@ typedef struct {
  * arrays on chip, so a single body of any marker count within the other limits
  * runs (band_capacity <= 2048; an MDF body <= 512 markers). */
 int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
+/* Ints of the cluster plan of one body (iblbm_ibm_args.cluster_plan), or 0
+ * when a body of lb_total markers cannot run on a cluster of that size (a
+ * CTA holds its markers' warps and one thread per node under their stencils:
+ * at most 152 markers with Peskin-4 on 8 CTAs).  No reference counterpart. */
+int iblbm_ibm_cluster_plan_ints(int lb_total, int delta_type, int cluster_size);
 /* Same band step for callers that cannot allocate device memory at call time
  * (a host framework that owns all device allocations, or a service that
  * forbids cudaMalloc after start-up).  No counterpart in the reference.  The
@@ -329,6 +343,8 @@ typedef struct {
     double dfc_rho_f;
     long long wait_limit;
     int test_skip_copy;
+    int *cluster_plan;  /* not used by the FP32 step yet: NULL / 0 */
+    int cluster_size;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,

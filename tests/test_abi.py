@@ -66,3 +66,15 @@ def test_rejects_bad_arguments_without_a_gpu():
     assert L.iblbm_dense_step_f32(None, None) == -1
     assert L.iblbm_ibm_step_f32(None, None) == -1
     assert L.iblbm_feq(None, None, 10, 0, None, None) == -1
+
+
+def test_cluster_plan_sizes():
+    """Which bodies the cluster form of the FP64 MDF step takes (no GPU needed)."""
+    from iblbm_b200._lib import lib
+    L = lib()
+    assert L.iblbm_ibm_cluster_plan_ints(126, 0, 8) > 0
+    assert L.iblbm_ibm_cluster_plan_ints(152, 0, 8) > 0
+    assert L.iblbm_ibm_cluster_plan_ints(153, 0, 8) == 0  # 20 markers x 25 slots + a warp > 512 threads
+    assert L.iblbm_ibm_cluster_plan_ints(392, 1, 8) > 0
+    assert L.iblbm_ibm_cluster_plan_ints(126, 0, 3) == 0
+    assert L.iblbm_ibm_cluster_plan_ints(4, 1, 8) == 0
