@@ -5,13 +5,13 @@
 // bound by that one SM's shared-memory pipe (gathers of band velocities and
 // marker forces).  Here the body's markers are split into C contiguous ranges,
 // one per CTA of a cluster of C CTAs on C SMs.  CTA c owns
-//   * its markers [m0, m1): their stencil slots (16-bit CTA-local node
-//     indices) and separable weights in registers;
+//   * its markers [m0, m1): their stencil slots (CTA-local node, weight);
 //   * its nodes: every band node under one of its markers' stencils, with that
 //     node's contribution list (marker, weight) in shared memory.
-// The per-thread state stays small so that the gathers of an interpolation or
-// a spread can all be in flight together (at 128 registers a thread that
-// held every weight could keep only a few of them in flight).
+// Both sit in shared memory, one column per thread, and are walked by compact
+// loops (a stencil row or four list entries per trip): the loop bodies stay
+// small enough for the instruction cache and the per-thread state small
+// enough that a trip's loads are in flight together.
 // A node under the stencils of markers of two CTAs is held by both; both run
 // the same operations on the same inputs, so both copies keep the same bits.
 // An iteration is
@@ -19,10 +19,12 @@
 //   -> each marker's force stored into every CTA's shared memory, and each
 //      marker warp's maximum squared slip into a slot of every CTA
 //   -> cluster barrier (release / acquire)
-//   -> residual = sqrt of the maximum over the slots (the same bits in every
-//      CTA, so every CTA takes the same branch), divergence check
 //   -> spread + relax + velocity update (node threads, forces of any marker
-//      read from the CTA's own copy) -> CTA barrier -> convergence check.
+//      read from the CTA's own copy), while one warp reduces the residual =
+//      sqrt of the maximum over the slots (the same bits in every CTA, so
+//      every CTA takes the same branch)
+//   -> CTA barrier -> divergence check (a diverged iteration's spread is
+//      undone: its force increments are dropped) -> convergence check.
 // Every sum runs over the same terms in the same order as the single-CTA step
 // (slot order for interpolation, list order for spreading), so every result is
 // bit-identical to it.  The force copies and residual slots are double-buffered
@@ -93,7 +95,8 @@ __host__ __device__ inline size_t cluster_smem_bytes(int Lb, int S, int C)
 {
     const ClusterDims d = cluster_dims(Lb, S, C);
     return up16(16 * (size_t)d.NLP) + up16(8 * (size_t)d.NLP) + up16(16 * 2 * (size_t)Lb) + 8 * 2 * 32 +
-           up16(8 * (size_t)S * d.NLP) + up16(4 * (size_t)S * d.NLP);
+           up16(8 * (size_t)S * d.NLP) + up16(4 * (size_t)S * d.NLP) + up16(8 * (size_t)S * d.NMP) +
+           up16(4 * (size_t)S * d.NMP);
 }
 
 // Whether a band step can run on a cluster of C CTAs: one fixed body under MDF
@@ -109,6 +112,7 @@ inline bool cluster_eligible(const iblbm_ibm_args& a)
     const ClusterDims d = cluster_dims(a.lb_total, S, C);
     if (d.MW * 32 + d.nm * S > IBM_THREADS || d.MW * C > 32) return false;
     if ((reinterpret_cast<uintptr_t>(a.cluster_plan) & 7) != 0) return false;
+    if (cluster_smem_bytes(a.lb_total, S, C) > (size_t)IBM_SMEM_LIMIT) return false;
     return ibm_smem<double>(a) <= (size_t)IBM_SMEM_LIMIT;  // the layout fits (no global-static form)
 }
 
@@ -251,20 +255,14 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_plan_kernel(const 
 }
 
 // ---- the step ---------------------------------------------------------------
-// Stencil slot k of a marker thread's packed 16-bit node indices.
-template <int S>
-__device__ __forceinline__ int cl_idx(const uint32_t (&ip)[(S + 1) / 2], int k)
-{
-    return (k & 1) ? (int)(ip[k >> 1] >> 16) : (int)(ip[k >> 1] & 0xffffu);
-}
-
 template <int A>
 __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm_ibm_args a, BcParams bc,
                                                                       const int* __restrict__ plan)
 {
-    constexpr int SW = Sten<A>::SW, S = Sten<A>::S, SP = (S + 1) / 2;
+    constexpr int SW = Sten<A>::SW, S = Sten<A>::S;
     extern __shared__ __align__(16) char smem_raw[];
     __shared__ int s_status;
+    __shared__ double s_res[2];  // the residual of an iteration (parity)
     const int C = (int)cl_nranks(), rank = (int)cl_rank();
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int Lb = a.lb_total;
@@ -292,36 +290,37 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
     double* s_ew = reinterpret_cast<double*>(sp);  // entry j of node i: weight s_ew[j * nls + i],
     sp += up16(8 * (size_t)S * d.NLP);
     int* s_el = reinterpret_cast<int*>(sp);          // marker s_el[j * nls + i]
+    sp += up16(4 * (size_t)S * d.NLP);
+    double* s_mw = reinterpret_cast<double*>(sp);    // slot k of marker i: weight s_mw[k * NMP + i],
+    sp += up16(8 * (size_t)S * d.NMP);
+    int* s_mi = reinterpret_cast<int*>(sp);          // CTA-local node s_mi[k * NMP + i]
+    const int NMP = d.NMP;
     const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
     const double dt = a.c.dt;
     const bool unit_dt = (a.c.dt == 1.0);
 
     // roles: marker threads tid < nm (warps 0 .. MW-1), node threads from MW * 32.
-    // A marker's stencil nodes (CTA-local indices, 16 bits each) and separable
-    // weights in registers; a node's list in shared memory.
+    // A marker's stencil (CTA-local node, weight wx * wy per slot) and a node's
+    // list (marker, weight per entry) in shared memory, one column per thread,
+    // walked by compact loops whose loads run ahead of the serial sums.
     const bool mk = tid < nm;
     const int ni = tid - MW * 32;
     const bool nd = ni >= 0 && ni < nl;
-    uint32_t ip[SP];
-#pragma unroll
-    for (int k = 0; k < SP; ++k) ip[k] = 0;
-    double hwx[SW], hwy[SW];  // a marker's separable weights: slot k weighs hwx[k / SW] * hwy[k % SW]
-#pragma unroll
-    for (int q = 0; q < SW; ++q) { hwx[q] = 0; hwy[q] = 0; }
     int len = 0, b = -1, own = 0, l = 0;
     double dvx = 0, dvy = 0, vs = 0;
     if (mk) {
         l = m0 + tid;
         const double* mw = reinterpret_cast<const double*>(rb + clo_mw(d));
-#pragma unroll
-        for (int k = 0; k < S; ++k) {
-            const uint32_t v = (uint32_t)rb[4 + k * d.NMP + tid];
-            ip[k >> 1] |= (k & 1) ? (v << 16) : v;
-        }
+        double hwx[SW], hwy[SW];
 #pragma unroll
         for (int q = 0; q < SW; ++q) {
-            hwx[q] = mw[q * d.NMP + tid];
-            hwy[q] = mw[(SW + q) * d.NMP + tid];
+            hwx[q] = mw[q * NMP + tid];
+            hwy[q] = mw[(SW + q) * NMP + tid];
+        }
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            s_mi[k * NMP + tid] = rb[4 + k * NMP + tid];
+            s_mw[k * NMP + tid] = hwx[k / SW] * hwy[k % SW];  // the single-CTA step's wgt(l, k)
         }
         dvx = a.dvel[2 * l];
         dvy = a.dvel[2 * l + 1];
@@ -376,8 +375,19 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
     cl_sync();
     double Rl = 0;
     if (mk) {
+        const int* mi = s_mi + tid;
+        const double* mwp = s_mw + tid;
+#pragma unroll 1
+        for (int gi = 0; gi < SW; ++gi) {
+            double v[SW], w[SW];
 #pragma unroll
-        for (int k = 0; k < S; ++k) Rl += s_bro[cl_idx<S>(ip, k)] * (hwx[k / SW] * hwy[k % SW]);
+            for (int gj = 0; gj < SW; ++gj) {
+                v[gj] = s_bro[mi[(gi * SW + gj) * NMP]];
+                w[gj] = mwp[(gi * SW + gj) * NMP];
+            }
+#pragma unroll
+            for (int gj = 0; gj < SW; ++gj) Rl += v[gj] * w[gj];
+        }
     }
     const uint32_t lf_base = smem_addr(s_lf), rb_base = smem_addr(s_rb);
     const int min_iter = max(1, min(a.mdf_min_iterations, a.mdf_iterations));
@@ -389,13 +399,39 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
         const int par = it & 1;
         unsigned long long key = 0;  // squared slip as its bit pattern
         if (mk) {
-            double ux = 0, uy = 0;
+            // slot order; one stencil row per trip, the next row's indices and
+            // weights loaded while this row's gathers and sums run
+            const int* mi = s_mi + tid;
+            const double* mwp = s_mw + tid;
+            int ni_[SW];
+            double w_[SW];
 #pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const double2 v = s_bw[cl_idx<S>(ip, k)];
-                const double w = hwx[k / SW] * hwy[k % SW];
-                ux += v.x * w;
-                uy += v.y * w;
+            for (int gj = 0; gj < SW; ++gj) {
+                ni_[gj] = mi[gj * NMP];
+                w_[gj] = mwp[gj * NMP];
+            }
+            double ux = 0, uy = 0;
+#pragma unroll 1
+            for (int gi = 0; gi < SW; ++gi) {
+                double2 v[SW];
+                double w[SW];
+#pragma unroll
+                for (int gj = 0; gj < SW; ++gj) {
+                    v[gj] = s_bw[ni_[gj]];
+                    w[gj] = w_[gj];
+                }
+                if (gi + 1 < SW) {
+#pragma unroll
+                    for (int gj = 0; gj < SW; ++gj) {
+                        ni_[gj] = mi[((gi + 1) * SW + gj) * NMP];
+                        w_[gj] = mwp[((gi + 1) * SW + gj) * NMP];
+                    }
+                }
+#pragma unroll
+                for (int gj = 0; gj < SW; ++gj) {
+                    ux += v[gj].x * w[gj];
+                    uy += v[gj].y * w[gj];
+                }
             }
             lux = ux;
             luy = uy;
@@ -415,15 +451,15 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
             }
         }
         cl_sync();
-        // residual = max_l sqrt(slip^2) = sqrt(max_l slip^2), max on the bit patterns
-        const double residual =
-            sqrt(__longlong_as_double((long long)warp_max_bits(lane < NSLOT ? s_rb[par * 32 + lane] : 0ull)));
-        last = residual;
-        if (it > 0 && residual > prev * 1.5) {
-            diverged = 1;
-            iter_count = it + 1;
-            break;
+        // residual = max_l sqrt(slip^2) = sqrt(max_l slip^2), max on the bit patterns:
+        // one warp reduces it while the node threads spread (a spread that the
+        // divergence check then rejects is undone below)
+        if (wid == 0) {
+            const double r =
+                sqrt(__longlong_as_double((long long)warp_max_bits(lane < NSLOT ? s_rb[par * 32 + lane] : 0ull)));
+            if (lane == 0) s_res[par] = r;
         }
+        const double ftx0 = ftx, fty0 = fty;
         if (nd) {
             // list order, four entries' loads in flight together
             const double2* F = s_lf + par * Lb;
@@ -453,6 +489,17 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
             s_bw[ni] = w;
         }
         __syncthreads();
+        const double residual = s_res[par];
+        last = residual;
+        if (it > 0 && residual > prev * 1.5) {
+            // diverged: this iteration's spread is not applied (the working
+            // velocities are not read again; the accumulated forces are restored)
+            ftx = ftx0;
+            fty = fty0;
+            diverged = 1;
+            iter_count = it + 1;
+            break;
+        }
         prev = residual;
         iter_count = it + 1;
         if ((it + 1) >= min_iter && residual < a.mdf_tol) {
