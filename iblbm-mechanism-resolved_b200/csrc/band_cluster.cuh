@@ -8,10 +8,11 @@
 //   * its markers [m0, m1): their stencil slots (CTA-local node, weight);
 //   * its nodes: every band node under one of its markers' stencils, with that
 //     node's contribution list (marker, weight) in shared memory.
-// Both sit in shared memory, one column per thread, and are walked by compact
-// loops (a stencil row or four list entries per trip): the loop bodies stay
-// small enough for the instruction cache and the per-thread state small
-// enough that a trip's loads are in flight together.
+// Both sit in shared memory, one column per thread, and are walked by
+// straight-line code (the whole stencil; a list's first CL_JU entries,
+// predicated on its length) so that their loads issue ahead of the serial sums:
+// measured standalone, a stencil walked one row per loop trip takes twice as
+// long as the unrolled one.
 // A node under the stencils of markers of two CTAs is held by both; both run
 // the same operations on the same inputs, so both copies keep the same bits.
 // An iteration is
@@ -51,6 +52,7 @@ namespace iblbm {
 
 constexpr int CL_MAX = 8;     // CTAs per cluster (the portable cluster size)
 constexpr int CL_HDR = 16;    // plan header ints: [C, S, Lb, nb, NMP, NLP, 0, 0, rank status x CL_MAX]
+constexpr int CL_JU = 8;      // list entries of a node spread by straight-line code
 
 // Plan sizes of one rank: markers per CTA (capacity NMP), nodes per CTA
 // (capacity NLP = markers x stencil slots, the most distinct nodes they cover).
@@ -266,35 +268,69 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
     const int C = (int)cl_nranks(), rank = (int)cl_rank();
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int Lb = a.lb_total;
-    // the plan holds iff it was built for this band, these sizes and every rank fits
-    bool valid = plan[0] == C && plan[1] == S && plan[2] == Lb && plan[3] == *a.band_count;
-    for (int r = 0; r < C; ++r) valid = valid && plan[8 + r] == 1;
-    if (!valid) {
+    const ClusterDims d = cluster_dims(Lb, S, C);
+    const int* rb = plan + CL_HDR + (size_t)rank * d.rank_ints;
+    const int MW = d.MW, NSLOT = C * MW, NMP = d.NMP, NLP = d.NLP;
+    // this rank's markers, split as the plan splits them
+    const int m0 = (int)((long long)rank * Lb / C), nm = (int)((long long)(rank + 1) * Lb / C) - m0;
+    const int ni = tid - MW * 32;
+    // First round of loads, all independent of one another (the step starts
+    // with its plan out of L2): the plan header, this rank's header and each
+    // thread's own column of the plan, whatever role the header then confirms.
+    int hv[4 + CL_MAX];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) hv[r] = plan[r];
+#pragma unroll
+    for (int r = 0; r < CL_MAX; ++r) hv[4 + r] = r < C ? plan[8 + r] : 1;
+    const int nb_now = *a.band_count;
+    const int nl = rb[2];
+    int slot[S];
+    double hwx[SW], hwy[SW];
+    double dvx = 0, dvy = 0;
+    int b = -1, own = 0, len = 0, n = 0;
+    if (tid < nm) {
+        const double* mw = reinterpret_cast<const double*>(rb + clo_mw(d));
+#pragma unroll
+        for (int k = 0; k < S; ++k) slot[k] = rb[4 + k * NMP + tid];
+#pragma unroll
+        for (int q = 0; q < SW; ++q) {
+            hwx[q] = mw[q * NMP + tid];
+            hwy[q] = mw[(SW + q) * NMP + tid];
+        }
+        dvx = a.dvel[2 * (m0 + tid)];
+        dvy = a.dvel[2 * (m0 + tid) + 1];
+    } else if (ni >= 0 && ni < NLP) {
+        b = rb[clo_nidx(d) + ni];
+        own = rb[clo_nown(d) + ni];
+        len = rb[clo_nlen(d) + ni];
+        n = rb[clo_nlat(d) + ni];
+    }
+    // the plan holds iff it was built for this band, these sizes and every rank
+    // fits: values every CTA reads alike, so all take the same branch
+    int ok = hv[0] == C && hv[1] == S && hv[2] == Lb && hv[3] == nb_now;
+#pragma unroll
+    for (int r = 0; r < CL_MAX; ++r) ok &= hv[4 + r] == 1;
+    if (!ok) {
         if (rank == 0) ibm_step_body<iblbm_ibm_args, double, false, A, IBM_MDF, false, false>(a, bc);
         return;
     }
-    const ClusterDims d = cluster_dims(Lb, S, C);
-    const int* rb = plan + CL_HDR + (size_t)rank * d.rank_ints;
-    const int nm = rb[0], m0 = rb[1], nl = rb[2];
     const int nls = (nl + 1) & ~1;  // row stride of the entry weights in shared memory
-    const int MW = d.MW, NSLOT = C * MW;
     char* sp = smem_raw;
     double2* s_bw = reinterpret_cast<double2*>(sp);
-    sp += up16(16 * (size_t)d.NLP);
+    sp += up16(16 * (size_t)NLP);
     double* s_bro = reinterpret_cast<double*>(sp);
-    sp += up16(8 * (size_t)d.NLP);
+    sp += up16(8 * (size_t)NLP);
     double2* s_lf = reinterpret_cast<double2*>(sp);
     sp += up16(16 * 2 * (size_t)Lb);
     unsigned long long* s_rb = reinterpret_cast<unsigned long long*>(sp);
     sp += 8 * 2 * 32;
     double* s_ew = reinterpret_cast<double*>(sp);  // entry j of node i: weight s_ew[j * nls + i],
-    sp += up16(8 * (size_t)S * d.NLP);
+    sp += up16(8 * (size_t)S * NLP);
     int* s_el = reinterpret_cast<int*>(sp);          // marker s_el[j * nls + i]
-    sp += up16(4 * (size_t)S * d.NLP);
+    sp += up16(4 * (size_t)S * NLP);
     double* s_mw = reinterpret_cast<double*>(sp);    // slot k of marker i: weight s_mw[k * NMP + i],
-    sp += up16(8 * (size_t)S * d.NMP);
+    sp += up16(8 * (size_t)S * NMP);
     int* s_mi = reinterpret_cast<int*>(sp);          // CTA-local node s_mi[k * NMP + i]
-    const int NMP = d.NMP;
     const Geom g{a.g.nx, a.g.ny, a.g.pitch, a.g.qstride};
     const double dt = a.c.dt;
     const bool unit_dt = (a.c.dt == 1.0);
@@ -302,43 +338,31 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
     // roles: marker threads tid < nm (warps 0 .. MW-1), node threads from MW * 32.
     // A marker's stencil (CTA-local node, weight wx * wy per slot) and a node's
     // list (marker, weight per entry) in shared memory, one column per thread,
-    // walked by compact loops whose loads run ahead of the serial sums.
+    // walked by straight-line code whose loads run ahead of the serial sums.
     const bool mk = tid < nm;
-    const int ni = tid - MW * 32;
     const bool nd = ni >= 0 && ni < nl;
-    int len = 0, b = -1, own = 0, l = 0;
-    double dvx = 0, dvy = 0, vs = 0;
+    const int l = m0 + tid;
+    double vs = 0;
     if (mk) {
-        l = m0 + tid;
-        const double* mw = reinterpret_cast<const double*>(rb + clo_mw(d));
-        double hwx[SW], hwy[SW];
-#pragma unroll
-        for (int q = 0; q < SW; ++q) {
-            hwx[q] = mw[q * NMP + tid];
-            hwy[q] = mw[(SW + q) * NMP + tid];
-        }
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-            s_mi[k * NMP + tid] = rb[4 + k * NMP + tid];
+            s_mi[k * NMP + tid] = slot[k];
             s_mw[k * NMP + tid] = hwx[k / SW] * hwy[k % SW];  // the single-CTA step's wgt(l, k)
         }
-        dvx = a.dvel[2 * l];
-        dvy = a.dvel[2 * l + 1];
         if (a.dvel_scale) {
             const double sc = *a.dvel_scale;
             dvx = dvx * sc;
             dvy = dvy * sc;
         }
     } else if (nd) {
-        b = rb[clo_nidx(d) + ni];
-        own = rb[clo_nown(d) + ni];
-        len = rb[clo_nlen(d) + ni];
+        // second round: the node's list and its post-streaming populations
         const double* ew = reinterpret_cast<const double*>(rb + clo_ew(d));
-        for (int j = 0; j < len; ++j) {
-            s_el[j * nls + ni] = rb[clo_el(d) + j * d.NLP + ni];
-            s_ew[j * nls + ni] = ew[j * d.NLP + ni];
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            const bool in = j < len;
+            s_el[j * nls + ni] = in ? rb[clo_el(d) + j * NLP + ni] : 0;
+            s_ew[j * nls + ni] = in ? ew[j * NLP + ni] : 0.0;
         }
-        const int n = rb[clo_nlat(d) + ni];
         double r, x, y;
         switch (a.c.bc) {
         case BC_DIRICHLET_NEUMANN: cl_node_moments<BC_DIRICHLET_NEUMANN>(a, g, bc, n, r, x, y); break;
@@ -377,17 +401,8 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
     if (mk) {
         const int* mi = s_mi + tid;
         const double* mwp = s_mw + tid;
-#pragma unroll 1
-        for (int gi = 0; gi < SW; ++gi) {
-            double v[SW], w[SW];
 #pragma unroll
-            for (int gj = 0; gj < SW; ++gj) {
-                v[gj] = s_bro[mi[(gi * SW + gj) * NMP]];
-                w[gj] = mwp[(gi * SW + gj) * NMP];
-            }
-#pragma unroll
-            for (int gj = 0; gj < SW; ++gj) Rl += v[gj] * w[gj];
-        }
+        for (int k = 0; k < S; ++k) Rl += s_bro[mi[k * NMP]] * mwp[k * NMP];
     }
     const uint32_t lf_base = smem_addr(s_lf), rb_base = smem_addr(s_rb);
     const int min_iter = max(1, min(a.mdf_min_iterations, a.mdf_iterations));
@@ -399,47 +414,29 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
         const int par = it & 1;
         unsigned long long key = 0;  // squared slip as its bit pattern
         if (mk) {
-            // slot order; one stencil row per trip, the next row's indices and
-            // weights loaded while this row's gathers and sums run
+            // slot order; indices and weights from shared memory, the whole
+            // stencil unrolled so that its loads issue ahead of the serial sums
             const int* mi = s_mi + tid;
             const double* mwp = s_mw + tid;
-            int ni_[SW];
-            double w_[SW];
-#pragma unroll
-            for (int gj = 0; gj < SW; ++gj) {
-                ni_[gj] = mi[gj * NMP];
-                w_[gj] = mwp[gj * NMP];
-            }
             double ux = 0, uy = 0;
-#pragma unroll 1
-            for (int gi = 0; gi < SW; ++gi) {
-                double2 v[SW];
-                double w[SW];
 #pragma unroll
-                for (int gj = 0; gj < SW; ++gj) {
-                    v[gj] = s_bw[ni_[gj]];
-                    w[gj] = w_[gj];
-                }
-                if (gi + 1 < SW) {
-#pragma unroll
-                    for (int gj = 0; gj < SW; ++gj) {
-                        ni_[gj] = mi[((gi + 1) * SW + gj) * NMP];
-                        w_[gj] = mwp[((gi + 1) * SW + gj) * NMP];
-                    }
-                }
-#pragma unroll
-                for (int gj = 0; gj < SW; ++gj) {
-                    ux += v[gj].x * w[gj];
-                    uy += v[gj].y * w[gj];
-                }
+            for (int k = 0; k < S; ++k) {
+                const double2 v = s_bw[mi[k * NMP]];
+                const double w = mwp[k * NMP];
+                ux += v.x * w;
+                uy += v.y * w;
             }
             lux = ux;
             luy = uy;
             const double ex = dvx - ux, ey = dvy - uy;
             key = (unsigned long long)__double_as_longlong(ex * ex + ey * ey);
             const double fx = 2.0 * Rl * (dvx - ux), fy = 2.0 * Rl * (dvy - uy);
-            lfx = unit_dt ? fx : fx / dt;
-            lfy = unit_dt ? fy : fy / dt;
+            lfx = fx;
+            lfy = fy;
+            if (!unit_dt) {  // x / 1.0 == x: the division only for other time steps
+                lfx = fx / dt;
+                lfy = fy / dt;
+            }
             const uint32_t la = lf_base + (uint32_t)(16 * (par * Lb + l));
             for (int p = 0; p < C; ++p) cl_store2(cl_map(la, (uint32_t)p), lfx, lfy);
         }
@@ -461,20 +458,22 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
         }
         const double ftx0 = ftx, fty0 = fty;
         if (nd) {
-            // list order, four entries' loads in flight together
+            // list order: the first CL_JU entries unrolled (predicated on the
+            // list length, so their loads issue together), the rest one by one
             const double2* F = s_lf + par * Lb;
             const int* el = s_el + ni;
             const double* ew = s_ew + ni;
             double ax = 0, ay = 0;
-            int j = 0;
-            for (; j + 4 <= len; j += 4) {
-                const int e0 = el[j * nls], e1 = el[(j + 1) * nls], e2 = el[(j + 2) * nls], e3 = el[(j + 3) * nls];
-                const double w0 = ew[j * nls], w1 = ew[(j + 1) * nls], w2 = ew[(j + 2) * nls], w3 = ew[(j + 3) * nls];
-                const double2 v0 = F[e0], v1 = F[e1], v2 = F[e2], v3 = F[e3];
-                ax += v0.x * w0; ax += v1.x * w1; ax += v2.x * w2; ax += v3.x * w3;
-                ay += v0.y * w0; ay += v1.y * w1; ay += v2.y * w2; ay += v3.y * w3;
+#pragma unroll
+            for (int j = 0; j < CL_JU; ++j) {
+                if (j < len) {
+                    const double2 v = F[el[j * nls]];
+                    const double w = ew[j * nls];
+                    ax += v.x * w;
+                    ay += v.y * w;
+                }
             }
-            for (; j < len; ++j) {
+            for (int j = CL_JU; j < len; ++j) {
                 const double2 v = F[el[j * nls]];
                 const double w = ew[j * nls];
                 ax += v.x * w;
