@@ -222,6 +222,12 @@ INIT_CASES = {
                settling_inertia_model="explicit_history", marker_spacing_factor=1.0),
 }
 
+# the stream-first schedule (iblbm/runtime/loop.py:60-61,77,86-87: collide once
+# before the loop, then at the end of every step) on the DFC cases, the one
+# method whose default schedule collides at the start of the step
+RUN_CASES["dfc_trt_hat_fixed_sf"] = dict(RUN_CASES["dfc_trt_hat_fixed"], stream_first=True)
+RUN_CASES["c3_dfc_bgk_p4_osc_sf"] = dict(RUN_CASES["c3_dfc_bgk_p4_osc"], stream_first=True, max_steps=120)
+
 
 def _import_reference(path):
     os.environ["IBLBM_GPU"] = "0"

@@ -46,9 +46,11 @@ def _device_still_exact(torch):
 def test_band_copy_wait_runs_out_and_reports(torch, precision):
     """The fixed body's restore copy is not issued while the band kernel waits
     for it with a 256-poll limit: the step reports status 6; the next normal
-    step reports 0, and the device still computes bit-exact results."""
+    step reports 0, and the device still computes bit-exact results.  (The
+    single-CTA step: the cluster form of the FP64 step restores nothing by bulk
+    copy.)"""
     from iblbm_b200.engine import Engine
-    e = Engine(_cfg(), precision=precision)
+    e = Engine(_cfg(), precision=precision, cluster=0)
     e.advance(5, outputs_last=False)  # the band is built and cached; later steps restore it by a bulk copy
     torch.cuda.synchronize()
     assert e.status() == 0
