@@ -970,7 +970,7 @@ def run_profile(args):
     import torch
     from iblbm_b200.engine import Engine
     eng = Engine(workload_config(collision=args.collision, max_steps=args.warmup + args.steps + 8),
-                 precision=args.precision)
+                 precision=args.precision, cluster=args.cluster)
     for _ in range(args.warmup + args.steps):
         eng._launch(False)
     eng.join()
@@ -1006,6 +1006,8 @@ def main():
     ap.add_argument("--collision", default="TRT", choices=["BGK", "TRT", "CM_MRT"])
     ap.add_argument("--form", default="chosen", choices=["chosen", "plain"])
     ap.add_argument("--precision", default=None, choices=["f64", "f32"], help="form used by the profile runs")
+    ap.add_argument("--cluster", type=int, default=None, choices=[0, 2, 4, 8],
+                    help="profile runs: CTAs of the FP64 MDF band step's cluster (0: one CTA; default: 8)")
     ap.add_argument("--accuracy-steps", type=int, default=SWEEP_STEPS,
                     help="steps of the sweep's FP32-vs-FP64 accuracy run (0: skip)")
     ap.add_argument("--accuracy-out", default=None, help="write the per-case accuracy table here (JSON)")
