@@ -91,8 +91,8 @@ class Engine:
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
             if cfg.time_integrator not in ("verlet", "euler_explicit"):
                 raise NotImplementedError(f"time_integrator='{cfg.time_integrator}' (verlet, euler_explicit)")
-            if cfg.ibm_method != "MDF":
-                raise NotImplementedError("multi-particle sedimentation is accelerated for MDF")
+            if cfg.ibm_method not in ("MDF", "DF"):
+                raise NotImplementedError("multi-particle sedimentation is accelerated for MDF and DF")
         # cfg.stream_first (iblbm/runtime/loop.py:60-61,77,86-87) moves each
         # collision from the start of a step to the end of the previous one, with
         # the same inputs: the fused pass (streaming ... collision) already runs
@@ -234,10 +234,12 @@ class Engine:
         self._torque_ij = None
         if st.particles is not None:
             self.dev_particles = True if device_particles is None else bool(device_particles)
-            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit":
-                # the torque, the angular Verlet step and the explicit Euler step run on the host
+            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method == "DF":
+                # the torque, the angular Verlet step, the explicit Euler step and DF's
+                # Lagrangian force sums run on the host
                 if device_particles:
-                    raise NotImplementedError("rotating particles and explicit Euler steps run on the host")
+                    raise NotImplementedError("rotating particles, explicit Euler steps and DF particles run on "
+                                              "the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -806,8 +808,24 @@ class Engine:
         reference (numpy over the dense N x 2 field: iblbm/ibm/multi_particle.py:199-202);
         with torques also T = -sum((i - cx) fy - (j - cy) fx) over the lattice, node
         indices as floats and the particle centre in lattice units (:203-208).
+        Under DF the reference sums the particle's marker forces instead
+        (iblbm/ibm/forcing.py:262-275): F = -sum(Lf ds), T = -sum((rx Lfy - ry Lfx) ds),
+        rx = (Lx - cx) / dx over the markers this step used.
         Returns (forces, torques or None)."""
         st = self.st
+        if self.method == "DF":
+            Lfx, Lfy = self.d_Lfx.cpu().numpy(), self.d_Lfy.cpu().numpy()
+            moff = self.d_moff.cpu().numpy()
+            out, tq = [], ([] if torques else None)
+            for p, part in enumerate(st.particles):
+                fx, fy = Lfx[moff[p]:moff[p + 1]], Lfy[moff[p]:moff[p + 1]]
+                La = float(part.Larea)
+                out.append(np.array([-float(np.sum(fx * La)), -float(np.sum(fy * La))]))
+                if torques:
+                    rx = (part.Lx - float(part.pos[0])) / st.dx
+                    ry = (part.Ly - float(part.pos[1])) / st.dy
+                    tq.append(-float(np.sum((rx * fy - ry * fx) * La)))
+            return out, tq
         nb = int(self.d_count.item())
         nodes = self.d_nodes[:nb].cpu().numpy()
         part = self.d_fib_part[: 2 * self.B * self.P].reshape(self.P, self.B, 2)[:, :nb].cpu().numpy()

@@ -436,11 +436,38 @@ class OracleSim:
         else:
             raise KeyError(cfg.ibm_method)
 
+    # iblbm/ibm/multi_particle.py:347-421 (DF): each particle's closure
+    # (ibm/forcing.py:125-275, CPU branch) on the same velocity field, its
+    # Eulerian force added to the total in particle order; the particle's force
+    # and torque are the negated Lagrangian sums -sum(Lf ds) and
+    # -sum((rx Lfy - ry Lfx) ds), rx = (Lx - cx) / dx; then the velocity
+    # correction with the total (ibm/dispatch.py:43-53)
+    def _apply_df_multi(self):
+        s, cfg = self.s, self.cfg
+        Eux, Euy = np.ascontiguousarray(s.U[:, 0]), np.ascontiguousarray(s.U[:, 1])
+        fib_total = np.zeros((s.nx * s.ny, 2))
+        for particle in s.particles:
+            La = float(particle.Larea)
+            fib_p, _, _, Lfx, Lfy, _ = ibm_df(
+                np.ascontiguousarray(particle.Lx), np.ascontiguousarray(particle.Ly),
+                np.ascontiguousarray(particle.desired_velocity), Eux, Euy, s.ro, s.dx, s.dy, s.dt, La, s.ny,
+                s.nx, cfg.delta_type, cfg.incompressible_lbgk)
+            fib_total += fib_p
+            particle._fib_force = np.array([-float(np.sum(Lfx * La)), -float(np.sum(Lfy * La))])
+            if cfg.enable_rotation:
+                rx = (particle.Lx - float(particle.pos[0])) / s.dx
+                ry = (particle.Ly - float(particle.pos[1])) / s.dy
+                particle._torque_new = -float(np.sum((rx * Lfy - ry * Lfx) * La))
+        s.fib = fib_total
+        velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
+
     # iblbm/ibm/multi_particle.py:424-455 (MDF) and 347-421 (DF, uncoupled)
     def _apply_ibm_multi(self):
         s, cfg = self.s, self.cfg
+        if cfg.ibm_method == "DF":
+            return self._apply_df_multi()
         if cfg.ibm_method != "MDF" or len(s.particles) < 2:
-            raise NotImplementedError("multi-particle oracle covers coupled MDF")
+            raise NotImplementedError("multi-particle oracle covers DF and coupled MDF")
         parts = [(np.ascontiguousarray(p.Lx), np.ascontiguousarray(p.Ly),
                   np.ascontiguousarray(p.desired_velocity), p.Larea) for p in s.particles]
         fib, fpart, stats = mdf_coupled(parts, s.U, s.ro, s.dx, s.dy, s.dt, s.ny, s.nx,

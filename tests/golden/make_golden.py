@@ -228,6 +228,12 @@ INIT_CASES = {
 RUN_CASES["dfc_trt_hat_fixed_sf"] = dict(RUN_CASES["dfc_trt_hat_fixed"], stream_first=True)
 RUN_CASES["c3_dfc_bgk_p4_osc_sf"] = dict(RUN_CASES["c3_dfc_bgk_p4_osc"], stream_first=True, max_steps=120)
 
+# two settling discs under DF (iblbm/ibm/multi_particle.py:347-421): Lagrangian force and
+# torque sums per particle; translation only, and with semi-implicit rotation
+RUN_CASES["c5_sed2_df_bgk_hat"] = dict(RUN_CASES["c5_sed2_mdf_cmmrt_p4"], ibm_method="DF", delta_type="hat",
+                                       collision_model="BGK", max_steps=200)
+RUN_CASES["c5r_sed2_df_rot_semi"] = dict(RUN_CASES["c5r_sed2_mdf_rot_semi"], ibm_method="DF", max_steps=200)
+
 
 def _import_reference(path):
     os.environ["IBLBM_GPU"] = "0"
