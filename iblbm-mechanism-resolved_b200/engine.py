@@ -91,8 +91,10 @@ class Engine:
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
             if cfg.time_integrator not in ("verlet", "euler_explicit"):
                 raise NotImplementedError(f"time_integrator='{cfg.time_integrator}' (verlet, euler_explicit)")
-            if cfg.ibm_method not in ("MDF", "DF"):
-                raise NotImplementedError("multi-particle sedimentation is accelerated for MDF and DF")
+            if cfg.ibm_method == "DFC" and any(abs(float(p.Larea) - float(st.particles[0].Larea)) > 1e-12
+                                               for p in st.particles):
+                # iblbm/ibm/strategies/dfc.py:73-74
+                raise ValueError("multi-particle DFC needs equal marker arc lengths")
         # cfg.stream_first (iblbm/runtime/loop.py:60-61,77,86-87) moves each
         # collision from the start of a step to the end of the previous one, with
         # the same inputs: the fused pass (streaming ... collision) already runs
@@ -172,6 +174,7 @@ class Engine:
         self.B = B = self._band_capacity(S)
         t = lambda n, dt=f64: torch.zeros(max(int(n), 1), dtype=dt, device=dev)
         self.d_moff = torch.as_tensor(moff, device=dev)
+        self.d_moff_set = torch.as_tensor(np.array([0, self.Lb], dtype=np.int32), device=dev)
         self.d_larea = torch.as_tensor(self.larea_h, device=dev)
         self.d_Lx, self.d_Ly, self.d_dv = t(self.Lb), t(self.Lb), t(2 * self.Lb)
         self._upload_markers()
@@ -234,12 +237,12 @@ class Engine:
         self._torque_ij = None
         if st.particles is not None:
             self.dev_particles = True if device_particles is None else bool(device_particles)
-            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method == "DF":
-                # the torque, the angular Verlet step, the explicit Euler step and DF's
-                # Lagrangian force sums run on the host
+            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method != "MDF":
+                # the torque, the angular Verlet step, the explicit Euler step and the
+                # Lagrangian force sums of DF and DFC run on the host
                 if device_particles:
-                    raise NotImplementedError("rotating particles, explicit Euler steps and DF particles run on "
-                                              "the host")
+                    raise NotImplementedError("rotating particles, explicit Euler steps and DF / DFC particles "
+                                              "run on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -382,8 +385,14 @@ class Engine:
         a.delta_type = DELTA_IDS[cfg.delta_type]
         a.rebuild = 1
         a.n_particles, a.lb_total = self.P, self.Lb
+        if self.method == "DFC" and self.P > 1:
+            # iblbm/ibm/strategies/dfc.py:56-110: every particle's markers as one point
+            # set with the first particle's arc length, lambda of that set each step
+            a.n_particles = 1
         a.moff, a.Lx, a.Ly, a.dvel, a.larea = (ptr(x) for x in (self.d_moff, self.d_Lx, self.d_Ly, self.d_dv,
                                                                  self.d_larea))
+        if self.method == "DFC" and self.P > 1:
+            a.moff = ptr(self.d_moff_set)
         a.dx, a.dy = self.st.dx, self.st.dy
         if self.tg and cfg.tg_with_ibm:
             a.dvel_scale = ptr(self.d_tg_cur)
@@ -810,9 +819,23 @@ class Engine:
         indices as floats and the particle centre in lattice units (:203-208).
         Under DF the reference sums the particle's marker forces instead
         (iblbm/ibm/forcing.py:262-275): F = -sum(Lf ds), T = -sum((rx Lfy - ry Lfx) ds),
-        rx = (Lx - cx) / dx over the markers this step used.
+        rx = (Lx - cx) / dx over the markers this step used; under DFC the sums of
+        its markers' Lagrangian forces F and of rx Fy - ry Fx.
         Returns (forces, torques or None)."""
         st = self.st
+        if self.method == "DFC":
+            # iblbm/ibm/strategies/dfc.py:114-128: sums of the markers' Lagrangian forces
+            fl = self.d_dfc_force[: 2 * self.Lb].reshape(self.Lb, 2).cpu().numpy()
+            moff = self.d_moff.cpu().numpy()
+            out, tq = [], ([] if torques else None)
+            for p, part in enumerate(st.particles):
+                f = fl[moff[p]:moff[p + 1]]
+                out.append(np.array([float(f[:, 0].sum()), float(f[:, 1].sum())]))
+                if torques:
+                    rx = (np.asarray(part.Lx) - float(part.pos[0])) / st.dx
+                    ry = (np.asarray(part.Ly) - float(part.pos[1])) / st.dy
+                    tq.append(float(np.sum(rx * f[:, 1] - ry * f[:, 0])))
+            return out, tq
         if self.method == "DF":
             Lfx, Lfy = self.d_Lfx.cpu().numpy(), self.d_Lfy.cpu().numpy()
             moff = self.d_moff.cpu().numpy()

@@ -461,11 +461,40 @@ class OracleSim:
         s.fib = fib_total
         velocity_correction(s.U, s.fib, s.ro, s.dt, cfg.incompressible_lbgk)
 
+    # iblbm/ibm/strategies/dfc.py:56-128 (DFC, apply_multi): every particle's markers as
+    # one point set (equal arc lengths required), lambda of that set each step, one
+    # correction, the moments again; a particle's force and torque are the sums of
+    # its markers' Lagrangian forces and of rx Fy - ry Fx, rx = (Lx - cx) / dx
+    def _apply_dfc_multi(self):
+        s, cfg = self.s, self.cfg
+        La = float(s.particles[0].Larea)
+        if any(abs(float(p.Larea) - La) > 1e-12 for p in s.particles):
+            raise ValueError("multi-particle DFC needs equal marker arc lengths")
+        Lx = np.ascontiguousarray(np.concatenate([p.Lx for p in s.particles]))
+        Ly = np.ascontiguousarray(np.concatenate([p.Ly for p in s.particles]))
+        dv = np.ascontiguousarray(np.concatenate([p.desired_velocity for p in s.particles]))
+        lam = dfc_lambda(Lx, Ly, La, s.dx, s.dy, s.ny, s.nx, cfg.delta_type)
+        s.fstar, s.dfc_force_lagr = dfc_correction(Lx, Ly, dv, s.fstar, lam, s.dx, s.dy, La, s.ny, s.nx,
+                                                   cfg.delta_type)
+        s.ro, s.U = macroscopic(s.fstar, cfg.incompressible_lbgk)
+        start = 0
+        for particle in s.particles:
+            end = start + len(particle.Lx)
+            fl = s.dfc_force_lagr[start:end]
+            particle._fib_force = np.array([float(fl[:, 0].sum()), float(fl[:, 1].sum())])
+            if cfg.enable_rotation:
+                rx = (np.asarray(particle.Lx) - float(particle.pos[0])) / s.dx
+                ry = (np.asarray(particle.Ly) - float(particle.pos[1])) / s.dy
+                particle._torque_new = float(np.sum(rx * fl[:, 1] - ry * fl[:, 0]))
+            start = end
+
     # iblbm/ibm/multi_particle.py:424-455 (MDF) and 347-421 (DF, uncoupled)
     def _apply_ibm_multi(self):
         s, cfg = self.s, self.cfg
         if cfg.ibm_method == "DF":
             return self._apply_df_multi()
+        if cfg.ibm_method == "DFC":
+            return self._apply_dfc_multi()
         if cfg.ibm_method != "MDF" or len(s.particles) < 2:
             raise NotImplementedError("multi-particle oracle covers DF and coupled MDF")
         parts = [(np.ascontiguousarray(p.Lx), np.ascontiguousarray(p.Ly),

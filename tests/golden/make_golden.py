@@ -234,6 +234,13 @@ RUN_CASES["c5_sed2_df_bgk_hat"] = dict(RUN_CASES["c5_sed2_mdf_cmmrt_p4"], ibm_me
                                        collision_model="BGK", max_steps=200)
 RUN_CASES["c5r_sed2_df_rot_semi"] = dict(RUN_CASES["c5r_sed2_mdf_rot_semi"], ibm_method="DF", max_steps=200)
 
+# two settling discs under DFC (iblbm/ibm/strategies/dfc.py:56-128): one correction over
+# both marker sets, per-particle Lagrangian force sums; translation only, and with
+# semi-implicit rotation
+RUN_CASES["c5_sed2_dfc_trt_p4"] = dict(RUN_CASES["c5_sed2_mdf_cmmrt_p4"], ibm_method="DFC", collision_model="TRT",
+                                       max_steps=200)
+RUN_CASES["c5r_sed2_dfc_rot_semi"] = dict(RUN_CASES["c5r_sed2_mdf_rot_semi"], ibm_method="DFC", max_steps=200)
+
 
 def _import_reference(path):
     os.environ["IBLBM_GPU"] = "0"
