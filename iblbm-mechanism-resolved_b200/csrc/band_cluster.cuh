@@ -55,7 +55,9 @@ constexpr int CL_HDR = 16;    // plan header ints: [C, S, Lb, nb, NMP, NLP, 0, 0
 constexpr int CL_JU = 8;      // list entries of a node spread by straight-line code
 
 // Plan sizes of one rank: markers per CTA (capacity NMP), nodes per CTA
-// (capacity NLP = markers x stencil slots, the most distinct nodes they cover).
+// (capacity NLP: the most distinct nodes the markers can cover, at most the
+// CTA's threads after its marker warps; a band whose ranks find more nodes
+// than that takes the single-CTA fallback).
 struct ClusterDims {
     int C, S, SW, nm, MW, NMP, NLP, rank_ints;
 };
@@ -70,7 +72,10 @@ __host__ __device__ inline ClusterDims cluster_dims(int Lb, int S, int C)
     d.nm = (Lb + C - 1) / C;
     d.MW = (d.nm + 31) / 32;
     d.NMP = cl_up2(d.nm);
-    d.NLP = cl_up2(d.nm * S);
+    // node capacity: the nodes the markers can cover, at most the CTA's threads
+    // after the marker warps (the plan checks the count it finds against it)
+    const int cover = d.nm * S, room = IBM_THREADS - 32 * d.MW;
+    d.NLP = cl_up2(cover < room ? cover : room);
     d.SW = S == 25 ? 5 : 3;
     // [nm, m0, nl, 0], slots int[S][NMP], separable weights double[2 SW][NMP]
     // (wx then wy), node band index, lattice index, owner flag, list length
@@ -103,7 +108,7 @@ __host__ __device__ inline size_t cluster_smem_bytes(int Lb, int S, int C)
 
 // Whether a band step can run on a cluster of C CTAs: one fixed body under MDF
 // (its lists cached between steps), the band layout in shared memory, and the
-// rank's marker warps plus one thread per node within one CTA.
+// rank's marker warps plus at least one warp of node threads within one CTA.
 inline bool cluster_eligible(const iblbm_ibm_args& a)
 {
     const int C = a.cluster_size;
@@ -112,7 +117,7 @@ inline bool cluster_eligible(const iblbm_ibm_args& a)
     if (a.field_ro || a.field_fstar || a.lb_total < C) return false;
     const int S = a.delta_type == 0 ? 25 : 9;
     const ClusterDims d = cluster_dims(a.lb_total, S, C);
-    if (d.MW * 32 + d.nm * S > IBM_THREADS || d.MW * C > 32) return false;
+    if (d.MW * 32 + 32 > IBM_THREADS || d.MW * C > 32) return false;
     if ((reinterpret_cast<uintptr_t>(a.cluster_plan) & 7) != 0) return false;
     if (cluster_smem_bytes(a.lb_total, S, C) > (size_t)IBM_SMEM_LIMIT) return false;
     return ibm_smem<double>(a) <= (size_t)IBM_SMEM_LIMIT;  // the layout fits (no global-static form)
@@ -204,7 +209,8 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_plan_kernel(const 
         int idx = block_exscan(cnt, ired, &nl);
         for (int b = b0; b < b1; ++b) loc[b] = loc[b] ? idx++ : -1;
         __syncthreads();
-        for (int b = tid; b < nb; b += IBM_THREADS) {
+        if (nl > d.NLP) bad = 1;  // more nodes than the CTA has node threads: the plan does not hold
+        for (int b = tid; b < nb && nl <= d.NLP; b += IBM_THREADS) {
             const int i = loc[b];
             if (i < 0) continue;
             const int u0 = cstart[b], n = cstart[b + 1] - u0;

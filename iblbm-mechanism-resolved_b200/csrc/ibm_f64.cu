@@ -45,7 +45,7 @@ extern "C" int iblbm_ibm_cluster_plan_ints(int lb_total, int delta_type, int clu
     if (cluster_size != 2 && cluster_size != 4 && cluster_size != 8) return 0;
     const int S = delta_type == 0 ? 25 : 9;
     const ClusterDims d = cluster_dims(lb_total, S, cluster_size);
-    if (lb_total < cluster_size || d.MW * 32 + d.nm * S > IBM_THREADS || d.MW * cluster_size > 32) return 0;
+    if (lb_total < cluster_size || d.MW * 32 + 32 > IBM_THREADS || d.MW * cluster_size > 32) return 0;
     if (cluster_smem_bytes(lb_total, S, cluster_size) > (size_t)IBM_SMEM_LIMIT) return 0;
     return (int)cluster_plan_ints(lb_total, S, cluster_size);
 }

@@ -205,8 +205,9 @@ typedef struct {
 int iblbm_ibm_step_f64(const iblbm_ibm_args *a, void *stream);
 /* Ints of the cluster plan of one body (iblbm_ibm_args.cluster_plan), or 0
  * when a body of lb_total markers cannot run on a cluster of that size (a
- * CTA holds its markers' warps and one thread per node under their stencils:
- * at most 152 markers with Peskin-4 on 8 CTAs).  No reference counterpart. */
+ * CTA holds its markers' warps and one thread per band node under their
+ * stencils; a band whose ranks cover more nodes than a CTA has threads left
+ * steps through the single-CTA fallback).  No reference counterpart. */
 int iblbm_ibm_cluster_plan_ints(int lb_total, int delta_type, int cluster_size);
 /* Same band step for callers that cannot allocate device memory at call time
  * (a host framework that owns all device allocations, or a service that

@@ -74,7 +74,9 @@ def test_cluster_plan_sizes():
     L = lib()
     assert L.iblbm_ibm_cluster_plan_ints(126, 0, 8) > 0
     assert L.iblbm_ibm_cluster_plan_ints(152, 0, 8) > 0
-    assert L.iblbm_ibm_cluster_plan_ints(153, 0, 8) == 0  # 20 markers x 25 slots + a warp > 512 threads
+    assert L.iblbm_ibm_cluster_plan_ints(153, 0, 8) > 0
+    assert L.iblbm_ibm_cluster_plan_ints(126, 0, 2) > 0
+    assert L.iblbm_ibm_cluster_plan_ints(1025, 0, 8) == 0  # 129 markers per CTA: 5 marker warps x 8 > 32 slots
     assert L.iblbm_ibm_cluster_plan_ints(392, 1, 8) > 0
     assert L.iblbm_ibm_cluster_plan_ints(126, 0, 3) == 0
     assert L.iblbm_ibm_cluster_plan_ints(4, 1, 8) == 0

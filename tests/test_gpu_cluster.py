@@ -93,3 +93,24 @@ def test_cluster_full_size_config2(torch):
     assert a.mdf_stats()["cluster"] and a.Lb == 126
     _same(a, b)
 
+
+
+def test_cluster_falls_back_when_nodes_exceed_the_threads(torch):
+    """A body of 251 markers (D = 80) on 2 CTAs: each rank's markers cover more
+    band nodes than a CTA has threads after its marker warps, so the plan does
+    not hold and the single-CTA step runs in the launch; the bits stay the same."""
+    a, b = _pair(torch, _cfg(cylinder_D_ratio=0.5), 2, steps=20)
+    assert a.Lb == 251
+    assert not a.mdf_stats()["cluster"]
+    assert a.d_plan[8:10].cpu().numpy().min() == 0
+    _same(a, b)
+
+
+@pytest.mark.parametrize("size", [2, 4])
+def test_cluster_sizes_full_size_config2(torch, size):
+    """Configuration 2 on 2 and 4 CTAs (63 and 32 markers per CTA)."""
+    import bench
+    cfg = bench.workload_config(max_steps=40)
+    a, b = _pair(torch, cfg, size, steps=40)
+    assert a.mdf_stats()["cluster"]
+    _same(a, b)
