@@ -28,7 +28,7 @@ from ._lib import (BC_IDS, COLL_IDS, DELTA_IDS, DELTA_RADIUS, IBM_IDS, BandView,
                    Geom, Ibm32Args, IbmArgs, TILES, check, lib, ptr)
 from .physics import (history_increment, mdf_relaxation_factor, net_gravity, oscillation_table,
                       rigid_markers)
-from .state import initial_velocity, initialize
+from .state import Particle, initial_velocity, initialize
 
 MDF_COUPLED_OMEGA_MAX = 0.8  # iblbm/ibm/multi_particle.py:33
 OUT_MOMENTS = 2  # output flag of a step that writes rho and U but not f*
@@ -84,9 +84,25 @@ class Engine:
             raise KeyError(f"unknown delta_type='{cfg.delta_type}'")
         if cfg.motion_type not in (None, "oscillating", "sedimentation"):
             raise ValueError(f"motion_type='{cfg.motion_type}' is not supported")
+        # the single-particle runtime (iblbm/runtime/scenarios/sedimentation_single.py):
+        # its disc steps as a one-particle set, with the single runtime's own force
+        # extraction, desired velocity and prescribed-velocity mode
+        self.single = cfg.motion_type == "sedimentation" and st.particles is None
+        if self.single:
+            if cfg.enable_rotation and cfg.rotation_coupling == "iterative" and cfg.ibm_method == "MDF":
+                raise NotImplementedError("iterative rotation coupling inside MDF is not on the accelerated path")
+            if cfg.settling_inertia_model not in ("none", "explicit_history", "feng_b2"):
+                raise NotImplementedError(f"settling_inertia_model='{cfg.settling_inertia_model}' for a single "
+                                          "particle is not on the accelerated path")
+            # iblbm/physics/sedimentation.py:97-128
+            cx, cy = cfg.cylinder_center
+            mass = cfg.rho_ratio * np.pi * st.lattice_r ** 2
+            st.particles = [Particle(pos=np.array([cx, cy], dtype=float), vel=np.zeros(2), vel_prev=np.zeros(2),
+                                     force=np.zeros(2), mass=mass, rho_ratio=cfg.rho_ratio, lattice_r=st.lattice_r,
+                                     r_domain=st.r, I_particle=0.5 * mass * st.lattice_r ** 2, Lx_c=st.Lx.copy(),
+                                     Ly_c=st.Ly.copy(), Lx=st.Lx.copy(), Ly=st.Ly.copy(), Lb=st.Lb, Larea=st.Larea,
+                                     desired_velocity=np.zeros((st.Lb, 2)), cx_init=cx, cy_init=cy)]
         if cfg.motion_type == "sedimentation":
-            if st.particles is None:
-                raise NotImplementedError("single-particle sedimentation runtime is not on the accelerated path")
             if cfg.settling_inertia_model == "full_volume":
                 raise NotImplementedError("full_volume inertia is not on the accelerated path")
             if cfg.time_integrator not in ("verlet", "euler_explicit"):
@@ -237,7 +253,8 @@ class Engine:
         self._torque_ij = None
         if st.particles is not None:
             self.dev_particles = True if device_particles is None else bool(device_particles)
-            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method != "MDF":
+            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method != "MDF" or \
+                    self.single:
                 # the torque, the angular Verlet step, the explicit Euler step and the
                 # Lagrangian force sums of DF and DFC run on the host
                 if device_particles:
@@ -698,6 +715,8 @@ class Engine:
             return self._sedimentation_step_euler(outputs)
         cfg, st = self.cfg, self.st
         rot = cfg.enable_rotation
+        if self.single and cfg.prescribed_velocity is not None:
+            return self._sedimentation_step_prescribed(outputs)
         for p in st.particles:  # runtime/scenarios/sedimentation_multi.py:36-80
             F = p.force + net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             vel_half = p.vel + 0.5 * st.dt * F / p.mass
@@ -712,10 +731,13 @@ class Engine:
             dv = np.empty((p.Lb, 2))
             dv[:, 0] = float(vel_half[0])
             dv[:, 1] = float(vel_half[1])
-            if rot and cfg.rotation_coupling == "semi_implicit" and p.omega != 0.0:
-                # U + omega x r with the last step's omega, physics/markers.py:41-60
-                dv[:, 0] += -p.omega * (p.Ly - float(p.pos[1])) / st.dx
-                dv[:, 1] += p.omega * (p.Lx - float(p.pos[0])) / st.dx
+            # U + omega x r (physics/markers.py:41-60) for semi-implicit coupling: the
+            # multi-particle runtime takes the last step's omega, the single-particle
+            # runtime this step's half-kicked one (sedimentation_single.py:148-158)
+            om = (p.omega_half if self.single else p.omega) if rot else 0.0
+            if rot and cfg.rotation_coupling == "semi_implicit" and om != 0.0:
+                dv[:, 0] += -om * (p.Ly - float(p.pos[1])) / st.dx
+                dv[:, 1] += om * (p.Lx - float(p.pos[0])) / st.dx
             p.desired_velocity = dv
             p.vel_half = vel_half
         self._upload_markers()
@@ -739,6 +761,31 @@ class Engine:
             p.vel_prev = p.vel.copy()
             p.vel = vel_new
             p.force = fp
+
+    def _sedimentation_step_prescribed(self, outputs):
+        """A single disc moved at cfg.prescribed_velocity
+        (runtime/scenarios/sedimentation_single.py:91-97,174-180): position and
+        markers advance, the desired velocity is the prescribed one, and after
+        the IB step the disc keeps that velocity and records the force."""
+        cfg, st = self.cfg, self.st
+        p = st.particles[0]
+        pv = np.array(cfg.prescribed_velocity, dtype=float)
+        p.pos = p.pos + st.dt * pv * st.dx
+        p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos)
+        dv = np.empty((p.Lb, 2))
+        dv[:, 0] = float(pv[0])
+        dv[:, 1] = float(pv[1])
+        p.desired_velocity = dv
+        p.vel_half = pv
+        self._upload_markers()
+        self._launch(outputs)
+        self.ttt += 1
+        if outputs:
+            self.last_out_step = self.ttt - 1
+        forces, _ = self.particle_forces()
+        p.vel = pv.copy()
+        p.fib_force = forces[0]
+        p.force = forces[0]
 
     def _l_int_z(self, p):
         """Angular momentum of the fluid inside particle p's disc from this step's
@@ -836,7 +883,7 @@ class Engine:
                     ry = (np.asarray(part.Ly) - float(part.pos[1])) / st.dy
                     tq.append(float(np.sum(rx * f[:, 1] - ry * f[:, 0])))
             return out, tq
-        if self.method == "DF":
+        if self.method == "DF" and not self.single:  # (the single runtime sums the field, below)
             Lfx, Lfy = self.d_Lfx.cpu().numpy(), self.d_Lfy.cpu().numpy()
             moff = self.d_moff.cpu().numpy()
             out, tq = [], ([] if torques else None)

@@ -40,6 +40,49 @@ def _sedimentation_record(p, ttt, d_lattice, g, cfg, dx, pid):
             "vy_star": float(p.vel[1] / u_g) if u_g > 1e-15 else 0.0}
 
 
+def _single_record(p, ttt, d_lattice, g, cfg, dx):
+    """The single-particle runtime's record (iblbm/diagnostics/internal_flow.py:156-214,
+    record_sedimentation_state, and runtime/scenarios/sedimentation_single.py:294-297):
+    distance fallen and velocities made dimensionless with u_g = sqrt(|rho_r - 1| g D),
+    and the hydrodynamic force."""
+    u_g = np.sqrt(abs(cfg.rho_ratio - 1.0) * g * d_lattice)
+    pos, vel = p.pos, p.vel
+    if u_g < 1e-15:
+        rec = {"step": int(ttt), "t_star": 0.0, "y_star": 0.0, "vy_star": 0.0, "vx_star": 0.0,
+               "x": float(pos[0]), "y": float(pos[1]), "vx": float(vel[0]), "vy": float(vel[1])}
+    else:
+        rec = {"step": int(ttt), "t_star": float(ttt * u_g / d_lattice),
+               "y_star": float((p.cy_init - pos[1]) / (d_lattice * dx)), "vy_star": float(-vel[1] / u_g),
+               "vx_star": float(vel[0] / u_g), "x": float(pos[0]), "y": float(pos[1]), "vx": float(vel[0]),
+               "vy": float(vel[1])}
+    rec["f_hydro_x"] = float(p.force[0])
+    rec["f_hydro_y"] = float(p.force[1])
+    return rec
+
+
+def _single_flow_diagnostics(rec, eng, cfg, d_lattice):
+    """The fluid inside the disc (sedimentation_single.py:298-322): residual
+    velocity, momentum and angular momentum from this step's fields."""
+    from .diagnostics import (compute_inside_residual, compute_internal_angular_momentum,
+                              compute_internal_momentum)
+    st = eng.read_state()
+    p = st.particles[0]
+    dx = st.dx
+    cx, cy = float(p.pos[0]), float(p.pos[1])
+    r_domain = st.lattice_r * dx
+    Eux, Euy = st.U[:, 0].reshape(st.ny, st.nx), st.U[:, 1].reshape(st.ny, st.nx)
+    ro = st.ro.reshape(st.ny, st.nx)
+    u_g = math.sqrt(abs(cfg.rho_ratio - 1.0) * st.gravity_lattice * d_lattice)
+    res = compute_inside_residual(Eux, Euy, dx, dx, cx, cy, d_lattice * dx, kappa=2.0, u_ref=max(float(u_g), 1e-12))
+    rec["inside_residual_mean"] = res["mean"]
+    rec["inside_residual_max"] = res["max"]
+    rec["inside_residual_mean_norm"] = res["mean_normalized"]
+    px, py = compute_internal_momentum(Eux, Euy, ro, dx, dx, cx, cy, r_domain)
+    rec["p_int_x"] = px
+    rec["p_int_y"] = py
+    rec["l_int_z"] = compute_internal_angular_momentum(Eux, Euy, ro, dx, dx, cx, cy, r_domain)
+
+
 def _stop_reason(p, cfg, dx):
     """iblbm/runtime/scenarios/sedimentation_common.py:19-66."""
     pos, r = p.pos, p.r_domain
@@ -83,6 +126,7 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
     ttt = 1
     ci = int(cfg.check_interval)
     sed = eng.st.particles is not None
+    single = eng.single
     d_lattice = 2.0 * eng.st.lattice_r
     # Without a stop rule, a callback or particle records nothing at a check
     # needs its values on the host before the run goes on: the Cd / Cl of many
@@ -126,7 +170,13 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
             ttt += 1
             continue
         if ttt % ci == 0:
-            if sed:
+            if single:
+                rec = _single_record(eng.st.particles[0], ttt, d_lattice, eng.st.gravity_lattice, cfg, eng.st.dx)
+                if cfg.diagnostics_interval and cfg.diagnostics_interval > 0 and ttt % cfg.diagnostics_interval == 0:
+                    _single_flow_diagnostics(rec, eng, cfg, d_lattice)
+                history.append(rec)
+                Cd = Cl = 0.0
+            elif sed:
                 rec = {"step": ttt, "particles": [
                     _sedimentation_record(p, ttt, d_lattice, eng.st.gravity_lattice, cfg, eng.st.dx, k)
                     for k, p in enumerate(eng.st.particles)]}
@@ -143,7 +193,10 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
                          elapsed=time.time() - t0, converged=converged)
             if sed:
                 p0 = eng.st.particles[0]
-                v = float(p0.vel[0]) if cfg.gravity_direction == "right" else float(p0.vel[1])
+                if single:  # sedimentation_single.py:332-345
+                    v = rec["vy_star"]
+                else:
+                    v = float(p0.vel[0]) if cfg.gravity_direction == "right" else float(p0.vel[1])
                 reason = "nan" if not math.isfinite(v) else _stop_reason(p0, cfg, eng.st.dx)
                 if reason is None and any(_near_wall(p, cfg, eng.st.dx) for p in eng.st.particles):
                     reason = "domain_bounds"
@@ -176,6 +229,12 @@ def run(cfg, verbose: bool = True, callback=None, save_dir=None, engine: Engine 
               "converged": converged, "final_step": ttt - 1, "termination_reason": termination}
     if sed:
         result["sedimentation_history"] = history
+    if single:
+        # the single-particle runtime keeps the disc on the state (iblbm/physics/sedimentation.py:109-128)
+        p = eng.st.particles[0]
+        state.particle_pos, state.particle_vel = p.pos.copy(), p.vel.copy()
+        state.particle_vel_prev, state.particle_force = p.vel_prev.copy(), p.force.copy()
+        state.particle_omega, state.particle_angle, state.particle_torque = p.omega, p.angle, p.torque
     elif eng.last_out_step > 0 and not eng.no_ibm:
         from .diagnostics import engine_slip
         result["slip"] = engine_slip(eng)  # marker slip of the last output step / U_ref

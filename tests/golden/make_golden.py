@@ -241,6 +241,47 @@ RUN_CASES["c5_sed2_dfc_trt_p4"] = dict(RUN_CASES["c5_sed2_mdf_cmmrt_p4"], ibm_me
                                        max_steps=200)
 RUN_CASES["c5r_sed2_dfc_rot_semi"] = dict(RUN_CASES["c5r_sed2_mdf_rot_semi"], ibm_method="DFC", max_steps=200)
 
+# Single settling discs (iblbm/runtime/scenarios/sedimentation_single.py): the
+# reference's single-particle runtime, whose state keeps the disc in
+# particle_pos / particle_vel / ... instead of a particle list.  Written as
+# sed1_<name>.npz: the engine is compared with them directly.
+_SED1_BASE = dict(Re=20, NN=81, xmax=1, ymax=4, cylinder_center=(0.47, 3.0), cylinder_D_ratio=0.25,
+                  lattice_u=0.05, inflow_u=0.0, bc_type="settling_channel", motion_type="sedimentation",
+                  rho_ratio=1.5, gravity=2e-5, marker_spacing_factor=1.0, max_steps=240, use_convergence=False,
+                  check_interval=40, mdf_iterations=20, mdf_min_iterations=5, mdf_tolerance=1e-6)
+SINGLE_CASES = {
+    # the layout of the bundled single-particle runs: DF + Peskin-4, BGK, explicit Euler, rotation
+    "df_euler_rot": dict(_SED1_BASE, delta_type="peskin4pt", ibm_method="DF", collision_model="BGK",
+                         settling_inertia_model="explicit_history", time_integrator="euler_explicit",
+                         enable_rotation=True, rotation_coupling="indirect"),
+    "mdf_verlet": dict(_SED1_BASE, delta_type="hat", ibm_method="MDF", collision_model="TRT",
+                       trt_magic_param=0.1875, settling_inertia_model="none"),
+    "dfc_verlet_semi_rot": dict(_SED1_BASE, delta_type="peskin4pt", ibm_method="DFC", collision_model="CM_MRT",
+                                settling_inertia_model="feng_b2", enable_rotation=True,
+                                rotation_coupling="semi_implicit"),
+    "df_prescribed": dict(_SED1_BASE, delta_type="hat", ibm_method="DF", collision_model="BGK",
+                          settling_inertia_model="none", prescribed_velocity=(0.0, -0.01)),
+    # with the fluid-inside-the-disc diagnostics every other check
+    "df_verlet_diag": dict(_SED1_BASE, delta_type="peskin4pt", ibm_method="DF", collision_model="TRT",
+                           trt_magic_param=0.1875, settling_inertia_model="explicit_history",
+                           diagnostics_interval=80),
+}
+
+
+def make_single(name, kw, out_dir):
+    from iblbm import SimConfig, run
+    res = run(SimConfig(**kw), verbose=False)
+    st = res["state"]
+    d = {"config_json": np.frombuffer(json.dumps(kw).encode(), dtype=np.uint8)}
+    for k, a in {"ro": st.ro, "U": st.U, "fib": st.fib, "fstar": st.fstar, "feq": st.feq}.items():
+        d[f"sha_{k}"] = np.frombuffer(bytes.fromhex(_sha(a)), dtype=np.uint8)
+    d["particle"] = np.array([*st.particle_pos, *st.particle_vel, *st.particle_force])
+    d["rotation"] = np.array([float(st.particle_omega), float(st.particle_angle), float(st.particle_torque)])
+    d["history_json"] = np.frombuffer(json.dumps(res["sedimentation_history"]).encode(), dtype=np.uint8)
+    d["final_step"] = np.array([res["final_step"]])
+    d["termination"] = np.frombuffer(res["termination_reason"].encode(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(out_dir, f"sed1_{name}.npz"), **d)
+
 
 def _import_reference(path):
     os.environ["IBLBM_GPU"] = "0"
@@ -430,6 +471,11 @@ def main():
             continue
         make_run(name, kw, HERE)
         print(f"run_{name}.npz written")
+    for name, kw in SINGLE_CASES.items():
+        if args.only not in (None, "sed1_" + name):
+            continue
+        make_single(name, kw, HERE)
+        print(f"sed1_{name}.npz written")
 
 
 if __name__ == "__main__":
