@@ -58,7 +58,7 @@ class IbmArgs(ctypes.Structure):
                 ("Lfy", _vp), ("dfc_force", _vp), ("stats", _vp), ("dstats", _vp), ("field_ro", _vp),
                 ("field_ux", _vp), ("field_uy", _vp), ("field_fstar", _vp), ("field_ustride", _i),
                 ("dvel_scale", _vp), ("dfc_rho_f", _d), ("wait_limit", ctypes.c_longlong), ("test_skip_copy", _i),
-                ("cluster_plan", _vp), ("cluster_size", _i)]
+                ("cluster_plan", _vp), ("cluster_size", _i), ("df_given_force", _i)]
 
 
 # The FP32 structs have the FP64 ones' fields in the same order (only pointee

@@ -685,7 +685,12 @@ __device__ __forceinline__ void ibm_step_body(const ARGS& a, const BcOf<SHIFTED>
     if (METHOD == IBM_DF) {
         // iblbm/ibm/df.py:93-154, summed over particles as ibm/multi_particle.py:404-421
         const bool incomp = a.c.incompressible != 0;
-        for (int l = tid; l < Lb; l += IBM_THREADS) {
+        for (int l = tid; l < Lb && a.df_given_force; l += IBM_THREADS) {
+            // the marker forces are given: only their spreading (Lux, Luy stay 0)
+            sh.Lfx[l] = (R)a.Lfx[l];
+            sh.Lfy[l] = (R)a.Lfy[l];
+        }
+        for (int l = tid; l < Lb && !a.df_given_force; l += IBM_THREADS) {
             R Rl, ux, uy;
             {
                 R dummy;
@@ -1565,6 +1570,7 @@ static int check_ibm_args(const ARGS* a, bool allow_gs = false)
     if (a->delta_type != 0 && a->delta_type != 1) return IBLBM_E_ARG;
     if (a->method != IBM_DF && a->method != IBM_MDF && a->method != IBM_DFC) return IBLBM_E_ARG;
     if ((a->method == IBM_DF || a->method == IBM_MDF) && !a->band_fib) return IBLBM_E_ARG;
+    if (a->df_given_force && (a->method != IBM_DF || !a->Lfx || !a->Lfy)) return IBLBM_E_ARG;
     if (a->method == IBM_DFC && (!a->band_df || !a->lambda || a->n_particles != 1)) return IBLBM_E_ARG;
     if (!a->xt_table && (!a->Lx || !a->Ly || !a->dvel)) return IBLBM_E_ARG;
     if (a->xt_table && (!a->Lx_c || !a->Ly_c || !a->step_counter || a->xt_len < 1)) return IBLBM_E_ARG;

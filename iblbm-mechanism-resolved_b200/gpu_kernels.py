@@ -100,10 +100,70 @@ def velocity_correction_gpu(U, fib, ro, dt, incompressible=False):
 # ---- immersed boundary: reference-shaped wrappers over the band kernel ---------
 _DELTA_TYPE_IDS = {"peskin4pt": 0, "hat": 1}
 _DELTA_STENCIL_A = {"peskin4pt": 2, "hat": 1}
+_BLOCK = 256
+
+
+def _grid(n):
+    """Launch grid of the reference's raw DF kernels (one thread per marker)."""
+    return ((int(n) + _BLOCK - 1) // _BLOCK,)
+
+
+class _RawKernel:
+    """The reference's raw-kernel call convention, kern(grid, block, args):
+    iblbm/gpu_kernels.py `_ibm_interp_force_kern` / `_ibm_spread_kern`, as
+    launched by iblbm/ibm/forcing.py:185-231 (the GPU branch of the per-particle
+    DF closure).  grid and block are accepted and ignored: the band step sizes
+    its own launch."""
+
+    def __init__(self, fn):
+        self._fn = fn
+
+    def __call__(self, grid, block, args):
+        return self._fn(*args)
+
+
+def _delta_name(delta_type_id):
+    return {v: k for k, v in _DELTA_TYPE_IDS.items()}[int(delta_type_id)]
+
+
+def _interp_force(Lx, Ly, desired_vel, Eux, Euy, Ro, dx, dy, dt, nx, ny, Lb, delta_type_id, stencil_a,
+                  incompressible, Lfx, Lfy, Lux, Luy):
+    """Per marker: interpolated velocity (Lux, Luy) and force
+    F = 2 rho (U_d - U) / dt (or 2 (U_d - U) / dt incompressible), written into
+    the given arrays; the DF band step on the given fields, bit for bit the
+    reference's CPU ibm_direct_forcing (iblbm/ibm/df.py:93-126)."""
+    nx, ny = int(nx), int(ny)
+    k = _band_call("DF", Lx, Ly, desired_vel, float(dx), float(dy), float(dt), 1.0, ny, nx,
+                   _delta_name(delta_type_id), bool(int(incompressible)), ro=_dev(Ro, "Ro").reshape(-1),
+                   ux=_dev(Eux, "Eux").reshape(-1), uy=_dev(Euy, "Euy").reshape(-1))
+    for dst, src in ((Lfx, "Lfx"), (Lfy, "Lfy"), (Lux, "Lux"), (Luy, "Luy")):
+        dst.reshape(-1).copy_(k[src][: int(Lb)])
+
+
+def _spread(Lfx, Lfy, Lx, Ly, dx, dy, Larea, nx, ny, Lb, delta_type_id, stencil_a, Efx, Efy):
+    """Add each marker's force, spread by its stencil weights times Larea, into
+    Efx / Efy ((ny, nx) fields; iblbm/ibm/df.py:128-154 order: stencil slot,
+    then marker)."""
+    torch = _t()
+    nx, ny = int(nx), int(ny)
+    dev = _dev(Lx, "Lx").device
+    N = nx * ny
+    ones = torch.ones(N, dtype=torch.float64, device=dev)
+    zeros = torch.zeros(N, dtype=torch.float64, device=dev)
+    k = _band_call("DF", Lx, Ly, None, float(dx), float(dy), 1.0, float(Larea), ny, nx, _delta_name(delta_type_id),
+                   False, ro=ones, ux=zeros, uy=zeros, given_force=(Lfx, Lfy))
+    nb = k["nb"]
+    f = k["fib"][: 2 * nb].reshape(nb, 2)
+    Efx.reshape(-1).index_add_(0, k["nodes_l"], f[:, 0])
+    Efy.reshape(-1).index_add_(0, k["nodes_l"], f[:, 1])
+
+
+_ibm_interp_force_kern = _RawKernel(_interp_force)
+_ibm_spread_kern = _RawKernel(_spread)
 
 
 def _band_call(method, Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_type, incompressible,
-               ro=None, ux=None, uy=None, ustride=1, fstar=None, lambda_k=None, rho_f=1.0):
+               ro=None, ux=None, uy=None, ustride=1, fstar=None, lambda_k=None, rho_f=1.0, given_force=None):
     """One band-kernel launch on caller-given fields (iblbm_ibm_step_f64 with
     field_*): returns the band's node list and outputs."""
     import numpy as np
@@ -150,6 +210,9 @@ def _band_call(method, Lx, Ly, desired_vel, dx, dy, dt, Larea, ny, nx, delta_typ
     a.list_cache = ptr(keep["lists"])
     a.band_capacity, a.box_capacity = B, N
     a.band_fib, a.band_df, a.scratch, a.iscratch = (ptr(keep[k]) for k in ("fib", "df", "scr", "iscr"))
+    if given_force is not None:  # spread the given marker forces (DF)
+        keep["Lfx"], keep["Lfy"] = (_dev(f, "Lf").reshape(-1).contiguous().clone() for f in given_force)
+        a.df_given_force = 1
     a.Lux, a.Luy, a.Lfx, a.Lfy, a.dfc_force = (ptr(keep[k]) for k in ("Lux", "Luy", "Lfx", "Lfy", "force"))
     a.stats, a.dstats = ptr(keep["stats"]), ptr(keep["dstats"])
     if fstar is not None:

@@ -190,6 +190,10 @@ typedef struct {
      * when the cluster ran the iterations. */
     int *cluster_plan;
     int cluster_size;
+    /* DF only: 1 spreads the marker forces given in Lfx / Lfy (inputs) instead
+     * of computing them from the velocity (the spreading half of the
+     * reference's raw DF kernels); Lux / Luy are then left 0 */
+    int df_given_force;
 } iblbm_ibm_args;
 
 /* Replaces: ibm_direct_forcing_gpu (iblbm/gpu_kernels.py:956-1042) called from
@@ -346,6 +350,7 @@ typedef struct {
     int test_skip_copy;
     int *cluster_plan;  /* not used by the FP32 step yet: NULL / 0 */
     int cluster_size;
+    int df_given_force;
     /* learned MDF warm start (single-body MDF only): mlp_mode bit 1 writes each
      * marker's 64 features before the MDF loop (mlp_features, lb_total x 64) and
      * the force it accumulates, sum over iterations of omega * Lf (mlp_targets,

@@ -82,6 +82,37 @@ def test_reference_shaped_ibm_wrappers(torch, units, delta):
     np.testing.assert_allclose(force.cpu().numpy(), u[f"dfc_{delta}_force"], rtol=1e-13, atol=1e-18)
 
 
+@pytest.mark.parametrize("delta", ["hat", "peskin4pt"])
+def test_raw_df_kernel_handles(torch, units, delta):
+    """_ibm_interp_force_kern and _ibm_spread_kern (the raw kernels the
+    reference's per-particle DF closure launches, iblbm/ibm/forcing.py:185-231)
+    with the reference's call convention: interpolated velocities equal to the
+    reference's own, and the spread of the computed marker forces equal to the
+    reference's DF field, bit for bit."""
+    from iblbm_b200 import gpu_kernels as gk
+    u = units
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    nx, ny, dx = int(u["i_nx"][0]), int(u["i_ny"][0]), float(u["i_dx"][0])
+    Lx, Ly, dv, La = d(u["i_Lx"]), d(u["i_Ly"]), d(u["i_dv"]), float(u["i_Larea"][0])
+    Eux, Euy, Ro = (d(u[k]).reshape(ny, nx) for k in ("i_Eux", "i_Euy", "i_Ro"))
+    Lb = int(Lx.numel())
+    for inc in (0, 1):
+        Lfx, Lfy, Lux, Luy = (torch.empty(Lb, dtype=torch.float64, device="cuda") for _ in range(4))
+        gk._ibm_interp_force_kern(gk._grid(Lb), (gk._BLOCK,),
+                                  (Lx, Ly, dv, Eux, Euy, Ro, dx, dx, 1.0, nx, ny, Lb, gk._DELTA_TYPE_IDS[delta],
+                                   gk._DELTA_STENCIL_A[delta], inc, Lfx, Lfy, Lux, Luy))
+        k = f"df_{delta}_{inc}"
+        np.testing.assert_array_equal(Lux.cpu().numpy(), u[k + "_Lux"])
+        np.testing.assert_array_equal(Luy.cpu().numpy(), u[k + "_Luy"])
+        Efx = torch.zeros(ny, nx, dtype=torch.float64, device="cuda")
+        Efy = torch.zeros_like(Efx)
+        gk._ibm_spread_kern(gk._grid(Lb), (gk._BLOCK,),
+                            (Lfx, Lfy, Lx, Ly, dx, dx, La, nx, ny, Lb, gk._DELTA_TYPE_IDS[delta],
+                             gk._DELTA_STENCIL_A[delta], Efx, Efy))
+        np.testing.assert_array_equal(Efx.cpu().numpy().ravel(), u[k + "_fib"][:, 0])
+        np.testing.assert_array_equal(Efy.cpu().numpy().ravel(), u[k + "_fib"][:, 1])
+
+
 def _cfg(kw):
     from iblbm_b200.config import SimConfig
     kw = dict(kw)
