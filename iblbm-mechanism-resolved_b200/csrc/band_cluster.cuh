@@ -1,9 +1,10 @@
 // band_cluster.cuh — the MDF band step of one fixed body spread over a
 // thread-block cluster (FP64 form).
 //
-// One CTA holds the whole band in the single-CTA step; its MDF iterations are
-// bound by that one SM's shared-memory pipe (gathers of band velocities and
-// marker forces).  Here the body's markers are split into C contiguous ranges,
+// One CTA holds the whole band in the single-CTA step; its MDF iterations wait
+// on that one SM's shared-memory pipe (gathers of band velocities and marker
+// forces) and on long per-thread chains.  Here the body's markers are split
+// into C contiguous ranges,
 // one per CTA of a cluster of C CTAs on C SMs.  CTA c owns
 //   * its markers [m0, m1): their stencil slots (CTA-local node, weight);
 //   * its nodes: every band node under one of its markers' stencils, with that
@@ -32,10 +33,11 @@
 // by iteration parity: a CTA that runs ahead writes the other buffer, and cannot
 // come back to this one before every CTA has passed the next cluster barrier.
 //
-// The per-CTA plan (marker ranges, node sets, lists in register order) is built
-// from the body's cached lists by ibm_cluster_plan_kernel right after each band
+// The per-CTA plan (marker ranges, node sets, lists, slot order) is built from
+// the body's cached lists by ibm_cluster_plan_kernel right after each band
 // rebuild.  When the plan does not hold (a list longer than the stencil, from
-// stencil slots clamped onto an edge node, or no band), the cluster's first CTA
+// stencil slots clamped onto an edge node; more nodes under a rank's markers
+// than the CTA has threads left; or no band), the cluster's first CTA
 // runs the single-CTA step instead and the others return, so the launch always
 // computes the step.
 //
