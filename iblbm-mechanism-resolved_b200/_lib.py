@@ -82,7 +82,11 @@ class ParticlesArgs(ctypes.Structure):
                 ("dt", _d), ("dx", _d), ("band_fib_part", _vp), ("band_count", _vp), ("band_capacity", _i),
                 ("forces_out", _vp), ("n_nodes", _i), ("band_nodes", _vp), ("pw_leaves", _i), ("pw_internal", _i),
                 ("pw_levels", _i), ("pw_leaf", _vp), ("pw_node", _vp), ("pw_level", _vp), ("pw_lut", _vp),
-                ("pw_span", _vp), ("pw_scratch", _vp)]
+                ("pw_span", _vp), ("pw_scratch", _vp), ("rotation", _i), ("semi_implicit", _i),
+                ("euler_trapezoidal", _i), ("nx", _i), ("dy", _d)]
+
+
+PARTICLE_STATE, PARTICLE_CONSTS = 21, 8  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)
 
 
 INERTIA_IDS = {"none": 0, "explicit_history": 1, "feng_b2": 2}

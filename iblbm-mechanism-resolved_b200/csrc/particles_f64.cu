@@ -4,16 +4,25 @@
 // (:36-80 half step, :83-111 full step) for up to 8 discs, in FP64 without
 // multiply-add contraction, with the same scalar expressions as the host step:
 //   half  F = F_h + G;  v_half = v + (0.5 dt) F / m [+ 0.5 c (v - v_prev)];
-//         x_next = x + (dt v_half) dx;  markers X = R(0) (X_c - X_0) + x_next;
-//         desired velocity v_half
+//         x_next = x + (dt v_half) dx;  [omega_half = omega + (0.5 dt) T / I;
+//         angle += dt omega_half];  markers X = R(angle) (X_c - X_0) + x_next;
+//         desired velocity v_half [+ omega x (X - x_next) / dx, semi-implicit]
 //   full  F_h = -sum over the band of the particle's spread force;
+//         [T = -sum of (i - x/dx) fy - (j - y/dy) fx;  omega = omega_half +
+//         (0.5 dt) T / I];
 //         v_new = v_half + (0.5 dt) (F_h + G) / m [+ 0.5 c (v - v_prev)]
 //         [+ (1 / rho_ratio) (v - v_prev)];  v_prev = v;  v = v_new;  x = x_next
 // (c = pi r^2 / m for the explicit-history inertia model, physics/inertia/
-// explicit_history.py:53-66; the rho-ratio term for feng_b2, feng_b2.py:33-48).
+// explicit_history.py:53-66; the rho-ratio term for feng_b2, feng_b2.py:33-48;
+// the angular kicks of physics/rigid_body.py:65-82, the marker rotation of
+// physics/markers.py:23-38 and the rigid-body velocity of :41-60).
 // One launch after the band kernel does the full step of this timestep and the
 // half step of the next, so the whole step stays on the device and can be
-// captured in a CUDA graph.
+// captured in a CUDA graph.  The explicit Euler step without rotation
+// (sedimentation_multi.py:126-190) is one launch after the band kernel too:
+//   v_new = v + dt F / m [+ c (v - v_prev)];  x_new = x + (dt v_new) dx, or
+//   x + (0.5 dt (v + v_new)) dx (trapezoidal);  [v_new += (1 / rho_ratio)
+//   (v - v_prev)];  then the next step's markers at x_new, desired velocity v_new.
 //
 // The force is -sum of the particle's spread force over the lattice.  The
 // reference sums its dense n_nodes x 2 field with numpy (np.sum: pairwise
@@ -24,8 +33,12 @@
 // a block without band entries sums to +0.0, and the inner nodes add their
 // children level by level.  Adding the zeros numpy adds would change no
 // partial sum, so the force equals numpy's bit for bit and the trajectories
-// equal the host step's.  Without a tree the sum runs in another fixed order
-// (deterministic, round-off apart from numpy's).
+// equal the host step's.  The torque is the same pairwise sum of its dense
+// moment-arm field (:203-208; its zero terms may be -0.0, which changes no
+// partial sum that is not itself zero).  Without a tree the sums run in
+// another fixed order (deterministic, round-off apart from numpy's).  The
+// rotated markers take the device's cos and sin of the angle, which may differ
+// from the host's in the last bit, so rotating runs are not bit for bit.
 #include <cstdint>
 #include "common.cuh"
 #include "../../include/iblbm_b200.h"
@@ -36,32 +49,39 @@ constexpr int PART_THREADS = 256;
 constexpr int PART_MAXP = 8;
 constexpr int PART_MAXB = 2048;  // band capacity limit of the band kernel
 
+// channel pc of the sums at band entry b (lattice index e): the force
+// components of the particles (pc < 2P), then their torque terms
 template <typename F>
-__device__ void particle_forces(const iblbm_particles_args& a, const F* fib, double* s_force)
+__device__ __forceinline__ double channel_value(const iblbm_particles_args& a, const F* fib, size_t pstride,
+                                                const double* s_ctr, int pc, int b, int e)
 {
-    __shared__ double red[2][PART_THREADS];
+    const int P2 = 2 * a.n_particles;
+    if (pc < P2) return (double)fib[(pc >> 1) * pstride + 2 * (size_t)b + (pc & 1)];
+    const int p = pc - P2;
+    const double fx = (double)fib[p * pstride + 2 * (size_t)b];
+    const double fy = (double)fib[p * pstride + 2 * (size_t)b + 1];
+    const double i = (double)(e % a.nx), j = (double)(e / a.nx);
+    return (i - s_ctr[2 * p]) * fy - (j - s_ctr[2 * p + 1]) * fx;
+}
+
+template <typename F>
+__device__ void particle_forces(const iblbm_particles_args& a, const F* fib, const double* s_ctr, int PC,
+                                double* s_force)
+{
+    __shared__ double red[PART_THREADS];
     const int nb = *a.band_count;
     const size_t pstride = 2 * (size_t)a.band_capacity;
-    for (int p = 0; p < a.n_particles; ++p) {
-        double sx = 0.0, sy = 0.0;
-        for (int b = threadIdx.x; b < nb; b += PART_THREADS) {
-            sx += (double)fib[p * pstride + 2 * b];
-            sy += (double)fib[p * pstride + 2 * b + 1];
-        }
-        red[0][threadIdx.x] = sx;
-        red[1][threadIdx.x] = sy;
+    for (int pc = 0; pc < PC; ++pc) {
+        double sum = 0.0;
+        for (int b = threadIdx.x; b < nb; b += PART_THREADS)
+            sum += channel_value(a, fib, pstride, s_ctr, pc, b, pc < 2 * a.n_particles ? 0 : a.band_nodes[b]);
+        red[threadIdx.x] = sum;
         __syncthreads();
         for (int w = PART_THREADS / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) {
-                red[0][threadIdx.x] += red[0][threadIdx.x + w];
-                red[1][threadIdx.x] += red[1][threadIdx.x + w];
-            }
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
             __syncthreads();
         }
-        if (threadIdx.x == 0) {
-            s_force[2 * p] = -red[0][0];
-            s_force[2 * p + 1] = -red[1][0];
-        }
+        if (threadIdx.x == 0) s_force[pc] = -red[0];
         __syncthreads();
     }
 }
@@ -79,11 +99,11 @@ __device__ __forceinline__ int pw_leaf_of(const iblbm_particles_args& a, int e)
 }
 
 template <typename F>
-__device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fib, double* s_force)
+__device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fib, const double* s_ctr, int PC,
+                                      double* s_force)
 {
     __shared__ int s_nodes[PART_MAXB];
     const int nb = min(*a.band_count, PART_MAXB);
-    const int P = a.n_particles, PC = 2 * P;
     const int L = a.pw_leaves;
     const size_t pstride = 2 * (size_t)a.band_capacity;
     double* v = a.pw_scratch;  // node id x PC
@@ -105,17 +125,17 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
         }
         const int cut = m - m % 8;
         for (int pc = 0; pc < PC; ++pc) {
-            const F* src = fib + (pc >> 1) * pstride + (pc & 1);
+            auto val = [&](int b) { return channel_value(a, fib, pstride, s_ctr, pc, b, s_nodes[b]); };
             double res;
             if (m < 8) {
                 res = 0.0;
-                for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+                for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
             } else {
                 double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
                 int b = lo;
-                for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += (double)src[2 * (size_t)b];
+                for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += val(b);
                 res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-                for (; b < nb && s_nodes[b] < off + m; ++b) res += (double)src[2 * (size_t)b];
+                for (; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
             }
             v[(size_t)li * PC + pc] = res;
         }
@@ -147,24 +167,45 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
 
 __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_particles_args a)
 {
-    __shared__ double s_force[2 * PART_MAXP];
+    __shared__ double s_force[3 * PART_MAXP];  // forces (2 per particle), then torques
+    __shared__ double s_ctr[2 * PART_MAXP];    // the centres in lattice units, for the torques
     __shared__ double s_next[2 * PART_MAXP], s_vh[2 * PART_MAXP];
+    __shared__ double s_rot[3 * PART_MAXP];    // cos, sin of the angle; omega of the rigid-body velocity
     const int P = a.n_particles;
     const double dt = a.dt, dx = a.dx;
-    if (a.phase & IBLBM_PARTICLES_FULL) {
-        if (a.pw_leaf) {
-            if (a.fib_f32) particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_force);
-            else particle_forces_exact(a, static_cast<const double*>(a.band_fib_part), s_force);
-        } else if (a.fib_f32) {
-            particle_forces(a, static_cast<const float*>(a.band_fib_part), s_force);
-        } else {
-            particle_forces(a, static_cast<const double*>(a.band_fib_part), s_force);
+    if (a.phase & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) {
+        const int PC = 2 * P + (a.rotation ? P : 0);
+        if (threadIdx.x < 2 * P) {
+            const int p = threadIdx.x >> 1, d = threadIdx.x & 1;
+            s_ctr[threadIdx.x] = a.state[IBLBM_PARTICLE_STATE * p + 10 + d] / (d ? a.dy : dx);
         }
+        __syncthreads();
+        if (a.pw_leaf) {
+            if (a.fib_f32) particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force);
+            else particle_forces_exact(a, static_cast<const double*>(a.band_fib_part), s_ctr, PC, s_force);
+        } else if (a.fib_f32) {
+            particle_forces(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force);
+        } else {
+            particle_forces(a, static_cast<const double*>(a.band_fib_part), s_ctr, PC, s_force);
+        }
+    }
+    if (a.phase & IBLBM_PARTICLES_FULL) {
         if (threadIdx.x < P) {
             const int p = threadIdx.x;
             double* s = a.state + IBLBM_PARTICLE_STATE * p;
             const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
             const double m = c[0], inv_rho = c[1], hc = c[2];
+            // this step's half-step values become current (the half step wrote them ahead)
+            s[6] = s[16];
+            s[7] = s[17];
+            if (a.rotation) {  // physics/rigid_body.py:77-82
+                s[13] = s[18];
+                s[14] = s[19];
+                s[20] = s[12];  // the omega this step's half step turned its markers with
+                const double T = s_force[2 * P + p];
+                s[12] = s[13] + ((0.5 * dt) * T) / c[7];
+                s[15] = T;
+            }
             for (int d = 0; d < 2; ++d) {
                 const double F = s_force[2 * p + d] + c[3 + d];
                 double vn = s[6 + d] + ((0.5 * dt) * F) / m;
@@ -179,6 +220,36 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
         }
         __syncthreads();
     }
+    if (a.phase & IBLBM_PARTICLES_EULER) {
+        if (threadIdx.x < P) {
+            const int p = threadIdx.x;
+            double* s = a.state + IBLBM_PARTICLE_STATE * p;
+            const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
+            const double m = c[0], inv_rho = c[1], hc = c[2];
+            for (int d = 0; d < 2; ++d) {
+                const double F = s_force[2 * p + d] + c[3 + d];
+                double vn = s[2 + d] + (dt * F) / m;
+                if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vn = vn + hc * (s[2 + d] - s[4 + d]);
+                const double xn = a.euler_trapezoidal ? s[d] + ((0.5 * dt) * (s[2 + d] + vn)) * dx
+                                                      : s[d] + (dt * vn) * dx;
+                if (a.model == IBLBM_INERTIA_FENG_B2) vn = vn + inv_rho * (s[2 + d] - s[4 + d]);
+                s[4 + d] = s[2 + d];      // v_prev = v
+                s[2 + d] = vn;            // v
+                s[6 + d] = vn;
+                s[16 + d] = vn;
+                s[8 + d] = s_force[2 * p + d];
+                s[d] = xn;
+                s[10 + d] = xn;
+                s_vh[2 * p + d] = vn;
+                s_next[2 * p + d] = xn;
+                if (a.forces_out) a.forces_out[2 * p + d] = s_force[2 * p + d];
+            }
+            s_rot[3 * p] = 1.0;
+            s_rot[3 * p + 1] = 0.0;
+            s_rot[3 * p + 2] = 0.0;
+        }
+        __syncthreads();
+    }
     if (a.phase & IBLBM_PARTICLES_HALF) {
         if (threadIdx.x < P) {
             const int p = threadIdx.x;
@@ -190,24 +261,41 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
                 double vh = s[2 + d] + ((0.5 * dt) * F) / m;
                 if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vh = vh + 0.5 * (hc * (s[2 + d] - s[4 + d]));
                 const double xn = s[d] + (dt * vh) * dx;
-                s[6 + d] = vh;
+                s[16 + d] = vh;
                 s[10 + d] = xn;
                 s_vh[2 * p + d] = vh;
                 s_next[2 * p + d] = xn;
             }
+            if (a.rotation) {  // physics/rigid_body.py:65-74
+                s[18] = s[12] + ((0.5 * dt) * s[15]) / c[7];
+                s[19] = s[14] + dt * s[18];
+            }
+            // R(0) = [[1, -0], [0, 1]] exactly, as the host's cos 0 and sin 0
+            s_rot[3 * p] = a.rotation ? cos(s[19]) : 1.0;
+            s_rot[3 * p + 1] = a.rotation ? sin(s[19]) : 0.0;
+            s_rot[3 * p + 2] = a.rotation && a.semi_implicit ? s[12] : 0.0;
         }
         __syncthreads();
+    }
+    if (a.phase & (IBLBM_PARTICLES_HALF | IBLBM_PARTICLES_EULER)) {
         const int Lb = a.moff[P];
         for (int l = threadIdx.x; l < Lb; l += PART_THREADS) {
             int p = 0;
             while (p + 1 < P && l >= a.moff[p + 1]) ++p;
             const double* c = a.consts + IBLBM_PARTICLE_CONSTS * p;
             const double rx = a.Lx_c[l] - c[5], ry = a.Ly_c[l] - c[6];
-            // R(0) = [[cos 0, -sin 0], [sin 0, cos 0]] = [[1, -0], [0, 1]]
-            a.Lx[l] = (1.0 * rx - 0.0 * ry) + s_next[2 * p];
-            a.Ly[l] = (0.0 * rx + 1.0 * ry) + s_next[2 * p + 1];
-            a.dvel[2 * l] = s_vh[2 * p];
-            a.dvel[2 * l + 1] = s_vh[2 * p + 1];
+            const double cs = s_rot[3 * p], sn = s_rot[3 * p + 1], om = s_rot[3 * p + 2];
+            const double X = (cs * rx - sn * ry) + s_next[2 * p];
+            const double Y = (sn * rx + cs * ry) + s_next[2 * p + 1];
+            double u = s_vh[2 * p], v = s_vh[2 * p + 1];
+            if (om != 0.0) {  // U + omega x r, physics/markers.py:41-60
+                u = u + ((-om) * (Y - s_next[2 * p + 1])) / dx;
+                v = v + (om * (X - s_next[2 * p])) / dx;
+            }
+            a.Lx[l] = X;
+            a.Ly[l] = Y;
+            a.dvel[2 * l] = u;
+            a.dvel[2 * l + 1] = v;
         }
     }
 }
@@ -220,11 +308,16 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
 {
     if (!a || a->n_particles < 1 || a->n_particles > PART_MAXP || !a->moff || !a->state || !a->consts)
         return IBLBM_E_ARG;
-    if ((a->phase & ~(IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_HALF)) || !a->phase) return IBLBM_E_ARG;
-    if ((a->phase & IBLBM_PARTICLES_FULL) && (!a->band_fib_part || !a->band_count || a->band_capacity < 1))
+    const int ph = a->phase;
+    if ((ph & ~(IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_HALF | IBLBM_PARTICLES_EULER)) || !ph) return IBLBM_E_ARG;
+    if ((ph & IBLBM_PARTICLES_EULER) && (ph != IBLBM_PARTICLES_EULER || a->rotation)) return IBLBM_E_ARG;
+    if ((ph & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) &&
+        (!a->band_fib_part || !a->band_count || a->band_capacity < 1))
         return IBLBM_E_ARG;
-    if ((a->phase & IBLBM_PARTICLES_HALF) && (!a->Lx_c || !a->Ly_c || !a->Lx || !a->Ly || !a->dvel))
+    if ((ph & (IBLBM_PARTICLES_HALF | IBLBM_PARTICLES_EULER)) &&
+        (!a->Lx_c || !a->Ly_c || !a->Lx || !a->Ly || !a->dvel))
         return IBLBM_E_ARG;
+    if (a->rotation && (!a->band_nodes || a->nx < 1 || !(a->dy > 0.0))) return IBLBM_E_ARG;
     if (a->model < IBLBM_INERTIA_NONE || a->model > IBLBM_INERTIA_FENG_B2) return IBLBM_E_ARG;
     if (a->pw_leaf && (!a->pw_node && a->pw_internal > 0)) return IBLBM_E_ARG;
     if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || !a->pw_lut || !a->pw_span ||

@@ -246,20 +246,26 @@ class Engine:
         self.d_pipe_status = torch.zeros(1, dtype=i32, device=dev)
         self.graphs = {}
         self._make_dense_variants()
-        # free particles: their Verlet step on the device by default (in the FP64
-        # form its force sums follow numpy's pairwise order, so it equals the
-        # host step bit for bit); device_particles=False keeps the host step
+        # free particles: their Verlet or explicit Euler step on the device by
+        # default (in the FP64 form its force and torque sums follow numpy's
+        # pairwise order, so it equals the host step bit for bit);
+        # device_particles=False keeps the host step.  Rotating FP64 runs keep
+        # the host step unless asked: their markers turn by the device's cos and
+        # sin, which may differ from the host's in the last bit
         self.dev_particles = False
         self._torque_ij = None
         if st.particles is not None:
-            self.dev_particles = True if device_particles is None else bool(device_particles)
-            if cfg.enable_rotation or cfg.time_integrator == "euler_explicit" or cfg.ibm_method != "MDF" or \
-                    self.single:
-                # the torque, the angular Verlet step, the explicit Euler step and the
-                # Lagrangian force sums of DF and DFC run on the host
+            rot = bool(cfg.enable_rotation)
+            euler = cfg.time_integrator == "euler_explicit"
+            default = not (rot and not self.f32)
+            self.dev_particles = default if device_particles is None else bool(device_particles)
+            if (rot and euler) or cfg.ibm_method != "MDF" or self.single:
+                # the Euler angular step (it needs the fluid's angular momentum inside
+                # each disc), the Lagrangian force sums of DF and DFC and the
+                # single-particle runtime run on the host
                 if device_particles:
-                    raise NotImplementedError("rotating particles, explicit Euler steps and DF / DFC particles "
-                                              "run on the host")
+                    raise NotImplementedError("rotating explicit Euler steps, DF / DFC particles and the "
+                                              "single-particle runtime run on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -271,13 +277,13 @@ class Engine:
         self.last_out_step = 0
 
     def _setup_device_particles(self):
-        from ._lib import INERTIA_IDS, ParticlesArgs
+        from ._lib import INERTIA_IDS, PARTICLE_CONSTS, PARTICLE_STATE, ParticlesArgs
         torch, st, cfg = self.torch, self.st, self.cfg
         if cfg.settling_inertia_model not in INERTIA_IDS:
             raise NotImplementedError(f"inertia model '{cfg.settling_inertia_model}' on the device")
         ps = st.particles
-        state = np.zeros((len(ps), 12))
-        consts = np.zeros((len(ps), 8))
+        state = np.zeros((len(ps), PARTICLE_STATE))
+        consts = np.zeros((len(ps), PARTICLE_CONSTS))
         for k, p in enumerate(ps):
             state[k, 0:2] = p.pos
             state[k, 2:4] = p.vel
@@ -285,9 +291,12 @@ class Engine:
             state[k, 6:8] = p.vel_half
             state[k, 8:10] = p.force
             state[k, 10:12] = p.pos
+            state[k, 12:16] = [p.omega, p.omega_half, p.angle, p.torque]
+            state[k, 16:18] = p.vel_half
+            state[k, 18:21] = [p.omega_half, p.angle, p.omega]
             g = net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             consts[k] = [p.mass, 1.0 / p.rho_ratio, np.pi * p.lattice_r ** 2 / p.mass, g[0], g[1], p.cx_init,
-                         p.cy_init, 0.0]
+                         p.cy_init, p.I_particle]
         self.d_pstate = torch.as_tensor(state.reshape(-1), device=self.dev)
         self.d_pconsts = torch.as_tensor(consts.reshape(-1), device=self.dev)
         self.d_Lxc_all = torch.as_tensor(np.concatenate([p.Lx_c for p in ps]), device=self.dev)
@@ -301,6 +310,14 @@ class Engine:
         a.dt, a.dx = float(st.dt), float(st.dx)
         a.band_fib_part, a.band_count, a.band_capacity = ptr(self.d_fib_part), ptr(self.d_count), self.B
         a.forces_out = ptr(self.d_pforces)
+        a.rotation = int(bool(cfg.enable_rotation))
+        a.semi_implicit = int(cfg.rotation_coupling == "semi_implicit")
+        a.euler_trapezoidal = int(cfg.sedimentation_euler_update_scheme == "trapezoidal")
+        a.nx, a.dy, a.n_nodes, a.band_nodes = st.nx, float(st.dy), self.N, ptr(self.d_nodes)
+        # Verlet: a half step before the first band kernel, then the full step of
+        # each timestep and the half step of the next; explicit Euler: the whole
+        # step after each band kernel, from the markers the host set up
+        self.part_phase = 4 if cfg.time_integrator == "euler_explicit" else 3
         if not self.f32:
             # the FP64 form sums the forces in numpy's pairwise order over the
             # dense lattice field, so the device step equals the host step bit
@@ -314,9 +331,8 @@ class Engine:
             self.d_pw_level = torch.as_tensor(levels, device=self.dev)
             self.d_pw_lut = torch.as_tensor(lut, device=self.dev)
             self.d_pw_span = torch.as_tensor(span.reshape(-1) if span.size else z2, device=self.dev)
-            self.d_pw_scratch = torch.zeros((len(leaves) + len(inner)) * 2 * len(ps), dtype=torch.float64,
+            self.d_pw_scratch = torch.zeros((len(leaves) + len(inner)) * 3 * len(ps), dtype=torch.float64,
                                             device=self.dev)
-            a.n_nodes, a.band_nodes = self.N, ptr(self.d_nodes)
             a.pw_leaves, a.pw_internal, a.pw_levels = len(leaves), len(inner), len(levels) - 1
             a.pw_leaf, a.pw_node, a.pw_level = ptr(self.d_pw_leaf), ptr(self.d_pw_node), ptr(self.d_pw_level)
             a.pw_lut, a.pw_span, a.pw_scratch = ptr(self.d_pw_lut), ptr(self.d_pw_span), ptr(self.d_pw_scratch)
@@ -329,12 +345,19 @@ class Engine:
         check(self.L.iblbm_particles_step_f64(ctypes.byref(a), stream), "iblbm_particles_step_f64")
 
     def pull_particles(self):
-        """Copy the device particle state (position, velocity, force of the last
-        completed step) into the host Particle objects."""
+        """Copy the device particle state of the last completed step (position,
+        velocities, force, angular velocity, angle, torque) into the host
+        Particle objects, with that step's markers and desired velocities."""
         if not self.dev_particles:
             return
         self.join()
-        s = self.d_pstate.reshape(-1, 12).cpu().numpy()
+        s = self.d_pstate.reshape(-1, _lib.PARTICLE_STATE).cpu().numpy()
+        euler = self.part_phase == 4
+        if euler:  # the device holds the markers the Euler step left for the next step
+            Lx, Ly = self.d_Lx.cpu().numpy(), self.d_Ly.cpu().numpy()
+            dv = self.d_dv[: 2 * self.Lb].reshape(-1, 2).cpu().numpy()
+            moff = self.d_moff.cpu().numpy()
+        rot, semi = bool(self.cfg.enable_rotation), self.cfg.rotation_coupling == "semi_implicit"
         for k, p in enumerate(self.st.particles):
             p.pos = s[k, 0:2].copy()
             p.vel = s[k, 2:4].copy()
@@ -342,6 +365,12 @@ class Engine:
             p.vel_half = s[k, 6:8].copy()
             p.force = s[k, 8:10].copy()
             p.fib_force = p.force.copy()
+            p.omega, p.omega_half, p.angle, p.torque = (float(x) for x in s[k, 12:16])
+            if euler:
+                p.Lx, p.Ly = Lx[moff[k]:moff[k + 1]].copy(), Ly[moff[k]:moff[k + 1]].copy()
+                p.desired_velocity = dv[moff[k]:moff[k + 1]].copy()
+            else:  # the markers of the last step (the device holds the next step's)
+                self._set_markers(p, p.vel_half, float(s[k, 20]) if rot and semi else 0.0)
 
     def _band_capacity(self, S):
         st = self.st
@@ -533,14 +562,17 @@ class Engine:
         if self.tg:
             self._tg_tick()
         if self.dev_particles and not self.part_started:
-            self._particles(s, 2)  # half step of the first timestep
+            if self.part_phase == 3:
+                self._particles(s, 2)  # half step of the first timestep
+            else:
+                self._upload_markers()  # the Euler step starts from the set-up markers
             self.part_started = True
         if self.no_ibm:
             self.rebuild_next = False
         else:
             self._ibm(s, excl_check=False)
         if self.dev_particles:
-            self._particles(s, 3)  # full step of this timestep, half step of the next
+            self._particles(s, self.part_phase)  # full step of this timestep (and half step of the next)
         if events:
             events[1].record()
         self._dense(self.dense_full, outputs, s)
@@ -561,7 +593,7 @@ class Engine:
         side.wait_event(self.ev_bulk)
         self._ibm(side.cuda_stream, excl_check=True)
         if self.dev_particles:
-            self._particles(side.cuda_stream, 3)
+            self._particles(side.cuda_stream, self.part_phase)
         self._dense(self.dense_box, outputs, side.cuda_stream)
         main.wait_event(self.ev_side)
         self.ev_side.record(side)
@@ -727,18 +759,11 @@ class Engine:
             if rot:  # angular half kick, physics/rigid_body.py:65-74
                 p.omega_half = p.omega + 0.5 * st.dt * p.torque / p.I_particle
                 p.angle += st.dt * p.omega_half
-            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=p.angle if rot else 0.0)
-            dv = np.empty((p.Lb, 2))
-            dv[:, 0] = float(vel_half[0])
-            dv[:, 1] = float(vel_half[1])
             # U + omega x r (physics/markers.py:41-60) for semi-implicit coupling: the
             # multi-particle runtime takes the last step's omega, the single-particle
             # runtime this step's half-kicked one (sedimentation_single.py:148-158)
             om = (p.omega_half if self.single else p.omega) if rot else 0.0
-            if rot and cfg.rotation_coupling == "semi_implicit" and om != 0.0:
-                dv[:, 0] += -om * (p.Ly - float(p.pos[1])) / st.dx
-                dv[:, 1] += om * (p.Lx - float(p.pos[0])) / st.dx
-            p.desired_velocity = dv
+            self._set_markers(p, vel_half, om if cfg.rotation_coupling == "semi_implicit" else 0.0)
             p.vel_half = vel_half
         self._upload_markers()
         self._launch(outputs)
@@ -761,6 +786,19 @@ class Engine:
             p.vel_prev = p.vel.copy()
             p.vel = vel_new
             p.force = fp
+
+    def _set_markers(self, p, vel, om):
+        """Particle p's markers at its position and angle (physics/markers.py:23-38)
+        and their desired velocity vel + om x (X - x) / dx (:41-60; om = 0.0: vel)."""
+        rot = self.cfg.enable_rotation
+        p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, p.pos, angle=p.angle if rot else 0.0)
+        dv = np.empty((p.Lb, 2))
+        dv[:, 0] = float(vel[0])
+        dv[:, 1] = float(vel[1])
+        if om != 0.0:
+            dv[:, 0] += -om * (p.Ly - float(p.pos[1])) / self.st.dx
+            dv[:, 1] += om * (p.Lx - float(p.pos[0])) / self.st.dx
+        p.desired_velocity = dv
 
     def _sedimentation_step_prescribed(self, outputs):
         """A single disc moved at cfg.prescribed_velocity
@@ -850,14 +888,7 @@ class Engine:
             p.vel = vel_new
             p.pos = pos_new
             p.force = fp
-            p.Lx, p.Ly = rigid_markers(p.Lx_c, p.Ly_c, p.cx_init, p.cy_init, pos_new, angle=p.angle if rot else 0.0)
-            dv = np.empty((p.Lb, 2))
-            dv[:, 0] = float(vel_new[0])
-            dv[:, 1] = float(vel_new[1])
-            if rot and p.omega != 0.0:  # U + omega x r, physics/markers.py:41-60
-                dv[:, 0] += -p.omega * (p.Ly - float(pos_new[1])) / st.dx
-                dv[:, 1] += p.omega * (p.Lx - float(pos_new[0])) / st.dx
-            p.desired_velocity = dv
+            self._set_markers(p, vel_new, p.omega if rot else 0.0)
 
     def particle_forces(self, torques=False):
         """-sum of each particle's spread force over the lattice, summed like the

@@ -402,19 +402,29 @@ int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *gra
                          int n, float lr, int step, float *loss, int apply, void *stream);
 
 /* ---- rigid particles of sedimentation runs on the device -------------------
- * Replaces the host Velocity-Verlet step of runtime/scenarios/
- * sedimentation_multi.py:36-111 (inertia models none / explicit_history /
- * feng_b2, no rotation).  Per particle, state holds IBLBM_PARTICLE_STATE
- * doubles: pos(2), vel(2), vel_prev(2), vel_half(2), force(2), pos_next(2);
- * consts holds IBLBM_PARTICLE_CONSTS doubles: mass, 1/rho_ratio, pi r^2/mass,
- * net gravity (2), initial centre (2), unused.  phase FULL finishes the current
- * step from the band kernel's per-particle forces (band_fib_part, particles x
- * band_capacity x 2, FP32 when fib_f32); phase HALF starts the next one: new
- * marker positions Lx, Ly and desired velocities dvel. */
-#define IBLBM_PARTICLE_STATE 12
+ * Replaces the host particle steps of runtime/scenarios/sedimentation_multi.py:
+ * the Velocity-Verlet step (:36-111, with the angular half and full kicks of
+ * physics/rigid_body.py:65-82 when rotation is on) and the explicit Euler step
+ * without rotation (:126-190, physics/rigid_body.py:84-98), inertia models
+ * none / explicit_history / feng_b2.  Per particle, state holds
+ * IBLBM_PARTICLE_STATE doubles: pos(2), vel(2), vel_prev(2), vel_half(2),
+ * force(2), pos_next(2), omega, omega_half, angle, torque, and the half step's
+ * look-ahead vel_half(2), omega_half, angle of the next step (pos_next,
+ * vel_half, omega_half and angle become current in its full step, so between
+ * launches the state is that of the last completed step), then the omega of
+ * the last step's rigid-body marker velocity; consts holds
+ * IBLBM_PARTICLE_CONSTS doubles: mass, 1/rho_ratio, pi r^2/mass, net gravity
+ * (2), initial centre (2), moment of inertia.  phase FULL finishes the
+ * current Verlet step from the band kernel's per-particle forces
+ * (band_fib_part, particles x band_capacity x 2, FP32 when fib_f32); phase HALF
+ * starts the next one: new marker positions Lx, Ly and desired velocities
+ * dvel; phase EULER (alone) does a whole explicit Euler step after the band
+ * kernel and leaves the next step's markers and desired velocities. */
+#define IBLBM_PARTICLE_STATE 21
 #define IBLBM_PARTICLE_CONSTS 8
 #define IBLBM_PARTICLES_FULL 1
 #define IBLBM_PARTICLES_HALF 2
+#define IBLBM_PARTICLES_EULER 4
 #define IBLBM_INERTIA_NONE 0
 #define IBLBM_INERTIA_EXPLICIT_HISTORY 1
 #define IBLBM_INERTIA_FENG_B2 2
@@ -451,6 +461,15 @@ typedef struct {
     const int *pw_lut;
     const int *pw_span;
     double *pw_scratch;
+    /* Rotation (Verlet only): the torque T = -sum over the lattice of
+     * (i - x/dx) fy - (j - y/dy) fx (node (i, j) = band_nodes entry e as
+     * (e % nx, e / nx), x, y the centre), summed like the forces; markers
+     * X = R(angle) (X_c - X_0) + x; semi_implicit adds omega x r to the desired
+     * velocity (physics/markers.py:41-60).  Needs band_nodes and nx.
+     * euler_trapezoidal: the position update of the Euler step with the mean of
+     * the old and new velocities (else the new one). */
+    int rotation, semi_implicit, euler_trapezoidal, nx;
+    double dy;
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);

@@ -42,6 +42,8 @@ def test_struct_layout_matches_c(tmp_path):
         for f in fl:
             cf = "lambda" if f == "lambda_" else f
             lines.append(f'printf("{st}.{f} %zu\\n", offsetof({st}, {cf}));')
+    lines.append('printf("IBLBM_PARTICLE_STATE %d\\n", IBLBM_PARTICLE_STATE);')
+    lines.append('printf("IBLBM_PARTICLE_CONSTS %d\\n", IBLBM_PARTICLE_CONSTS);')
     lines.append("return 0;}")
     probe.write_text("\n".join(lines))
     exe = tmp_path / "probe"
@@ -55,6 +57,8 @@ def test_struct_layout_matches_c(tmp_path):
         assert int(out[st]) == ctypes.sizeof(cls), st
         for f, _ in cls._fields_:
             assert int(out[f"{st}.{f}"]) == getattr(cls, f).offset, (st, f)
+    assert int(out["IBLBM_PARTICLE_STATE"]) == _lib.PARTICLE_STATE
+    assert int(out["IBLBM_PARTICLE_CONSTS"]) == _lib.PARTICLE_CONSTS
 
 
 def test_rejects_bad_arguments_without_a_gpu():

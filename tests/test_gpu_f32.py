@@ -234,16 +234,18 @@ def test_f32_config1_geometry_long(torch):
     _check_forces(r64, r32)
 
 
+@pytest.mark.parametrize("name", ["c5_sed2_mdf_cmmrt_p4", "c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_device_particles_match_host_step(torch, precision):
-    """The Verlet step on the device against the host step (bit-exact to the
-    reference in FP64).  In the FP64 form the device sums each particle's
-    force in numpy's pairwise order over the lattice, so trajectories, forces,
-    fields and the sedimentation records are equal bit for bit; the FP32 form
-    sums in a fixed order of its own (trajectories within 1e-9 relative)."""
+def test_device_particles_match_host_step(torch, precision, name):
+    """The Verlet and explicit Euler steps on the device against the host step
+    (bit-exact to the reference in FP64).  In the FP64 form the device sums
+    each particle's force in numpy's pairwise order over the lattice, so
+    trajectories, forces, fields and the sedimentation records are equal bit
+    for bit; the FP32 form sums in a fixed order of its own (trajectories
+    within 1e-9 relative)."""
     from iblbm_b200 import run
     from iblbm_b200.engine import Engine
-    cfg = _cfg(RUN_CASES["c5_sed2_mdf_cmmrt_p4"])
+    cfg = _cfg(RUN_CASES[name])
     host = run(cfg, verbose=False, engine=Engine(cfg, precision=precision, device_particles=False))
     dev = run(cfg, verbose=False, engine=Engine(cfg, precision=precision, device_particles=True))
     assert dev["engine"].status() == 0 and dev["engine"].dev_particles
@@ -252,6 +254,8 @@ def test_device_particles_match_host_step(torch, precision):
             np.testing.assert_array_equal(p.pos, q.pos)
             np.testing.assert_array_equal(p.vel, q.vel)
             np.testing.assert_array_equal(p.force, q.force)
+            np.testing.assert_array_equal(p.Lx, q.Lx)
+            np.testing.assert_array_equal(p.desired_velocity, q.desired_velocity)
         assert dev["sedimentation_history"] == host["sedimentation_history"]
         for k in ("ro", "U", "fstar", "fib"):
             np.testing.assert_array_equal(getattr(dev["state"], k), getattr(host["state"], k), err_msg=k)
@@ -259,6 +263,37 @@ def test_device_particles_match_host_step(torch, precision):
         for p, q in zip(dev["state"].particles, host["state"].particles):
             np.testing.assert_allclose(p.pos, q.pos, rtol=1e-9, atol=0)
             np.testing.assert_allclose(p.vel, q.vel, rtol=1e-9, atol=1e-9 * float(np.max(np.abs(q.vel))))
+
+
+@pytest.mark.parametrize("name", ["c5r_sed2_mdf_rot_indirect", "c5r_sed2_mdf_rot_semi", "c5r_sed2_mdf_rot_iterative"])
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_device_rotation_matches_host_step(torch, precision, name):
+    """Rotating discs with the Verlet step on the device (torque summed like
+    the forces, angular half and full kicks, markers turned by the device's cos
+    and sin) against the host step.  The torque sums follow numpy's order in
+    the FP64 form; cos and sin may differ from the host's in the last bit, so
+    the bar is round-off: FP64 within 1e-12 relative (equal bit for bit in
+    the measured runs), FP32 (whose device sums run in another order)
+    positions and velocities within 1e-9 relative, angles, angular velocities
+    and torques within 1e-6 of their magnitudes."""
+    from iblbm_b200 import run
+    from iblbm_b200.engine import Engine
+    cfg = _cfg(RUN_CASES[name])
+    host = run(cfg, verbose=False, engine=Engine(cfg, precision=precision, device_particles=False))
+    dev = run(cfg, verbose=False, engine=Engine(cfg, precision=precision, device_particles=True))
+    assert dev["engine"].status() == 0 and dev["engine"].dev_particles
+    for p, q in zip(dev["state"].particles, host["state"].particles):
+        print(f"{name} {precision}: angle {p.angle:.17e} / {q.angle:.17e}, omega {p.omega:.17e} / {q.omega:.17e}, "
+              f"pos {np.max(np.abs(p.pos - q.pos)):.3e}")
+        assert q.angle != 0.0 and q.omega != 0.0
+        tol, atol = (1e-12, 1e-12) if precision == "f64" else (1e-9, 1e-6)
+        np.testing.assert_allclose(p.pos, q.pos, rtol=tol, atol=0)
+        np.testing.assert_allclose(p.vel, q.vel, rtol=tol, atol=tol * float(np.max(np.abs(q.vel))))
+        assert abs(p.angle - q.angle) <= atol * abs(q.angle)
+        assert abs(p.omega - q.omega) <= atol * abs(q.omega)
+        assert abs(p.torque - q.torque) <= atol * abs(q.torque)
+    # default: FP32 rotating runs step on the device, FP64 ones on the host
+    assert Engine(cfg, precision=precision).dev_particles == (precision == "f32")
 
 
 @pytest.mark.parametrize("tile", ["node", "rows4", "pipe4x2", "pipe8x2"])
