@@ -83,10 +83,11 @@ class ParticlesArgs(ctypes.Structure):
                 ("forces_out", _vp), ("n_nodes", _i), ("band_nodes", _vp), ("pw_leaves", _i), ("pw_internal", _i),
                 ("pw_levels", _i), ("pw_leaf", _vp), ("pw_node", _vp), ("pw_level", _vp), ("pw_lut", _vp),
                 ("pw_span", _vp), ("pw_scratch", _vp), ("rotation", _i), ("semi_implicit", _i),
-                ("euler_trapezoidal", _i), ("nx", _i), ("dy", _d)]
+                ("euler_trapezoidal", _i), ("nx", _i), ("dy", _d), ("rho", _vp), ("U", _vp), ("moments_f32", _i),
+                ("ny", _i), ("lint_scratch", _vp), ("lint_capacity", _i)]
 
 
-PARTICLE_STATE, PARTICLE_CONSTS = 21, 8  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)
+PARTICLE_STATE, PARTICLE_CONSTS = 22, 9  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)
 
 
 INERTIA_IDS = {"none": 0, "explicit_history": 1, "feng_b2": 2}

@@ -18,11 +18,16 @@
 // physics/markers.py:23-38 and the rigid-body velocity of :41-60).
 // One launch after the band kernel does the full step of this timestep and the
 // half step of the next, so the whole step stays on the device and can be
-// captured in a CUDA graph.  The explicit Euler step without rotation
-// (sedimentation_multi.py:126-190) is one launch after the band kernel too:
+// captured in a CUDA graph.  The explicit Euler step (sedimentation_multi.py:
+// 126-190) is one launch after the band kernel too (after the whole lattice
+// pass when rotating):
+//   [L = the fluid's angular momentum inside the disc from this step's rho, U;
+//   omega_new = omega + (L - L_prev + dt T) / I;  angle += dt omega_new, or
+//   0.5 dt (omega + omega_new) (trapezoidal)];
 //   v_new = v + dt F / m [+ c (v - v_prev)];  x_new = x + (dt v_new) dx, or
 //   x + (0.5 dt (v + v_new)) dx (trapezoidal);  [v_new += (1 / rho_ratio)
-//   (v - v_prev)];  then the next step's markers at x_new, desired velocity v_new.
+//   (v - v_prev)];  then the next step's markers at x_new (turned by the
+//   angle), desired velocity v_new [+ omega_new x r].
 //
 // The force is -sum of the particle's spread force over the lattice.  The
 // reference sums its dense n_nodes x 2 field with numpy (np.sum: pairwise
@@ -165,12 +170,131 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
     __syncthreads();
 }
 
+// numpy's pairwise summation of n values (the tree of the file comment):
+// leaves of at most 128 values, each summed in 8 strided accumulators and a
+// tail, a longer range split at half its length rounded down to a multiple of 8
+__device__ double pw_block(const double* v, int n)
+{
+    if (n < 8) {
+        double res = 0.0;
+        for (int i = 0; i < n; ++i) res += v[i];
+        return res;
+    }
+    double r[8];
+    for (int k = 0; k < 8; ++k) r[k] = v[k];
+    int i = 8;
+    for (; i < n - n % 8; i += 8)
+        for (int k = 0; k < 8; ++k) r[k] += v[i + k];
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += v[i];
+    return res;
+}
+
+__device__ void pw_collect(int off, int n, int* loff, int* llen, int& cnt)
+{
+    if (n <= 128) {
+        loff[cnt] = off;
+        llen[cnt] = n;
+        ++cnt;
+        return;
+    }
+    int n2 = n / 2;
+    n2 -= n2 % 8;
+    pw_collect(off, n2, loff, llen, cnt);
+    pw_collect(off + n2, n - n2, loff, llen, cnt);
+}
+
+__device__ double pw_fold(int n, const double* lsum, int& li)
+{
+    if (n <= 128) return lsum[li++];
+    int n2 = n / 2;
+    n2 -= n2 % 8;
+    const double x = pw_fold(n2, lsum, li);
+    const double y = pw_fold(n - n2, lsum, li);
+    return x + y;
+}
+
+constexpr int PW_MAXLEAVES = 512;  // every leaf but a lone one holds at least 64 values
+constexpr int LINT_MAX = 64 * (PW_MAXLEAVES - 1);
+
+// The fluid's angular momentum inside a disc (centre px, py, radius r) from
+// this step's rho and U: diagnostics/internal_flow.py:220-262 as the host
+// restates it — the box of half-width int(r/dx) + 2 around the rounded centre
+// (round half to even), clipped to the lattice, the nodes with
+// RX^2 + RY^2 <= (r/dx)^2 in row order, each value (RX rho) uy - (RY rho) ux,
+// summed pairwise.  Block-wide; the sum is returned to thread 0.
+template <typename T>
+__device__ double disc_angular_momentum(const iblbm_particles_args& a, const T* rho, const T* U, double px,
+                                        double py, double r)
+{
+    __shared__ int s_base, s_nleaves;
+    __shared__ int s_wcount[PART_THREADS / 32];
+    __shared__ int s_loff[PW_MAXLEAVES], s_llen[PW_MAXLEAVES];
+    __shared__ double s_lsum[PW_MAXLEAVES];
+    const double dx = a.dx;
+    const double ci = px / dx, cj = py / dx, rl = r / dx;
+    const int ii = (int)rint(ci), jj = (int)rint(cj), rr = (int)rl + 2;
+    const int i0 = max(0, ii - rr), i1 = min(a.nx, ii + rr + 1);
+    const int j0 = max(0, jj - rr), j1 = min(a.ny, jj + rr + 1);
+    const int W = max(0, i1 - i0), H = max(0, j1 - j0), nbox = W * H;
+    const double r2 = rl * rl;
+    const int cap = min(a.lint_capacity, LINT_MAX);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int c0 = 0; c0 < nbox; c0 += PART_THREADS) {
+        const int k = c0 + (int)threadIdx.x;
+        bool in = false;
+        double val = 0.0;
+        if (k < nbox) {
+            const int i = i0 + k % W, j = j0 + k / W;
+            const double RX = (double)i - ci, RY = (double)j - cj;
+            in = RX * RX + RY * RY <= r2;
+            if (in) {
+                const size_t e = (size_t)j * a.nx + i;
+                const double ro = (double)rho[e], ux = (double)U[2 * e], uy = (double)U[2 * e + 1];
+                val = (RX * ro) * uy - (RY * ro) * ux;
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) s_wcount[w] = __popc(bal);
+        __syncthreads();
+        int off = s_base + __popc(bal & ((1u << lane) - 1u));
+        for (int q = 0; q < w; ++q) off += s_wcount[q];
+        if (in && off < cap) a.lint_scratch[off] = val;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = s_base;
+            for (int q = 0; q < PART_THREADS / 32; ++q) t += s_wcount[q];
+            s_base = t;
+        }
+        __syncthreads();
+    }
+    const int n = min(s_base, cap);
+    if (threadIdx.x == 0) {
+        int cnt = 0;
+        if (n > 0) pw_collect(0, n, s_loff, s_llen, cnt);
+        s_nleaves = cnt;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < s_nleaves; l += PART_THREADS) s_lsum[l] = pw_block(a.lint_scratch + s_loff[l], s_llen[l]);
+    __syncthreads();
+    double total = 0.0;
+    if (threadIdx.x == 0 && n > 0) {
+        int li = 0;
+        total = pw_fold(n, s_lsum, li);
+    }
+    __syncthreads();
+    return total;
+}
+
 __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_particles_args a)
 {
     __shared__ double s_force[3 * PART_MAXP];  // forces (2 per particle), then torques
     __shared__ double s_ctr[2 * PART_MAXP];    // the centres in lattice units, for the torques
     __shared__ double s_next[2 * PART_MAXP], s_vh[2 * PART_MAXP];
     __shared__ double s_rot[3 * PART_MAXP];    // cos, sin of the angle; omega of the rigid-body velocity
+    __shared__ double s_lint[PART_MAXP];       // the fluid's angular momentum inside each disc
     const int P = a.n_particles;
     const double dt = a.dt, dx = a.dx;
     if (a.phase & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) {
@@ -221,6 +345,19 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
         __syncthreads();
     }
     if (a.phase & IBLBM_PARTICLES_EULER) {
+        if (a.rotation) {
+            for (int p = 0; p < P; ++p) {
+                const double* s = a.state + IBLBM_PARTICLE_STATE * p;
+                const double r = a.consts[IBLBM_PARTICLE_CONSTS * p + 8];
+                const double l = a.moments_f32
+                    ? disc_angular_momentum(a, static_cast<const float*>(a.rho), static_cast<const float*>(a.U),
+                                            s[0], s[1], r)
+                    : disc_angular_momentum(a, static_cast<const double*>(a.rho), static_cast<const double*>(a.U),
+                                            s[0], s[1], r);
+                if (threadIdx.x == 0) s_lint[p] = 0.0 + l;
+            }
+            __syncthreads();
+        }
         if (threadIdx.x < P) {
             const int p = threadIdx.x;
             double* s = a.state + IBLBM_PARTICLE_STATE * p;
@@ -244,9 +381,20 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
                 s_next[2 * p + d] = xn;
                 if (a.forces_out) a.forces_out[2 * p + d] = s_force[2 * p + d];
             }
-            s_rot[3 * p] = 1.0;
-            s_rot[3 * p + 1] = 0.0;
-            s_rot[3 * p + 2] = 0.0;
+            if (a.rotation) {  // physics/rigid_body.py:101-121
+                const double T = s_force[2 * P + p];
+                const double dl = s_lint[p] - s[21];
+                s[21] = s_lint[p];
+                const double om = s[12] + (dl + dt * T) / c[7];
+                s[14] = a.euler_trapezoidal ? s[14] + (0.5 * dt) * (s[12] + om) : s[14] + dt * om;
+                s[15] = T;
+                s[12] = om;
+                s[19] = s[14];
+            }
+            // R(0) = [[1, -0], [0, 1]] exactly, as the host's cos 0 and sin 0
+            s_rot[3 * p] = a.rotation ? cos(s[14]) : 1.0;
+            s_rot[3 * p + 1] = a.rotation ? sin(s[14]) : 0.0;
+            s_rot[3 * p + 2] = a.rotation ? s[12] : 0.0;
         }
         __syncthreads();
     }
@@ -310,7 +458,10 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
         return IBLBM_E_ARG;
     const int ph = a->phase;
     if ((ph & ~(IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_HALF | IBLBM_PARTICLES_EULER)) || !ph) return IBLBM_E_ARG;
-    if ((ph & IBLBM_PARTICLES_EULER) && (ph != IBLBM_PARTICLES_EULER || a->rotation)) return IBLBM_E_ARG;
+    if ((ph & IBLBM_PARTICLES_EULER) && ph != IBLBM_PARTICLES_EULER) return IBLBM_E_ARG;
+    if ((ph & IBLBM_PARTICLES_EULER) && a->rotation &&
+        (!a->rho || !a->U || a->ny < 1 || !a->lint_scratch || a->lint_capacity < 1 || a->lint_capacity > LINT_MAX))
+        return IBLBM_E_ARG;
     if ((ph & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) &&
         (!a->band_fib_part || !a->band_count || a->band_capacity < 1))
         return IBLBM_E_ARG;

@@ -253,19 +253,17 @@ class Engine:
         # the host step unless asked: their markers turn by the device's cos and
         # sin, which may differ from the host's in the last bit
         self.dev_particles = False
+        self.part_after_lattice = self.moments_always = False
         self._torque_ij = None
         if st.particles is not None:
             rot = bool(cfg.enable_rotation)
-            euler = cfg.time_integrator == "euler_explicit"
             default = not (rot and not self.f32)
             self.dev_particles = default if device_particles is None else bool(device_particles)
-            if (rot and euler) or cfg.ibm_method != "MDF" or self.single:
-                # the Euler angular step (it needs the fluid's angular momentum inside
-                # each disc), the Lagrangian force sums of DF and DFC and the
-                # single-particle runtime run on the host
+            if cfg.ibm_method != "MDF" or self.single:
+                # the Lagrangian force sums of DF and DFC and the single-particle
+                # runtime run on the host
                 if device_particles:
-                    raise NotImplementedError("rotating explicit Euler steps, DF / DFC particles and the "
-                                              "single-particle runtime run on the host")
+                    raise NotImplementedError("DF / DFC particles and the single-particle runtime run on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -293,10 +291,10 @@ class Engine:
             state[k, 10:12] = p.pos
             state[k, 12:16] = [p.omega, p.omega_half, p.angle, p.torque]
             state[k, 16:18] = p.vel_half
-            state[k, 18:21] = [p.omega_half, p.angle, p.omega]
+            state[k, 18:22] = [p.omega_half, p.angle, p.omega, p.l_int_prev]
             g = net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             consts[k] = [p.mass, 1.0 / p.rho_ratio, np.pi * p.lattice_r ** 2 / p.mass, g[0], g[1], p.cx_init,
-                         p.cy_init, p.I_particle]
+                         p.cy_init, p.I_particle, p.r_domain]
         self.d_pstate = torch.as_tensor(state.reshape(-1), device=self.dev)
         self.d_pconsts = torch.as_tensor(consts.reshape(-1), device=self.dev)
         self.d_Lxc_all = torch.as_tensor(np.concatenate([p.Lx_c for p in ps]), device=self.dev)
@@ -318,6 +316,16 @@ class Engine:
         # each timestep and the half step of the next; explicit Euler: the whole
         # step after each band kernel, from the markers the host set up
         self.part_phase = 4 if cfg.time_integrator == "euler_explicit" else 3
+        # a rotating Euler step reads this step's rho and U (the fluid's angular
+        # momentum inside each disc): every step writes them, and the particle
+        # launch follows the whole lattice pass
+        self.part_after_lattice = self.part_phase == 4 and bool(cfg.enable_rotation)
+        self.moments_always = self.part_after_lattice
+        if self.part_after_lattice:
+            cap = max((2 * (int(p.r_domain / st.dx) + 2) + 1) ** 2 for p in ps)
+            self.d_lint = torch.zeros(cap, dtype=torch.float64, device=self.dev)
+            a.rho, a.U, a.moments_f32, a.ny = ptr(self.ro_out), ptr(self.U_out), int(self.f32), st.ny
+            a.lint_scratch, a.lint_capacity = ptr(self.d_lint), cap
         if not self.f32:
             # the FP64 form sums the forces in numpy's pairwise order over the
             # dense lattice field, so the device step equals the host step bit
@@ -366,6 +374,7 @@ class Engine:
             p.force = s[k, 8:10].copy()
             p.fib_force = p.force.copy()
             p.omega, p.omega_half, p.angle, p.torque = (float(x) for x in s[k, 12:16])
+            p.l_int_prev = float(s[k, 21])
             if euler:
                 p.Lx, p.Ly = Lx[moff[k]:moff[k + 1]].copy(), Ly[moff[k]:moff[k + 1]].copy()
                 p.desired_velocity = dv[moff[k]:moff[k + 1]].copy()
@@ -546,6 +555,8 @@ class Engine:
         self.rebuild_next = False
 
     def _dense(self, variant, outputs, stream):
+        if not outputs and self.moments_always:
+            outputs = OUT_MOMENTS
         da = variant[self.parity][2 if outputs == OUT_MOMENTS else (1 if outputs else 0)]
         if self.f32:
             check(self.L.iblbm_dense_step_f32(ctypes.byref(da), stream), "iblbm_dense_step_f32")
@@ -571,11 +582,13 @@ class Engine:
             self.rebuild_next = False
         else:
             self._ibm(s, excl_check=False)
-        if self.dev_particles:
+        if self.dev_particles and not self.part_after_lattice:
             self._particles(s, self.part_phase)  # full step of this timestep (and half step of the next)
         if events:
             events[1].record()
         self._dense(self.dense_full, outputs, s)
+        if self.dev_particles and self.part_after_lattice:
+            self._particles(s, self.part_phase)
         if events:
             events[2].record()
         self.parity ^= 1
@@ -592,7 +605,7 @@ class Engine:
         side = self.side
         side.wait_event(self.ev_bulk)
         self._ibm(side.cuda_stream, excl_check=True)
-        if self.dev_particles:
+        if self.dev_particles and not self.part_after_lattice:
             self._particles(side.cuda_stream, self.part_phase)
         self._dense(self.dense_box, outputs, side.cuda_stream)
         main.wait_event(self.ev_side)
@@ -602,6 +615,9 @@ class Engine:
         self._dense(self.dense_bulk, outputs, main.cuda_stream)
         if bulk_events:
             bulk_events[1].record(main)
+        if self.dev_particles and self.part_after_lattice:
+            main.wait_event(self.ev_side)  # this step's box pass
+            self._particles(main.cuda_stream, self.part_phase)
         self.ev_bulk.record(main)
         self.parity ^= 1
 

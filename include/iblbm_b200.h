@@ -405,23 +405,25 @@ int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *gra
  * Replaces the host particle steps of runtime/scenarios/sedimentation_multi.py:
  * the Velocity-Verlet step (:36-111, with the angular half and full kicks of
  * physics/rigid_body.py:65-82 when rotation is on) and the explicit Euler step
- * without rotation (:126-190, physics/rigid_body.py:84-98), inertia models
- * none / explicit_history / feng_b2.  Per particle, state holds
+ * (:126-190, physics/rigid_body.py:84-121), inertia models none /
+ * explicit_history / feng_b2.  Per particle, state holds
  * IBLBM_PARTICLE_STATE doubles: pos(2), vel(2), vel_prev(2), vel_half(2),
  * force(2), pos_next(2), omega, omega_half, angle, torque, and the half step's
  * look-ahead vel_half(2), omega_half, angle of the next step (pos_next,
  * vel_half, omega_half and angle become current in its full step, so between
  * launches the state is that of the last completed step), then the omega of
- * the last step's rigid-body marker velocity; consts holds
+ * the last step's rigid-body marker velocity, and the fluid's angular
+ * momentum inside the disc at the last Euler step; consts holds
  * IBLBM_PARTICLE_CONSTS doubles: mass, 1/rho_ratio, pi r^2/mass, net gravity
- * (2), initial centre (2), moment of inertia.  phase FULL finishes the
+ * (2), initial centre (2), moment of inertia, disc radius (domain units).  phase FULL finishes the
  * current Verlet step from the band kernel's per-particle forces
  * (band_fib_part, particles x band_capacity x 2, FP32 when fib_f32); phase HALF
  * starts the next one: new marker positions Lx, Ly and desired velocities
  * dvel; phase EULER (alone) does a whole explicit Euler step after the band
- * kernel and leaves the next step's markers and desired velocities. */
-#define IBLBM_PARTICLE_STATE 21
-#define IBLBM_PARTICLE_CONSTS 8
+ * kernel (with rotation: after the whole lattice pass) and leaves the next
+ * step's markers and desired velocities. */
+#define IBLBM_PARTICLE_STATE 22
+#define IBLBM_PARTICLE_CONSTS 9
 #define IBLBM_PARTICLES_FULL 1
 #define IBLBM_PARTICLES_HALF 2
 #define IBLBM_PARTICLES_EULER 4
@@ -470,6 +472,18 @@ typedef struct {
      * the old and new velocities (else the new one). */
     int rotation, semi_implicit, euler_trapezoidal, nx;
     double dy;
+    /* Rotating Euler steps (physics/rigid_body.py:101-121): the change of the
+     * fluid's angular momentum inside each disc, sum over the lattice nodes
+     * within the disc radius of (i - x/dx) rho uy - (j - y/dx) rho ux, taken
+     * from this step's rho and U (n_nodes and n_nodes x 2, FP32 when
+     * moments_f32) over the box of diagnostics/internal_flow.py:220-262 and
+     * summed like numpy sums the masked values.  The launch follows the whole
+     * lattice pass.  lint_scratch: lint_capacity doubles, at least the
+     * largest box, (2 (int(r/dx) + 2) + 1)^2. */
+    const void *rho, *U;
+    int moments_f32, ny;
+    double *lint_scratch;
+    int lint_capacity;
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);

@@ -265,13 +265,16 @@ def test_device_particles_match_host_step(torch, precision, name):
             np.testing.assert_allclose(p.vel, q.vel, rtol=1e-9, atol=1e-9 * float(np.max(np.abs(q.vel))))
 
 
-@pytest.mark.parametrize("name", ["c5r_sed2_mdf_rot_indirect", "c5r_sed2_mdf_rot_semi", "c5r_sed2_mdf_rot_iterative"])
+@pytest.mark.parametrize("name", ["c5r_sed2_mdf_rot_indirect", "c5r_sed2_mdf_rot_semi", "c5r_sed2_mdf_rot_iterative",
+                                  "c5e_sed2_mdf_euler_rot"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_device_rotation_matches_host_step(torch, precision, name):
-    """Rotating discs with the Verlet step on the device (torque summed like
-    the forces, angular half and full kicks, markers turned by the device's cos
-    and sin) against the host step.  The torque sums follow numpy's order in
-    the FP64 form; cos and sin may differ from the host's in the last bit, so
+    """Rotating discs with the Verlet or explicit Euler step on the device
+    (torque summed like the forces, angular kicks or the Euler angular step with
+    the fluid's angular momentum inside each disc, markers turned by the
+    device's cos and sin) against the host step.  The torque and angular
+    momentum sums follow numpy's order in the FP64 form (the latter in the FP32
+    form too); cos and sin may differ from the host's in the last bit, so
     the bar is round-off: FP64 within 1e-12 relative (equal bit for bit in
     the measured runs), FP32 (whose device sums run in another order)
     positions and velocities within 1e-9 relative, angles, angular velocities
