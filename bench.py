@@ -966,11 +966,14 @@ def run_b200(args):
 
 def run_profile(args):
     """A short eager run for ncu captures: warm-up steps, then args.steps timesteps
-    (two kernel launches each), no graphs, no baseline, no clock sampling."""
+    of configuration 2 (or 3, 5: --profile-config), no graphs, no baseline, no
+    clock sampling."""
     import torch
     from iblbm_b200.engine import Engine
-    eng = Engine(workload_config(collision=args.collision, max_steps=args.warmup + args.steps + 8),
-                 precision=args.precision, cluster=args.cluster)
+    n = args.warmup + args.steps + 8
+    cfg = {2: lambda: workload_config(collision=args.collision, max_steps=n), 3: lambda: config3(max_steps=n),
+           5: lambda: config5(max_steps=n)}[args.profile_config]()
+    eng = Engine(cfg, precision=args.precision, cluster=args.cluster)
     for _ in range(args.warmup + args.steps):
         eng._launch(False)
     eng.join()
@@ -1003,6 +1006,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--profile", action="store_true", help="short eager run for ncu captures")
     ap.add_argument("--profile-batch", action="store_true", help="short eager batched run for ncu captures")
+    ap.add_argument("--profile-config", type=int, default=2, choices=[2, 3, 5],
+                    help="profile runs: configuration 2 (fixed cylinder), 3 (oscillating DFC) or 5 (two settling discs)")
     ap.add_argument("--collision", default="TRT", choices=["BGK", "TRT", "CM_MRT"])
     ap.add_argument("--form", default="chosen", choices=["chosen", "plain"])
     ap.add_argument("--precision", default=None, choices=["f64", "f32"], help="form used by the profile runs")

@@ -103,13 +103,38 @@ __device__ __forceinline__ int pw_leaf_of(const iblbm_particles_args& a, int e)
     return l;
 }
 
+constexpr int PW_MAXLEVELS = 64;
+constexpr size_t PART_DYN_SMEM = 2 * PART_MAXB * sizeof(double);  // a particle's band forces
+
+// first k in [A, B) with pred(k) (pred false then true along k), B if none:
+// the 32 lanes of a warp probe 32 evenly spaced points per round
+template <typename Pred>
+__device__ int warp_first_true(int A, int B, Pred pred)
+{
+    const int lane = threadIdx.x & 31;
+    int lo = A, hi = B;  // the answer lies in [lo, hi]
+    while (lo < hi) {
+        const int step = (hi - lo + 31) / 32;
+        const int k = lo + lane * step;
+        const unsigned m = __ballot_sync(0xffffffffu, k < hi && pred(k));
+        if (m) {
+            const int j = __ffs(m) - 1;
+            hi = lo + j * step;
+            if (j) lo += (j - 1) * step + 1;
+        } else {  // every probe below hi was false
+            lo += ((hi - 1 - lo) / step) * step + 1;
+        }
+    }
+    return lo;
+}
+
 template <typename F>
 __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fib, const double* s_ctr, int PC,
-                                      double* s_force)
+                                      double* s_force, double* s_f)
 {
     __shared__ int s_nodes[PART_MAXB];
     const int nb = min(*a.band_count, PART_MAXB);
-    const int L = a.pw_leaves;
+    const int P = a.n_particles, L = a.pw_leaves;
     const size_t pstride = 2 * (size_t)a.band_capacity;
     double* v = a.pw_scratch;  // node id x PC
     for (int b = threadIdx.x; b < nb; b += PART_THREADS) s_nodes[b] = a.band_nodes[b];
@@ -120,32 +145,63 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
         return;
     }
     const int l0 = pw_leaf_of(a, s_nodes[0]), l1 = pw_leaf_of(a, s_nodes[nb - 1]);
-    for (int li = l0 + (int)threadIdx.x; li <= l1; li += PART_THREADS) {
-        const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
-        int lo = 0, hi = nb;  // first band entry at or after off
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (s_nodes[mid] < off) lo = mid + 1;
-            else hi = mid;
-        }
-        const int cut = m - m % 8;
-        for (int pc = 0; pc < PC; ++pc) {
-            auto val = [&](int b) { return channel_value(a, fib, pstride, s_ctr, pc, b, s_nodes[b]); };
-            double res;
-            if (m < 8) {
-                res = 0.0;
-                for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
-            } else {
-                double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                int b = lo;
-                for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += val(b);
-                res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-                for (; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
-            }
-            v[(size_t)li * PC + pc] = res;
+    // a level's nodes are disjoint and left to right, so those meeting the window
+    // are one run [s_klo, s_kend); one warp per level finds it
+    __shared__ int s_klo[PW_MAXLEVELS], s_kend[PW_MAXLEVELS];
+    for (int d = (int)threadIdx.x >> 5; d < a.pw_levels; d += PART_THREADS / 32) {
+        const int A = a.pw_level[d], B = a.pw_level[d + 1];
+        const int klo = warp_first_true(A, B, [&](int k) { return a.pw_span[2 * k + 1] >= l0; });
+        const int kend = warp_first_true(klo, B, [&](int k) { return a.pw_span[2 * k] > l1; });
+        if ((threadIdx.x & 31) == 0) {
+            s_klo[d] = klo;
+            s_kend[d] = kend;
         }
     }
     __syncthreads();
+    // one particle at a time: its band forces staged in shared memory (s_f: fx
+    // then fy, PART_MAXB each), so the leaves' ordered sums read no global memory
+    for (int p = 0; p < P; ++p) {
+        for (int b = threadIdx.x; b < nb; b += PART_THREADS) {
+            s_f[b] = (double)fib[p * pstride + 2 * (size_t)b];
+            s_f[PART_MAXB + b] = (double)fib[p * pstride + 2 * (size_t)b + 1];
+        }
+        __syncthreads();
+        const int nch = a.rotation ? 3 : 2;
+        const double cx = s_ctr[2 * p], cy = s_ctr[2 * p + 1];
+        for (int li = l0 + (int)threadIdx.x; li <= l1; li += PART_THREADS) {
+            const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
+            int lo = 0, hi = nb;  // first band entry at or after off
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (s_nodes[mid] < off) lo = mid + 1;
+                else hi = mid;
+            }
+            const int cut = m - m % 8;
+            for (int ch = 0; ch < nch; ++ch) {
+                // fx, fy, or the torque term (i - cx) fy - (j - cy) fx
+                auto val = [&](int b) -> double {
+                    if (ch < 2) return s_f[ch * PART_MAXB + b];
+                    const int e = s_nodes[b];
+                    const double i = (double)(e % a.nx), j = (double)(e / a.nx);
+                    return (i - cx) * s_f[PART_MAXB + b] - (j - cy) * s_f[b];
+                };
+                double res;
+                if (m < 8) {
+                    res = 0.0;
+                    for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
+                } else {
+                    double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                    int b = lo;
+                    for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += val(b);
+                    res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+                    for (; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
+                }
+                const int pc = ch < 2 ? 2 * p + ch : 2 * P + p;
+                v[(size_t)li * PC + pc] = res;
+            }
+        }
+        __syncthreads();
+    }
     // a child is in the window when its leaves meet [l0, l1]; outside it sums to +0.0
     auto in_window = [&](int id) {
         if (id < L) return id >= l0 && id <= l1;
@@ -153,8 +209,7 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
         return a.pw_span[2 * k + 1] >= l0 && a.pw_span[2 * k] <= l1;
     };
     for (int d = 0; d < a.pw_levels; ++d) {
-        for (int k = a.pw_level[d] + threadIdx.x; k < a.pw_level[d + 1]; k += PART_THREADS) {
-            if (a.pw_span[2 * k + 1] < l0 || a.pw_span[2 * k] > l1) continue;
+        for (int k = s_klo[d] + threadIdx.x; k < s_kend[d]; k += PART_THREADS) {
             const int c0 = a.pw_node[2 * k], c1 = a.pw_node[2 * k + 1];
             const bool w0 = in_window(c0), w1 = in_window(c1);
             for (int pc = 0; pc < PC; ++pc) {
@@ -305,8 +360,11 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
         }
         __syncthreads();
         if (a.pw_leaf) {
-            if (a.fib_f32) particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force);
-            else particle_forces_exact(a, static_cast<const double*>(a.band_fib_part), s_ctr, PC, s_force);
+            extern __shared__ double s_dyn[];  // PART_DYN_SMEM bytes with a summation tree
+            if (a.fib_f32)
+                particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force, s_dyn);
+            else
+                particle_forces_exact(a, static_cast<const double*>(a.band_fib_part), s_ctr, PC, s_force, s_dyn);
         } else if (a.fib_f32) {
             particle_forces(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force);
         } else {
@@ -474,7 +532,15 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
     if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || !a->pw_lut || !a->pw_span ||
                        a->pw_leaves < 1 || a->pw_internal < 0 || a->pw_levels < 0 || a->n_nodes < 1))
         return IBLBM_E_ARG;
-    if (a->pw_leaf && a->band_capacity > PART_MAXB) return IBLBM_E_CAPACITY;
-    particles_kernel<<<1, PART_THREADS, 0, (cudaStream_t)stream>>>(*a);
+    if (a->pw_leaf && (a->band_capacity > PART_MAXB || a->pw_levels > PW_MAXLEVELS)) return IBLBM_E_CAPACITY;
+    const size_t dyn = a->pw_leaf ? PART_DYN_SMEM : 0;
+    static bool attr = false;  // the staging buffers need more than the default 48 KB in all
+    if (!attr) {
+        if (cudaFuncSetAttribute(particles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)PART_DYN_SMEM) != cudaSuccess)
+            return IBLBM_E_LAUNCH;
+        attr = true;
+    }
+    particles_kernel<<<1, PART_THREADS, dyn, (cudaStream_t)stream>>>(*a);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
