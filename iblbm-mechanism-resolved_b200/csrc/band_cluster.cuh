@@ -544,14 +544,9 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_cluster_kernel(const iblbm
 template <int A>
 static int launch_cluster_plan(const iblbm_ibm_args& a, void* stream)
 {
-    static bool configured = false;
     auto K = ibm_cluster_plan_kernel<A>;
     const size_t smem = sizeof(int) * (MAX_BAND + 64);
-    if (!configured) {
-        if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        configured = true;
-    }
+    if (smem_limit_once<ibm_cluster_plan_kernel<A>>((int)smem) != cudaSuccess) return IBLBM_E_LAUNCH;
     K<<<a.cluster_size, IBM_THREADS, smem, (cudaStream_t)stream>>>(a, a.cluster_plan, a.cluster_size);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
@@ -559,13 +554,8 @@ static int launch_cluster_plan(const iblbm_ibm_args& a, void* stream)
 template <int A>
 static int launch_cluster_step(const iblbm_ibm_args& a, const BcParams& bc, void* stream)
 {
-    static bool configured = false;
     auto K = ibm_cluster_kernel<A>;
-    if (!configured) {
-        if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT) != cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        configured = true;
-    }
+    if (smem_limit_once<ibm_cluster_kernel<A>>(IBM_SMEM_LIMIT) != cudaSuccess) return IBLBM_E_LAUNCH;
     const int S = Sten<A>::S;
     const size_t smem = std::max(ibm_smem<double>(a), cluster_smem_bytes(a.lb_total, S, a.cluster_size));
     cudaLaunchConfig_t cfg = {};

@@ -1512,12 +1512,8 @@ __global__ void __launch_bounds__(IBM_THREADS, 1) ibm_batch_kernel(const ARGS* _
 template <class ARGS, class BCP, void (*K)(const ARGS, BCP)>
 static cudaError_t launch_ibm(const ARGS& a, const BCP& bc, size_t smem, void* stream)
 {
-    static bool configured = false;
-    if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    const cudaError_t e = smem_limit_once<K>(IBM_SMEM_LIMIT);
+    if (e != cudaSuccess) return e;
     K<<<1, IBM_THREADS, smem, (cudaStream_t)stream>>>(a, bc);
     return cudaGetLastError();
 }

@@ -8,10 +8,22 @@
 // components e in {0, +-1} are exact and written as the adds/subtracts they are.
 #pragma once
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "../../include/iblbm_b200.h"
 
 namespace iblbm {
+
+// Raises kernel K's dynamic shared-memory limit to bytes, once per process and
+// thread-safe; later calls return the first call's result.
+template <auto K>
+inline cudaError_t smem_limit_once(int bytes)
+{
+    static std::once_flag flag;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(flag, [&] { err = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); });
+    return err;
+}
 
 // D2Q9 ordering of iblbm/lbm/lattice.py:45-55: 0; E,N,W,S; NE,NW,SW,SE
 __host__ __device__ constexpr int ex_(int q) { return q == 1 || q == 5 || q == 8 ? 1 : (q == 3 || q == 6 || q == 7 ? -1 : 0); }

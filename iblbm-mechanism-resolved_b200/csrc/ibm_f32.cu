@@ -3,6 +3,7 @@
 // band_kernel.cuh instantiated with R = float: band moments from g = f - w
 // (rho = 1 + sum g), interpolation, spreading and MDF relaxation in FP32, the
 // MDF residual norm in FP64; per-marker outputs are written as FP64.
+#include <mutex>
 #include <algorithm>
 #include "band_kernel.cuh"
 
@@ -45,12 +46,7 @@ extern "C" int iblbm_ibm_step_f32_batch(const iblbm_ibm32_args* host_args, const
         smem = std::max(smem, ibm_smem<float>(host_args[b]));
     }
     auto K = ibm_batch_kernel<iblbm_ibm32_args, float, true>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT) != cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        configured = true;
-    }
+    if (smem_limit_once<ibm_batch_kernel<iblbm_ibm32_args, float, true>>(IBM_SMEM_LIMIT) != cudaSuccess) return IBLBM_E_LAUNCH;
     K<<<n, IBM_THREADS, smem, (cudaStream_t)stream>>>(dev_args);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

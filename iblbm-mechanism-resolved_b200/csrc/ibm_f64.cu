@@ -84,12 +84,7 @@ extern "C" int iblbm_ibm_step_f64_batch(const iblbm_ibm_args* host_args, const i
         smem = std::max(smem, ibm_smem<double>(host_args[b]));
     }
     auto K = ibm_batch_kernel<iblbm_ibm_args, double, false>;
-    static std::once_flag configured;
-    cudaError_t attr = cudaSuccess;
-    std::call_once(configured, [&] {
-        attr = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, IBM_SMEM_LIMIT);
-    });
-    if (attr != cudaSuccess) return IBLBM_E_LAUNCH;
+    if (smem_limit_once<ibm_batch_kernel<iblbm_ibm_args, double, false>>(IBM_SMEM_LIMIT) != cudaSuccess) return IBLBM_E_LAUNCH;
     K<<<n, IBM_THREADS, smem, (cudaStream_t)stream>>>(dev_args);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }

@@ -11,6 +11,7 @@
 // tensor cores (mlp.cuh tc_gemm64); the 64 -> 2 output layer stays on CUDA
 // cores.  Inference: 128 samples per CTA.
 #include <cstdint>
+#include "common.cuh"
 #include "mlp.cuh"
 #include "../../include/iblbm_b200.h"
 
@@ -224,13 +225,7 @@ extern "C" int iblbm_mlp_infer(const float* params, const float* x, int n, float
     if (!params || !x || !y || n < 0) return IBLBM_E_ARG;
     if (n == 0) return IBLBM_OK;
     const size_t smem = sizeof(float) * (size_t)(2 * INFER_ROWS * MLP_LD + INFER_ROWS * 2);
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        configured = true;
-    }
+    if (iblbm::smem_limit_once<mlp_infer_kernel>((int)smem) != cudaSuccess) return IBLBM_E_LAUNCH;
     mlp_infer_kernel<<<(n + INFER_ROWS - 1) / INFER_ROWS, INFER_THREADS, smem, (cudaStream_t)stream>>>(params, x, n,
                                                                                                       y);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
@@ -241,13 +236,7 @@ extern "C" int iblbm_mlp_train_step(float* params, float* adam_m, float* adam_v,
 {
     if (!params || !grad || !x || !t || n < 1 || step < 1) return IBLBM_E_ARG;
     if (apply && (!adam_m || !adam_v)) return IBLBM_E_ARG;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) !=
-            cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        configured = true;
-    }
+    if (iblbm::smem_limit_once<mlp_grad_kernel>((int)TRAIN_SMEM) != cudaSuccess) return IBLBM_E_LAUNCH;
     // Adam bias corrections 1 / (1 - beta^step)
     const float c1 = (float)(1.0 / (1.0 - pow((double)ADAM_B1, step)));
     const float c2 = (float)(1.0 / (1.0 - pow((double)ADAM_B2, step)));

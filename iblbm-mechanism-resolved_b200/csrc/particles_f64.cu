@@ -534,13 +534,8 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
         return IBLBM_E_ARG;
     if (a->pw_leaf && (a->band_capacity > PART_MAXB || a->pw_levels > PW_MAXLEVELS)) return IBLBM_E_CAPACITY;
     const size_t dyn = a->pw_leaf ? PART_DYN_SMEM : 0;
-    static bool attr = false;  // the staging buffers need more than the default 48 KB in all
-    if (!attr) {
-        if (cudaFuncSetAttribute(particles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)PART_DYN_SMEM) != cudaSuccess)
-            return IBLBM_E_LAUNCH;
-        attr = true;
-    }
+    // the staging buffer takes static + dynamic shared memory past 48 KB
+    if (smem_limit_once<particles_kernel>((int)PART_DYN_SMEM) != cudaSuccess) return IBLBM_E_LAUNCH;
     particles_kernel<<<1, PART_THREADS, dyn, (cudaStream_t)stream>>>(*a);
     return cudaGetLastError() == cudaSuccess ? IBLBM_OK : IBLBM_E_LAUNCH;
 }
