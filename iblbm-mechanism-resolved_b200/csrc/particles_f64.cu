@@ -104,7 +104,10 @@ __device__ __forceinline__ int pw_leaf_of(const iblbm_particles_args& a, int e)
 }
 
 constexpr int PW_MAXLEVELS = 64;
-constexpr size_t PART_DYN_SMEM = 2 * PART_MAXB * sizeof(double);  // a particle's band forces
+constexpr int PW_SV = 6144;  // window partial sums held in shared memory (doubles)
+constexpr int PW_SN = 2048;  // window inner nodes whose children are held in shared memory
+// a particle's band forces, the window's partial sums and its inner nodes' children
+constexpr size_t PART_DYN_SMEM = (2 * PART_MAXB + PW_SV) * sizeof(double) + 2 * PW_SN * sizeof(int);
 
 // first k in [A, B) with pred(k) (pred false then true along k), B if none:
 // the 32 lanes of a warp probe 32 evenly spaced points per round
@@ -147,7 +150,7 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
     const int l0 = pw_leaf_of(a, s_nodes[0]), l1 = pw_leaf_of(a, s_nodes[nb - 1]);
     // a level's nodes are disjoint and left to right, so those meeting the window
     // are one run [s_klo, s_kend); one warp per level finds it
-    __shared__ int s_klo[PW_MAXLEVELS], s_kend[PW_MAXLEVELS];
+    __shared__ int s_klo[PW_MAXLEVELS], s_kend[PW_MAXLEVELS], s_base[PW_MAXLEVELS + 1];
     for (int d = (int)threadIdx.x >> 5; d < a.pw_levels; d += PART_THREADS / 32) {
         const int A = a.pw_level[d], B = a.pw_level[d + 1];
         const int klo = warp_first_true(A, B, [&](int k) { return a.pw_span[2 * k + 1] >= l0; });
@@ -158,6 +161,25 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
         }
     }
     __syncthreads();
+    // window-local ids: the window's leaves first, then its inner nodes level by level
+    const int WL = l1 - l0 + 1;
+    if (threadIdx.x == 0) {
+        int t = WL;
+        for (int d = 0; d < a.pw_levels; ++d) {
+            s_base[d] = t;
+            t += s_kend[d] - s_klo[d];
+        }
+        s_base[a.pw_levels] = t;
+    }
+    __syncthreads();
+    const int WN = s_base[a.pw_levels];  // window nodes, leaves included
+    // the partial sums of the window live in shared memory when they fit (sv:
+    // PW_SV doubles; lc: the window-local children of up to PW_SN inner nodes),
+    // else in the global scratch v
+    const bool fast = (size_t)WN * PC <= PW_SV && WN - WL <= PW_SN;
+    double* sv = s_f + 2 * PART_MAXB;
+    int* lc = reinterpret_cast<int*>(sv + PW_SV);
+    auto vref = [&](int li, int pc) -> double& { return fast ? sv[(li - l0) * PC + pc] : v[(size_t)li * PC + pc]; };
     // one particle at a time: its band forces staged in shared memory (s_f: fx
     // then fy, PART_MAXB each), so the leaves' ordered sums read no global memory
     for (int p = 0; p < P; ++p) {
@@ -166,39 +188,60 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
             s_f[PART_MAXB + b] = (double)fib[p * pstride + 2 * (size_t)b + 1];
         }
         __syncthreads();
-        const int nch = a.rotation ? 3 : 2;
+        const bool rot = a.rotation != 0;
         const double cx = s_ctr[2 * p], cy = s_ctr[2 * p + 1];
         for (int li = l0 + (int)threadIdx.x; li <= l1; li += PART_THREADS) {
             const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
-            int lo = 0, hi = nb;  // first band entry at or after off
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (s_nodes[mid] < off) lo = mid + 1;
+            int b = 0, hi = nb;  // first band entry at or after off
+            while (b < hi) {
+                const int mid = (b + hi) >> 1;
+                if (s_nodes[mid] < off) b = mid + 1;
                 else hi = mid;
             }
-            const int cut = m - m % 8;
-            for (int ch = 0; ch < nch; ++ch) {
-                // fx, fy, or the torque term (i - cx) fy - (j - cy) fx
-                auto val = [&](int b) -> double {
-                    if (ch < 2) return s_f[ch * PART_MAXB + b];
-                    const int e = s_nodes[b];
-                    const double i = (double)(e % a.nx), j = (double)(e / a.nx);
-                    return (i - cx) * s_f[PART_MAXB + b] - (j - cy) * s_f[b];
-                };
-                double res;
-                if (m < 8) {
-                    res = 0.0;
-                    for (int b = lo; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
-                } else {
-                    double r[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                    int b = lo;
-                    for (; b < nb && s_nodes[b] < off + cut; ++b) r[(s_nodes[b] - off) & 7] += val(b);
-                    res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-                    for (; b < nb && s_nodes[b] < off + m; ++b) res += val(b);
+            // fx, fy and the torque term (i - cx) fy - (j - cy) fx of entry b
+            auto terms = [&](int e, double& fx, double& fy, double& t) {
+                fx = s_f[e];
+                fy = s_f[PART_MAXB + e];
+                if (rot) {
+                    const int n = s_nodes[e];
+                    t = ((double)(n % a.nx) - cx) * fy - ((double)(n / a.nx) - cy) * fx;
                 }
-                const int pc = ch < 2 ? 2 * p + ch : 2 * P + p;
-                v[(size_t)li * PC + pc] = res;
+            };
+            double res0 = 0.0, res1 = 0.0, res2 = 0.0;
+            double fx, fy, t = 0.0;
+            if (m >= 8) {
+                // numpy's 8 strided accumulators, in registers: the entries of each
+                // 8-position block go to the lanes of their positions, in order
+                const int cut = off + (m - m % 8);
+                double r0[8], r1[8], r2[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) r0[k] = r1[k] = r2[k] = 0.0;
+                while (b < nb && s_nodes[b] < cut) {
+                    const int q0 = off + ((s_nodes[b] - off) & ~7);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        if (b < nb && s_nodes[b] == q0 + k) {
+                            terms(b, fx, fy, t);
+                            r0[k] += fx;
+                            r1[k] += fy;
+                            r2[k] += t;
+                            ++b;
+                        }
+                    }
+                }
+                res0 = ((r0[0] + r0[1]) + (r0[2] + r0[3])) + ((r0[4] + r0[5]) + (r0[6] + r0[7]));
+                res1 = ((r1[0] + r1[1]) + (r1[2] + r1[3])) + ((r1[4] + r1[5]) + (r1[6] + r1[7]));
+                res2 = ((r2[0] + r2[1]) + (r2[2] + r2[3])) + ((r2[4] + r2[5]) + (r2[6] + r2[7]));
             }
+            for (; b < nb && s_nodes[b] < off + m; ++b) {  // the tail (or a leaf of under 8)
+                terms(b, fx, fy, t);
+                res0 += fx;
+                res1 += fy;
+                res2 += t;
+            }
+            vref(li, 2 * p) = res0;
+            vref(li, 2 * p + 1) = res1;
+            if (rot) vref(li, 2 * P + p) = res2;
         }
         __syncthreads();
     }
@@ -208,20 +251,54 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
         const int k = id - L;
         return a.pw_span[2 * k + 1] >= l0 && a.pw_span[2 * k] <= l1;
     };
-    for (int d = 0; d < a.pw_levels; ++d) {
-        for (int k = s_klo[d] + threadIdx.x; k < s_kend[d]; k += PART_THREADS) {
-            const int c0 = a.pw_node[2 * k], c1 = a.pw_node[2 * k + 1];
-            const bool w0 = in_window(c0), w1 = in_window(c1);
-            for (int pc = 0; pc < PC; ++pc) {
-                const double x0 = w0 ? v[(size_t)c0 * PC + pc] : 0.0;
-                const double x1 = w1 ? v[(size_t)c1 * PC + pc] : 0.0;
-                v[(size_t)(L + k) * PC + pc] = x0 + x1;
-            }
+    const int root = a.pw_internal > 0 ? L + a.pw_internal - 1 : 0;
+    if (fast) {
+        // window-local ids of the children of every window inner node (-1: outside
+        // the window, adds +0.0), read once, then the levels in shared memory
+        auto local = [&](int id) {
+            if (id < L) return id >= l0 && id <= l1 ? id - l0 : -1;
+            const int k = id - L;
+            for (int d = 0; d < a.pw_levels; ++d)
+                if (k >= s_klo[d] && k < s_kend[d]) return s_base[d] + k - s_klo[d];
+            return -1;
+        };
+        for (int u = WL + (int)threadIdx.x; u < WN; u += PART_THREADS) {
+            int d = 0;
+            while (u >= s_base[d + 1]) ++d;
+            const int k = s_klo[d] + u - s_base[d];
+            lc[2 * (u - WL)] = local(a.pw_node[2 * k]);
+            lc[2 * (u - WL) + 1] = local(a.pw_node[2 * k + 1]);
         }
         __syncthreads();
+        for (int d = 0; d < a.pw_levels; ++d) {
+            for (int u = s_base[d] + (int)threadIdx.x; u < s_base[d + 1]; u += PART_THREADS) {
+                const int c0 = lc[2 * (u - WL)], c1 = lc[2 * (u - WL) + 1];
+                for (int pc = 0; pc < PC; ++pc) {
+                    const double x0 = c0 >= 0 ? sv[c0 * PC + pc] : 0.0;
+                    const double x1 = c1 >= 0 ? sv[c1 * PC + pc] : 0.0;
+                    sv[u * PC + pc] = x0 + x1;
+                }
+            }
+            __syncthreads();
+        }
+        // the root meets the window (it holds every leaf)
+        const int r = local(root);
+        if (threadIdx.x < PC) s_force[threadIdx.x] = -(0.0 + sv[r * PC + threadIdx.x]);
+    } else {
+        for (int d = 0; d < a.pw_levels; ++d) {
+            for (int k = s_klo[d] + threadIdx.x; k < s_kend[d]; k += PART_THREADS) {
+                const int c0 = a.pw_node[2 * k], c1 = a.pw_node[2 * k + 1];
+                const bool w0 = in_window(c0), w1 = in_window(c1);
+                for (int pc = 0; pc < PC; ++pc) {
+                    const double x0 = w0 ? v[(size_t)c0 * PC + pc] : 0.0;
+                    const double x1 = w1 ? v[(size_t)c1 * PC + pc] : 0.0;
+                    v[(size_t)(L + k) * PC + pc] = x0 + x1;
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x < PC) s_force[threadIdx.x] = -(0.0 + v[(size_t)root * PC + threadIdx.x]);
     }
-    const int root = a.pw_internal > 0 ? L + a.pw_internal - 1 : 0;
-    if (threadIdx.x < PC) s_force[threadIdx.x] = -(0.0 + v[(size_t)root * PC + threadIdx.x]);
     __syncthreads();
 }
 
