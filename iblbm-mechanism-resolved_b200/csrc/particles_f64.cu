@@ -106,8 +106,8 @@ __device__ __forceinline__ int pw_leaf_of(const iblbm_particles_args& a, int e)
 constexpr int PW_MAXLEVELS = 64;
 constexpr int PW_SV = 6144;  // window partial sums held in shared memory (doubles)
 constexpr int PW_SN = 2048;  // window inner nodes whose children are held in shared memory
-// a particle's band forces, the window's partial sums and its inner nodes' children
-constexpr size_t PART_DYN_SMEM = (2 * PART_MAXB + PW_SV) * sizeof(double) + 2 * PW_SN * sizeof(int);
+// two particles' band forces, the window's partial sums and its inner nodes' children
+constexpr size_t PART_DYN_SMEM = (4 * PART_MAXB + PW_SV) * sizeof(double) + 2 * PW_SN * sizeof(int);
 
 // first k in [A, B) with pred(k) (pred false then true along k), B if none:
 // the 32 lanes of a warp probe 32 evenly spaced points per round
@@ -177,19 +177,27 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
     // PW_SV doubles; lc: the window-local children of up to PW_SN inner nodes),
     // else in the global scratch v
     const bool fast = (size_t)WN * PC <= PW_SV && WN - WL <= PW_SN;
-    double* sv = s_f + 2 * PART_MAXB;
+    double* sv = s_f + 4 * PART_MAXB;
     int* lc = reinterpret_cast<int*>(sv + PW_SV);
     auto vref = [&](int li, int pc) -> double& { return fast ? sv[(li - l0) * PC + pc] : v[(size_t)li * PC + pc]; };
-    // one particle at a time: its band forces staged in shared memory (s_f: fx
-    // then fy, PART_MAXB each), so the leaves' ordered sums read no global memory
-    for (int p = 0; p < P; ++p) {
-        for (int b = threadIdx.x; b < nb; b += PART_THREADS) {
-            s_f[b] = (double)fib[p * pstride + 2 * (size_t)b];
-            s_f[PART_MAXB + b] = (double)fib[p * pstride + 2 * (size_t)b + 1];
-        }
+    // two particles at a time: their band forces staged in shared memory (s_f: fx,
+    // fy of the first, then of the second, PART_MAXB each), so the leaves' ordered
+    // sums read no global memory and each leaf's entries are walked once per pair
+    const bool rot = a.rotation != 0;
+    for (int p0 = 0; p0 < P; p0 += 2) {
+        const int np = min(2, P - p0);
+        for (int b = threadIdx.x; b < nb; b += PART_THREADS)
+            for (int q = 0; q < np; ++q) {
+                s_f[(2 * q) * PART_MAXB + b] = (double)fib[(p0 + q) * pstride + 2 * (size_t)b];
+                s_f[(2 * q + 1) * PART_MAXB + b] = (double)fib[(p0 + q) * pstride + 2 * (size_t)b + 1];
+            }
         __syncthreads();
-        const bool rot = a.rotation != 0;
-        const double cx = s_ctr[2 * p], cy = s_ctr[2 * p + 1];
+        double cx[2], cy[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            cx[q] = q < np ? s_ctr[2 * (p0 + q)] : 0.0;
+            cy[q] = q < np ? s_ctr[2 * (p0 + q) + 1] : 0.0;
+        }
         for (int li = l0 + (int)threadIdx.x; li <= l1; li += PART_THREADS) {
             const int off = a.pw_leaf[2 * li], m = a.pw_leaf[2 * li + 1];
             int b = 0, hi = nb;  // first band entry at or after off
@@ -198,50 +206,57 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
                 if (s_nodes[mid] < off) b = mid + 1;
                 else hi = mid;
             }
-            // fx, fy and the torque term (i - cx) fy - (j - cy) fx of entry b
-            auto terms = [&](int e, double& fx, double& fy, double& t) {
-                fx = s_f[e];
-                fy = s_f[PART_MAXB + e];
+            // channel 3 q + c of particle p0 + q: c = 0 fx, 1 fy, 2 the torque term
+            // (i - cx) fy - (j - cy) fx; entry e's terms added to accumulator k
+            double res[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) res[c] = 0.0;
+            auto add = [&](int e, double (&acc)[6]) {
+                double i = 0.0, j = 0.0;
                 if (rot) {
                     const int n = s_nodes[e];
-                    t = ((double)(n % a.nx) - cx) * fy - ((double)(n / a.nx) - cy) * fx;
+                    i = (double)(n % a.nx);
+                    j = (double)(n / a.nx);
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (q < np) {
+                        const double fx = s_f[(2 * q) * PART_MAXB + e], fy = s_f[(2 * q + 1) * PART_MAXB + e];
+                        acc[3 * q] += fx;
+                        acc[3 * q + 1] += fy;
+                        if (rot) acc[3 * q + 2] += (i - cx[q]) * fy - (j - cy[q]) * fx;
+                    }
                 }
             };
-            double res0 = 0.0, res1 = 0.0, res2 = 0.0;
-            double fx, fy, t = 0.0;
             if (m >= 8) {
                 // numpy's 8 strided accumulators, in registers: the entries of each
                 // 8-position block go to the lanes of their positions, in order
                 const int cut = off + (m - m % 8);
-                double r0[8], r1[8], r2[8];
+                double r[8][6];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) r0[k] = r1[k] = r2[k] = 0.0;
+                for (int k = 0; k < 8; ++k)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) r[k][c] = 0.0;
                 while (b < nb && s_nodes[b] < cut) {
                     const int q0 = off + ((s_nodes[b] - off) & ~7);
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
                         if (b < nb && s_nodes[b] == q0 + k) {
-                            terms(b, fx, fy, t);
-                            r0[k] += fx;
-                            r1[k] += fy;
-                            r2[k] += t;
+                            add(b, r[k]);
                             ++b;
                         }
                     }
                 }
-                res0 = ((r0[0] + r0[1]) + (r0[2] + r0[3])) + ((r0[4] + r0[5]) + (r0[6] + r0[7]));
-                res1 = ((r1[0] + r1[1]) + (r1[2] + r1[3])) + ((r1[4] + r1[5]) + (r1[6] + r1[7]));
-                res2 = ((r2[0] + r2[1]) + (r2[2] + r2[3])) + ((r2[4] + r2[5]) + (r2[6] + r2[7]));
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    res[c] = ((r[0][c] + r[1][c]) + (r[2][c] + r[3][c])) + ((r[4][c] + r[5][c]) + (r[6][c] + r[7][c]));
             }
-            for (; b < nb && s_nodes[b] < off + m; ++b) {  // the tail (or a leaf of under 8)
-                terms(b, fx, fy, t);
-                res0 += fx;
-                res1 += fy;
-                res2 += t;
+            for (; b < nb && s_nodes[b] < off + m; ++b) add(b, res);  // the tail (or a leaf of under 8)
+            for (int q = 0; q < np; ++q) {
+                vref(li, 2 * (p0 + q)) = res[3 * q];
+                vref(li, 2 * (p0 + q) + 1) = res[3 * q + 1];
+                if (rot) vref(li, 2 * P + p0 + q) = res[3 * q + 2];
             }
-            vref(li, 2 * p) = res0;
-            vref(li, 2 * p + 1) = res1;
-            if (rot) vref(li, 2 * P + p) = res2;
         }
         __syncthreads();
     }
