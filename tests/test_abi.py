@@ -72,6 +72,38 @@ def test_rejects_bad_arguments_without_a_gpu():
     assert L.iblbm_feq(None, None, 10, 0, None, None) == -1
 
 
+def test_particle_step_rejects_bad_arguments_without_a_gpu():
+    """The particle step's phase and rotation checks run on the host before any
+    launch (the pointers here are never dereferenced)."""
+    import ctypes
+    from iblbm_b200 import _lib
+    L = _lib.lib()
+    fake = ctypes.c_void_p(16)
+
+    def args(**over):
+        a = _lib.ParticlesArgs()
+        a.n_particles, a.model, a.band_capacity, a.nx, a.ny, a.dy = 2, 0, 10, 10, 10, 1.0
+        for f in ("moff", "state", "consts", "band_fib_part", "band_count", "Lx_c", "Ly_c", "Lx", "Ly", "dvel",
+                  "band_nodes", "rho", "U", "lint_scratch"):
+            setattr(a, f, fake)
+        a.lint_capacity = 100
+        for k, v in over.items():
+            setattr(a, k, v)
+        return a
+
+    E_ARG = -1
+    step = lambda a: L.iblbm_particles_step_f64(ctypes.byref(a), None)
+    assert step(args(phase=0)) == E_ARG
+    assert step(args(phase=4 | 1)) == E_ARG          # Euler is a whole step on its own
+    assert step(args(phase=8)) == E_ARG
+    assert step(args(phase=2, rotation=1, band_nodes=None)) == E_ARG
+    assert step(args(phase=2, rotation=1, dy=0.0)) == E_ARG
+    assert step(args(phase=4, rotation=1, rho=None)) == E_ARG
+    assert step(args(phase=4, rotation=1, lint_capacity=0)) == E_ARG
+    assert step(args(phase=4, rotation=1, lint_capacity=1 << 20)) == E_ARG
+    assert step(args(phase=3, n_particles=9)) == E_ARG
+
+
 def test_cluster_plan_sizes():
     """Which bodies the cluster form of the FP64 MDF step takes (no GPU needed)."""
     from iblbm_b200._lib import lib
