@@ -285,14 +285,14 @@ __device__ void particle_forces_exact(const iblbm_particles_args& a, const F* fi
             lc[2 * (u - WL) + 1] = local(a.pw_node[2 * k + 1]);
         }
         __syncthreads();
-        for (int d = 0; d < a.pw_levels; ++d) {
-            for (int u = s_base[d] + (int)threadIdx.x; u < s_base[d + 1]; u += PART_THREADS) {
+        for (int d = 0; d < a.pw_levels; ++d) {  // one thread per node and channel
+            const int n0 = s_base[d], cnt = (s_base[d + 1] - n0) * PC;
+            for (int x = threadIdx.x; x < cnt; x += PART_THREADS) {
+                const int u = n0 + x / PC, pc = x % PC;
                 const int c0 = lc[2 * (u - WL)], c1 = lc[2 * (u - WL) + 1];
-                for (int pc = 0; pc < PC; ++pc) {
-                    const double x0 = c0 >= 0 ? sv[c0 * PC + pc] : 0.0;
-                    const double x1 = c1 >= 0 ? sv[c1 * PC + pc] : 0.0;
-                    sv[u * PC + pc] = x0 + x1;
-                }
+                const double x0 = c0 >= 0 ? sv[c0 * PC + pc] : 0.0;
+                const double x1 = c1 >= 0 ? sv[c1 * PC + pc] : 0.0;
+                sv[u * PC + pc] = x0 + x1;
             }
             __syncthreads();
         }
