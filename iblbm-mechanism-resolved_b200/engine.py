@@ -270,6 +270,11 @@ class Engine:
         self.side = torch.cuda.Stream(self.dev, priority=-1)
         self.ev_bulk = torch.cuda.Event()
         self.ev_side = torch.cuda.Event()
+        # the particle step runs beside the box pass (both only read the band
+        # step's output) on a stream of its own
+        self.pstream = torch.cuda.Stream(self.dev, priority=-1) if self.dev_particles else None
+        self.ev_band = torch.cuda.Event()
+        self.ev_part = torch.cuda.Event()
         self.overlap = not self.tg  # the per-step decay factor needs one stream
         self.rebuild_next = True
         self.last_out_step = 0
@@ -605,8 +610,12 @@ class Engine:
         side = self.side
         side.wait_event(self.ev_bulk)
         self._ibm(side.cuda_stream, excl_check=True)
-        if self.dev_particles and not self.part_after_lattice:
-            self._particles(side.cuda_stream, self.part_phase)
+        beside = self.dev_particles and not self.part_after_lattice
+        if beside:
+            self.ev_band.record(side)
+            self.pstream.wait_event(self.ev_band)
+            self._particles(self.pstream.cuda_stream, self.part_phase)
+            self.ev_part.record(self.pstream)
         self._dense(self.dense_box, outputs, side.cuda_stream)
         main.wait_event(self.ev_side)
         self.ev_side.record(side)
@@ -615,6 +624,8 @@ class Engine:
         self._dense(self.dense_bulk, outputs, main.cuda_stream)
         if bulk_events:
             bulk_events[1].record(main)
+        if beside:
+            main.wait_event(self.ev_part)  # the next band step reads the markers it wrote
         if self.dev_particles and self.part_after_lattice:
             main.wait_event(self.ev_side)  # this step's box pass
             self._particles(main.cuda_stream, self.part_phase)
