@@ -604,7 +604,9 @@ class Engine:
 
         Dependencies (n = this step): band(n) and box(n) wait for bulk(n-1);
         bulk(n) waits for box(n-1).  Reads of f_post(n-1) and writes of f_post(n)
-        therefore never race, and the ping-pong buffers are safe to reuse."""
+        therefore never race, and the ping-pong buffers are safe to reuse.  A
+        device particle step runs on its own stream after band(n), beside box(n);
+        bulk(n)'s event waits for it, so band(n+1) reads the markers it wrote."""
         torch = self.torch
         main = torch.cuda.current_stream(self.dev)
         side = self.side
