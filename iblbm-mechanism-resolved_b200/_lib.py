@@ -84,10 +84,11 @@ class ParticlesArgs(ctypes.Structure):
                 ("pw_levels", _i), ("pw_leaf", _vp), ("pw_node", _vp), ("pw_level", _vp), ("pw_lut", _vp),
                 ("pw_span", _vp), ("pw_scratch", _vp), ("rotation", _i), ("semi_implicit", _i),
                 ("euler_trapezoidal", _i), ("nx", _i), ("dy", _d), ("rho", _vp), ("U", _vp), ("moments_f32", _i),
-                ("ny", _i), ("lint_scratch", _vp), ("lint_capacity", _i)]
+                ("ny", _i), ("lint_scratch", _vp), ("lint_capacity", _i), ("lagrangian", _i), ("Lfx", _vp),
+                ("Lfy", _vp), ("dfc_force", _vp)]
 
 
-PARTICLE_STATE, PARTICLE_CONSTS = 22, 9  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)
+PARTICLE_STATE, PARTICLE_CONSTS = 22, 10  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)
 
 
 INERTIA_IDS = {"none": 0, "explicit_history": 1, "feng_b2": 2}

@@ -43,7 +43,9 @@
 // partial sum that is not itself zero).  Without a tree the sums run in
 // another fixed order (deterministic, round-off apart from numpy's).  The
 // rotated markers take the device's cos and sin of the angle, which may differ
-// from the host's in the last bit, so rotating runs are not bit for bit.
+// from the host's in the last bit, so rotating runs are not bit for bit.  DF and
+// DFC particles take their forces and torques from their markers' forces
+// instead, each a pairwise sum over the particle's markers (lagrangian_sums).
 #include <cstdint>
 #include "common.cuh"
 #include "../../include/iblbm_b200.h"
@@ -364,6 +366,30 @@ __device__ double pw_fold(int n, const double* lsum, int& li)
 constexpr int PW_MAXLEAVES = 512;  // every leaf but a lone one holds at least 64 values
 constexpr int LINT_MAX = 64 * (PW_MAXLEAVES - 1);
 
+// numpy's pairwise sum of vals[0 .. n), n <= LINT_MAX (global memory the block
+// wrote before a __syncthreads); block-wide, the sum is returned to thread 0
+__device__ double block_pairwise_sum(const double* vals, int n)
+{
+    __shared__ int s_nleaves;
+    __shared__ int s_loff[PW_MAXLEAVES], s_llen[PW_MAXLEAVES];
+    __shared__ double s_lsum[PW_MAXLEAVES];
+    if (threadIdx.x == 0) {
+        int cnt = 0;
+        if (n > 0) pw_collect(0, n, s_loff, s_llen, cnt);
+        s_nleaves = cnt;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < s_nleaves; l += PART_THREADS) s_lsum[l] = pw_block(vals + s_loff[l], s_llen[l]);
+    __syncthreads();
+    double total = 0.0;
+    if (threadIdx.x == 0 && n > 0) {
+        int li = 0;
+        total = pw_fold(n, s_lsum, li);
+    }
+    __syncthreads();
+    return total;
+}
+
 // The fluid's angular momentum inside a disc (centre px, py, radius r) from
 // this step's rho and U: diagnostics/internal_flow.py:220-262 as the host
 // restates it — the box of half-width int(r/dx) + 2 around the rounded centre
@@ -374,10 +400,8 @@ template <typename T>
 __device__ double disc_angular_momentum(const iblbm_particles_args& a, const T* rho, const T* U, double px,
                                         double py, double r)
 {
-    __shared__ int s_base, s_nleaves;
+    __shared__ int s_base;
     __shared__ int s_wcount[PART_THREADS / 32];
-    __shared__ int s_loff[PW_MAXLEAVES], s_llen[PW_MAXLEAVES];
-    __shared__ double s_lsum[PW_MAXLEAVES];
     const double dx = a.dx;
     const double ci = px / dx, cj = py / dx, rl = r / dx;
     const int ii = (int)rint(ci), jj = (int)rint(cj), rr = (int)rl + 2;
@@ -417,22 +441,45 @@ __device__ double disc_angular_momentum(const iblbm_particles_args& a, const T* 
         }
         __syncthreads();
     }
-    const int n = min(s_base, cap);
-    if (threadIdx.x == 0) {
-        int cnt = 0;
-        if (n > 0) pw_collect(0, n, s_loff, s_llen, cnt);
-        s_nleaves = cnt;
+    return block_pairwise_sum(a.lint_scratch, min(s_base, cap));
+}
+
+// Each particle's force and torque from its markers' forces, summed like the
+// reference: DF (iblbm/ibm/forcing.py:262-275) F = -sum(Lf ds), T =
+// -sum((rx Lfy - ry Lfx) ds); DFC (iblbm/ibm/strategies/dfc.py:114-128) F =
+// sum(f), T = sum(rx fy - ry fx); rx = (X - x)/dx, ry = (Y - y)/dy over the
+// markers of this step, each sum numpy's pairwise sum of the particle's values.
+__device__ void lagrangian_sums(const iblbm_particles_args& a, double* s_force)
+{
+    const int P = a.n_particles;
+    const bool rot = a.rotation != 0, df = a.lagrangian == IBLBM_LAGRANGIAN_DF;
+    const int cap = min(a.lint_capacity, LINT_MAX);
+    double* buf = a.lint_scratch;
+    for (int p = 0; p < P; ++p) {
+        const int m0 = a.moff[p], n = min(a.moff[p + 1] - m0, cap);
+        const double* st = a.state + IBLBM_PARTICLE_STATE * p;
+        const double px = st[10], py = st[11];
+        const double ds = a.consts[IBLBM_PARTICLE_CONSTS * p + 9];
+        for (int c = 0; c < (rot ? 3 : 2); ++c) {
+            for (int l = threadIdx.x; l < n; l += PART_THREADS) {
+                const int m = m0 + l;
+                const double fx = df ? a.Lfx[m] : a.dfc_force[2 * m];
+                const double fy = df ? a.Lfy[m] : a.dfc_force[2 * m + 1];
+                double v;
+                if (c < 2) {
+                    v = c == 0 ? fx : fy;
+                } else {
+                    const double rx = (a.Lx[m] - px) / a.dx, ry = (a.Ly[m] - py) / a.dy;
+                    v = rx * fy - ry * fx;
+                }
+                buf[l] = df ? v * ds : v;
+            }
+            __syncthreads();
+            const double t = 0.0 + block_pairwise_sum(buf, n);
+            if (threadIdx.x == 0) s_force[c < 2 ? 2 * p + c : 2 * P + p] = df ? -t : t;
+            __syncthreads();
+        }
     }
-    __syncthreads();
-    for (int l = threadIdx.x; l < s_nleaves; l += PART_THREADS) s_lsum[l] = pw_block(a.lint_scratch + s_loff[l], s_llen[l]);
-    __syncthreads();
-    double total = 0.0;
-    if (threadIdx.x == 0 && n > 0) {
-        int li = 0;
-        total = pw_fold(n, s_lsum, li);
-    }
-    __syncthreads();
-    return total;
 }
 
 __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_particles_args a)
@@ -451,7 +498,9 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
             s_ctr[threadIdx.x] = a.state[IBLBM_PARTICLE_STATE * p + 10 + d] / (d ? a.dy : dx);
         }
         __syncthreads();
-        if (a.pw_leaf) {
+        if (a.lagrangian) {
+            lagrangian_sums(a, s_force);
+        } else if (a.pw_leaf) {
             extern __shared__ double s_dyn[];  // PART_DYN_SMEM bytes with a summation tree
             if (a.fib_f32)
                 particle_forces_exact(a, static_cast<const float*>(a.band_fib_part), s_ctr, PC, s_force, s_dyn);
@@ -619,6 +668,11 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
         (!a->Lx_c || !a->Ly_c || !a->Lx || !a->Ly || !a->dvel))
         return IBLBM_E_ARG;
     if (a->rotation && (!a->band_nodes || a->nx < 1 || !(a->dy > 0.0))) return IBLBM_E_ARG;
+    if (a->lagrangian < 0 || a->lagrangian > IBLBM_LAGRANGIAN_DFC) return IBLBM_E_ARG;
+    if (a->lagrangian && (ph & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) &&
+        (!a->lint_scratch || a->lint_capacity < 1 || a->lint_capacity > LINT_MAX || !a->Lx || !a->Ly ||
+         (a->lagrangian == IBLBM_LAGRANGIAN_DF ? (!a->Lfx || !a->Lfy) : !a->dfc_force)))
+        return IBLBM_E_ARG;
     if (a->model < IBLBM_INERTIA_NONE || a->model > IBLBM_INERTIA_FENG_B2) return IBLBM_E_ARG;
     if (a->pw_leaf && (!a->pw_node && a->pw_internal > 0)) return IBLBM_E_ARG;
     if (a->pw_leaf && (!a->band_nodes || !a->pw_scratch || !a->pw_level || !a->pw_lut || !a->pw_span ||

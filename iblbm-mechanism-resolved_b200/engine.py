@@ -259,11 +259,10 @@ class Engine:
             rot = bool(cfg.enable_rotation)
             default = not (rot and not self.f32)
             self.dev_particles = default if device_particles is None else bool(device_particles)
-            if cfg.ibm_method != "MDF" or self.single:
-                # the Lagrangian force sums of DF and DFC and the single-particle
-                # runtime run on the host
+            if self.single:
+                # the single-particle runtime (its own force extraction) runs on the host
                 if device_particles:
-                    raise NotImplementedError("DF / DFC particles and the single-particle runtime run on the host")
+                    raise NotImplementedError("the single-particle runtime runs on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -299,7 +298,7 @@ class Engine:
             state[k, 18:22] = [p.omega_half, p.angle, p.omega, p.l_int_prev]
             g = net_gravity(p.rho_ratio, p.lattice_r, st.gravity_lattice, cfg.gravity_direction)
             consts[k] = [p.mass, 1.0 / p.rho_ratio, np.pi * p.lattice_r ** 2 / p.mass, g[0], g[1], p.cx_init,
-                         p.cy_init, p.I_particle, p.r_domain]
+                         p.cy_init, p.I_particle, p.r_domain, float(p.Larea)]
         self.d_pstate = torch.as_tensor(state.reshape(-1), device=self.dev)
         self.d_pconsts = torch.as_tensor(consts.reshape(-1), device=self.dev)
         self.d_Lxc_all = torch.as_tensor(np.concatenate([p.Lx_c for p in ps]), device=self.dev)
@@ -326,12 +325,18 @@ class Engine:
         # launch follows the whole lattice pass
         self.part_after_lattice = self.part_phase == 4 and bool(cfg.enable_rotation)
         self.moments_always = self.part_after_lattice
+        # DF and DFC particles: force and torque from the markers' forces
+        # (iblbm/ibm/forcing.py:262-275, iblbm/ibm/strategies/dfc.py:114-128)
+        a.lagrangian = {"DF": 1, "DFC": 2}.get(self.method, 0)
+        a.Lfx, a.Lfy, a.dfc_force = ptr(self.d_Lfx), ptr(self.d_Lfy), ptr(self.d_dfc_force)
+        cap = max(p.Lb for p in ps) if a.lagrangian else 0
         if self.part_after_lattice:
-            cap = max((2 * (int(p.r_domain / st.dx) + 2) + 1) ** 2 for p in ps)
-            self.d_lint = torch.zeros(cap, dtype=torch.float64, device=self.dev)
+            cap = max([cap] + [(2 * (int(p.r_domain / st.dx) + 2) + 1) ** 2 for p in ps])
             a.rho, a.U, a.moments_f32, a.ny = ptr(self.ro_out), ptr(self.U_out), int(self.f32), st.ny
+        if cap:
+            self.d_lint = torch.zeros(cap, dtype=torch.float64, device=self.dev)
             a.lint_scratch, a.lint_capacity = ptr(self.d_lint), cap
-        if not self.f32:
+        if not self.f32 and not a.lagrangian:
             # the FP64 form sums the forces in numpy's pairwise order over the
             # dense lattice field, so the device step equals the host step bit
             # for bit; the FP32 form keeps the cheaper fixed-order sum

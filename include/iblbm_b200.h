@@ -415,7 +415,8 @@ int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *gra
  * the last step's rigid-body marker velocity, and the fluid's angular
  * momentum inside the disc at the last Euler step; consts holds
  * IBLBM_PARTICLE_CONSTS doubles: mass, 1/rho_ratio, pi r^2/mass, net gravity
- * (2), initial centre (2), moment of inertia, disc radius (domain units).  phase FULL finishes the
+ * (2), initial centre (2), moment of inertia, disc radius (domain units),
+ * marker arc length.  phase FULL finishes the
  * current Verlet step from the band kernel's per-particle forces
  * (band_fib_part, particles x band_capacity x 2, FP32 when fib_f32); phase HALF
  * starts the next one: new marker positions Lx, Ly and desired velocities
@@ -423,13 +424,15 @@ int iblbm_mlp_train_step(float *params, float *adam_m, float *adam_v, float *gra
  * kernel (with rotation: after the whole lattice pass) and leaves the next
  * step's markers and desired velocities. */
 #define IBLBM_PARTICLE_STATE 22
-#define IBLBM_PARTICLE_CONSTS 9
+#define IBLBM_PARTICLE_CONSTS 10
 #define IBLBM_PARTICLES_FULL 1
 #define IBLBM_PARTICLES_HALF 2
 #define IBLBM_PARTICLES_EULER 4
 #define IBLBM_INERTIA_NONE 0
 #define IBLBM_INERTIA_EXPLICIT_HISTORY 1
 #define IBLBM_INERTIA_FENG_B2 2
+#define IBLBM_LAGRANGIAN_DF 1
+#define IBLBM_LAGRANGIAN_DFC 2
 typedef struct {
     int n_particles, phase, model, fib_f32;
     const int *moff;
@@ -484,6 +487,13 @@ typedef struct {
     int moments_f32, ny;
     double *lint_scratch;
     int lint_capacity;
+    /* lagrangian: IBLBM_LAGRANGIAN_DF / _DFC take each particle's force and
+     * torque from its markers' forces instead of the band field (multi-particle
+     * DF: Lfx, Lfy times the particle's arc length, consts[9]; DFC: dfc_force,
+     * markers x 2), summed over its markers like numpy; lint_scratch then holds
+     * at least the most markers of a particle. */
+    int lagrangian;
+    const double *Lfx, *Lfy, *dfc_force;
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);

@@ -234,12 +234,14 @@ def test_f32_config1_geometry_long(torch):
     _check_forces(r64, r32)
 
 
-@pytest.mark.parametrize("name", ["c5_sed2_mdf_cmmrt_p4", "c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap"])
+@pytest.mark.parametrize("name", ["c5_sed2_mdf_cmmrt_p4", "c5e_sed2_mdf_euler_none", "c5e_sed2_mdf_euler_feng_trap",
+                                  "c5_sed2_df_bgk_hat", "c5_sed2_dfc_trt_p4"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_device_particles_match_host_step(torch, precision, name):
     """The Verlet and explicit Euler steps on the device against the host step
-    (bit-exact to the reference in FP64).  In the FP64 form the device sums
-    each particle's force in numpy's pairwise order over the lattice, so
+    (bit-exact to the reference in FP64), MDF, DF and DFC particles.  In the
+    FP64 form the device sums each particle's force in numpy's pairwise order
+    over the lattice (MDF) or over its markers (DF, DFC; both forms), so
     trajectories, forces, fields and the sedimentation records are equal bit
     for bit; the FP32 form sums in a fixed order of its own (trajectories
     within 1e-9 relative)."""
@@ -266,7 +268,7 @@ def test_device_particles_match_host_step(torch, precision, name):
 
 
 @pytest.mark.parametrize("name", ["c5r_sed2_mdf_rot_indirect", "c5r_sed2_mdf_rot_semi", "c5r_sed2_mdf_rot_iterative",
-                                  "c5e_sed2_mdf_euler_rot"])
+                                  "c5e_sed2_mdf_euler_rot", "c5r_sed2_df_rot_semi", "c5r_sed2_dfc_rot_semi"])
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_device_rotation_matches_host_step(torch, precision, name):
     """Rotating discs with the Verlet or explicit Euler step on the device
