@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
             // R(0) = [[1, -0], [0, 1]] exactly, as the host's cos 0 and sin 0
             s_rot[3 * p] = a.rotation ? cos(s[19]) : 1.0;
             s_rot[3 * p + 1] = a.rotation ? sin(s[19]) : 0.0;
-            s_rot[3 * p + 2] = a.rotation && a.semi_implicit ? s[12] : 0.0;
+            s_rot[3 * p + 2] = a.rotation && a.semi_implicit ? (a.half_kick_omega ? s[18] : s[12]) : 0.0;
         }
         __syncthreads();
     }

@@ -259,10 +259,10 @@ class Engine:
             rot = bool(cfg.enable_rotation)
             default = not (rot and not self.f32)
             self.dev_particles = default if device_particles is None else bool(device_particles)
-            if self.single:
-                # the single-particle runtime (its own force extraction) runs on the host
+            if self.single and cfg.prescribed_velocity is not None:
+                # a disc moved at a prescribed velocity steps on the host
                 if device_particles:
-                    raise NotImplementedError("the single-particle runtime runs on the host")
+                    raise NotImplementedError("a prescribed-velocity disc steps on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -327,7 +327,9 @@ class Engine:
         self.moments_always = self.part_after_lattice
         # DF and DFC particles: force and torque from the markers' forces
         # (iblbm/ibm/forcing.py:262-275, iblbm/ibm/strategies/dfc.py:114-128)
-        a.lagrangian = {"DF": 1, "DFC": 2}.get(self.method, 0)
+        # (the single-particle runtime sums the DF field like MDF's)
+        a.lagrangian = {"DF": 0 if self.single else 1, "DFC": 2}.get(self.method, 0)
+        a.half_kick_omega = int(self.single)
         a.Lfx, a.Lfy, a.dfc_force = ptr(self.d_Lfx), ptr(self.d_Lfy), ptr(self.d_dfc_force)
         cap = max(p.Lb for p in ps) if a.lagrangian else 0
         if self.part_after_lattice:
@@ -389,7 +391,8 @@ class Engine:
                 p.Lx, p.Ly = Lx[moff[k]:moff[k + 1]].copy(), Ly[moff[k]:moff[k + 1]].copy()
                 p.desired_velocity = dv[moff[k]:moff[k + 1]].copy()
             else:  # the markers of the last step (the device holds the next step's)
-                self._set_markers(p, p.vel_half, float(s[k, 20]) if rot and semi else 0.0)
+                om = p.omega_half if self.single else float(s[k, 20])
+                self._set_markers(p, p.vel_half, om if rot and semi else 0.0)
 
     def _band_capacity(self, S):
         st = self.st

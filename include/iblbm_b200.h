@@ -494,6 +494,10 @@ typedef struct {
      * at least the most markers of a particle. */
     int lagrangian;
     const double *Lfx, *Lfy, *dfc_force;
+    /* half_kick_omega: the semi-implicit marker velocity takes the step's
+     * half-kicked omega, as the single-particle runtime does
+     * (runtime/scenarios/sedimentation_single.py:148-158), not the last step's. */
+    int half_kick_omega;
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);
