@@ -85,7 +85,8 @@ class ParticlesArgs(ctypes.Structure):
                 ("pw_span", _vp), ("pw_scratch", _vp), ("rotation", _i), ("semi_implicit", _i),
                 ("euler_trapezoidal", _i), ("nx", _i), ("dy", _d), ("rho", _vp), ("U", _vp), ("moments_f32", _i),
                 ("ny", _i), ("lint_scratch", _vp), ("lint_capacity", _i), ("lagrangian", _i), ("Lfx", _vp),
-                ("Lfy", _vp), ("dfc_force", _vp), ("half_kick_omega", _i)]
+                ("Lfy", _vp), ("dfc_force", _vp), ("half_kick_omega", _i),
+                ("prescribed", _i), ("prescribed_velocity", _d * 2)]
 
 
 PARTICLE_STATE, PARTICLE_CONSTS = 22, 10  # doubles per particle (IBLBM_PARTICLE_STATE / _CONSTS)

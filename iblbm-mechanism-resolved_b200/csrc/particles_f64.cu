@@ -530,6 +530,13 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
                 s[15] = T;
             }
             for (int d = 0; d < 2; ++d) {
+                if (a.prescribed) {  // sedimentation_single.py:174-180: the velocity stays
+                    s[2 + d] = a.prescribed_velocity[d];
+                    s[8 + d] = s_force[2 * p + d];
+                    s[d] = s[10 + d];
+                    if (a.forces_out) a.forces_out[2 * p + d] = s_force[2 * p + d];
+                    continue;
+                }
                 const double F = s_force[2 * p + d] + c[3 + d];
                 double vn = s[6 + d] + ((0.5 * dt) * F) / m;
                 if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vn = vn + 0.5 * (hc * (s[2 + d] - s[4 + d]));
@@ -607,6 +614,7 @@ __global__ void __launch_bounds__(PART_THREADS) particles_kernel(const iblbm_par
                 const double F = s[8 + d] + c[3 + d];
                 double vh = s[2 + d] + ((0.5 * dt) * F) / m;
                 if (a.model == IBLBM_INERTIA_EXPLICIT_HISTORY) vh = vh + 0.5 * (hc * (s[2 + d] - s[4 + d]));
+                if (a.prescribed) vh = a.prescribed_velocity[d];  // sedimentation_single.py:91-97
                 const double xn = s[d] + (dt * vh) * dx;
                 s[16 + d] = vh;
                 s[10 + d] = xn;
@@ -669,6 +677,7 @@ extern "C" int iblbm_particles_step_f64(const iblbm_particles_args* a, void* str
         return IBLBM_E_ARG;
     if (a->rotation && (!a->band_nodes || a->nx < 1 || !(a->dy > 0.0))) return IBLBM_E_ARG;
     if (a->lagrangian < 0 || a->lagrangian > IBLBM_LAGRANGIAN_DFC) return IBLBM_E_ARG;
+    if (a->prescribed && (a->rotation || (ph & IBLBM_PARTICLES_EULER))) return IBLBM_E_ARG;
     if (a->lagrangian && (ph & (IBLBM_PARTICLES_FULL | IBLBM_PARTICLES_EULER)) &&
         (!a->lint_scratch || a->lint_capacity < 1 || a->lint_capacity > LINT_MAX || !a->Lx || !a->Ly ||
          (a->lagrangian == IBLBM_LAGRANGIAN_DF ? (!a->Lfx || !a->Lfy) : !a->dfc_force)))

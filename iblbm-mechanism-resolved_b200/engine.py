@@ -259,10 +259,12 @@ class Engine:
             rot = bool(cfg.enable_rotation)
             default = not (rot and not self.f32)
             self.dev_particles = default if device_particles is None else bool(device_particles)
-            if self.single and cfg.prescribed_velocity is not None:
-                # a disc moved at a prescribed velocity steps on the host
+            if self.single and cfg.prescribed_velocity is not None and (rot or cfg.time_integrator != "verlet"):
+                # a disc moved at a prescribed velocity steps on the host with
+                # rotation or the Euler integrator set (the host step ignores both)
                 if device_particles:
-                    raise NotImplementedError("a prescribed-velocity disc steps on the host")
+                    raise NotImplementedError("a prescribed-velocity disc with rotation or explicit Euler set "
+                                              "steps on the host")
                 self.dev_particles = False
             if self.dev_particles:
                 self._setup_device_particles()
@@ -330,6 +332,9 @@ class Engine:
         # (the single-particle runtime sums the DF field like MDF's)
         a.lagrangian = {"DF": 0 if self.single else 1, "DFC": 2}.get(self.method, 0)
         a.half_kick_omega = int(self.single)
+        if self.single and cfg.prescribed_velocity is not None:
+            a.prescribed = 1
+            a.prescribed_velocity[0], a.prescribed_velocity[1] = (float(x) for x in cfg.prescribed_velocity)
         a.Lfx, a.Lfy, a.dfc_force = ptr(self.d_Lfx), ptr(self.d_Lfy), ptr(self.d_dfc_force)
         cap = max(p.Lb for p in ps) if a.lagrangian else 0
         if self.part_after_lattice:

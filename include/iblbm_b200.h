@@ -498,6 +498,12 @@ typedef struct {
      * half-kicked omega, as the single-particle runtime does
      * (runtime/scenarios/sedimentation_single.py:148-158), not the last step's. */
     int half_kick_omega;
+    /* prescribed: the disc moves at prescribed_velocity (lattice units per step,
+     * runtime/scenarios/sedimentation_single.py:91-97,174-180): the half step
+     * moves it and its markers, whose desired velocity is that velocity, and the
+     * full step records the force and keeps the velocity; no rotation. */
+    int prescribed;
+    double prescribed_velocity[2];
 } iblbm_particles_args;
 
 int iblbm_particles_step_f64(const iblbm_particles_args *a, void *stream);

@@ -49,11 +49,12 @@ def test_single_particle_runtime_matches_reference(torch, name):
     assert res["termination_reason"] == bytes(g["termination"]).decode()
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if c != "df_prescribed"])
+@pytest.mark.parametrize("name", CASES)
 def test_single_particle_runtime_on_the_device(torch, name):
     """The same runs with the disc stepped by the device particle step (forces
     summed over the band field, or over the markers under DFC, in numpy's order;
-    the semi-implicit marker velocity from the half-kicked omega): the disc
+    the semi-implicit marker velocity from the half-kicked omega; the
+    prescribed-velocity mode): the disc
     within 1e-12 relative of the reference's run (equal bits without rotation,
     whose device cos and sin may round differently from numpy's)."""
     from iblbm_b200 import run
@@ -62,6 +63,8 @@ def test_single_particle_runtime_on_the_device(torch, name):
     g = dict(np.load(os.path.join(GOLD, f"sed1_{name}.npz")))
     kw = json.loads(bytes(g["config_json"]).decode())
     kw["cylinder_center"] = tuple(kw["cylinder_center"])
+    if kw.get("prescribed_velocity") is not None:
+        kw["prescribed_velocity"] = tuple(kw["prescribed_velocity"])
     cfg = SimConfig(**kw)
     eng = Engine(cfg, device_particles=True)
     assert eng.dev_particles
