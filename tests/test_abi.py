@@ -102,6 +102,11 @@ def test_particle_step_rejects_bad_arguments_without_a_gpu():
     assert step(args(phase=4, rotation=1, lint_capacity=0)) == E_ARG
     assert step(args(phase=4, rotation=1, lint_capacity=1 << 20)) == E_ARG
     assert step(args(phase=3, n_particles=9)) == E_ARG
+    assert step(args(phase=3, lagrangian=3)) == E_ARG
+    assert step(args(phase=3, lagrangian=1, Lfx=None)) == E_ARG     # DF sums need the marker forces
+    assert step(args(phase=3, lagrangian=2, dfc_force=None)) == E_ARG
+    assert step(args(phase=3, prescribed=1, rotation=1)) == E_ARG   # a prescribed disc does not turn
+    assert step(args(phase=4, prescribed=1)) == E_ARG
 
 
 def test_cluster_plan_sizes():
